@@ -1,0 +1,81 @@
+"""Loader of the CUDA library and the ctypes signatures of its C ABI (include/field_b200.h).
+
+There is no fallback: ``lib()`` raises ``RuntimeError`` when ``libfield_b200.so`` is missing or no
+CUDA device is visible, so every product call fails loudly instead of computing elsewhere.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import threading
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "libfield_b200.so"
+
+_lock = threading.Lock()
+_LIBS: dict[str, ct.CDLL] = {}
+
+P, I, I64, D, F, U64 = ct.c_void_p, ct.c_int, ct.c_int64, ct.c_double, ct.c_float, ct.c_uint64
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    # runtime
+    "fb_abi_version": (I, []),
+    "fb_device_arch": (I, []),
+    # EDT, device pointers
+    "fb_edt_scratch_bytes": (I64, [I, I, I, I]),
+    "fb_edt_squared_device": (I, [P, I, I, I, I, P, P, I64, P]),
+    "fb_edt_pair_device": (I, [P, I, I, I, D, P, P, P, I64, P]),
+    "fb_edt_validate_device": (I, [P, I, I, I, P, I64, P]),
+    # EDT, host pointers (reference names)
+    "edt_squared_large": (I, [P, I, I, I, P]),
+    "edt_squared": (I, [P, I, I, I, P]),
+    "edt_pair_create": (P, [I, I, I]),
+    "edt_pair_query": (I, [P, P, D, P, P]),
+    "edt_pair_destroy": (None, [P]),
+}
+
+
+def _bind(L: ct.CDLL) -> ct.CDLL:
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
+def load(path: str | Path | None = None) -> ct.CDLL:
+    """The CUDA library at ``path`` (default: the in-tree build), loaded once per path."""
+    p = Path(path).resolve() if path is not None else LIBRARY
+    key = str(p)
+    with _lock:
+        if key not in _LIBS:
+            if not p.exists():
+                raise RuntimeError(f"CUDA library {p} is not built; run __graft_entry__.build() "
+                                   "(there is no CPU fallback)")
+            _LIBS[key] = _bind(ct.CDLL(key))
+        return _LIBS[key]
+
+
+def lib(path=None) -> ct.CDLL:
+    """The CUDA library, after checking that a CUDA device is present."""
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("field_b200 needs a CUDA device (sm_100a); there is no CPU fallback")
+    return load(path)
+
+
+def stream_handle(stream=None) -> int:
+    """Raw cudaStream_t of a torch stream (default: the current stream)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def check(status: int, what: str) -> None:
+    if status == 1:
+        raise ValueError(f"{what}: invalid input (status 1)")
+    if status:
+        raise RuntimeError(f"{what}: native failure (status {status})")

@@ -1,0 +1,337 @@
+"""CPU oracle for the block-sparse SDF field path -- TEST INFRASTRUCTURE ONLY.
+
+ctypes bindings to ``oracle/liboracle.so`` (a C restatement of the reference algorithms, each
+function citing the reference file:line it follows) plus NumPy restatements of the reference's
+Python-level semantics.  Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker: the product library never calls it.
+
+``ref_library(name)`` loads the reference's own CPU libraries compiled from its sources into
+``oracle/_ref/`` (see oracle/Makefile); they pin the restatements where the reference is C++.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIB = None
+
+NODE = np.dtype([("lo", "<i4", (3,)), ("shape", "<i4", (3,)), ("stored_shape", "<i4", (3,)),
+                 ("children", "<i4", (2,)), ("offset", "<i8")])
+CSG_INSN = np.dtype([("op", "<i4"), ("left", "<i4"), ("right", "<i4"), ("pad", "<i4"), ("offset", "<f8")])
+PRIM = np.dtype([("type", "<i4"), ("flags", "<i4"), ("p", "<f8", (12,)), ("A", "<f8", (12,)),
+                 ("s", "<f8"), ("off", "<f8")])
+INSN = np.dtype([("op", "<i4"), ("arg", "<i4"), ("k", "<f8")])
+
+
+def lib():
+    """The compiled oracle (built on demand with make when missing)."""
+    global _LIB
+    if _LIB is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            import subprocess
+            subprocess.run(["make", "-C", str(HERE), "liboracle.so"], check=True, capture_output=True)
+        L = ct.CDLL(str(path))
+        P, I, I64, D, F = ct.c_void_p, ct.c_int, ct.c_int64, ct.c_double, ct.c_float
+        sig = {
+            "or_edt_squared": [P, I, I, I, P],
+            "or_edt_squared_brute": [P, I, I, I, P],
+            "or_edt_signed": [P, I, I, I, D, P, P],
+            "or_classify_dense": [P, I64, I64, I64, I64, F, P, P],
+            "or_tiles_dense": [P, I64, I64, I64, I64, P, I64, P],
+            "or_csg_execute": [P, ct.c_int32, P, P, ct.c_int32, P],
+            "or_eval_points": [P, ct.c_int32, P, ct.c_int32, P, I64, P],
+            "or_classify_program": [P, ct.c_int32, P, ct.c_int32, D, D, D, D, I, I, I, I, F, P, P],
+            "or_tiles_program": [P, ct.c_int32, P, ct.c_int32, D, D, D, D, I, I, I, I, P, I64, P],
+            "or_pack_nodes": [P], "or_pack_samples": [P], "or_pack_copy": [P, P, I64, P, I64],
+            "or_pack_free": [P], "or_threads": [],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ct.c_int
+        L.or_pack.argtypes = [P, P, I]
+        L.or_pack.restype = P
+        L.or_pack_nodes.restype = ct.c_int64
+        L.or_pack_samples.restype = ct.c_int64
+        L.or_pack_free.restype = None
+        _LIB = L
+    return _LIB
+
+
+def threads() -> int:
+    return int(lib().or_threads())
+
+
+# ----------------------------------------------------------------------------------------- EDT
+def edt_squared(binary, brute=False):
+    """int32 squared distance of every voxel to the nearest zero of ``binary``
+    (src/field_engine/field_edt_integer_v1.py:14-26)."""
+    b = np.ascontiguousarray(binary, dtype=np.uint8)
+    out = np.empty(b.shape, np.int32)
+    fn = lib().or_edt_squared_brute if brute else lib().or_edt_squared
+    rc = fn(b.ctypes.data, *b.shape, out.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle EDT status {rc}")
+    return out
+
+
+def edt_signed(mask, pitch, with_squared=False):
+    """Signed float32 distance, negative inside ``mask``, half-pitch corrected
+    (src/field_engine/edt_persistent_pair_v1/edt.cu:36-42)."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    out = np.empty(m.shape, np.float32)
+    pair = np.empty((2,) + m.shape, np.int32)
+    rc = lib().or_edt_signed(m.ctypes.data, *m.shape, float(pitch), out.ctypes.data, pair.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle EDT status {rc}")
+    return (out, pair) if with_squared else out
+
+
+def edt_signed_numpy(mask, pitch, pair):
+    """The reference's NumPy signed reconstruction from a squared pair
+    (src/field_engine/field_edt_integer_v1.py:40-43)."""
+    outside = (np.sqrt(pair[0].astype(np.float64)) * pitch).astype(np.float32)
+    inside = (np.sqrt(pair[1].astype(np.float64)) * pitch).astype(np.float32)
+    signed = (outside - inside).astype(np.float32)
+    return (signed - np.sign(signed) * np.float32(0.5 * pitch)).astype(np.float32)
+
+
+# ----------------------------------------------------------------------------------------- dense classify
+def classify_dense(dense, pitch, block):
+    """dict(kind, active_ids, tiles, ...) exactly as
+    src/field_engine/faltkarna_v1_mesh_to_sdf.py:660-692 returns it."""
+    import math
+    d = np.ascontiguousarray(dense, dtype=np.float32)
+    nx, ny, nz = d.shape
+    n_bx, n_by, n_bz = -(-nx // block), -(-ny // block), -(-nz // block)
+    margin = math.sqrt(3.0) * block * pitch
+    kind = np.empty(n_bx * n_by * n_bz, np.int32)
+    cma = np.empty(n_bx * n_by * n_bz, np.float32)
+    rc = lib().or_classify_dense(d.ctypes.data, nx, ny, nz, block, float(np.float32(margin)), kind.ctypes.data,
+                                 cma.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle classify status {rc}")
+    active = np.where(kind == 0)[0].astype(np.int32)
+    tiles = np.empty((len(active), block, block, block), np.float32)
+    if len(active):
+        rc = lib().or_tiles_dense(d.ctypes.data, nx, ny, nz, block, active.ctypes.data, len(active),
+                                  tiles.ctypes.data)
+        if rc:
+            raise ValueError(f"oracle tiles status {rc}")
+    return dict(kind=kind, active_ids=active, tiles=tiles, n_bx=n_bx, n_by=n_by, n_bz=n_bz,
+                n_blocks=int(len(kind)), n_active=int(len(active)), margin_mm=margin, corner_min_abs=cma)
+
+
+# ----------------------------------------------------------------------------------------- CSG
+def encode_program(instructions, nfields):
+    """Encode ('union'|'difference'|'offset', left, right) triples into the reference's 24-byte
+    records (src/field_engine/field_csg_batch_v1.py:59-64)."""
+    enc = np.zeros(len(instructions), CSG_INSN)
+    for i, (op, left, right) in enumerate(instructions):
+        enc[i]["op"] = {"union": 0, "difference": 1, "offset": 2}[op]
+        enc[i]["left"] = left
+        if op == "offset":
+            enc[i]["offset"] = right
+        else:
+            enc[i]["right"] = right
+    return enc
+
+
+def csg_execute(fields, instructions):
+    """Dense float32 result of the ordered program; raises ValueError(status) like the reference
+    (src/field_engine/csg_batch_native_v1/execute.cpp:10-53)."""
+    arrs = [np.ascontiguousarray(f, dtype=np.float32) for f in fields]
+    shape = np.array(arrs[0].shape, np.int32)
+    ptrs = (ct.c_void_p * len(arrs))(*(a.ctypes.data for a in arrs))
+    enc = encode_program(instructions, len(arrs))
+    out = np.empty(arrs[0].shape, np.float32)
+    rc = lib().or_csg_execute(ptrs, len(arrs), shape.ctypes.data, enc.ctypes.data, len(enc), out.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle CSG status {rc}")
+    return out
+
+
+# ----------------------------------------------------------------------------------------- packing
+def pack(samples, threshold=512):
+    """(nodes, payload) with the reference's split decisions
+    (src/field_engine/adaptive_pack_native_v1/pack.cpp:18-69)."""
+    a = np.ascontiguousarray(samples, dtype=np.float32)
+    shape = np.array(a.shape, np.int32)
+    h = lib().or_pack(a.ctypes.data, shape.ctypes.data, int(threshold))
+    if not h:
+        raise ValueError("oracle packing refused the input")
+    try:
+        nodes = np.empty(lib().or_pack_nodes(h), NODE)
+        payload = np.empty(lib().or_pack_samples(h), np.float32)
+        if lib().or_pack_copy(h, nodes.ctypes.data, len(nodes), payload.ctypes.data, len(payload)):
+            raise RuntimeError("oracle pack copy failed")
+    finally:
+        lib().or_pack_free(h)
+    return nodes, payload
+
+
+def samples_at(nodes, payload, indices):
+    """Exact sample bits at integer indices by walking the packed tree
+    (src/field_engine/adaptive_sample_blocks_v1.py:103-128)."""
+    idx = np.asarray(indices, dtype=np.int64)
+    out = np.empty(len(idx), np.float32)
+    pending = [(0, np.arange(len(idx)))]
+    while pending:
+        nid, sel = pending.pop()
+        if not len(sel):
+            continue
+        node = nodes[nid]
+        left, right = node["children"]
+        if left < 0:
+            local = idx[sel] - node["lo"]
+            local[:, node["stored_shape"] == 1] = 0
+            lin = np.ravel_multi_index(local.T, tuple(node["stored_shape"]))
+            out[sel] = payload[node["offset"] + lin]
+        else:
+            b = nodes[left]
+            inl = np.all((idx[sel] >= b["lo"]) & (idx[sel] < b["lo"] + b["shape"]), axis=1)
+            pending.append((int(right), sel[~inl]))
+            pending.append((int(left), sel[inl]))
+    return out
+
+
+def query_trilinear(nodes, payload, shape, origin, pitch, points):
+    """float32 trilinear value on the fine grid, coordinates clipped into the grid, eight samples
+    gathered across leaves, interpolated by scipy.ndimage.map_coordinates(order=1, mode='nearest')
+    (src/field_engine/adaptive_sample_blocks_v1.py:130-151)."""
+    import itertools
+    from scipy import ndimage
+    pts = np.asarray(points, dtype=np.float64)
+    out = np.empty(len(pts), np.float32)
+    offsets = np.array(list(itertools.product((0, 1), repeat=3)), dtype=np.int64)
+    shp = np.array(shape)
+    for start in range(0, len(pts), 4096):
+        batch = pts[start:start + 4096]
+        c = np.clip((batch - np.asarray(origin, np.float64)) / pitch, 0, shp - 1)
+        lower = np.floor(c).astype(np.int64)
+        frac = c - lower
+        nb = np.minimum(lower[:, None, :] + offsets, shp - 1)
+        corners = samples_at(nodes, payload, nb.reshape(-1, 3)).reshape(-1, 2, 2, 2)
+        q = np.vstack((np.arange(len(batch)), frac.T))
+        out[start:start + len(batch)] = ndimage.map_coordinates(corners, q, order=1, mode="nearest")
+    return out
+
+
+# ----------------------------------------------------------------------------------------- analytic
+def eval_points(prims, prog, points):
+    """float64 program values at (N, 3) float64 points (src/field_engine/ikarus_v1/expr.py:263-385)."""
+    P = np.ascontiguousarray(prims, PRIM)
+    G = np.ascontiguousarray(prog, INSN)
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    out = np.empty(len(pts), np.float64)
+    rc = lib().or_eval_points(P.ctypes.data, len(P), G.ctypes.data, len(G), pts.ctypes.data, len(pts),
+                              out.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle eval status {rc}")
+    return out
+
+
+def classify_program(prims, prog, meta):
+    """(kind int32, corner_min_abs float64) of every block, float64 corners
+    (src/field_engine/faltkarna_v1.py:129-164)."""
+    P = np.ascontiguousarray(prims, PRIM)
+    G = np.ascontiguousarray(prog, INSN)
+    kind = np.empty(meta.n_blocks, np.int32)
+    cma = np.empty(meta.n_blocks, np.float64)
+    rc = lib().or_classify_program(P.ctypes.data, len(P), G.ctypes.data, len(G), meta.x0, meta.y0, meta.z0,
+                                   meta.pitch, meta.nx, meta.ny, meta.nz, meta.block,
+                                   float(np.float32(meta.margin_mm)), kind.ctypes.data, cma.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle classify status {rc}")
+    return kind, cma
+
+
+def tiles_program(prims, prog, meta, active_ids):
+    """float64 leaf values (n_active, B, B, B) of the given blocks (src/field_engine/faltkarna_v1.py:167-190)."""
+    P = np.ascontiguousarray(prims, PRIM)
+    G = np.ascontiguousarray(prog, INSN)
+    act = np.ascontiguousarray(active_ids, np.int32)
+    b = meta.block
+    out = np.empty((len(act), b, b, b), np.float64)
+    rc = lib().or_tiles_program(P.ctypes.data, len(P), G.ctypes.data, len(G), meta.x0, meta.y0, meta.z0,
+                                meta.pitch, meta.nx, meta.ny, meta.nz, b, act.ctypes.data, len(act),
+                                out.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle tiles status {rc}")
+    return out
+
+
+# ----------------------------------------------------------------------------------------- reference libs
+def ref_library(name):
+    """A reference CPU library compiled from the reference's own sources into oracle/_ref/
+    (``pack``, ``csg_batch`` or ``mesh_sdf``); None when it was not built on this machine."""
+    path = HERE / "_ref" / f"libref_{name}.so"
+    if not path.exists():
+        return None
+    return ct.CDLL(str(path))
+
+
+def ref_classify_dense(dense, pitch, block, nthreads=0):
+    """The reference's meshsdf_classify_cpu + meshsdf_tiles_cpu (OpenMP), same dict as
+    src/field_engine/mesh_sdf_native_v1.py:121-141."""
+    import math
+    L = ref_library("mesh_sdf")
+    if L is None:
+        raise RuntimeError("oracle/_ref/libref_mesh_sdf.so is not built")
+    P, I64 = ct.c_void_p, ct.c_int64
+    L.meshsdf_classify_cpu.argtypes = [P, I64, I64, I64, I64, ct.c_float, P, ct.c_int]
+    L.meshsdf_classify_cpu.restype = ct.c_int
+    L.meshsdf_tiles_cpu.argtypes = [P, I64, I64, I64, I64, P, I64, P, ct.c_int]
+    L.meshsdf_tiles_cpu.restype = ct.c_int
+    d = np.ascontiguousarray(dense, dtype=np.float32)
+    nx, ny, nz = d.shape
+    n_bx, n_by, n_bz = -(-nx // block), -(-ny // block), -(-nz // block)
+    margin = math.sqrt(3.0) * block * pitch
+    kind = np.empty(n_bx * n_by * n_bz, np.int32)
+    rc = L.meshsdf_classify_cpu(d.ctypes.data, nx, ny, nz, block, float(np.float32(margin)), kind.ctypes.data,
+                                int(nthreads))
+    if rc:
+        raise RuntimeError(f"reference classify status {rc}")
+    active = np.where(kind == 0)[0].astype(np.int32)
+    tiles = np.empty((len(active), block, block, block), np.float32)
+    if len(active):
+        rc = L.meshsdf_tiles_cpu(d.ctypes.data, nx, ny, nz, block, active.ctypes.data, len(active),
+                                 tiles.ctypes.data, int(nthreads))
+        if rc:
+            raise RuntimeError(f"reference tiles status {rc}")
+    return dict(kind=kind, active_ids=active, tiles=tiles, n_bx=n_bx, n_by=n_by, n_bz=n_bz,
+                n_blocks=int(len(kind)), n_active=int(len(active)), margin_mm=margin)
+
+
+def ref_pack(samples, threshold=512):
+    """The reference's adaptive_pack compiled from pack.cpp: (nodes, payload)."""
+    L = ref_library("pack")
+    if L is None:
+        raise RuntimeError("oracle/_ref/libref_pack.so is not built")
+    L.adaptive_pack.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int]
+    L.adaptive_pack.restype = ct.c_void_p
+    for name in ("adaptive_nodes", "adaptive_samples"):
+        getattr(L, name).argtypes = [ct.c_void_p]
+        getattr(L, name).restype = ct.c_int64
+    L.adaptive_copy.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_int64]
+    L.adaptive_copy.restype = ct.c_int
+    L.adaptive_free.argtypes = [ct.c_void_p]
+    L.adaptive_free.restype = None
+    a = np.ascontiguousarray(samples, dtype=np.float32)
+    shape = np.array(a.shape, np.int32)
+    h = L.adaptive_pack(a.ctypes.data, shape.ctypes.data, int(threshold))
+    if not h:
+        raise ValueError("reference packing refused the input")
+    try:
+        nodes = np.empty(L.adaptive_nodes(h), NODE)
+        payload = np.empty(L.adaptive_samples(h), np.float32)
+        if L.adaptive_copy(h, nodes.ctypes.data, len(nodes), payload.ctypes.data, len(payload)):
+            raise RuntimeError("reference pack copy failed")
+    finally:
+        L.adaptive_free(h)
+    return nodes, payload
