@@ -1,0 +1,1336 @@
+// Block-sparse field build on sm_100a: block classification, stream compaction and fused
+// leaf-tile evaluation with min/max CSG, for analytic recipes and for dense sampled fields.
+//
+// Analytic pipeline (all stream-ordered, no host round trip between kernels):
+//   k_prepare_prims  float32 mirror of the primitive table + per-primitive Lipschitz bound.
+//   k_cull           warp per region: walks the parent region's CSG chain list and keeps only the
+//                    elements that can influence the region (Lipschitz interval arithmetic, exact
+//                    for min/max: a skipped element is strictly dominated everywhere in the
+//                    region, and an element that strictly dominates resets the list).  Two levels:
+//                    128-voxel coarse regions from the full chain, 32-voxel superblocks from those.
+//   k_classify       thread per block: culls the superblock list to the block, evaluates the 8
+//                    corners in float32 in block-local coordinates, decides kind -1/0/+1 by the
+//                    reference rule, re-evaluating in float64 when a corner value lies within the
+//                    guard band of 0 or of the margin.
+//   k_compact        single-pass decoupled look-back scan: ascending active block ids + count.
+//   k_leaf<B>        warp per active block: block-level culling, float64 -> float32 localisation of
+//                    each surviving primitive, float32 evaluation of all B^3 voxels, float64 recheck
+//                    inside the guard band, vectorised 128-bit tile stores.
+// Reference semantics: src/field_engine/faltkarna_v1.py:51-82 (grid and layout), :129-164
+// (classification rule), :167-190 (tile order), :277 (ascending compaction); dense input
+// src/field_engine/faltkarna_v1_mesh_to_sdf.py:602-657.
+#include "common.cuh"
+#include "prims.cuh"
+#include <algorithm>
+#include <cmath>
+
+// Grid geometry of one build, fb_geom in include/field_b200.h.
+struct FbGeom {
+    double x0, y0, z0, pitch;
+    int32_t nx, ny, nz, block;
+    float margin, guard;
+    int32_t reserved[2];
+};
+static_assert(sizeof(FbGeom) == 64, "fb_geom layout");
+
+namespace {
+
+constexpr float kBig = 1.0e6f;  // background of interior (-) and exterior (+) blocks, faltkarna_v1.py:46
+constexpr int kCapCoarse = 1024;
+constexpr int kCapSuper = 256;
+constexpr int kCapBlock = 48;
+constexpr int kSuperEdge = 32;    // voxels per superblock edge
+constexpr int kCoarseDiv = 4;     // superblocks per coarse-region edge
+constexpr int kTile = 2048;       // compaction tile (256 threads x 8)
+constexpr int kLeafWarps = 4;     // warps per CTA in k_leaf
+
+
+struct Geo {
+    double x0, y0, z0, pitch;
+    float fx0, fy0, fz0, fpitch;
+    int nx, ny, nz, B;
+    int nbx, nby, nbz;
+    int64_t nblocks;
+    int S, nsx, nsy, nsz;
+    int64_t nsuper;
+    int ncx, ncy, ncz;
+    int64_t ncoarse;
+    float margin, guard, eps;
+};
+
+Geo make_geo(const FbGeom& g) {
+    Geo o{};
+    o.x0 = g.x0; o.y0 = g.y0; o.z0 = g.z0; o.pitch = g.pitch;
+    o.fx0 = (float)g.x0; o.fy0 = (float)g.y0; o.fz0 = (float)g.z0; o.fpitch = (float)g.pitch;
+    o.nx = g.nx; o.ny = g.ny; o.nz = g.nz; o.B = g.block;
+    o.nbx = (g.nx + g.block - 1) / g.block;
+    o.nby = (g.ny + g.block - 1) / g.block;
+    o.nbz = (g.nz + g.block - 1) / g.block;
+    o.nblocks = (int64_t)o.nbx * o.nby * o.nbz;
+    o.S = std::max(1, kSuperEdge / g.block);
+    o.nsx = (o.nbx + o.S - 1) / o.S;
+    o.nsy = (o.nby + o.S - 1) / o.S;
+    o.nsz = (o.nbz + o.S - 1) / o.S;
+    o.nsuper = (int64_t)o.nsx * o.nsy * o.nsz;
+    o.ncx = (o.nsx + kCoarseDiv - 1) / kCoarseDiv;
+    o.ncy = (o.nsy + kCoarseDiv - 1) / kCoarseDiv;
+    o.ncz = (o.nsz + kCoarseDiv - 1) / kCoarseDiv;
+    o.ncoarse = (int64_t)o.ncx * o.ncy * o.ncz;
+    o.margin = g.margin;
+    o.guard = g.guard;
+    o.eps = 4.0f * g.guard;
+    return o;
+}
+
+bool geom_ok(const FbGeom& g) {
+    if (!(g.pitch > 0) || !std::isfinite(g.pitch) || !std::isfinite(g.x0) || !std::isfinite(g.y0) ||
+        !std::isfinite(g.z0))
+        return false;
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || g.nx > 16384 || g.ny > 16384 || g.nz > 16384) return false;
+    if (g.block != 4 && g.block != 8 && g.block != 16) return false;
+    if (!(g.margin >= 0) || !(g.guard >= 0)) return false;
+    return true;
+}
+
+// ------------------------------------------------------------------------------------ scratch
+struct Plan {
+    int64_t primf, pool, off, len, status, misc, total;
+    int64_t pool_full, pool_coarse, pool_super;  // element offsets inside pool
+    int64_t ntiles;
+};
+
+int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
+
+Plan make_plan(const Geo& G, int n_prims, int n_chain) {
+    Plan p{};
+    int64_t at = 0;
+    p.primf = at; at += align256((int64_t)std::max(n_prims, 1) * sizeof(PrimF));
+    p.pool_full = 0;
+    p.pool_coarse = n_chain;
+    p.pool_super = p.pool_coarse + G.ncoarse * kCapCoarse;
+    const int64_t pool_elems = p.pool_super + G.nsuper * kCapSuper;
+    p.pool = at; at += align256(pool_elems * 4);
+    p.off = at; at += align256((G.ncoarse + G.nsuper) * 8);
+    p.len = at; at += align256((G.ncoarse + G.nsuper) * 4);
+    p.ntiles = (G.nblocks + kTile - 1) / kTile;
+    p.status = at; at += align256(p.ntiles * 8);
+    p.misc = at; at += 256;  // [0] ticket, [1] error flag
+    p.total = at;
+    return p;
+}
+
+// Compaction needs only the status words and the misc block.
+int64_t compact_scratch(int64_t nblocks) { return align256((nblocks + kTile - 1) / kTile * 8) + 256; }
+
+// ------------------------------------------------------------------------------------ prepare
+__global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const FbPrim P = prims[i];
+    PrimF F;
+    F.type = P.type;
+    F.s = (float)P.s;
+    F.off = (float)P.off;
+    F.pad0 = F.pad1 = F.pad2 = 0.f;
+    bool ident = true;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) ident &= P.A[r * 4 + c] == (r == c ? 1.0 : 0.0);
+    F.ident = ident ? 1 : 0;
+    for (int j = 0; j < 12; ++j) F.A[j] = (float)P.A[j];
+    // Lipschitz bound of x -> f(A x + t): sqrt of the Gershgorin bound on A^T A.
+    double G[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += P.A[k * 4 + r] * P.A[k * 4 + c];
+            G[r][c] = s;
+        }
+    double row = 0;
+    for (int r = 0; r < 3; ++r) row = fmax(row, fabs(G[r][0]) + fabs(G[r][1]) + fabs(G[r][2]));
+    double canon = 1.0;
+    for (int j = 0; j < 12; ++j) F.p[j] = 0.f;
+    const double* p = P.p;
+    switch (P.type) {
+    case P_CONE:
+        canon = 2.0 + fabs(p[1] - p[0]) / p[2];
+        F.p[0] = (float)p[0]; F.p[1] = (float)p[1]; F.p[2] = (float)p[2]; F.p[3] = (float)(1.0 / p[2]);
+        break;
+    case P_FRUSTUM: {
+        const double z1 = p[0], hx0 = p[1], hy0 = p[2], hx1 = p[3], hy1 = p[4], cx1 = p[5], cy1 = p[6];
+        const double kx = (hx1 - hx0) / z1, ky = (hy1 - hy0) / z1, kcx = cx1 / z1, kcy = cy1 / z1;
+        const double a[4] = {-(kx + kcx), -(kx - kcx), -(ky + kcy), -(ky - kcy)};
+        F.p[0] = (float)z1; F.p[1] = (float)hx0; F.p[2] = (float)hy0;
+        for (int j = 0; j < 4; ++j) {
+            F.p[3 + j] = (float)a[j];
+            F.p[7 + j] = (float)(1.0 / sqrt(1.0 + a[j] * a[j]));
+        }
+        break;
+    }
+    case P_CAPSULE: {
+        const double bb = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+        for (int j = 0; j < 4; ++j) F.p[j] = (float)p[j];
+        F.p[4] = bb > 0 ? (float)(1.0 / bb) : 0.f;
+        break;
+    }
+    default:
+        for (int j = 0; j < 12; ++j) F.p[j] = (float)p[j];
+    }
+    F.lip = (float)(fabs(P.s) * sqrt(row) * canon * (1.0 + 1e-6));
+    out[i] = F;
+}
+
+__global__ void k_full_list(uint32_t* __restrict__ list, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) list[i] = (uint32_t)i << 2;
+}
+
+// ------------------------------------------------------------------------------------ culling
+// One interval step of the chain walk.  Returns 0 skip, 1 keep, 2 reset to "set", 3 reset to
+// "set negated".  [alo, ahi] bounds the accumulator over the region.
+__device__ __forceinline__ int interval_step(int op, float k, float plo, float phi, float& alo, float& ahi) {
+    switch (op) {
+    case CH_SET:
+        alo = plo; ahi = phi;
+        return 2;
+    case CH_SETNEG:
+        alo = -phi; ahi = -plo;
+        return 3;
+    case CH_UNION:
+        if (plo > ahi + k) return 0;
+        if (phi < alo - k) { alo = plo; ahi = phi; return 2; }
+        alo = fminf(alo, plo) - 0.25f * k;
+        ahi = fminf(ahi, phi);
+        return 1;
+    case CH_INTERSECT:
+        if (phi < alo - k) return 0;
+        if (plo > ahi + k) { alo = plo; ahi = phi; return 2; }
+        alo = fmaxf(alo, plo);
+        ahi = fmaxf(ahi, phi) + 0.25f * k;
+        return 1;
+    case CH_SUBTRACT:
+        if (-plo < alo - k) return 0;
+        if (-phi > ahi + k) { alo = -phi; ahi = -plo; return 3; }
+        alo = fmaxf(alo, -phi);
+        ahi = fmaxf(ahi, -plo) + 0.25f * k;
+        return 1;
+    default:  // offset
+        alo -= k; ahi -= k;
+        return 1;
+    }
+}
+
+__device__ __forceinline__ int effective_op(uint32_t entry, int op) {
+    const uint32_t mode = entry & 3u;
+    return mode == 1u ? CH_SET : (mode == 2u ? CH_SETNEG : op);
+}
+
+// Interval of one chain element's primitive around (cx, cy, cz) with radius R.
+__device__ __forceinline__ void element_interval(const PrimF& P, float cx, float cy, float cz, float R, float eps,
+                                                 float& lo, float& hi) {
+    const float v = primf_world(P, cx, cy, cz);
+    const float r = fmaf(P.lip, R, eps + 1e-6f * fabsf(v));
+    lo = v - r;
+    hi = v + r;
+}
+
+// A hard (k == 0) union / intersection / subtraction: consecutive ones of the same kind form a
+// run whose result is an order-free min or max of the accumulator and the run's elements.
+__device__ __forceinline__ bool runnable(int op, float k) {
+    return k == 0.f && (op == CH_UNION || op == CH_INTERSECT || op == CH_SUBTRACT);
+}
+
+struct Elem {
+    uint32_t ent;
+    int op;
+    float k;
+    float lo, hi;  // bounds of the value the combine sees (-p for a subtraction)
+};
+
+__device__ __forceinline__ Elem load_elem(const uint32_t* __restrict__ in, int e, const FbInsn* __restrict__ chain,
+                                          const PrimF* __restrict__ primf, float cx, float cy, float cz, float R,
+                                          float eps, bool with_bounds) {
+    Elem E;
+    E.ent = in[e];
+    const FbInsn I = chain[E.ent >> 2];
+    E.op = effective_op(E.ent, I.op);
+    E.k = (float)I.k;
+    E.lo = E.hi = 0.f;
+    if (with_bounds && E.op != CH_OFFSET) {
+        float lo, hi;
+        element_interval(primf[I.arg], cx, cy, cz, R, eps, lo, hi);
+        if (E.op == CH_SUBTRACT || E.op == CH_SETNEG) { E.lo = -hi; E.hi = -lo; }
+        else { E.lo = lo; E.hi = hi; }
+    }
+    return E;
+}
+
+// Run decision.  union: result = min(acc, run); an element whose lower bound exceeds
+// H = min(acc_hi, min run hi) is never the minimum and is dropped; when min run hi < acc_lo the
+// accumulator so far is dominated everywhere and dropped (the run restarts the list).
+// intersection / subtraction: the mirror image with max.  All comparisons are strict, so every
+// decision is exact for the float values the bounds enclose.
+struct RunState {
+    float bound;   // H (union) or L (max kinds)
+    bool reset;
+};
+
+__device__ __forceinline__ RunState run_decide(int op, float agg, float alo, float ahi) {
+    RunState r;
+    if (op == CH_UNION) {
+        r.reset = agg < alo;
+        r.bound = r.reset ? agg : fminf(ahi, agg);
+    } else {
+        r.reset = agg > ahi;
+        r.bound = r.reset ? agg : fmaxf(alo, agg);
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool run_keep(int op, const Elem& E, float bound) {
+    return op == CH_UNION ? !(E.lo > bound) : !(E.hi < bound);
+}
+
+// Warp-cooperative chain walk over `in` for the region centred at (cx, cy, cz) with radius R.
+// Hard runs are decided with two warp-parallel passes (aggregate bound, then keep/drop with
+// ballot compaction); other elements (offsets, smooth booleans, sets) step one at a time.
+// Returns the kept count (may exceed cap: then the output is incomplete and must not be used).
+__device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn* __restrict__ chain,
+                         const PrimF* __restrict__ primf, float cx, float cy, float cz, float R, float eps,
+                         uint32_t* __restrict__ out, int cap) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    float alo = 0.f, ahi = 0.f;
+    int n = 0;
+    int i = 0;
+    while (i < n_in) {
+        const Elem head = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, false);
+        if (!runnable(head.op, head.k)) {
+            const Elem E = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, true);
+            float plo = E.lo, phi = E.hi;  // back to the primitive's own bounds
+            if (E.op == CH_SUBTRACT || E.op == CH_SETNEG) { plo = -E.hi; phi = -E.lo; }
+            const int act = interval_step(E.op, E.k, plo, phi, alo, ahi);
+            if (act) {
+                uint32_t rec = E.ent;
+                if (act == 2) { n = 0; rec = (E.ent & ~3u) | 1u; }
+                if (act == 3) { n = 0; rec = (E.ent & ~3u) | 2u; }
+                if (n < cap && lane == 0) out[n] = rec;
+                ++n;
+            }
+            ++i;
+            continue;
+        }
+        const int op = head.op;
+        // end of the run
+        int j = i + 1;
+        while (j < n_in) {
+            const int e = j + lane;
+            bool same = false;
+            if (e < n_in) {
+                const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, false);
+                same = E.op == op && runnable(E.op, E.k);
+            }
+            const unsigned stop = __ballot_sync(0xffffffffu, !same);
+            if (stop) { j += __ffs(stop) - 1; break; }
+            j += 32;
+        }
+        j = min(j, n_in);
+        // pass 1: aggregate bound of the run
+        float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
+        for (int b = i; b < j; b += 32) {
+            const int e = b + lane;
+            if (e < j) {
+                const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+                agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float t = __shfl_xor_sync(0xffffffffu, agg, o);
+            agg = op == CH_UNION ? fminf(agg, t) : fmaxf(agg, t);
+        }
+        const RunState rs = run_decide(op, agg, alo, ahi);
+        if (rs.reset) n = 0;
+        bool first = rs.reset;
+        float klo = 3.0e38f, khi = -3.0e38f;
+        // pass 2: keep / drop, ballot compaction in chain order
+        for (int b = i; b < j; b += 32) {
+            const int e = b + lane;
+            bool keep = false;
+            Elem E;
+            if (e < j) {
+                E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+                keep = run_keep(op, E, rs.bound);
+                if (keep) { klo = fminf(klo, E.lo); khi = fmaxf(khi, E.hi); }
+            }
+            const unsigned kept = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int pos = n + __popc(kept & below);
+                uint32_t rec = E.ent;
+                if (first && pos == 0) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
+                if (pos < cap) out[pos] = rec;
+            }
+            if (kept) first = false;
+            n += __popc(kept);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            klo = fminf(klo, __shfl_xor_sync(0xffffffffu, klo, o));
+            khi = fmaxf(khi, __shfl_xor_sync(0xffffffffu, khi, o));
+        }
+        if (op == CH_UNION) {
+            alo = rs.reset ? klo : fminf(alo, klo);
+            ahi = rs.bound;
+        } else {
+            alo = rs.bound;
+            ahi = rs.reset ? khi : fmaxf(ahi, khi);
+        }
+        i = j;
+    }
+    return n;
+}
+
+// The same walk by one thread (block-level culling in k_classify).
+__device__ int seq_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn* __restrict__ chain,
+                        const PrimF* __restrict__ primf, float cx, float cy, float cz, float R, float eps,
+                        uint32_t* __restrict__ out, int cap) {
+    float alo = 0.f, ahi = 0.f;
+    int n = 0;
+    int i = 0;
+    while (i < n_in) {
+        const Elem head = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, false);
+        if (!runnable(head.op, head.k)) {
+            const Elem E = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, true);
+            float plo = E.lo, phi = E.hi;  // back to the primitive's own bounds
+            if (E.op == CH_SUBTRACT || E.op == CH_SETNEG) { plo = -E.hi; phi = -E.lo; }
+            const int act = interval_step(E.op, E.k, plo, phi, alo, ahi);
+            if (act) {
+                uint32_t rec = E.ent;
+                if (act == 2) { n = 0; rec = (E.ent & ~3u) | 1u; }
+                if (act == 3) { n = 0; rec = (E.ent & ~3u) | 2u; }
+                if (n < cap) out[n] = rec;
+                ++n;
+            }
+            ++i;
+            continue;
+        }
+        const int op = head.op;
+        int j = i + 1;
+        while (j < n_in) {
+            const Elem E = load_elem(in, j, chain, primf, cx, cy, cz, R, eps, false);
+            if (!(E.op == op && runnable(E.op, E.k))) break;
+            ++j;
+        }
+        float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
+        for (int e = i; e < j; ++e) {
+            const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+            agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+        }
+        const RunState rs = run_decide(op, agg, alo, ahi);
+        if (rs.reset) n = 0;
+        bool first = rs.reset;
+        float klo = 3.0e38f, khi = -3.0e38f;
+        for (int e = i; e < j; ++e) {
+            const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+            if (!run_keep(op, E, rs.bound)) continue;
+            klo = fminf(klo, E.lo);
+            khi = fmaxf(khi, E.hi);
+            uint32_t rec = E.ent;
+            if (first) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
+            first = false;
+            if (n < cap) out[n] = rec;
+            ++n;
+        }
+        if (op == CH_UNION) {
+            alo = rs.reset ? klo : fminf(alo, klo);
+            ahi = rs.bound;
+        } else {
+            alo = rs.bound;
+            ahi = rs.reset ? khi : fmaxf(ahi, khi);
+        }
+        i = j;
+    }
+    return n;
+}
+
+// Level cull.  Regions of `edge` voxels on a (rnx, rny, rnz) grid; parent region = coords / div
+// on a (pnx, pny, pnz) grid (parent_off == nullptr: the single full list [0, n_full)).
+__global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
+                       uint32_t* __restrict__ pool, const int64_t* __restrict__ parent_off,
+                       const int32_t* __restrict__ parent_len, int n_full, int div, int pny, int pnz,
+                       int64_t* __restrict__ off, int32_t* __restrict__ len, int64_t pool_base, int cap, int edge,
+                       int rnx, int rny, int rnz) {
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nreg = (int64_t)rnx * rny * rnz;
+    if (r >= nreg) return;
+    const int rz = (int)(r % rnz), ry = (int)((r / rnz) % rny), rx = (int)(r / ((int64_t)rnz * rny));
+    int64_t poff = 0;
+    int plen = n_full;
+    if (parent_off) {
+        const int64_t pr = ((int64_t)(rx / div) * pny + ry / div) * pnz + rz / div;
+        poff = parent_off[pr];
+        plen = parent_len[pr];
+    }
+    const float half = 0.5f * edge;
+    const float cx = G.fx0 + (rx * edge + half) * G.fpitch;
+    const float cy = G.fy0 + (ry * edge + half) * G.fpitch;
+    const float cz = G.fz0 + (rz * edge + half) * G.fpitch;
+    const float R = 1.7320509f * half * G.fpitch;
+    uint32_t* dst = pool + pool_base + r * cap;
+    const int n = warp_walk(pool + poff, plen, chain, primf, cx, cy, cz, R, G.eps, dst, cap);
+    if ((threadIdx.x & 31) == 0) {
+        if (n <= cap) {
+            off[r] = pool_base + r * cap;
+            len[r] = n;
+        } else {  // overflow: the region keeps its parent's list (still exact, only slower)
+            off[r] = poff;
+            len[r] = plen;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------ localisation
+// Block-local float32 record of one primitive: L = A * origin + t in float64, rounded once.
+__device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double ox, double oy, double oz, int op,
+                                         float k, LocalPrim& out) {
+    out.type = F.type;
+    out.op = op;
+    out.ident = F.ident;
+    out.k = k;
+    out.s = F.s;
+    out.off = F.off;
+    const double* A = D.A;
+    out.L[0] = (float)fma(A[0], ox, fma(A[1], oy, fma(A[2], oz, A[3])));
+    out.L[1] = (float)fma(A[4], ox, fma(A[5], oy, fma(A[6], oz, A[7])));
+    out.L[2] = (float)fma(A[8], ox, fma(A[9], oy, fma(A[10], oz, A[11])));
+    out.L[3] = 0.f;
+    out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
+    out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
+    out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
+#pragma unroll
+    for (int j = 0; j < 12; ++j) out.p[j] = F.p[j];
+}
+
+// ------------------------------------------------------------------------------------ classify
+// float64 value of a block list at a world point (guard-band recheck).
+__device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, int n, const FbInsn* __restrict__ chain,
+                              const FbPrim* __restrict__ prims, double x, double y, double z) {
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const uint32_t e = list[i];
+        const FbInsn I = chain[e >> 2];
+        const int op = effective_op(e, I.op);
+        const double v = op == CH_OFFSET ? 0.0 : prim_world_d(prims[I.arg], x, y, z);
+        acc = chain_apply_d(op, acc, v, I.k);
+    }
+    return acc;
+}
+
+template <bool kChain>
+__global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restrict__ prims,
+                                                  const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
+                                                  int n_chain, const uint32_t* __restrict__ pool,
+                                                  const int64_t* __restrict__ sb_off,
+                                                  const int32_t* __restrict__ sb_len, int32_t* __restrict__ kind,
+                                                  float* __restrict__ cma) {
+    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (b >= G.nblocks) return;
+    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
+    const int B = G.B;
+    float v[8];
+    double vd[8];
+    bool use_d = false;
+    if (kChain) {
+        const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
+        const uint32_t* plist = pool + sb_off[s];
+        const int plen = sb_len[s];
+        // block-level cull of the superblock list
+        uint32_t blist[kCapBlock];
+        const float half = 0.5f * B;
+        const float cx = G.fx0 + (bi * B + half) * G.fpitch;
+        const float cy = G.fy0 + (bj * B + half) * G.fpitch;
+        const float cz = G.fz0 + (bk * B + half) * G.fpitch;
+        const float R = 1.7320509f * half * G.fpitch;
+        const int n = seq_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, blist, kCapBlock);
+        const uint32_t* list = n <= kCapBlock ? blist : plist;
+        const int len = n <= kCapBlock ? n : plen;
+        const double ox = G.x0 + (double)(bi * B) * G.pitch;
+        const double oy = G.y0 + (double)(bj * B) * G.pitch;
+        const double oz = G.z0 + (double)(bk * B) * G.pitch;
+        const float side = (float)B * G.fpitch;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = 0.f;
+        for (int i = 0; i < len; ++i) {
+            const uint32_t e = list[i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            const float k = (float)I.k;
+            if (op == CH_OFFSET) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) v[c] -= k;
+                continue;
+            }
+            LocalPrim P;
+            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const float pv = local_eval(P, (c & 1) ? side : 0.f, ((c >> 1) & 1) ? side : 0.f,
+                                            ((c >> 2) & 1) ? side : 0.f);
+                v[c] = chain_apply(op, v[c], pv, k);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float a = fabsf(v[c]);
+            use_d |= a < G.guard || fabsf(a - G.margin) < G.guard || !(a == a);
+        }
+        if (use_d) {
+            for (int c = 0; c < 8; ++c) {
+                const int64_t ix = (int64_t)bi * B + (c & 1) * B, iy = (int64_t)bj * B + ((c >> 1) & 1) * B,
+                              iz = (int64_t)bk * B + ((c >> 2) & 1) * B;
+                vd[c] = list_eval_d(list, len, chain, prims, rn_add(G.x0, rn_mul((double)ix, G.pitch)),
+                                    rn_add(G.y0, rn_mul((double)iy, G.pitch)), rn_add(G.z0, rn_mul((double)iz, G.pitch)));
+            }
+        }
+    } else {
+        use_d = true;
+        for (int c = 0; c < 8; ++c) {
+            const int64_t ix = (int64_t)bi * B + (c & 1) * B, iy = (int64_t)bj * B + ((c >> 1) & 1) * B,
+                          iz = (int64_t)bk * B + ((c >> 2) & 1) * B;
+            vd[c] = program_eval_d(prims, chain, n_chain, rn_add(G.x0, rn_mul((double)ix, G.pitch)),
+                                   rn_add(G.y0, rn_mul((double)iy, G.pitch)), rn_add(G.z0, rn_mul((double)iz, G.pitch)));
+        }
+    }
+    bool pos = false, neg = false;
+    int kd;
+    if (use_d) {
+        double mn = 1.0e30;
+        for (int c = 0; c < 8; ++c) {
+            mn = fmin(mn, fabs(vd[c]));
+            if (vd[c] >= 0.0) pos = true; else neg = true;
+        }
+        kd = (pos && neg) ? 0 : (mn <= (double)G.margin ? 0 : (neg ? -1 : 1));
+        cma[b] = (float)mn;
+    } else {
+        float mn = 1.0e30f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            mn = fminf(mn, fabsf(v[c]));
+            if (v[c] >= 0.f) pos = true; else neg = true;
+        }
+        kd = (pos && neg) ? 0 : (mn <= G.margin ? 0 : (neg ? -1 : 1));
+        cma[b] = mn;
+    }
+    kind[b] = kd;
+}
+
+// ------------------------------------------------------------------------------------ compaction
+// Single-pass scan with decoupled look-back over tiles of kTile block kinds.  Tiles are claimed in
+// order from a ticket counter, so every predecessor is already running when a tile waits on it;
+// each wait is bounded and a timeout raises the error flag instead of hanging.
+__device__ __forceinline__ unsigned long long ld_status(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kind, int64_t n,
+                                                 int32_t* __restrict__ active, int32_t* __restrict__ count,
+                                                 unsigned long long* __restrict__ status, int* __restrict__ misc,
+                                                 int64_t ntiles) {
+    __shared__ int s_tile;
+    __shared__ int s_warp[8];
+    __shared__ long long s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&misc[0], 1);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t base = tile * kTile + (int64_t)threadIdx.x * 8;
+    unsigned flags = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int64_t i = base + j;
+        if (i < n && kind[i] == 0) flags |= 1u << j;
+    }
+    const int c = __popc(flags);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    int wbase = 0, total = 0;
+    for (int w = 0; w < 8; ++w) {
+        if (w < warp) wbase += s_warp[w];
+        total += s_warp[w];
+    }
+    const int excl = wbase + incl - c;
+    constexpr unsigned long long kAgg = 1ull << 62, kInc = 2ull << 62, kMask = (1ull << 62) - 1;
+    if (threadIdx.x == 0) {
+        long long prefix = 0;
+        if (tile == 0) {
+            atomicExch(&status[0], kInc | (unsigned long long)total);
+        } else {
+            atomicExch(&status[tile], kAgg | (unsigned long long)total);
+            int64_t j = tile - 1;
+            long long spins = 0;
+            while (j >= 0) {
+                const unsigned long long s = ld_status(&status[j]);
+                const unsigned long long flag = s & ~kMask;
+                if (flag == 0) {
+                    if (++spins > (1ll << 24)) {
+                        atomicExch(&misc[1], 1);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                prefix += (long long)(s & kMask);
+                if (flag == kInc) break;
+                --j;
+            }
+            __threadfence();
+            atomicExch(&status[tile], kInc | (unsigned long long)(prefix + total));
+        }
+        s_prefix = prefix;
+        if (tile == ntiles - 1) count[0] = (int32_t)(prefix + total);
+    }
+    __syncthreads();
+    const long long start = s_prefix + excl;
+    int k = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if (flags & (1u << j)) active[start + k++] = (int32_t)(base + j);
+}
+
+// ------------------------------------------------------------------------------------ leaf eval
+
+// Canonical primitive of a fixed type (the switch is taken once per primitive and group of
+// voxels, not once per voxel, which keeps the evaluation loop small enough for the i-cache).
+template <int T>
+__device__ __forceinline__ float canon_t(const float* __restrict__ p, float x, float y, float z) {
+    if (T == P_SPHERE) return sqrtf(fmaf(x, x, fmaf(y, y, z * z))) - p[0];
+    if (T == P_BOX) {
+        const float qx = fabsf(x) - p[0], qy = fabsf(y) - p[1], qz = fabsf(z) - p[2];
+        const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f), oz = fmaxf(qz, 0.f);
+        return sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.f);
+    }
+    if (T == P_CAPSULE) {
+        const float h = fminf(fmaxf(fmaf(x, p[0], fmaf(y, p[1], z * p[2])) * p[4], 0.f), 1.f);
+        const float dx = fmaf(-p[0], h, x), dy = fmaf(-p[1], h, y), dz = fmaf(-p[2], h, z);
+        return sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - p[3];
+    }
+    if (T == P_TORUS) {
+        const float qx = sqrtf(fmaf(x, x, y * y)) - p[0];
+        return sqrtf(fmaf(qx, qx, z * z)) - p[1];
+    }
+    return canon_f(T, p, x, y, z);
+}
+
+// VG voxels along z of one lane: values of primitive P at block offsets (dx, dy, dz0 + k*pz).
+template <int VG, int T>
+__device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+    const float* p = P.p;
+    if (P.ident) {
+        const float x = P.L[0] + dx, y = P.L[1] + dy;
+#pragma unroll
+        for (int k = 0; k < VG; ++k) v[k] = fmaf(P.s, canon_t<T>(p, x, y, P.L[2] + dz[k]), -P.off);
+    } else {
+        const float bx = fmaf(P.A[0], dx, fmaf(P.A[1], dy, P.L[0]));
+        const float by = fmaf(P.A[3], dx, fmaf(P.A[4], dy, P.L[1]));
+        const float bz = fmaf(P.A[6], dx, fmaf(P.A[7], dy, P.L[2]));
+#pragma unroll
+        for (int k = 0; k < VG; ++k)
+            v[k] = fmaf(P.s, canon_t<T>(p, fmaf(P.A[2], dz[k], bx), fmaf(P.A[5], dz[k], by), fmaf(P.A[8], dz[k], bz)),
+                        -P.off);
+    }
+}
+
+template <int VG>
+__device__ __forceinline__ void eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+    switch (P.type) {
+    case P_SPHERE: eval_group_t<VG, P_SPHERE>(P, dx, dy, dz, v); break;
+    case P_BOX: eval_group_t<VG, P_BOX>(P, dx, dy, dz, v); break;
+    case P_CAPSULE: eval_group_t<VG, P_CAPSULE>(P, dx, dy, dz, v); break;
+    case P_TORUS: eval_group_t<VG, P_TORUS>(P, dx, dy, dz, v); break;
+    case P_CYLINDER: eval_group_t<VG, P_CYLINDER>(P, dx, dy, dz, v); break;
+    case P_CONE: eval_group_t<VG, P_CONE>(P, dx, dy, dz, v); break;
+    case P_HALFSPACE: eval_group_t<VG, P_HALFSPACE>(P, dx, dy, dz, v); break;
+    case P_FRUSTUM: eval_group_t<VG, P_FRUSTUM>(P, dx, dy, dz, v); break;
+    default: eval_group_t<VG, P_CYL_INF>(P, dx, dy, dz, v);
+    }
+}
+
+// acc = op(acc, v) for the VG voxels; the operator switch is taken once.
+template <int VG>
+__device__ __forceinline__ void combine_group(int op, float k, float* acc, const float* v) {
+    if (k > 0.f) {
+#pragma unroll
+        for (int j = 0; j < VG; ++j) acc[j] = chain_apply(op, acc[j], v[j], k);
+        return;
+    }
+    switch (op) {
+    case CH_SET:
+#pragma unroll
+        for (int j = 0; j < VG; ++j) acc[j] = v[j];
+        break;
+    case CH_SETNEG:
+#pragma unroll
+        for (int j = 0; j < VG; ++j) acc[j] = -v[j];
+        break;
+    case CH_UNION:
+#pragma unroll
+        for (int j = 0; j < VG; ++j) acc[j] = sel_min(acc[j], v[j]);
+        break;
+    case CH_INTERSECT:
+#pragma unroll
+        for (int j = 0; j < VG; ++j) acc[j] = sel_max(acc[j], v[j]);
+        break;
+    default:  // subtraction
+#pragma unroll
+        for (int j = 0; j < VG; ++j) acc[j] = sel_max(acc[j], -v[j]);
+    }
+}
+
+__device__ __noinline__ double guard_value(const uint32_t* __restrict__ list, int len, const FbInsn* __restrict__ chain,
+                                           const FbPrim* __restrict__ prims, const Geo& G, int64_t ix, int64_t iy,
+                                           int64_t iz) {
+    return list_eval_d(list, len, chain, prims, rn_add(G.x0, rn_mul((double)ix, G.pitch)),
+                       rn_add(G.y0, rn_mul((double)iy, G.pitch)), rn_add(G.z0, rn_mul((double)iz, G.pitch)));
+}
+
+// float32 operations of one localised primitive evaluation (affine + canonical formula + scale),
+// counting an FMA as two; the executed-work basis of the float32-pipe roofline.
+__device__ __forceinline__ unsigned prim_flops(int type, int ident) {
+    const unsigned affine = ident ? 3u : 18u;
+    unsigned f;
+    switch (type) {
+    case P_SPHERE: f = 7; break;      // 2 fma + mul + sqrt + sub
+    case P_BOX: f = 19; break;
+    case P_CYLINDER: f = 15; break;
+    case P_CONE: f = 22; break;
+    case P_HALFSPACE: f = 5; break;
+    case P_FRUSTUM: f = 30; break;
+    case P_CAPSULE: f = 22; break;
+    case P_TORUS: f = 12; break;
+    default: f = 5;
+    }
+    return affine + f + 2;
+}
+
+// Leaf tile of one block whose culled list is longer than the shared staging: every primitive is
+// localised on the fly (rare; kept out of line so the fast loop stays small).
+template <int B, int VG>
+__device__ __noinline__ void leaf_block_slow(const Geo& G, const FbPrim* __restrict__ prims,
+                                             const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
+                                             const uint32_t* __restrict__ list, int len, int bi, int bj, int bk,
+                                             float* __restrict__ out) {
+    constexpr int kVox = B * B * B;
+    constexpr int kGroups = kVox / (32 * VG);
+    const int lane = threadIdx.x & 31;
+    const double ox = G.x0 + (double)(bi * B) * G.pitch;
+    const double oy = G.y0 + (double)(bj * B) * G.pitch;
+    const double oz = G.z0 + (double)(bk * B) * G.pitch;
+    for (int g = 0; g < kGroups; ++g) {
+        const int v0 = (g * 32 + lane) * VG;
+        const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
+        const float dx = li * G.fpitch, dy = lj * G.fpitch;
+        float dz[VG], acc[VG], v[VG];
+        for (int k = 0; k < VG; ++k) {
+            dz[k] = (lk0 + k) * G.fpitch;
+            acc[k] = 0.f;
+        }
+        for (int i = 0; i < len; ++i) {
+            const uint32_t e = list[i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            if (op == CH_OFFSET) {
+                for (int k = 0; k < VG; ++k) acc[k] -= (float)I.k;
+                continue;
+            }
+            LocalPrim P;
+            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, P);
+            eval_group<VG>(P, dx, dy, dz, v);
+            combine_group<VG>(op, P.k, acc, v);
+        }
+        for (int k = 0; k < VG; ++k)
+            if (!(fabsf(acc[k]) >= G.guard))
+                acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li, (int64_t)bj * B + lj,
+                                            (int64_t)bk * B + lk0 + k);
+        if (VG == 4) reinterpret_cast<float4*>(out)[g * 32 + lane] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        else reinterpret_cast<float2*>(out)[g * 32 + lane] = make_float2(acc[0], acc[1]);
+    }
+}
+
+// Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
+// voxels along z (VG = 4, or 2 for 4^3 blocks) and stores each group with one vector store.
+template <int B>
+__global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim* __restrict__ prims,
+                                                             const PrimF* __restrict__ primf,
+                                                             const FbInsn* __restrict__ chain,
+                                                             const uint32_t* __restrict__ pool,
+                                                             const int64_t* __restrict__ sb_off,
+                                                             const int32_t* __restrict__ sb_len,
+                                                             const int32_t* __restrict__ active,
+                                                             const int32_t* __restrict__ count, int64_t capacity,
+                                                             float* __restrict__ tiles,
+                                                             unsigned long long* __restrict__ work) {
+    constexpr int kVox = B * B * B;
+    constexpr int VG = B == 4 ? 2 : 4;
+    constexpr int kGroups = kVox / (32 * VG);
+    __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
+    __shared__ uint32_t s_list[kLeafWarps][kCapBlock];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t n_active = min((int64_t)count[0], capacity);
+    LocalPrim* sp = s_prim[warp];
+    uint32_t* sl = s_list[warp];
+    for (int64_t a = gwarp; a < n_active; a += nwarps) {
+        const int64_t blk = active[a];
+        float* out = tiles + a * kVox;
+        if (blk < 0 || blk >= G.nblocks) {  // an id outside the grid (a corrupted list) reads as exterior
+            for (int v = lane; v < kVox; v += 32) out[v] = kBig;
+            continue;
+        }
+        const int bk = (int)(blk % G.nbz), bj = (int)((blk / G.nbz) % G.nby), bi = (int)(blk / ((int64_t)G.nbz * G.nby));
+        const double ox = G.x0 + (double)(bi * B) * G.pitch;
+        const double oy = G.y0 + (double)(bj * B) * G.pitch;
+        const double oz = G.z0 + (double)(bk * B) * G.pitch;
+        const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
+        const uint32_t* plist = pool + sb_off[s];
+        const int plen = sb_len[s];
+        const float half = 0.5f * B;
+        const float cx = G.fx0 + (bi * B + half) * G.fpitch;
+        const float cy = G.fy0 + (bj * B + half) * G.fpitch;
+        const float cz = G.fz0 + (bk * B + half) * G.fpitch;
+        const float R = 1.7320509f * half * G.fpitch;
+        __syncwarp();
+        const int nk = warp_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, sl, kCapBlock);
+        __syncwarp();
+        const bool fits = nk <= kCapBlock;
+        const uint32_t* list = fits ? sl : plist;
+        const int len = fits ? nk : plen;
+        if (work) {  // executed primitive evaluations and their float32 operation count
+            unsigned long long evals = 0, flops = 0;
+            for (int i = lane; i < len; i += 32) {
+                const FbInsn I = chain[list[i] >> 2];
+                const int op = effective_op(list[i], I.op);
+                if (op == CH_OFFSET) { flops += 1; continue; }
+                evals += 1;
+                flops += prim_flops(primf[I.arg].type, primf[I.arg].ident) + (I.k > 0 ? 8 : 1);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                evals += __shfl_xor_sync(0xffffffffu, evals, o);
+                flops += __shfl_xor_sync(0xffffffffu, flops, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&work[0], evals * kVox);
+                atomicAdd(&work[1], flops * kVox);
+            }
+        }
+        if (!fits) {
+            leaf_block_slow<B, VG>(G, prims, primf, chain, list, len, bi, bj, bk, out);
+            continue;
+        }
+        for (int i = lane; i < len; i += 32) {
+            const uint32_t e = list[i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            if (op == CH_OFFSET) {
+                sp[i].op = op;
+                sp[i].k = (float)I.k;
+            } else {
+                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
+            }
+        }
+        __syncwarp();
+        for (int g = 0; g < kGroups; ++g) {
+            const int v0 = (g * 32 + lane) * VG;
+            const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
+            const float dx = li * G.fpitch, dy = lj * G.fpitch;
+            float dz[VG], acc[VG], v[VG];
+#pragma unroll
+            for (int k = 0; k < VG; ++k) {
+                dz[k] = (lk0 + k) * G.fpitch;
+                acc[k] = 0.f;
+            }
+            for (int i = 0; i < len; ++i) {
+                const LocalPrim& P = sp[i];
+                const int op = P.op;
+                if (op == CH_OFFSET) {
+#pragma unroll
+                    for (int k = 0; k < VG; ++k) acc[k] -= P.k;
+                    continue;
+                }
+                eval_group<VG>(P, dx, dy, dz, v);
+                combine_group<VG>(op, P.k, acc, v);
+            }
+            // guard band: float64 recheck so the sign never disagrees with the float64 value
+            bool near = false;
+#pragma unroll
+            for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
+            if (near) {
+                for (int k = 0; k < VG; ++k)
+                    if (!(fabsf(acc[k]) >= G.guard))
+                        acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
+                                                    (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
+            }
+            if (VG == 4) reinterpret_cast<float4*>(out)[g * 32 + lane] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+            else reinterpret_cast<float2*>(out)[g * 32 + lane] = make_float2(acc[0], acc[1]);
+        }
+    }
+}
+
+// Leaf tiles of a general postfix program: float64 per voxel, no culling.
+template <int B>
+__global__ void __launch_bounds__(128) k_leaf_program(Geo G, const FbPrim* __restrict__ prims,
+                                                      const FbInsn* __restrict__ prog, int n_prog,
+                                                      const int32_t* __restrict__ active,
+                                                      const int32_t* __restrict__ count, int64_t capacity,
+                                                      float* __restrict__ tiles) {
+    constexpr int kVox = B * B * B;
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t n_active = min((int64_t)count[0], capacity);
+    for (int64_t a = gwarp; a < n_active; a += nwarps) {
+        const int64_t blk = active[a];
+        float* out = tiles + a * kVox;
+        if (blk < 0 || blk >= G.nblocks) {
+            for (int v = lane; v < kVox; v += 32) out[v] = kBig;
+            continue;
+        }
+        const int bk = (int)(blk % G.nbz), bj = (int)((blk / G.nbz) % G.nby), bi = (int)(blk / ((int64_t)G.nbz * G.nby));
+        for (int v = lane; v < kVox; v += 32) {
+            const int li = v / (B * B), lj = (v / B) % B, lk = v % B;
+            const double x = rn_add(G.x0, rn_mul((double)(bi * B + li), G.pitch));
+            const double y = rn_add(G.y0, rn_mul((double)(bj * B + lj), G.pitch));
+            const double z = rn_add(G.z0, rn_mul((double)(bk * B + lk), G.pitch));
+            out[v] = (float)program_eval_d(prims, prog, n_prog, x, y, z);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------ dense input
+__global__ void k_classify_dense(const float* __restrict__ dense, int64_t nx, int64_t ny, int64_t nz, int B,
+                                 int nby, int nbz, int64_t nblocks, float margin, int32_t* __restrict__ kind,
+                                 float* __restrict__ cma) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nblocks) return;
+    const int64_t bk = t % nbz, bj = (t / nbz) % nby, bi = t / ((int64_t)nbz * nby);
+    float mn = 1.0e30f;
+    bool pos = false, neg = false;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int64_t cx = min(bi * B + (c & 1) * B, nx - 1);
+        const int64_t cy = min(bj * B + ((c >> 1) & 1) * B, ny - 1);
+        const int64_t cz = min(bk * B + ((c >> 2) & 1) * B, nz - 1);
+        const float v = dense[(cx * ny + cy) * nz + cz];
+        mn = fminf(mn, fabsf(v));
+        if (v >= 0.0f) pos = true; else neg = true;
+    }
+    if (cma) cma[t] = mn;
+    kind[t] = (pos && neg) ? 0 : ((mn <= margin) ? 0 : (neg ? -1 : 1));
+}
+
+// Warp per active block; each lane copies voxels with the index clamped to n-1.
+__global__ void k_tiles_dense(const float* __restrict__ dense, int64_t nx, int64_t ny, int64_t nz, int B, int nby,
+                              int nbz, const int32_t* __restrict__ active, const int32_t* __restrict__ count,
+                              int64_t capacity, float* __restrict__ tiles) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t n_active = min((int64_t)count[0], capacity);
+    const int b3 = B * B * B;
+    for (int64_t a = gwarp; a < n_active; a += nwarps) {
+        const int64_t lin = active[a];
+        const int64_t bk = lin % nbz, bi = lin / ((int64_t)nbz * nby), bj = (lin / nbz) % nby;
+        for (int v = lane; v < b3; v += 32) {
+            const int li = v / (B * B), lj = (v / B) % B, lk = v % B;
+            const int64_t vx = min(bi * B + li, nx - 1), vy = min(bj * B + lj, ny - 1), vz = min(bk * B + lk, nz - 1);
+            tiles[a * b3 + v] = dense[(vx * ny + vy) * nz + vz];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------ reconstruction
+__global__ void k_slot_map(const int32_t* __restrict__ active, int64_t n_active, int32_t* __restrict__ slot) {
+    const int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (a < n_active) slot[active[a]] = (int32_t)a;
+}
+
+// Dense (nx, ny, nz) field: tile values for active blocks, -BIG / +BIG elsewhere
+// (src/field_engine/faltkarna_v1.py:302-350, cropped to the grid).
+__global__ void k_reconstruct(const int32_t* __restrict__ kind, const int32_t* __restrict__ slot,
+                              const float* __restrict__ tiles, int64_t nx, int64_t ny, int64_t nz, int B, int nby,
+                              int nbz, float big, float* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nx * ny * nz) return;
+    const int64_t z = i % nz, y = (i / nz) % ny, x = i / (nz * ny);
+    const int64_t blk = ((x / B) * nby + y / B) * nbz + z / B;
+    const int32_t s = slot[blk];
+    float v;
+    if (s >= 0) v = tiles[(int64_t)s * B * B * B + ((x % B) * B + (y % B)) * B + (z % B)];
+    else v = kind[blk] < 0 ? -big : big;
+    out[i] = v;
+}
+
+// Sum of trunc(v * scale) over negative values, in int64 (determinism-safe checksum,
+// src/field_engine/faltkarna_v1.py:250-255).
+__global__ void k_checksum_i64(const float* __restrict__ v, int64_t n, double scale, unsigned long long* out) {
+    long long acc = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = v[i];
+        if (x < 0.0f) acc += (long long)((double)x * scale);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, (unsigned long long)acc);
+}
+
+// ------------------------------------------------------------------------------------ host side
+struct Scratch {
+    PrimF* primf;
+    uint32_t* pool;
+    int64_t* off;
+    int32_t* len;
+    unsigned long long* status;
+    int* misc;
+};
+
+Scratch carve(void* base, const Plan& p, const Geo& G) {
+    char* b = static_cast<char*>(base);
+    Scratch s;
+    s.primf = reinterpret_cast<PrimF*>(b + p.primf);
+    s.pool = reinterpret_cast<uint32_t*>(b + p.pool);
+    s.off = reinterpret_cast<int64_t*>(b + p.off);
+    s.len = reinterpret_cast<int32_t*>(b + p.len);
+    s.status = reinterpret_cast<unsigned long long*>(b + p.status);
+    s.misc = reinterpret_cast<int*>(b + p.misc);
+    (void)G;
+    return s;
+}
+
+int launch_compact(const int32_t* kind, int64_t nblocks, int32_t* active, int32_t* count, unsigned long long* status,
+                   int* misc, cudaStream_t st) {
+    const int64_t ntiles = (nblocks + kTile - 1) / kTile;
+    FB_CUDA(cudaMemsetAsync(status, 0, ntiles * 8, st));
+    FB_CUDA(cudaMemsetAsync(misc, 0, 256, st));
+    k_compact<<<(unsigned)ntiles, 256, 0, st>>>(kind, nblocks, active, count, status, misc, ntiles);
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* chain, int n_chain, int mode,
+                  int32_t* kind, float* cma, int32_t* active, int32_t* count, void* scratch, int64_t scratch_len,
+                  cudaStream_t st) {
+    if (!geom_ok(g) || !prims || !chain || n_prims < 1 || n_chain < 1 || !kind || !cma || !active || !count ||
+        !scratch)
+        return FB_INVALID;
+    const Geo G = make_geo(g);
+    const Plan P = make_plan(G, n_prims, n_chain);
+    if (scratch_len < P.total) return FB_INVALID;
+    Scratch S = carve(scratch, P, G);
+    k_prepare_prims<<<fb_div_up(n_prims, 128), 128, 0, st>>>(prims, n_prims, S.primf);
+    FB_LAUNCH();
+    if (mode == 1) {
+        k_full_list<<<fb_div_up(n_chain, 256), 256, 0, st>>>(S.pool + P.pool_full, n_chain);
+        FB_LAUNCH();
+        const int coarse_edge = kSuperEdge * kCoarseDiv;
+        // coarse regions from the full chain
+        k_cull<<<fb_div_up(G.ncoarse * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, nullptr, nullptr, n_chain, 1,
+                                                               1, 1, S.off, S.len, P.pool_coarse, kCapCoarse,
+                                                               G.S * G.B * kCoarseDiv, G.ncx, G.ncy, G.ncz);
+        FB_LAUNCH();
+        (void)coarse_edge;
+        // superblocks from their coarse region
+        k_cull<<<fb_div_up(G.nsuper * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off, S.len, 0, kCoarseDiv,
+                                                              G.ncy, G.ncz, S.off + G.ncoarse, S.len + G.ncoarse,
+                                                              P.pool_super, kCapSuper, G.S * G.B, G.nsx, G.nsy, G.nsz);
+        FB_LAUNCH();
+        k_classify<true><<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, S.primf, chain, n_chain, S.pool,
+                                                                    S.off + G.ncoarse, S.len + G.ncoarse, kind, cma);
+    } else {
+        k_classify<false><<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, S.primf, chain, n_chain, S.pool,
+                                                                     S.off + G.ncoarse, S.len + G.ncoarse, kind, cma);
+    }
+    FB_LAUNCH();
+    return launch_compact(kind, G.nblocks, active, count, S.status, S.misc, st);
+}
+
+int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* chain, int n_chain, int mode,
+              const int32_t* active, const int32_t* count, float* tiles, int64_t capacity, void* scratch,
+              int64_t scratch_len, cudaStream_t st, unsigned long long* work = nullptr) {
+    if (!geom_ok(g) || !prims || !chain || n_prims < 1 || n_chain < 1 || !active || !count || !tiles || !scratch ||
+        capacity < 0)
+        return FB_INVALID;
+    const Geo G = make_geo(g);
+    const Plan P = make_plan(G, n_prims, n_chain);
+    if (scratch_len < P.total) return FB_INVALID;
+    Scratch S = carve(scratch, P, G);
+    const int grid = fb_sm_count() * 16;
+    const int64_t* sb_off = S.off + G.ncoarse;
+    const int32_t* sb_len = S.len + G.ncoarse;
+    if (mode != 1) {
+        switch (G.B) {
+        case 4: k_leaf_program<4><<<grid, 128, 0, st>>>(G, prims, chain, n_chain, active, count, capacity, tiles); break;
+        case 8: k_leaf_program<8><<<grid, 128, 0, st>>>(G, prims, chain, n_chain, active, count, capacity, tiles); break;
+        default: k_leaf_program<16><<<grid, 128, 0, st>>>(G, prims, chain, n_chain, active, count, capacity, tiles);
+        }
+    } else {
+        switch (G.B) {
+        case 4:
+            k_leaf<4><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, count,
+                                                       capacity, tiles, work);
+            break;
+        case 8:
+            k_leaf<8><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, count,
+                                                       capacity, tiles, work);
+            break;
+        default:
+            k_leaf<16><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active,
+                                                        count, capacity, tiles, work);
+        }
+    }
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Scratch bytes of one analytic build (classify + leaf) for this geometry and program size.
+int64_t fb_field_scratch_bytes(const FbGeom* g, int32_t n_prims, int32_t n_chain) {
+    if (!g || !geom_ok(*g) || n_prims < 1 || n_chain < 1) return -1;
+    const Geo G = make_geo(*g);
+    return make_plan(G, n_prims, n_chain).total;
+}
+
+// Classification + compaction of an analytic recipe.  mode 1: `chain` is the left-deep chain
+// (CH_* ops, culled); mode 0: `chain` is a general postfix program (OP_* ops, float64, no culling).
+// Writes kind[n_blocks], corner_min_abs[n_blocks], active[<= n_blocks] ascending and count[0].
+int fb_field_classify_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prims, const FbInsn* d_chain,
+                             int32_t n_chain, int32_t mode, int32_t* d_kind, float* d_cma, int32_t* d_active,
+                             int32_t* d_count, void* d_scratch, int64_t scratch_len, void* stream) noexcept {
+    if (!g) return FB_INVALID;
+    return classify_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_kind, d_cma, d_active, d_count, d_scratch,
+                         scratch_len, static_cast<cudaStream_t>(stream));
+}
+
+// Leaf tiles of the first min(count, capacity) active blocks, tile order (li, lj, lk).  Uses the
+// culling lists left in `d_scratch` by fb_field_classify_device for the same recipe and geometry.
+int fb_field_leaf_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prims, const FbInsn* d_chain,
+                         int32_t n_chain, int32_t mode, const int32_t* d_active, const int32_t* d_count, float* d_tiles,
+                         int64_t capacity, void* d_scratch, int64_t scratch_len, void* stream) noexcept {
+    if (!g) return FB_INVALID;
+    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_active, d_count, d_tiles, capacity, d_scratch,
+                     scratch_len, static_cast<cudaStream_t>(stream));
+}
+
+// fb_field_leaf_device plus a count of the executed work: d_work[0] += primitive evaluations,
+// d_work[1] += float32 operations (two uint64 counters, accumulated).
+int fb_field_leaf_work_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prims, const FbInsn* d_chain,
+                              int32_t n_chain, int32_t mode, const int32_t* d_active, const int32_t* d_count,
+                              float* d_tiles, int64_t capacity, void* d_scratch, int64_t scratch_len,
+                              uint64_t* d_work, void* stream) noexcept {
+    if (!g || !d_work) return FB_INVALID;
+    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_active, d_count, d_tiles, capacity, d_scratch,
+                     scratch_len, static_cast<cudaStream_t>(stream), reinterpret_cast<unsigned long long*>(d_work));
+}
+
+// Whole analytic build in one stream-ordered call (classify, compact, leaf tiles); tiles beyond
+// `capacity` active blocks are not written (count still reports the full number).
+int fb_field_build_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prims, const FbInsn* d_chain,
+                          int32_t n_chain, int32_t mode, int32_t* d_kind, float* d_cma, int32_t* d_active,
+                          int32_t* d_count, float* d_tiles, int64_t capacity, void* d_scratch, int64_t scratch_len,
+                          void* stream) noexcept {
+    if (!g) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = classify_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_kind, d_cma, d_active, d_count, d_scratch,
+                           scratch_len, st);
+    if (rc) return rc;
+    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_active, d_count, d_tiles, capacity, d_scratch,
+                     scratch_len, st);
+}
+
+// Scratch bytes of a dense classification (compaction state only).
+int64_t fb_dense_scratch_bytes(int64_t nx, int64_t ny, int64_t nz, int32_t block) {
+    if (nx < 1 || ny < 1 || nz < 1 || block < 1 || block > 1024) return -1;
+    const int64_t nb = ((nx + block - 1) / block) * ((ny + block - 1) / block) * ((nz + block - 1) / block);
+    return align256(nb / kTile * 8 + 8) + 256 + 256;
+}
+
+// Dense-input classification, compaction and tile gather: the reference's k_classify_dense /
+// k_eval_tile_dense and meshsdf_classify_cpu / meshsdf_tiles_cpu
+// (src/field_engine/mesh_sdf_native_v1/field.cpp:229-273) on the device.  d_cma may be null.
+int fb_dense_classify_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, int32_t block, float margin,
+                             int32_t* d_kind, float* d_cma, int32_t* d_active, int32_t* d_count, float* d_tiles,
+                             int64_t capacity, void* d_scratch, int64_t scratch_len, void* stream) noexcept {
+    if (!d_dense || !d_kind || !d_active || !d_count || nx < 1 || ny < 1 || nz < 1 || block < 1 || block > 1024 ||
+        !d_scratch || capacity < 0 || (capacity > 0 && !d_tiles))
+        return FB_INVALID;
+    if (scratch_len < fb_dense_scratch_bytes(nx, ny, nz, block)) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nby = (int)((ny + block - 1) / block), nbz = (int)((nz + block - 1) / block);
+    const int64_t nblocks = ((nx + block - 1) / block) * nby * nbz;
+    k_classify_dense<<<fb_div_up(nblocks, 256), 256, 0, st>>>(d_dense, nx, ny, nz, block, nby, nbz, nblocks, margin,
+                                                              d_kind, d_cma);
+    FB_LAUNCH();
+    char* b = static_cast<char*>(d_scratch);
+    const int64_t ntiles = (nblocks + kTile - 1) / kTile;
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(b);
+    int* misc = reinterpret_cast<int*>(b + align256(ntiles * 8));
+    if (int rc = launch_compact(d_kind, nblocks, d_active, d_count, status, misc, st)) return rc;
+    if (capacity > 0) {
+        k_tiles_dense<<<fb_sm_count() * 8, 256, 0, st>>>(d_dense, nx, ny, nz, block, nby, nbz, d_active, d_count,
+                                                          capacity, d_tiles);
+        FB_LAUNCH();
+    }
+    return FB_OK;
+}
+
+// Dense reconstruction of a sparse field; d_slot is caller scratch of n_blocks int32.
+int fb_field_reconstruct_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
+                                int64_t nx, int64_t ny, int64_t nz, int32_t block, float big, int32_t* d_slot,
+                                float* d_out, void* stream) noexcept {
+    if (!d_kind || !d_slot || !d_out || nx < 1 || ny < 1 || nz < 1 || block < 1 || n_active < 0 ||
+        (n_active > 0 && (!d_active || !d_tiles)))
+        return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nby = (int)((ny + block - 1) / block), nbz = (int)((nz + block - 1) / block);
+    const int64_t nblocks = ((nx + block - 1) / block) * nby * nbz;
+    FB_CUDA(cudaMemsetAsync(d_slot, 0xff, nblocks * 4, st));
+    if (n_active > 0) {
+        k_slot_map<<<fb_div_up(n_active, 256), 256, 0, st>>>(d_active, n_active, d_slot);
+        FB_LAUNCH();
+    }
+    k_reconstruct<<<fb_div_up(nx * ny * nz, 256), 256, 0, st>>>(d_kind, d_slot, d_tiles, nx, ny, nz, block, nby, nbz,
+                                                                big, d_out);
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+// int64 fixed-point checksum of the negative values (accumulates into d_out[0]).
+int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64_t* d_out, void* stream) noexcept {
+    if (!d_values || !d_out || n < 0) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n == 0) return FB_OK;
+    k_checksum_i64<<<std::min<int64_t>(fb_div_up(n, 256), fb_sm_count() * 8), 256, 0, st>>>(
+        d_values, n, scale, reinterpret_cast<unsigned long long*>(d_out));
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+// Error flag of the last compaction (1 when a bounded wait gave up), read from the scratch.
+int fb_field_compact_error(const FbGeom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, void* stream) {
+    if (!g || !geom_ok(*g) || !d_scratch) return FB_INVALID;
+    const Geo G = make_geo(*g);
+    const Plan P = make_plan(G, n_prims, n_chain);
+    int flags[2] = {0, 0};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    FB_CUDA(cudaMemcpyAsync(flags, static_cast<const char*>(d_scratch) + P.misc, 8, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    return flags[1] ? FB_TIMEOUT : FB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,275 @@
+// Primitive records and their evaluation on the device: float32 (bulk, block-localised) and
+// float64 (guard-band recheck, general programs).
+//
+// A primitive's world value is  s * f(A x + t) - off  with f the canonical primitive centred on
+// its own origin (the host compiler folds transforms, scales, axis projections and leaf offsets
+// into A, t, s, off).  Canonical formulas: sphere, box, cylinder, cone, halfspace and rect_frustum
+// follow src/field_engine/ikarus_v1/expr.py:268-340 (box also faltkarna_v1.py:91-99), the
+// unbounded z cylinder faltkarna_v1.py:102-104; capsule and torus are the textbook closed forms.
+#pragma once
+#include <cstdint>
+
+enum : int32_t { P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF };
+enum : int32_t { OP_PUSH = 0, OP_UNION, OP_INTERSECT, OP_SUBTRACT, OP_OFFSET };
+enum : int32_t { CH_SET = 0, CH_SETNEG, CH_UNION, CH_INTERSECT, CH_SUBTRACT, CH_OFFSET };
+
+// Host-compiled record (216 bytes, float64), the C-ABI layout of fb_prim in include/field_b200.h.
+struct FbPrim {
+    int32_t type, flags;
+    double p[12];
+    double A[12];  // rows of the 3x4 world -> canonical map
+    double s, off;
+};
+static_assert(sizeof(FbPrim) == 216, "fb_prim layout");
+
+// One program / chain instruction (16 bytes), fb_insn in include/field_b200.h.
+struct FbInsn {
+    int32_t op, arg;
+    double k;
+};
+static_assert(sizeof(FbInsn) == 16, "fb_insn layout");
+
+// float32 mirror used for interval culling in world coordinates (128 bytes).
+struct __align__(16) PrimF {
+    int32_t type, ident;
+    float s, off, lip, pad0, pad1, pad2;
+    float A[12];
+    float p[12];
+};
+
+// Block-localised float32 record: q = L + A_lin * d, d the offset from the block origin.
+struct __align__(16) LocalPrim {
+    int32_t type, op, ident, pad;
+    float k, s, off, pad1;
+    float L[4];
+    float A[12];   // A_lin rows (9 used)
+    float p[12];
+};
+
+// ------------------------------------------------------------------------------------ float32
+__device__ __forceinline__ float sel_min(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float sel_max(float a, float b) { return a > b ? a : b; }
+
+__device__ __forceinline__ float canon_f(int type, const float* __restrict__ p, float x, float y, float z) {
+    switch (type) {
+    case P_SPHERE:
+        return sqrtf(fmaf(x, x, fmaf(y, y, z * z))) - p[0];
+    case P_BOX: {
+        const float qx = fabsf(x) - p[0], qy = fabsf(y) - p[1], qz = fabsf(z) - p[2];
+        const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f), oz = fmaxf(qz, 0.f);
+        return sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.f);
+    }
+    case P_CYLINDER: {
+        const float qx = sqrtf(fmaf(x, x, y * y)) - p[0], qy = fabsf(z) - p[1];
+        const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f);
+        return sqrtf(fmaf(ox, ox, oy * oy)) + fminf(fmaxf(qx, qy), 0.f);
+    }
+    case P_CONE: {  // p = {r1, r2, h, 1/h}
+        const float t = fminf(fmaxf((z + 0.5f * p[2]) * p[3], 0.f), 1.f);
+        const float qx = sqrtf(fmaf(x, x, y * y)) - fmaf(p[1] - p[0], t, p[0]);
+        const float qy = fabsf(z) - 0.5f * p[2];
+        const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f);
+        return sqrtf(fmaf(ox, ox, oy * oy)) + fminf(fmaxf(qx, qy), 0.f);
+    }
+    case P_HALFSPACE:
+        return fmaf(x, p[0], fmaf(y, p[1], z * p[2]));
+    case P_FRUSTUM: {  // p = {z1, hx0, hy0, a1, a2, a3, a4, 1/n1, 1/n2, 1/n3, 1/n4}
+        float d = fmaxf(-z, z - p[0]);
+        d = fmaxf(d, (fmaf(p[3], z, x) - p[1]) * p[7]);
+        d = fmaxf(d, (fmaf(p[4], z, -x) - p[1]) * p[8]);
+        d = fmaxf(d, (fmaf(p[5], z, y) - p[2]) * p[9]);
+        d = fmaxf(d, (fmaf(p[6], z, -y) - p[2]) * p[10]);
+        return d;
+    }
+    case P_CAPSULE: {  // p = {bx, by, bz, r, 1/|b|^2 (0 if degenerate)}
+        const float h = fminf(fmaxf(fmaf(x, p[0], fmaf(y, p[1], z * p[2])) * p[4], 0.f), 1.f);
+        const float dx = fmaf(-p[0], h, x), dy = fmaf(-p[1], h, y), dz = fmaf(-p[2], h, z);
+        return sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - p[3];
+    }
+    case P_TORUS: {
+        const float qx = sqrtf(fmaf(x, x, y * y)) - p[0];
+        return sqrtf(fmaf(qx, qx, z * z)) - p[1];
+    }
+    case P_CYL_INF:
+        return sqrtf(fmaf(x, x, y * y)) - p[0];
+    default:
+        return __int_as_float(0x7fc00000);
+    }
+}
+
+// World-coordinate float32 value (culling intervals only).
+__device__ __forceinline__ float primf_world(const PrimF& P, float x, float y, float z) {
+    const float lx = fmaf(P.A[0], x, fmaf(P.A[1], y, fmaf(P.A[2], z, P.A[3])));
+    const float ly = fmaf(P.A[4], x, fmaf(P.A[5], y, fmaf(P.A[6], z, P.A[7])));
+    const float lz = fmaf(P.A[8], x, fmaf(P.A[9], y, fmaf(P.A[10], z, P.A[11])));
+    return fmaf(P.s, canon_f(P.type, P.p, lx, ly, lz), -P.off);
+}
+
+// Block-localised float32 value at offset (dx, dy, dz) from the block origin.
+__device__ __forceinline__ float local_eval(const LocalPrim& P, float dx, float dy, float dz) {
+    float x, y, z;
+    if (P.ident) {
+        x = P.L[0] + dx;
+        y = P.L[1] + dy;
+        z = P.L[2] + dz;
+    } else {
+        x = fmaf(P.A[0], dx, fmaf(P.A[1], dy, fmaf(P.A[2], dz, P.L[0])));
+        y = fmaf(P.A[3], dx, fmaf(P.A[4], dy, fmaf(P.A[5], dz, P.L[1])));
+        z = fmaf(P.A[6], dx, fmaf(P.A[7], dy, fmaf(P.A[8], dz, P.L[2])));
+    }
+    return fmaf(P.s, canon_f(P.type, P.p, x, y, z), -P.off);
+}
+
+// Hard / polynomial-smooth booleans in float32; on equality the second operand wins, as in NumPy.
+__device__ __forceinline__ float combine_f(int op, float a, float b, float k) {
+    if (op == CH_UNION) {
+        const float m = sel_min(a, b);
+        if (k <= 0.f) return m;
+        const float h = fmaxf(k - fabsf(a - b), 0.f) / k;
+        return m - h * h * k * 0.25f;
+    }
+    if (op == CH_INTERSECT) {
+        const float m = sel_max(a, b);
+        if (k <= 0.f) return m;
+        const float h = fmaxf(k - fabsf(a - b), 0.f) / k;
+        return m + h * h * k * 0.25f;
+    }
+    const float m = sel_max(a, -b);
+    if (k <= 0.f) return m;
+    const float h = fmaxf(k - fabsf(a + b), 0.f) / k;
+    return m + h * h * k * 0.25f;
+}
+
+// Apply one chain element (effective op) with primitive value v to the accumulator.
+__device__ __forceinline__ float chain_apply(int op, float acc, float v, float k) {
+    switch (op) {
+    case CH_SET: return v;
+    case CH_SETNEG: return -v;
+    case CH_OFFSET: return acc - k;
+    default: return combine_f(op, acc, v, k);
+    }
+}
+
+// ------------------------------------------------------------------------------------ float64
+// Every operation rounds once, in the written order (no contraction), so the values equal the
+// CPU float64 evaluation of the same program bit for bit.
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double rn_max(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double rn_min(double a, double b) { return a < b ? a : b; }
+
+static __device__ __noinline__ double canon_d(int type, const double* __restrict__ p, double x, double y, double z) {
+    switch (type) {
+    case P_SPHERE:
+        return rn_sub(__dsqrt_rn(rn_add(rn_add(rn_mul(x, x), rn_mul(y, y)), rn_mul(z, z))), p[0]);
+    case P_BOX: {
+        const double qx = rn_sub(fabs(x), p[0]), qy = rn_sub(fabs(y), p[1]), qz = rn_sub(fabs(z), p[2]);
+        const double ox = rn_max(qx, 0.0), oy = rn_max(qy, 0.0), oz = rn_max(qz, 0.0);
+        const double out = __dsqrt_rn(rn_add(rn_add(rn_mul(ox, ox), rn_mul(oy, oy)), rn_mul(oz, oz)));
+        return rn_add(out, rn_min(rn_max(qx, rn_max(qy, qz)), 0.0));
+    }
+    case P_CYLINDER: {
+        const double rad = __dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y)));
+        const double qx = rn_sub(rad, p[0]), qy = rn_sub(fabs(z), p[1]);
+        const double ox = rn_max(qx, 0.0), oy = rn_max(qy, 0.0);
+        return rn_add(__dsqrt_rn(rn_add(rn_mul(ox, ox), rn_mul(oy, oy))), rn_min(rn_max(qx, qy), 0.0));
+    }
+    case P_CONE: {
+        const double rad = __dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y))), h = p[2];
+        const double t = rn_min(rn_max(rn_div(rn_add(z, rn_div(h, 2.0)), h), 0.0), 1.0);
+        const double r_at = rn_add(p[0], rn_mul(rn_sub(p[1], p[0]), t));
+        const double qy = rn_sub(fabs(z), rn_div(h, 2.0)), qx = rn_sub(rad, r_at);
+        const double ox = rn_max(qx, 0.0), oy = rn_max(qy, 0.0);
+        return rn_add(__dsqrt_rn(rn_add(rn_mul(ox, ox), rn_mul(oy, oy))), rn_min(rn_max(qx, qy), 0.0));
+    }
+    case P_HALFSPACE:
+        return rn_add(rn_add(rn_mul(x, p[0]), rn_mul(y, p[1])), rn_mul(z, p[2]));
+    case P_FRUSTUM: {
+        const double z1 = p[0], hx0 = p[1], hy0 = p[2], hx1 = p[3], hy1 = p[4], cx1 = p[5], cy1 = p[6];
+        const double kx = rn_div(rn_sub(hx1, hx0), z1), ky = rn_div(rn_sub(hy1, hy0), z1);
+        const double kcx = rn_div(cx1, z1), kcy = rn_div(cy1, z1);
+        const double d_zlo = -z, d_zhi = rn_sub(z, z1);
+        const double a1 = -rn_add(kx, kcx), n1 = __dsqrt_rn(rn_add(1.0, rn_mul(a1, a1)));
+        const double a2 = -rn_sub(kx, kcx), n2 = __dsqrt_rn(rn_add(1.0, rn_mul(a2, a2)));
+        const double a3 = -rn_add(ky, kcy), n3 = __dsqrt_rn(rn_add(1.0, rn_mul(a3, a3)));
+        const double a4 = -rn_sub(ky, kcy), n4 = __dsqrt_rn(rn_add(1.0, rn_mul(a4, a4)));
+        const double d_xhi = rn_div(rn_sub(rn_add(x, rn_mul(a1, z)), hx0), n1);
+        const double d_xlo = rn_div(rn_sub(rn_add(-x, rn_mul(a2, z)), hx0), n2);
+        const double d_yhi = rn_div(rn_sub(rn_add(y, rn_mul(a3, z)), hy0), n3);
+        const double d_ylo = rn_div(rn_sub(rn_add(-y, rn_mul(a4, z)), hy0), n4);
+        return rn_max(rn_max(rn_max(d_zlo, d_zhi), rn_max(d_xhi, d_xlo)), rn_max(d_yhi, d_ylo));
+    }
+    case P_CAPSULE: {
+        const double bx = p[0], by = p[1], bz = p[2];
+        const double bb = rn_add(rn_add(rn_mul(bx, bx), rn_mul(by, by)), rn_mul(bz, bz));
+        const double h = bb > 0.0 ? rn_min(rn_max(rn_div(rn_add(rn_add(rn_mul(x, bx), rn_mul(y, by)), rn_mul(z, bz)), bb), 0.0), 1.0)
+                                  : 0.0;
+        const double dx = rn_sub(x, rn_mul(bx, h)), dy = rn_sub(y, rn_mul(by, h)), dz = rn_sub(z, rn_mul(bz, h));
+        return rn_sub(__dsqrt_rn(rn_add(rn_add(rn_mul(dx, dx), rn_mul(dy, dy)), rn_mul(dz, dz))), p[3]);
+    }
+    case P_TORUS: {
+        const double qx = rn_sub(__dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y))), p[0]);
+        return rn_sub(__dsqrt_rn(rn_add(rn_mul(qx, qx), rn_mul(z, z))), p[1]);
+    }
+    case P_CYL_INF:
+        return rn_sub(__dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y))), p[0]);
+    default:
+        return __longlong_as_double(0x7ff8000000000000ll);
+    }
+}
+
+__device__ __forceinline__ double prim_world_d(const FbPrim& P, double x, double y, double z) {
+    const double* A = P.A;
+    const double lx = rn_add(rn_add(rn_add(rn_mul(A[0], x), rn_mul(A[1], y)), rn_mul(A[2], z)), A[3]);
+    const double ly = rn_add(rn_add(rn_add(rn_mul(A[4], x), rn_mul(A[5], y)), rn_mul(A[6], z)), A[7]);
+    const double lz = rn_add(rn_add(rn_add(rn_mul(A[8], x), rn_mul(A[9], y)), rn_mul(A[10], z)), A[11]);
+    return rn_sub(rn_mul(P.s, canon_d(P.type, P.p, lx, ly, lz)), P.off);
+}
+
+__device__ __forceinline__ double combine_d(int op, double a, double b, double k) {
+    if (op == OP_UNION) {
+        if (k <= 0.0) return rn_min(a, b);
+        const double h = rn_div(rn_max(rn_sub(k, fabs(rn_sub(a, b))), 0.0), k);
+        return rn_sub(rn_min(a, b), rn_mul(rn_mul(rn_mul(h, h), k), 0.25));
+    }
+    if (op == OP_INTERSECT) {
+        if (k <= 0.0) return rn_max(a, b);
+        const double h = rn_div(rn_max(rn_sub(k, fabs(rn_sub(a, b))), 0.0), k);
+        return rn_add(rn_max(a, b), rn_mul(rn_mul(rn_mul(h, h), k), 0.25));
+    }
+    if (k <= 0.0) return rn_max(a, -b);
+    const double h = rn_div(rn_max(rn_sub(k, fabs(rn_add(a, b))), 0.0), k);
+    return rn_add(rn_max(a, -b), rn_mul(rn_mul(rn_mul(h, h), k), 0.25));
+}
+
+__device__ __forceinline__ double chain_apply_d(int op, double acc, double v, double k) {
+    switch (op) {
+    case CH_SET: return v;
+    case CH_SETNEG: return -v;
+    case CH_OFFSET: return rn_sub(acc, k);
+    case CH_UNION: return combine_d(OP_UNION, acc, v, k);
+    case CH_INTERSECT: return combine_d(OP_INTERSECT, acc, v, k);
+    default: return combine_d(OP_SUBTRACT, acc, v, k);
+    }
+}
+
+// General postfix program in float64 at one world point (stack depth <= 32).
+static __device__ double program_eval_d(const FbPrim* __restrict__ prims, const FbInsn* __restrict__ prog, int n,
+                                 double x, double y, double z) {
+    double st[32];
+    int sp = 0;
+    for (int i = 0; i < n; ++i) {
+        const FbInsn I = prog[i];
+        if (I.op == OP_PUSH) {
+            if (sp < 32) st[sp++] = prim_world_d(prims[I.arg], x, y, z);
+        } else if (I.op == OP_OFFSET) {
+            if (sp > 0) st[sp - 1] = rn_sub(st[sp - 1], I.k);
+        } else if (sp > 1) {
+            const double b = st[--sp];
+            st[sp - 1] = combine_d(I.op, st[sp - 1], b, I.k);
+        }
+    }
+    return sp == 1 ? st[0] : __longlong_as_double(0x7ff8000000000000ll);
+}

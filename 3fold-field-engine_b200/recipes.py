@@ -1,0 +1,151 @@
+"""Seeded synthetic workloads with the shapes, sizes and value distributions of the benchmark
+configurations (no external dataset is involved).
+
+* ``plain_union``  -- spheres (centres U[0.1,0.9]^3, radii U[0.02,0.1]) and axis-aligned boxes
+  (half extents U[0.02,0.08]) in a unit-cube domain, one hard union; 256^3 at pitch 1/256, 8^3
+  leaves, seed 0 for the plain single build.
+* ``milled_part``  -- the plain method at scale: spheres, boxes, capsules and tori in equal numbers
+  with the same distributions scaled by 1/4, unioned, then milling-tool capsules (radius
+  U[0.005,0.02], straight sweeps with endpoints U[0.05,0.95]^3) subtracted in order.
+* ``obstacle_grid``-- a uint8 occupancy grid of random boxes, scaled to a target fill fraction.
+* ``batch_recipes``-- many independent recipes: primitive counts log-uniform in [8, 2048], domains
+  from {64, 128, 256, 512}^3, each part followed by tool subtractions.
+* ``tangent_pairs``-- adversarial near-tangent sphere pairs (gap U[0, 0.5]*pitch) and thin box walls.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import expr as X
+from .grid import GridMeta
+
+
+def _unit_vectors(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def parts(rng, n_sphere, n_box, n_capsule=0, n_torus=0, scale=1.0, lo=0.1, hi=0.9):
+    """Primitive nodes: spheres, boxes, capsules, tori with the plain-build distributions x scale."""
+    out = []
+    c = rng.uniform(lo, hi, size=(n_sphere, 3))
+    r = rng.uniform(0.02, 0.1, size=n_sphere) * scale
+    out += [X.sphere(float(r[i]), c[i]) for i in range(n_sphere)]
+    c = rng.uniform(lo, hi, size=(n_box, 3))
+    h = rng.uniform(0.02, 0.08, size=(n_box, 3)) * scale
+    out += [X.box(h[i], c[i]) for i in range(n_box)]
+    if n_capsule:
+        c = rng.uniform(lo, hi, size=(n_capsule, 3))
+        d = _unit_vectors(rng, n_capsule) * rng.uniform(0.02, 0.08, size=(n_capsule, 1)) * scale
+        r = rng.uniform(0.01, 0.04, size=n_capsule) * scale
+        out += [X.capsule(c[i] - d[i], c[i] + d[i], float(r[i])) for i in range(n_capsule)]
+    if n_torus:
+        c = rng.uniform(lo, hi, size=(n_torus, 3))
+        R = rng.uniform(0.04, 0.1, size=n_torus) * scale
+        rr = R * rng.uniform(0.15, 0.4, size=n_torus)
+        axes = rng.integers(0, 3, size=n_torus)
+        out += [X.torus(float(R[i]), float(rr[i]), "xyz"[axes[i]], c[i]) for i in range(n_torus)]
+    return out
+
+
+def tools(rng, n, r_lo=0.005, r_hi=0.02, lo=0.05, hi=0.95):
+    """Milling-tool passes: capsules along random straight sweeps."""
+    a = rng.uniform(lo, hi, size=(n, 3))
+    b = rng.uniform(lo, hi, size=(n, 3))
+    r = rng.uniform(r_lo, r_hi, size=n)
+    return [X.capsule(a[i], b[i], float(r[i])) for i in range(n)]
+
+
+def plain_union(seed=0, n=256, block=8, n_sphere=32, n_box=32):
+    """(recipe, GridMeta) of the plain single build."""
+    rng = np.random.default_rng(seed)
+    nodes = parts(rng, n_sphere, n_box)
+    meta = GridMeta(0.0, 0.0, 0.0, 1.0 / n, n, n, n, block)
+    return X.union_all(nodes), meta
+
+
+def milled_part(seed=1, n=1024, block=8, n_parts=3584, n_tools=512):
+    """(recipe, GridMeta) of the plain method at scale: n_parts primitives in equal mix, unioned,
+    minus n_tools milling capsules."""
+    rng = np.random.default_rng(seed)
+    q = n_parts // 4
+    nodes = parts(rng, q, q, q, n_parts - 3 * q, scale=0.25)
+    order = rng.permutation(len(nodes))
+    recipe = X.union_all([nodes[i] for i in order])
+    recipe = X.subtract_all(recipe, tools(rng, n_tools))
+    meta = GridMeta(0.0, 0.0, 0.0, 1.0 / n, n, n, n, block)
+    return recipe, meta
+
+
+def _raster_boxes(n, centres, half):
+    g = np.zeros((n, n, n), np.uint8)
+    lo = np.clip(np.floor(centres - half), 0, n).astype(int)
+    hi = np.clip(np.ceil(centres + half), 0, n).astype(int)
+    for i in range(len(centres)):
+        g[lo[i, 0]:hi[i, 0], lo[i, 1]:hi[i, 1], lo[i, 2]:hi[i, 2]] = 1
+    return g
+
+
+def obstacle_grid(seed=2, n=512, n_boxes=2000, fill=0.08):
+    """uint8 (n, n, n) occupancy of n_boxes random boxes whose size is scaled (bisection on a coarse
+    raster, then on the full one) so that the filled fraction is close to ``fill``."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0, 1, size=(n_boxes, 3))
+    shape = rng.uniform(0.5, 1.5, size=(n_boxes, 3))
+
+    def frac(res, s):
+        return _raster_boxes(res, centres * res, shape * s * res).mean()
+    lo, hi = 0.0, 0.5
+    coarse = max(32, n // 4)
+    for _ in range(24):
+        s = 0.5 * (lo + hi)
+        lo, hi = (s, hi) if frac(coarse, s) < fill else (lo, s)
+    lo, hi = 0.5 * lo, 2.0 * hi
+    for _ in range(10 if n <= 256 else 7):
+        s = 0.5 * (lo + hi)
+        lo, hi = (s, hi) if frac(n, s) < fill else (lo, s)
+    return _raster_boxes(n, centres * n, shape * 0.5 * (lo + hi) * n)
+
+
+def batch_recipes(count=256, seed=3, sizes=(64, 128, 256, 512), tool_fraction=0.125):
+    """List of (recipe, n, n_prims): primitive counts log-uniform in [8, 2048], cubic domains
+    drawn uniformly from ``sizes``; a fraction of the primitives are milling tools subtracted
+    after the union of the parts."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n_prims = int(round(math.exp(rng.uniform(math.log(8), math.log(2048)))))
+        n = int(rng.choice(sizes))
+        n_tools = int(n_prims * tool_fraction)
+        n_parts = max(1, n_prims - n_tools)
+        # keep the part count per unit volume bounded: primitive size shrinks with the count
+        scale = float(min(1.0, (64.0 / n_parts) ** (1.0 / 3.0)))
+        q = n_parts // 4
+        nodes = parts(rng, n_parts - 3 * q, q, q, q, scale=scale)
+        recipe = X.union_all(nodes)
+        if n_tools:
+            recipe = X.subtract_all(recipe, tools(rng, n_tools, 0.005 * max(scale, 0.25), 0.02 * max(scale, 0.25)))
+        out.append((recipe, n, n_parts + n_tools))
+    return out
+
+
+def tangent_pairs(seed=4, n_pairs=1000, pitch=1.0 / 512, walls=64):
+    """Adversarial thin features: sphere pairs whose gap is U[0, 0.5]*pitch and box walls half a
+    voxel thick, in the unit cube.  Returns a recipe (union of everything)."""
+    rng = np.random.default_rng(seed)
+    nodes = []
+    for _ in range(n_pairs):
+        c = rng.uniform(0.1, 0.9, size=3)
+        r1, r2 = rng.uniform(0.004, 0.02, size=2)
+        d = _unit_vectors(rng, 1)[0]
+        gap = rng.uniform(0.0, 0.5) * pitch
+        nodes.append(X.sphere(r1, c))
+        nodes.append(X.sphere(r2, c + d * (r1 + r2 + gap)))
+    for _ in range(walls):
+        c = rng.uniform(0.1, 0.9, size=3)
+        h = rng.uniform(0.01, 0.05, size=3)
+        h[rng.integers(0, 3)] = 0.25 * pitch
+        nodes.append(X.box(h, c))
+    return X.union_all(nodes)

@@ -1,0 +1,395 @@
+#!/usr/bin/env python3
+"""Benchmark of the block-sparse SDF field hot path: one JSON line on rank 0.
+
+Workload (the plain method at scale, synthetic and seeded): a 1024^3 grid (pitch 1/1024, 8^3 leaf
+blocks) built from 3584 primitives (spheres, boxes, capsules, tori in equal numbers) unioned and
+then 512 milling-tool capsules subtracted, plus the exact int32 squared EDT of a 512^3 uint8
+obstacle grid of 2000 random boxes (~8 % fill), distances to the obstacles.  One step = one field
+build (cull + classify + compact + fused leaf evaluation with CSG) + one EDT, inputs resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: leaf voxels produced per second over the whole step (Gvox/s), all ranks.  Each rank builds
+its own replica (the path shards by recipe with no exchange: weak scaling).  Timing: CUDA events
+per step on the launching stream, L2 flushed between steps outside the events, max over ranks.
+`--impl reference` times the reference algorithm on the host cores instead (the CPU oracle port of
+the reference's float64 evaluator and integer EDT, OpenMP, on a bounded sample of the same
+workload, extrapolated to the full workload).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "leaf Gvox/s batched vs plain at ≤1e-5·pitch err; EDT GB/s; serve p50/p99 ms"
+UNIT = "Gvox/s"
+EDT_BYTES_PER_VOXEL = 13  # 1 B mask + 4 B output + 8 B int32 intermediate round trip
+LAUNCHES_PER_STEP = 10    # prepare, full list, 2 x cull, classify, compact, leaf, 3 x EDT
+WORKLOAD = "plain_at_scale_1024^3_3584prims_512tools_B8+edt_512^3_2000boxes"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=1024, help="grid edge of the field build")
+    ap.add_argument("--edt-n", type=int, default=512, help="grid edge of the EDT")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------ workload
+def workload(n, edt_n):
+    import field_b200.recipes as R
+    import field_b200.expr as X
+    recipe, meta = R.milled_part(seed=1, n=n, block=8)
+    comp = X.compile_recipe(recipe)
+    mask = R.obstacle_grid(seed=2, n=edt_n, n_boxes=2000, fill=0.08)
+    return comp, meta, mask
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_of(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    f = REPO / "profiles" / "ncu_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------------------------------ CPU leg
+def cpu_sample(comp, meta, mask, n_active=None, n_classify=8000, n_tiles=200, seed=0):
+    """Reference-algorithm CPU time of one full step, extrapolated from a bounded sample: float64
+    8-corner classification of n_classify random blocks, leaf evaluation of up to n_tiles of the
+    active blocks among them (every primitive at every point, as the reference kernels do), plus
+    the full integer EDT of the obstacle grid (OpenMP).  When n_active is None it is estimated from
+    the sampled active fraction.  Returns (seconds per step, description, threads, n_active)."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    blocks = np.sort(rng.choice(meta.n_blocks, size=min(n_classify, meta.n_blocks), replace=False)).astype(np.int64)
+    t0 = time.perf_counter()
+    kinds, _ = oracle.classify_blocks(comp.prims, comp.program, meta, blocks)
+    t_cls = (time.perf_counter() - t0) / len(blocks)
+    sampled_active = blocks[kinds == 0]
+    if n_active is None:
+        n_active = int(round(len(sampled_active) / len(blocks) * meta.n_blocks))
+    pick = sampled_active[:n_tiles].astype(np.int32)
+    t_tile = 0.0
+    if len(pick):
+        t0 = time.perf_counter()
+        oracle.tiles_program(comp.prims, comp.program, meta, pick)
+        t_tile = (time.perf_counter() - t0) / len(pick)
+    t0 = time.perf_counter()
+    oracle.edt_squared(1 - mask)  # distance to the obstacles: sites are the nonzero voxels
+    t_edt = time.perf_counter() - t0
+    total = t_cls * meta.n_blocks + t_tile * n_active + t_edt
+    desc = (f"float64 classify of {len(blocks)} random blocks + leaf eval of {len(pick)} sampled active blocks "
+            f"(extrapolated to {meta.n_blocks} blocks / {n_active} active) + full {mask.shape[0]}^3 integer EDT")
+    return total, desc, oracle.threads(), n_active
+
+
+# ------------------------------------------------------------------------------------------ ours
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import field_b200.build as B
+    import field_b200.edt as E
+    import field_b200._lib as L
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    comp, meta, mask_np = workload(args.n, args.edt_n)
+    builder = B.FieldBuilder(comp, meta, device=dev)
+    stream = torch.cuda.current_stream()
+    # sizing run: exact active count, then a fixed tile buffer
+    df = builder.build()
+    n_active = int(df.n_active)
+    del df
+    b3 = meta.block ** 3
+    tiles = torch.empty((max(n_active, 1), b3), dtype=torch.float32, device=dev)
+    mask = torch.from_numpy(mask_np).to(dev)
+    edt_out = torch.empty(mask.shape, dtype=torch.int32, device=dev)
+    edt_scratch = torch.empty(int(L.lib().fb_edt_scratch_bytes(*mask.shape, 0)), dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    edt_voxels = int(np.prod(mask.shape))
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        builder.classify(stream)
+        if ev:
+            ev[1].record(stream)
+        builder.leaf(tiles, n_active, stream=stream)
+        if ev:
+            ev[2].record(stream)
+        E.squared_distance_device(mask, sites_nonzero=True, out=edt_out, scratch=edt_scratch, stream=stream)
+        if ev:
+            ev[3].record(stream)
+
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    assert int(builder.count.item()) == n_active, "active count changed between builds"
+    assert builder.compact_error() == 0
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        step(events[k])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    t_cls = [e[0].elapsed_time(e[1]) for e in events]
+    t_leaf = [e[1].elapsed_time(e[2]) for e in events]
+    t_edt = [e[2].elapsed_time(e[3]) for e in events]
+    t_step = [e[0].elapsed_time(e[3]) for e in events]
+    total_ms = float(sum(t_step))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    leaf_voxels = n_active * b3
+    value = leaf_voxels * world * args.steps / (total_ms * 1e-3) / 1e9
+
+    # executed work of the leaf kernel and the float32 peak (untimed)
+    work = torch.zeros(2, dtype=torch.int64, device=dev)
+    builder.classify(stream)
+    L.lib().fb_field_leaf_work_device(*builder._args(), builder.active.data_ptr(), builder.count.data_ptr(),
+                                      tiles.data_ptr(), n_active, builder.scratch.data_ptr(), builder.scratch.numel(),
+                                      work.data_ptr(), L.stream_handle(stream))
+    torch.cuda.synchronize()
+    evals, flops = (int(x) for x in work.cpu().numpy())
+    probe = torch.empty(L.lib().fb_sm_count_c() * 8, dtype=torch.float32, device=dev)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nflop = L.lib().fb_fp32_peak_launch(probe.data_ptr(), probe.numel(), 4096, L.stream_handle(stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = max(best, nflop / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    fp32_peak = best
+    hbm_peak, hbm_src = measured_peaks()
+
+    med = lambda xs: float(statistics.median(xs))
+    leaf_ms, edt_ms, cls_ms = med(t_leaf), med(t_edt), med(t_cls)
+    leaf_tflops = flops / (leaf_ms * 1e-3) / 1e12
+    leaf_gbs = leaf_voxels * 4 / (leaf_ms * 1e-3) / 1e9
+    edt_gbs = edt_voxels * EDT_BYTES_PER_VOXEL / (edt_ms * 1e-3) / 1e9
+    shares = {"classify": cls_ms, "leaf": leaf_ms, "edt": edt_ms}
+    dominant = max(shares, key=shares.get)
+    if dominant == "edt":
+        roof = {"kernel": "edt (k_edt_bits + k_edt_zy + k_edt_x)", "bound": "hbm", "achieved": edt_gbs,
+                "peak": hbm_peak, "unit": "GB/s", "frac": edt_gbs / hbm_peak,
+                "traffic": traffic_of("edt"), "basis": f"{EDT_BYTES_PER_VOXEL} B/voxel"}
+    else:
+        fp32_frac = leaf_tflops / fp32_peak
+        hbm_frac = leaf_gbs / hbm_peak
+        if fp32_frac >= hbm_frac:
+            roof = {"kernel": "k_leaf<8>", "bound": "fp32", "achieved": leaf_tflops, "peak": fp32_peak,
+                    "unit": "TFLOP/s", "frac": fp32_frac, "traffic": traffic_of("k_leaf"),
+                    "basis": "executed float32 ops of the culled primitive evaluations (FMA = 2); peak = FFMA probe"}
+        else:
+            roof = {"kernel": "k_leaf<8>", "bound": "hbm", "achieved": leaf_gbs, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm_frac, "traffic": traffic_of("k_leaf"), "basis": "4 B tile store per leaf voxel"}
+    roof["peak_source"] = hbm_src if roof["bound"] == "hbm" else "measured in this run (FFMA probe)"
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 guard band); int32 EDT", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [meta.nx, meta.ny, meta.nz], "block": meta.block,
+                   "primitives": int(len(comp.prims)), "chain": int(len(comp.chain)), "n_blocks": int(meta.n_blocks),
+                   "n_active": n_active, "leaf_voxels": leaf_voxels, "edt_grid": list(mask.shape),
+                   "edt_fill": float(mask_np.mean()), "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between steps, outside the per-step events"},
+        "phases_ms_median": {"classify": cls_ms, "leaf": leaf_ms, "edt": edt_ms},
+        "leaf": {"gvox_s": leaf_voxels / (leaf_ms * 1e-3) / 1e9, "tflops_executed": leaf_tflops,
+                 "evals_per_voxel": evals / max(leaf_voxels, 1), "fp32_peak_tflops": fp32_peak,
+                 "gbs_tile_store": leaf_gbs},
+        "edt": {"gbs": edt_gbs, "ms": edt_ms, "frac_hbm": edt_gbs / hbm_peak, "voxels": edt_voxels},
+        "roofline": roof,
+        "clocks": clk,
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+    }
+
+    if rank == 0 and not args.no_e2e:
+        result["e2e"] = e2e_leg(comp, meta, mask_np, dev)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        secs, desc, cores, _ = cpu_sample(comp, meta, mask_np, n_active=n_active)
+        result["cpu_baseline"] = {"value": leaf_voxels / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+                                  "sample": desc, "seconds_per_step": secs}
+    return result
+
+
+def e2e_leg(comp, meta, mask_np, dev, steps=2):
+    """The same step through the public host API: build_field -> SparseField (host arrays) and
+    NativeEDTLarge.squared_distance on a host mask; host<->device copies inside the timed region."""
+    import torch
+    import field_b200.build as B
+    import field_b200.edt as E
+    native = E.NativeEDTLarge()
+    binary = ~mask_np.astype(bool)  # zero sites = the obstacles
+    times = []
+    h2d = d2h = 0
+    leaf = 0
+    for _ in range(steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sf = B.build_field(comp, meta, device=dev)
+        sq = native.squared_distance(binary)
+        t = time.perf_counter() - t0
+        times.append(t)
+        leaf = sf.tiles.size
+        h2d = comp.prims.nbytes + comp.chain.nbytes + binary.size
+        d2h = sf.kind.nbytes + sf.corner_min_abs.nbytes + sf.active_ids.nbytes + sf.tiles.nbytes + sq.nbytes + 4
+    times = times[1:]
+    return {"value": leaf / statistics.median(times) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "seconds_per_step": statistics.median(times),
+            "api": "field_b200.build.build_field + field_b200.edt.NativeEDTLarge.squared_distance"}
+
+
+# ------------------------------------------------------------------------------------------ reference arm
+def run_reference(args, rank, world):
+    """The reference algorithm on the host cores only (no GPU code on this path)."""
+    if rank != 0:
+        return None
+    comp, meta, mask_np = workload(args.n, args.edt_n)
+    secs, estimates = [], []
+    desc = cores = None
+    for i in range(max(args.warmup, 3) + args.steps):
+        s, desc, cores, n_active = cpu_sample(comp, meta, mask_np, n_classify=4000, n_tiles=100, seed=i)
+        if i >= max(args.warmup, 3):
+            secs.append(s)
+            estimates.append(n_active)
+    sec = float(statistics.median(secs))
+    n_active = int(statistics.median(estimates))
+    leaf_voxels = n_active * meta.block ** 3
+    value = leaf_voxels / sec / 1e9
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 evaluator, int32 EDT", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [meta.nx, meta.ny, meta.nz], "block": meta.block,
+                   "n_active_estimate": n_active, "leaf_voxels": leaf_voxels, "edt_grid": list(mask_np.shape)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, rank, world)
+        else:
+            res = run_ours(args, rank, world, local_rank)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

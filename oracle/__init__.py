@@ -47,6 +47,7 @@ def lib():
             "or_eval_points": [P, ct.c_int32, P, ct.c_int32, P, I64, P],
             "or_classify_program": [P, ct.c_int32, P, ct.c_int32, D, D, D, D, I, I, I, I, F, P, P],
             "or_tiles_program": [P, ct.c_int32, P, ct.c_int32, D, D, D, D, I, I, I, I, P, I64, P],
+            "or_classify_blocks": [P, ct.c_int32, P, ct.c_int32, D, D, D, D, I, I, I, I, F, P, I64, P, P],
             "or_pack_nodes": [P], "or_pack_samples": [P], "or_pack_copy": [P, P, I64, P, I64],
             "or_pack_free": [P], "or_threads": [],
         }
@@ -246,6 +247,22 @@ def classify_program(prims, prog, meta):
     rc = lib().or_classify_program(P.ctypes.data, len(P), G.ctypes.data, len(G), meta.x0, meta.y0, meta.z0,
                                    meta.pitch, meta.nx, meta.ny, meta.nz, meta.block,
                                    float(np.float32(meta.margin_mm)), kind.ctypes.data, cma.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle classify status {rc}")
+    return kind, cma
+
+
+def classify_blocks(prims, prog, meta, blocks):
+    """(kind, corner_min_abs) of the listed blocks only (faltkarna_v1.py:129-164)."""
+    P = np.ascontiguousarray(prims, PRIM)
+    G = np.ascontiguousarray(prog, INSN)
+    b = np.ascontiguousarray(blocks, np.int64)
+    kind = np.empty(len(b), np.int32)
+    cma = np.empty(len(b), np.float64)
+    rc = lib().or_classify_blocks(P.ctypes.data, len(P), G.ctypes.data, len(G), meta.x0, meta.y0, meta.z0,
+                                  meta.pitch, meta.nx, meta.ny, meta.nz, meta.block,
+                                  float(np.float32(meta.margin_mm)), b.ctypes.data, len(b), kind.ctypes.data,
+                                  cma.ctypes.data)
     if rc:
         raise ValueError(f"oracle classify status {rc}")
     return kind, cma

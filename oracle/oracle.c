@@ -514,7 +514,7 @@ typedef struct {
 } or_insn;
 
 enum { OP_PUSH = 0, OP_UNION = 1, OP_INTERSECT = 2, OP_SUBTRACT = 3, OP_OFFSET = 4 };
-enum { P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS };
+enum { P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF };
 
 static double or_max(double a, double b) { return a > b ? a : b; }
 static double or_min(double a, double b) { return a < b ? a : b; }
@@ -578,6 +578,8 @@ static double or_prim_local(const or_prim *P, double x, double y, double z) {
         double qx = sqrt(x * x + y * y) - p[0];
         return sqrt(qx * qx + z * z) - p[1];
     }
+    case P_CYL_INF: /* unbounded z cylinder, src/field_engine/faltkarna_v1.py:102-104 */
+        return sqrt(x * x + y * y) - p[0];
     default:
         return NAN;
     }
@@ -672,6 +674,35 @@ int or_classify_program(const or_prim *prims, int32_t nprim, const or_insn *prog
         }
         if (cma) cma[t] = mn;
         kind[t] = (pos && neg) ? 0 : ((mn <= m) ? 0 : (neg ? -1 : 1));
+    }
+    return OR_OK;
+}
+
+/* The same classification for a list of block ids only (a bounded sample for CPU timing). */
+int or_classify_blocks(const or_prim *prims, int32_t nprim, const or_insn *prog, int32_t ninsn, double x0,
+                       double y0, double z0, double pitch, int nx, int ny, int nz, int block, float margin,
+                       const int64_t *blocks, int64_t n, int32_t *kind, double *cma) {
+    if (!prims || !prog || !blocks || !kind || nx < 1 || ny < 1 || nz < 1 || block < 1 || n < 0) return OR_INVALID;
+    int64_t nby = (ny + block - 1) / block, nbz = (nz + block - 1) / block;
+    double m = (double)margin;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t s = 0; s < n; ++s) {
+        int64_t t = blocks[s];
+        int64_t bk = t % nbz, bj = (t / nbz) % nby, bi = t / (nbz * nby);
+        double mn = 1.0e30;
+        int pos = 0, neg = 0;
+        for (int c = 0; c < 8; ++c) {
+            int64_t ix = bi * block + (c & 1) * block;
+            int64_t iy = bj * block + ((c >> 1) & 1) * block;
+            int64_t iz = bk * block + ((c >> 2) & 1) * block;
+            double v = or_program_eval(prims, nprim, prog, ninsn, x0 + (double)ix * pitch,
+                                       y0 + (double)iy * pitch, z0 + (double)iz * pitch);
+            double a = fabs(v);
+            if (a < mn) mn = a;
+            if (v >= 0.0) pos = 1; else neg = 1;
+        }
+        if (cma) cma[s] = mn;
+        kind[s] = (pos && neg) ? 0 : ((mn <= m) ? 0 : (neg ? -1 : 1));
     }
     return OR_OK;
 }

@@ -1,0 +1,130 @@
+"""CUDA field build parity against the float64 oracle and the reference's dense classifier (GPU)."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import Golden, sha
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def fb():
+    import field_b200.build as B
+    return B
+
+
+def _check_against_oracle(recipe, meta, fb, tol_frac=1e-5):
+    import field_b200.expr as X
+    comp = X.compile_recipe(recipe)
+    sf = fb.build_field(comp, meta)
+    kind, cma = oracle.classify_program(comp.prims, comp.program, meta)
+    assert (sf.kind == kind).all(), f"{int((sf.kind != kind).sum())} block decisions differ"
+    active = np.where(kind == 0)[0].astype(np.int32)
+    assert (sf.active_ids == active).all()
+    assert np.allclose(sf.corner_min_abs, cma, rtol=1e-5, atol=1e-5 * meta.pitch)
+    exact = oracle.tiles_program(comp.prims, comp.program, meta, active)
+    err = np.abs(sf.tiles.astype(np.float64) - exact).max() if len(active) else 0.0
+    sign = int(np.count_nonzero((sf.tiles >= 0) != (exact >= 0)))
+    assert sign == 0
+    assert err <= tol_frac * meta.pitch, (err, err / meta.pitch)
+    return sf, err
+
+
+@pytest.mark.parametrize("block", [4, 8, 16])
+def test_plain_union_small_matches_oracle(fb, block):
+    import field_b200.recipes as R
+    recipe, meta = R.plain_union(seed=0, n=96, block=block)
+    _check_against_oracle(recipe, meta, fb)
+
+
+def test_mixed_primitives_and_tools_match_oracle(fb):
+    import field_b200.recipes as R
+    import field_b200.expr as X
+    from field_b200.grid import GridMeta
+    rng = np.random.default_rng(11)
+    nodes = R.parts(rng, 10, 10, 10, 10, scale=0.6)
+    recipe = X.subtract_all(X.union_all(nodes), R.tools(rng, 12, 0.01, 0.03))
+    meta = GridMeta(-0.03, 0.01, 0.0, 1.0 / 112, 120, 100, 112, 8)
+    _check_against_oracle(recipe, meta, fb)
+
+
+def test_transforms_smooth_ops_and_offsets_match_oracle(fb):
+    import field_b200.expr as X
+    from field_b200.grid import GridMeta
+    t = X.union(X.subtract(X.cylinder(0.3, 0.8), X.box((0.2, 0.2, 0.2), (0.05, 0.0, 0.1)), k=0.05),
+                X.rotate(X.sphere(0.2, (-0.1, 0.05, -0.08)), "y", 37.0), k=0.08)
+    t = X.intersect(t, X.offset(X.cone(0.2, 0.45, 1.0, axis="x"), -0.02))
+    t = X.subtract(t, X.scale(X.torus(0.2, 0.05, "y", (0.1, 0.0, 0.0)), 1.3))
+    meta = GridMeta(-0.6, -0.6, -0.6, 1.2 / 100, 101, 101, 101, 8)
+    _check_against_oracle(t, meta, fb)
+
+
+def test_general_program_tree_matches_oracle(fb):
+    import field_b200.expr as X
+    from field_b200.grid import GridMeta
+    # intersect(A, union(B, C)) does not reduce to a chain: runs as a float64 postfix program
+    t = X.intersect(X.sphere(0.4), X.union(X.box((0.5, 0.1, 0.5)), X.cylinder(0.15, 1.0, axis="x")))
+    assert X.compile_recipe(t).chain is None
+    meta = GridMeta(-0.5, -0.5, -0.5, 1.0 / 64, 65, 64, 66, 8)
+    _check_against_oracle(t, meta, fb)
+
+
+def test_testfalt_volume_gate_and_planted_fault(fb):
+    """Box minus cylinder: volume within 3 % of the analytic value; the corrupted block index must
+    fail the gate (src/field_engine/faltkarna_v1_g7_fix.py:36-48, faltkarna_v1_selftest_v1.py:86-102)."""
+    import math
+    from field_b200.grid import GridMeta, konservering_check
+    HX, HY, HZ, R = 20.0, 15.0, 10.0, 6.0
+    vol = 8.0 * HX * HY * HZ - math.pi * R * R * (2.0 * HZ)
+    pitch, pad = 0.25, 1.0  # the reference's gate pitch (faltkarna_v1_g7_fix.py:230)
+    nx = int(round((2 * HX + 2 * pad) / pitch)) + 1
+    ny = int(round((2 * HY + 2 * pad) / pitch)) + 1
+    nz = int(round((2 * HZ + 2 * pad) / pitch)) + 1
+    meta = GridMeta(-HX - pad, -HY - pad, -HZ - pad, pitch, nx, ny, nz, 8)
+    sf = fb.klassificera_och_evaluera_testfalt(meta, HX, HY, HZ, R)
+    comp = fb.X.compile_recipe(fb.testfalt(HX, HY, HZ, R))
+    kind, _ = oracle.classify_program(comp.prims, comp.program, meta)
+    assert (sf.kind == kind).all()
+    dense = fb.rekonstruera_tat(sf)
+    assert konservering_check(float(np.sum(dense < 0)) * pitch ** 3, vol, 0.03)["GRON"]
+    bad = fb.klassificera_och_evaluera_testfalt(meta, HX, HY, HZ, R, corrupt_index=True)
+    dense_bad = fb.rekonstruera_tat(bad)
+    assert not konservering_check(float(np.sum(dense_bad < 0)) * pitch ** 3, vol, 0.03)["GRON"]
+
+
+def test_reconstruction_matches_numpy(fb):
+    import field_b200.recipes as R
+    from field_b200.grid import BIG
+    recipe, meta = R.plain_union(seed=5, n=80, block=8)
+    sf = fb.build_field(recipe, meta)
+    dense = fb.rekonstruera_tat(sf)
+    b = meta.block
+    px, py, pz = meta.n_bx * b, meta.n_by * b, meta.n_bz * b
+    kind_grid = sf.kind.reshape(meta.n_bx, meta.n_by, meta.n_bz)
+    padded = np.empty((px, py, pz), np.float32)
+    view = padded.reshape(meta.n_bx, b, meta.n_by, b, meta.n_bz, b).transpose(0, 2, 4, 1, 3, 5)
+    view[:] = np.where(kind_grid < 0, -BIG, BIG).astype(np.float32)[:, :, :, None, None, None]
+    bi, bj, bk = np.unravel_index(sf.active_ids, (meta.n_bx, meta.n_by, meta.n_bz))
+    view[bi, bj, bk] = sf.tiles
+    assert dense.tobytes() == np.ascontiguousarray(padded[:meta.nx, :meta.ny, :meta.nz]).tobytes()
+
+
+def test_dense_classifier_matches_compiled_reference(fb):
+    g = Golden("classify_golden")
+    for name in g.names("dense/"):
+        meta = g.meta[name]
+        dense = g.z[f"field/{meta['field']}"]
+        r = fb.klassificera_och_evaluera_fran_tatt_falt(None, dense, meta["pitch"], meta["block"])
+        assert (r["kind"] == g.z[f"{name}__kind"]).all(), name
+        assert sha(r["tiles"]) == meta["tiles_sha256"], name
+        assert r["n_active"] == meta["n_active"]
+
+
+def test_checksum_is_deterministic(fb):
+    rng = np.random.default_rng(0)
+    v = rng.normal(size=1_000_003).astype(np.float32)
+    a = fb.checksum_i64(v)
+    b = fb.checksum_i64(v)
+    expect = int(np.sum(np.trunc(v[v < 0].astype(np.float64) * 1e6).astype(np.int64)))
+    assert a == b == expect
