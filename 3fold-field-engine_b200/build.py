@@ -107,7 +107,8 @@ class FieldBuilder:
 
     def leaf(self, tiles, capacity, active=None, stream=None):
         act = self.active if active is None else active
-        st = self.lib.fb_field_leaf_device(*self._args(), act.data_ptr(), self.count.data_ptr(), tiles.data_ptr(),
+        st = self.lib.fb_field_leaf_device(*self._args(), self.kind.data_ptr(), act.data_ptr(), self.count.data_ptr(),
+                                           tiles.data_ptr(),
                                            int(capacity), self.scratch.data_ptr(), self.scratch.numel(),
                                            _lib.stream_handle(stream))
         _lib.check(st, "field leaf")

@@ -85,19 +85,75 @@ __global__ void __launch_bounds__(256) k_edt_bits(const uint8_t* __restrict__ ma
     }
 }
 
-// Exact 1-D min-plus along a staged column: best = min_t g[c +- t] + t^2.  Stops once t^2 >= best,
-// since no farther candidate can be strictly smaller.
-__device__ __forceinline__ int32_t window_min(const int32_t* col, int pos, int len, int stride) {
-    int32_t best = col[pos * stride];
+// ------------------------------------------------------------------------------------------
+// Exact 1-D min-plus along a staged column, out(q) = min_s col(s) + (q - s)^2.
+//
+// The smallest minimiser s*(q) is non-decreasing in q (for q1 < q2 a smaller minimiser of q2
+// would contradict the minimality of s*(q1); the squares' cross terms decide it).  So:
+//   step A: every kSample-th target q gets (value, smallest minimiser) by a window search that
+//           stops once t^2 exceeds the best value (no farther source can tie or win);
+//   step B: every other target scans only [s*(q_a), s*(q_b)] between its two sampled neighbours,
+//           all targets of an interval sharing each loaded source.
+// Both steps are exact; the cost is ~window/kSample + interval width per target instead of
+// ~2*window per target.
+// ------------------------------------------------------------------------------------------
+constexpr int kSample = 8;
+
+// (value, smallest minimiser) at q; col is this lane's column (stride 32 in shared memory).
+__device__ __forceinline__ int32_t window_argmin(const int32_t* col, int q, int len, int& arg) {
+    int32_t best = col[q * 32];
+    int bi = q;
     for (int t = 1; t < len; ++t) {
         const int32_t tt = t * t;
-        if (tt >= best) break;
-        const int lo = pos - t, hi = pos + t;
+        if (tt > best) break;
+        const int lo = q - t, hi = q + t;
         if (lo < 0 && hi >= len) break;
-        if (lo >= 0) best = min(best, col[lo * stride] + tt);
-        if (hi < len) best = min(best, col[hi * stride] + tt);
+        if (hi < len) {  // a larger index wins only when strictly better
+            const int32_t v = col[hi * 32] + tt;
+            if (v < best) { best = v; bi = hi; }
+        }
+        if (lo >= 0) {   // a smaller index wins ties
+            const int32_t v = col[lo * 32] + tt;
+            if (v <= best) { best = v; bi = lo; }
+        }
     }
+    arg = bi;
     return best;
+}
+
+// One column pass over a shared-memory block col[len][32]; lanes are columns, warps split the
+// targets.  `sidx` is shared scratch of ceil(len / kSample) * 32 int16.  `store(q, v)` receives
+// every result.  Contains a __syncthreads(): every thread of the CTA must call it.
+template <typename Store>
+__device__ __forceinline__ void column_pass(const int32_t* col, int16_t* sidx, int len, Store store) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int nsamp = (len + kSample - 1) / kSample;
+    for (int m = warp; m < nsamp; m += nwarps) {
+        int arg;
+        const int32_t v = window_argmin(col + lane, m * kSample, len, arg);
+        sidx[m * 32 + lane] = (int16_t)arg;
+        store(m * kSample, v);
+    }
+    __syncthreads();
+    for (int m = warp; m < nsamp; m += nwarps) {
+        const int q0 = m * kSample;
+        const int nt = min(kSample - 1, len - 1 - q0);  // targets q0+1 .. q0+nt
+        if (nt <= 0) continue;
+        const int lo = sidx[m * 32 + lane];
+        const int hi = m + 1 < nsamp ? sidx[(m + 1) * 32 + lane] : len - 1;
+        int32_t best[kSample - 1];
+#pragma unroll
+        for (int i = 0; i < kSample - 1; ++i) best[i] = 0x7fffffff;
+        for (int s = lo; s <= hi; ++s) {
+            const int32_t f = col[s * 32 + lane];
+            const int d = q0 + 1 - s;
+#pragma unroll
+            for (int i = 0; i < kSample - 1; ++i) best[i] = min(best[i], f + (d + i) * (d + i));
+        }
+#pragma unroll
+        for (int i = 0; i < kSample - 1; ++i)
+            if (i < nt) store(q0 + 1 + i, best[i]);
+    }
 }
 
 // z pass (from bit words) + y pass.  grid = (W, nx, polarities); dynamic smem = ny * 32 * 4 bytes.
@@ -141,11 +197,12 @@ __global__ void __launch_bounds__(kThreads) k_edt_zy(const uint32_t* __restrict_
         col[y * 32 + lane] = value;
     }
     __syncthreads();
-    if (z >= nz) return;
     int32_t* out = g + (int64_t)pol * nx * ny * nz;
-    for (int y = warp; y < ny; y += nwarps) {
-        out[((int64_t)x * ny + y) * nz + z] = window_min(col + lane, y, ny, 32);
-    }
+    int16_t* sidx = reinterpret_cast<int16_t*>(col + ny * 32);
+    const bool live = z < nz;
+    column_pass(col, sidx, ny, [&](int y, int32_t v) {
+        if (live) out[((int64_t)x * ny + y) * nz + z] = v;
+    });
 }
 
 // Correctly rounded signed distance of one voxel from its two squared distances, the reference's
@@ -165,36 +222,41 @@ __device__ __forceinline__ float signed_from_pair(int32_t sq_out, int32_t sq_in,
 __global__ void __launch_bounds__(kThreads) k_edt_x(const int32_t* __restrict__ g, int32_t* __restrict__ out,
                                                     float* __restrict__ signed_out, int nx, int ny, int nz,
                                                     int paired, double pitch, float half) {
-    extern __shared__ int32_t col[];  // [npol][nx][32]
+    // shared: col[npol][nx][32], then (paired) res0[nx][32], then sidx
+    extern __shared__ int32_t col[];
     const int w = blockIdx.x, y = blockIdx.y;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int z = 32 * w + lane;
+    const bool live = z < nz;
     const int64_t size = (int64_t)nx * ny * nz;
     const int npol = paired ? 2 : 1;
     const int pol0 = paired ? 0 : blockIdx.z;
     for (int p = 0; p < npol; ++p) {
         const int32_t* src = g + (int64_t)(pol0 + p) * size;
         for (int x = warp; x < nx; x += nwarps)
-            col[(p * nx + x) * 32 + lane] = z < nz ? src[((int64_t)x * ny + y) * nz + z] : 0;
+            col[(p * nx + x) * 32 + lane] = live ? src[((int64_t)x * ny + y) * nz + z] : 0;
     }
+    int32_t* res0 = col + npol * nx * 32;
+    int16_t* sidx = reinterpret_cast<int16_t*>(res0 + (paired ? nx * 32 : 0));
     __syncthreads();
-    if (z >= nz) return;
     if (!paired) {
         int32_t* dst = out + (int64_t)pol0 * size;
-        for (int x = warp; x < nx; x += nwarps)
-            dst[((int64_t)x * ny + y) * nz + z] = window_min(col + lane, x, nx, 32);
+        column_pass(col, sidx, nx, [&](int x, int32_t v) {
+            if (live) dst[((int64_t)x * ny + y) * nz + z] = v;
+        });
         return;
     }
-    for (int x = warp; x < nx; x += nwarps) {
-        const int32_t so = window_min(col + lane, x, nx, 32);
-        const int32_t si = window_min(col + nx * 32 + lane, x, nx, 32);
-        const int64_t v = ((int64_t)x * ny + y) * nz + z;
-        signed_out[v] = signed_from_pair(so, si, pitch, half);
-        if (out) {
-            out[v] = so;
-            out[size + v] = si;
-        }
-    }
+    column_pass(col, sidx, nx, [&](int x, int32_t v) {
+        res0[x * 32 + lane] = v;
+        if (live && out) out[((int64_t)x * ny + y) * nz + z] = v;
+    });
+    __syncthreads();
+    column_pass(col + nx * 32, sidx, nx, [&](int x, int32_t v) {
+        if (!live) return;
+        const int64_t i = ((int64_t)x * ny + y) * nz + z;
+        signed_out[i] = signed_from_pair(res0[x * 32 + lane], v, pitch, half);
+        if (out) out[size + i] = v;
+    });
 }
 
 bool shape_ok(int nx, int ny, int nz) {
@@ -214,11 +276,15 @@ int64_t scratch_bytes(int nx, int ny, int nz, int npol) {
     return 256 + bits + (int64_t)npol * size * 4;
 }
 
+int sidx_bytes(int len) { return (len + kSample - 1) / kSample * 32 * 2; }
+
 int configure_once() {
     static int done = 0;
     if (done) return FB_OK;
-    FB_CUDA(cudaFuncSetAttribute(k_edt_zy, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxAxis * 32 * 4));
-    FB_CUDA(cudaFuncSetAttribute(k_edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxAxis * 32 * 4));
+    FB_CUDA(cudaFuncSetAttribute(k_edt_zy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kMaxAxis * 32 * 4 + sidx_bytes(kMaxAxis)));
+    FB_CUDA(cudaFuncSetAttribute(k_edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 3 * kMaxAxis * 32 * 4 + sidx_bytes(kMaxAxis)));
     done = 1;
     return FB_OK;
 }
@@ -248,14 +314,16 @@ int enqueue(const uint8_t* d_mask, int nx, int ny, int nz, int paired, int sites
     const int32_t sentinel = sentinel_of(nx, ny, nz);
     // Single polarity measuring to zero bytes = the set bits flipped.
     const int invert = paired ? 0 : (sites_nonzero ? 0 : 1);
-    k_edt_zy<<<dim3(W, nx, npol), kThreads, ny * 32 * 4, stream>>>(bits, g, nx, ny, nz, W, invert, sentinel);
+    k_edt_zy<<<dim3(W, nx, npol), kThreads, ny * 32 * 4 + sidx_bytes(ny), stream>>>(bits, g, nx, ny, nz, W, invert,
+                                                                                     sentinel);
     FB_LAUNCH();
     const float half = (float)(0.5 * pitch);
     if (paired) {
-        k_edt_x<<<dim3(W, ny, 1), kThreads, 2 * nx * 32 * 4, stream>>>(g, out_sq, out_signed, nx, ny, nz, 1, pitch,
-                                                                       half);
+        k_edt_x<<<dim3(W, ny, 1), kThreads, 3 * nx * 32 * 4 + sidx_bytes(nx), stream>>>(g, out_sq, out_signed, nx, ny,
+                                                                                         nz, 1, pitch, half);
     } else {
-        k_edt_x<<<dim3(W, ny, 1), kThreads, nx * 32 * 4, stream>>>(g, out_sq, nullptr, nx, ny, nz, 0, pitch, half);
+        k_edt_x<<<dim3(W, ny, 1), kThreads, nx * 32 * 4 + sidx_bytes(nx), stream>>>(g, out_sq, nullptr, nx, ny, nz, 0,
+                                                                                     pitch, half);
     }
     FB_LAUNCH();
     (void)size;

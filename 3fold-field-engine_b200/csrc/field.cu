@@ -40,7 +40,7 @@ constexpr int kCapCoarse = 1024;
 constexpr int kCapSuper = 256;
 constexpr int kCapBlock = 48;
 constexpr int kSuperEdge = 32;    // voxels per superblock edge
-constexpr int kCoarseDiv = 4;     // superblocks per coarse-region edge
+constexpr int kCoarseDiv = 2;     // superblocks per coarse-region edge
 constexpr int kTile = 2048;       // compaction tile (256 threads x 8)
 constexpr int kLeafWarps = 4;     // warps per CTA in k_leaf
 
@@ -95,6 +95,7 @@ bool geom_ok(const FbGeom& g) {
 // ------------------------------------------------------------------------------------ scratch
 struct Plan {
     int64_t primf, pool, off, len, status, misc, total;
+    int64_t blk_off, blk_len, blk_pool, blk_cap;  // per-block culled lists of active blocks
     int64_t pool_full, pool_coarse, pool_super;  // element offsets inside pool
     int64_t ntiles;
 };
@@ -114,7 +115,11 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     p.len = at; at += align256((G.ncoarse + G.nsuper) * 4);
     p.ntiles = (G.nblocks + kTile - 1) / kTile;
     p.status = at; at += align256(p.ntiles * 8);
-    p.misc = at; at += 256;  // [0] ticket, [1] error flag
+    p.misc = at; at += 256;  // [0] ticket, [1] error flag, [2] block-list pool cursor
+    p.blk_off = at; at += align256(G.nblocks * 4);
+    p.blk_len = at; at += align256(G.nblocks * 4);
+    p.blk_cap = std::max<int64_t>(G.nblocks * 12, 4096);
+    p.blk_pool = at; at += align256(p.blk_cap * 4);
     p.total = at;
     return p;
 }
@@ -250,7 +255,7 @@ __device__ __forceinline__ Elem load_elem(const uint32_t* __restrict__ in, int e
                                           const PrimF* __restrict__ primf, float cx, float cy, float cz, float R,
                                           float eps, bool with_bounds) {
     Elem E;
-    E.ent = in[e];
+    E.ent = in ? in[e] : (uint32_t)e << 2;  // a null list is the whole chain in order
     const FbInsn I = chain[E.ent >> 2];
     E.op = effective_op(E.ent, I.op);
     E.k = (float)I.k;
@@ -474,7 +479,7 @@ __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __r
     const float cz = G.fz0 + (rz * edge + half) * G.fpitch;
     const float R = 1.7320509f * half * G.fpitch;
     uint32_t* dst = pool + pool_base + r * cap;
-    const int n = warp_walk(pool + poff, plen, chain, primf, cx, cy, cz, R, G.eps, dst, cap);
+    const int n = warp_walk(parent_off ? pool + poff : nullptr, plen, chain, primf, cx, cy, cz, R, G.eps, dst, cap);
     if ((threadIdx.x & 31) == 0) {
         if (n <= cap) {
             off[r] = pool_base + r * cap;
@@ -523,32 +528,46 @@ __device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, in
     return acc;
 }
 
+// Threads of one superblock are consecutive (a warp never spans two superblocks in the chain
+// mode), so the walk over the superblock's list runs in lockstep with broadcast loads.
+__host__ __device__ __forceinline__ int threads_per_super(int S) { return ((S * S * S + 31) / 32) * 32; }
+
 template <bool kChain>
 __global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restrict__ prims,
                                                   const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
                                                   int n_chain, const uint32_t* __restrict__ pool,
                                                   const int64_t* __restrict__ sb_off,
                                                   const int32_t* __restrict__ sb_len, int32_t* __restrict__ kind,
-                                                  float* __restrict__ cma) {
-    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (b >= G.nblocks) return;
-    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
+                                                  float* __restrict__ cma, int32_t* __restrict__ blk_off,
+                                                  int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool,
+                                                  int64_t blk_cap, int* __restrict__ blk_cursor) {
+    const int S = G.S;
+    const int T = threads_per_super(S);
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t s_id = t / T;
+    const int local = (int)(t % T);
+    if (s_id >= G.nsuper || local >= S * S * S) return;
+    const int sz = (int)(s_id % G.nsz), sy = (int)((s_id / G.nsz) % G.nsy), sx = (int)(s_id / ((int64_t)G.nsz * G.nsy));
+    const int bi = sx * S + local / (S * S), bj = sy * S + (local / S) % S, bk = sz * S + local % S;
+    if (bi >= G.nbx || bj >= G.nby || bk >= G.nbz) return;
+    const int64_t b = ((int64_t)bi * G.nby + bj) * G.nbz + bk;
     const int B = G.B;
     float v[8];
     double vd[8];
     bool use_d = false;
+    uint32_t blist[kCapBlock];
+    int nblist = -1;
     if (kChain) {
-        const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
-        const uint32_t* plist = pool + sb_off[s];
-        const int plen = sb_len[s];
+        const uint32_t* plist = pool + sb_off[s_id];
+        const int plen = sb_len[s_id];
         // block-level cull of the superblock list
-        uint32_t blist[kCapBlock];
         const float half = 0.5f * B;
         const float cx = G.fx0 + (bi * B + half) * G.fpitch;
         const float cy = G.fy0 + (bj * B + half) * G.fpitch;
         const float cz = G.fz0 + (bk * B + half) * G.fpitch;
         const float R = 1.7320509f * half * G.fpitch;
         const int n = seq_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, blist, kCapBlock);
+        nblist = n;
         const uint32_t* list = n <= kCapBlock ? blist : plist;
         const int len = n <= kCapBlock ? n : plen;
         const double ox = G.x0 + (double)(bi * B) * G.pitch;
@@ -619,6 +638,18 @@ __global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restric
         cma[b] = mn;
     }
     kind[b] = kd;
+    if (kChain && kd == 0) {  // keep the culled list for the leaf pass
+        int len = -1;
+        if (nblist >= 0 && nblist <= kCapBlock) {
+            const int slot = atomicAdd(blk_cursor, nblist);
+            if ((int64_t)slot + nblist <= blk_cap) {
+                for (int i = 0; i < nblist; ++i) blk_pool[slot + i] = blist[i];
+                blk_off[b] = slot;
+                len = nblist;
+            }
+        }
+        blk_len[b] = len;  // -1: the leaf pass culls from the superblock list itself
+    }
 }
 
 // ------------------------------------------------------------------------------------ compaction
@@ -708,20 +739,21 @@ __global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kin
 // voxels, not once per voxel, which keeps the evaluation loop small enough for the i-cache).
 template <int T>
 __device__ __forceinline__ float canon_t(const float* __restrict__ p, float x, float y, float z) {
-    if (T == P_SPHERE) return sqrtf(fmaf(x, x, fmaf(y, y, z * z))) - p[0];
+    // z-dependent terms outermost: across a group of voxels along z the x/y parts are shared
+    if (T == P_SPHERE) return sqrtf(fmaf(z, z, fmaf(x, x, y * y))) - p[0];
     if (T == P_BOX) {
         const float qx = fabsf(x) - p[0], qy = fabsf(y) - p[1], qz = fabsf(z) - p[2];
         const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f), oz = fmaxf(qz, 0.f);
-        return sqrtf(fmaf(ox, ox, fmaf(oy, oy, oz * oz))) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.f);
+        return sqrtf(fmaf(oz, oz, fmaf(ox, ox, oy * oy))) + fminf(fmaxf(qz, fmaxf(qx, qy)), 0.f);
     }
     if (T == P_CAPSULE) {
-        const float h = fminf(fmaxf(fmaf(x, p[0], fmaf(y, p[1], z * p[2])) * p[4], 0.f), 1.f);
+        const float h = fminf(fmaxf(fmaf(z, p[2], fmaf(x, p[0], y * p[1])) * p[4], 0.f), 1.f);
         const float dx = fmaf(-p[0], h, x), dy = fmaf(-p[1], h, y), dz = fmaf(-p[2], h, z);
-        return sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - p[3];
+        return sqrtf(fmaf(dz, dz, fmaf(dx, dx, dy * dy))) - p[3];
     }
     if (T == P_TORUS) {
         const float qx = sqrtf(fmaf(x, x, y * y)) - p[0];
-        return sqrtf(fmaf(qx, qx, z * z)) - p[1];
+        return sqrtf(fmaf(z, z, qx * qx)) - p[1];
     }
     return canon_f(T, p, x, y, z);
 }
@@ -817,6 +849,20 @@ __device__ __forceinline__ unsigned prim_flops(int type, int ident) {
     return affine + f + 2;
 }
 
+// One lane's group of VG consecutive voxels: vector stores, coalesced across the warp.
+template <int VG>
+__device__ __forceinline__ void store_group(float* out, int group, const float* acc) {
+    if (VG == 8) {
+        float4* o = reinterpret_cast<float4*>(out) + 2 * group;
+        o[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        o[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+    } else if (VG == 4) {
+        reinterpret_cast<float4*>(out)[group] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+        reinterpret_cast<float2*>(out)[group] = make_float2(acc[0], acc[1]);
+    }
+}
+
 // Leaf tile of one block whose culled list is longer than the shared staging: every primitive is
 // localised on the fly (rare; kept out of line so the fast loop stays small).
 template <int B, int VG>
@@ -856,8 +902,7 @@ __device__ __noinline__ void leaf_block_slow(const Geo& G, const FbPrim* __restr
             if (!(fabsf(acc[k]) >= G.guard))
                 acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li, (int64_t)bj * B + lj,
                                             (int64_t)bk * B + lk0 + k);
-        if (VG == 4) reinterpret_cast<float4*>(out)[g * 32 + lane] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-        else reinterpret_cast<float2*>(out)[g * 32 + lane] = make_float2(acc[0], acc[1]);
+        store_group<VG>(out, g * 32 + lane, acc);
     }
 }
 
@@ -873,9 +918,13 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim
                                                              const int32_t* __restrict__ active,
                                                              const int32_t* __restrict__ count, int64_t capacity,
                                                              float* __restrict__ tiles,
-                                                             unsigned long long* __restrict__ work) {
+                                                             unsigned long long* __restrict__ work,
+                                                             const int32_t* __restrict__ kind,
+                                                             const int32_t* __restrict__ blk_off,
+                                                             const int32_t* __restrict__ blk_len,
+                                                             const uint32_t* __restrict__ blk_pool, int64_t blk_cap) {
     constexpr int kVox = B * B * B;
-    constexpr int VG = B == 4 ? 2 : 4;
+    constexpr int VG = B == 4 ? 2 : 8;
     constexpr int kGroups = kVox / (32 * VG);
     __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
     __shared__ uint32_t s_list[kLeafWarps][kCapBlock];
@@ -896,20 +945,32 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim
         const double ox = G.x0 + (double)(bi * B) * G.pitch;
         const double oy = G.y0 + (double)(bj * B) * G.pitch;
         const double oz = G.z0 + (double)(bk * B) * G.pitch;
-        const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
-        const uint32_t* plist = pool + sb_off[s];
-        const int plen = sb_len[s];
-        const float half = 0.5f * B;
-        const float cx = G.fx0 + (bi * B + half) * G.fpitch;
-        const float cy = G.fy0 + (bj * B + half) * G.fpitch;
-        const float cz = G.fz0 + (bk * B + half) * G.fpitch;
-        const float R = 1.7320509f * half * G.fpitch;
-        __syncwarp();
-        const int nk = warp_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, sl, kCapBlock);
-        __syncwarp();
-        const bool fits = nk <= kCapBlock;
-        const uint32_t* list = fits ? sl : plist;
-        const int len = fits ? nk : plen;
+        // the block's culled list, as the classification left it; cull again if it is not there
+        const uint32_t* list;
+        int len;
+        bool fits = true;
+        int stored = kind[blk] == 0 ? blk_len[blk] : -1;
+        const int64_t soff = stored >= 0 ? (int64_t)blk_off[blk] : 0;
+        if (stored < 0 || stored > kCapBlock || soff < 0 || soff + stored > blk_cap) stored = -1;
+        if (stored >= 0) {
+            list = blk_pool + soff;
+            len = stored;
+        } else {
+            const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
+            const uint32_t* plist = pool + sb_off[s];
+            const int plen = sb_len[s];
+            const float half = 0.5f * B;
+            const float cx = G.fx0 + (bi * B + half) * G.fpitch;
+            const float cy = G.fy0 + (bj * B + half) * G.fpitch;
+            const float cz = G.fz0 + (bk * B + half) * G.fpitch;
+            const float R = 1.7320509f * half * G.fpitch;
+            __syncwarp();
+            const int nk = warp_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, sl, kCapBlock);
+            __syncwarp();
+            fits = nk <= kCapBlock;
+            list = fits ? sl : plist;
+            len = fits ? nk : plen;
+        }
         if (work) {  // executed primitive evaluations and their float32 operation count
             unsigned long long evals = 0, flops = 0;
             for (int i = lane; i < len; i += 32) {
@@ -975,8 +1036,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim
                         acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
                                                     (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
             }
-            if (VG == 4) reinterpret_cast<float4*>(out)[g * 32 + lane] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-            else reinterpret_cast<float2*>(out)[g * 32 + lane] = make_float2(acc[0], acc[1]);
+            store_group<VG>(out, g * 32 + lane, acc);
         }
     }
 }
@@ -1089,6 +1149,9 @@ __global__ void k_checksum_i64(const float* __restrict__ v, int64_t n, double sc
 
 // ------------------------------------------------------------------------------------ host side
 struct Scratch {
+    int32_t* blk_off;
+    int32_t* blk_len;
+    uint32_t* blk_pool;
     PrimF* primf;
     uint32_t* pool;
     int64_t* off;
@@ -1106,6 +1169,9 @@ Scratch carve(void* base, const Plan& p, const Geo& G) {
     s.len = reinterpret_cast<int32_t*>(b + p.len);
     s.status = reinterpret_cast<unsigned long long*>(b + p.status);
     s.misc = reinterpret_cast<int*>(b + p.misc);
+    s.blk_off = reinterpret_cast<int32_t*>(b + p.blk_off);
+    s.blk_len = reinterpret_cast<int32_t*>(b + p.blk_len);
+    s.blk_pool = reinterpret_cast<uint32_t*>(b + p.blk_pool);
     (void)G;
     return s;
 }
@@ -1147,21 +1213,24 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
                                                               G.ncy, G.ncz, S.off + G.ncoarse, S.len + G.ncoarse,
                                                               P.pool_super, kCapSuper, G.S * G.B, G.nsx, G.nsy, G.nsz);
         FB_LAUNCH();
-        k_classify<true><<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, S.primf, chain, n_chain, S.pool,
-                                                                    S.off + G.ncoarse, S.len + G.ncoarse, kind, cma);
+        FB_CUDA(cudaMemsetAsync(S.misc, 0, 256, st));
+        k_classify<true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+            G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
+            S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
     } else {
-        k_classify<false><<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, S.primf, chain, n_chain, S.pool,
-                                                                     S.off + G.ncoarse, S.len + G.ncoarse, kind, cma);
+        k_classify<false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+            G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
+            S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
     }
     FB_LAUNCH();
     return launch_compact(kind, G.nblocks, active, count, S.status, S.misc, st);
 }
 
 int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* chain, int n_chain, int mode,
-              const int32_t* active, const int32_t* count, float* tiles, int64_t capacity, void* scratch,
-              int64_t scratch_len, cudaStream_t st, unsigned long long* work = nullptr) {
-    if (!geom_ok(g) || !prims || !chain || n_prims < 1 || n_chain < 1 || !active || !count || !tiles || !scratch ||
-        capacity < 0)
+              const int32_t* kind, const int32_t* active, const int32_t* count, float* tiles, int64_t capacity,
+              void* scratch, int64_t scratch_len, cudaStream_t st, unsigned long long* work = nullptr) {
+    if (!geom_ok(g) || !prims || !chain || n_prims < 1 || n_chain < 1 || !kind || !active || !count || !tiles ||
+        !scratch || capacity < 0)
         return FB_INVALID;
     const Geo G = make_geo(g);
     const Plan P = make_plan(G, n_prims, n_chain);
@@ -1180,15 +1249,18 @@ int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* c
         switch (G.B) {
         case 4:
             k_leaf<4><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, count,
-                                                       capacity, tiles, work);
+                                                       capacity, tiles, work, kind, S.blk_off, S.blk_len, S.blk_pool,
+                                                       P.blk_cap);
             break;
         case 8:
             k_leaf<8><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, count,
-                                                       capacity, tiles, work);
+                                                       capacity, tiles, work, kind, S.blk_off, S.blk_len, S.blk_pool,
+                                                       P.blk_cap);
             break;
         default:
             k_leaf<16><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active,
-                                                        count, capacity, tiles, work);
+                                                        count, capacity, tiles, work, kind, S.blk_off, S.blk_len,
+                                                        S.blk_pool, P.blk_cap);
         }
     }
     FB_LAUNCH();
@@ -1220,21 +1292,22 @@ int fb_field_classify_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_p
 // Leaf tiles of the first min(count, capacity) active blocks, tile order (li, lj, lk).  Uses the
 // culling lists left in `d_scratch` by fb_field_classify_device for the same recipe and geometry.
 int fb_field_leaf_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prims, const FbInsn* d_chain,
-                         int32_t n_chain, int32_t mode, const int32_t* d_active, const int32_t* d_count, float* d_tiles,
-                         int64_t capacity, void* d_scratch, int64_t scratch_len, void* stream) noexcept {
+                         int32_t n_chain, int32_t mode, const int32_t* d_kind, const int32_t* d_active,
+                         const int32_t* d_count, float* d_tiles, int64_t capacity, void* d_scratch, int64_t scratch_len,
+                         void* stream) noexcept {
     if (!g) return FB_INVALID;
-    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_active, d_count, d_tiles, capacity, d_scratch,
+    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_kind, d_active, d_count, d_tiles, capacity, d_scratch,
                      scratch_len, static_cast<cudaStream_t>(stream));
 }
 
 // fb_field_leaf_device plus a count of the executed work: d_work[0] += primitive evaluations,
 // d_work[1] += float32 operations (two uint64 counters, accumulated).
 int fb_field_leaf_work_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prims, const FbInsn* d_chain,
-                              int32_t n_chain, int32_t mode, const int32_t* d_active, const int32_t* d_count,
-                              float* d_tiles, int64_t capacity, void* d_scratch, int64_t scratch_len,
-                              uint64_t* d_work, void* stream) noexcept {
+                              int32_t n_chain, int32_t mode, const int32_t* d_kind, const int32_t* d_active,
+                              const int32_t* d_count, float* d_tiles, int64_t capacity, void* d_scratch,
+                              int64_t scratch_len, uint64_t* d_work, void* stream) noexcept {
     if (!g || !d_work) return FB_INVALID;
-    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_active, d_count, d_tiles, capacity, d_scratch,
+    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_kind, d_active, d_count, d_tiles, capacity, d_scratch,
                      scratch_len, static_cast<cudaStream_t>(stream), reinterpret_cast<unsigned long long*>(d_work));
 }
 
@@ -1249,8 +1322,8 @@ int fb_field_build_device(const FbGeom* g, const FbPrim* d_prims, int32_t n_prim
     int rc = classify_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_kind, d_cma, d_active, d_count, d_scratch,
                            scratch_len, st);
     if (rc) return rc;
-    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_active, d_count, d_tiles, capacity, d_scratch,
-                     scratch_len, st);
+    return leaf_impl(*g, d_prims, n_prims, d_chain, n_chain, mode, d_kind, d_active, d_count, d_tiles, capacity,
+                     d_scratch, scratch_len, st);
 }
 
 // Scratch bytes of a dense classification (compaction state only).

@@ -242,7 +242,8 @@ def run_ours(args, rank, world, local_rank):
     # executed work of the leaf kernel and the float32 peak (untimed)
     work = torch.zeros(2, dtype=torch.int64, device=dev)
     builder.classify(stream)
-    L.lib().fb_field_leaf_work_device(*builder._args(), builder.active.data_ptr(), builder.count.data_ptr(),
+    L.lib().fb_field_leaf_work_device(*builder._args(), builder.kind.data_ptr(), builder.active.data_ptr(),
+                                      builder.count.data_ptr(),
                                       tiles.data_ptr(), n_active, builder.scratch.data_ptr(), builder.scratch.numel(),
                                       work.data_ptr(), L.stream_handle(stream))
     torch.cuda.synchronize()
