@@ -1,0 +1,142 @@
+/*
+ * field_b200.h -- C ABI of libfield_b200.so, the B200-native (sm_100a) block-sparse SDF field path.
+ *
+ * Conventions (the reference's native contract, src/field_engine/edt_native_v1/edt.cu:18-19 and
+ * src/field_engine/csg_batch_native_v1/execute.cpp):
+ *   - every entry point is extern "C" and noexcept; integer status: 0 ok, 1 invalid input,
+ *     2 runtime / CUDA failure, 3-5 the CSG codes of execute.cpp/gather.cpp, 6 a bounded device
+ *     wait gave up (the context stays usable);
+ *   - arguments are validated before any output is written;
+ *   - handles are created and destroyed explicitly; a handle that failed stays failed;
+ *   - *_device entry points take device pointers and a cudaStream_t (as void*), enqueue their
+ *     kernels on that stream and return without synchronising; they allocate nothing -- the
+ *     caller passes scratch sized by the matching *_scratch_bytes function;
+ *   - entry points without the _device suffix take host pointers and are synchronous, with the
+ *     reference's names and arguments.
+ * Paths in citations are relative to the reference project root.
+ */
+#ifndef FIELD_B200_H
+#define FIELD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------ records */
+
+/* Grid of one build: vertex-centred samples at x0 + i*pitch, blocks of block^3 voxels (4, 8 or 16),
+ * margin = float32(sqrt(3)*block*pitch), guard = float64-recheck band.
+ * Mirrors GridMeta, src/field_engine/faltkarna_v1.py:50-64. */
+typedef struct fb_geom {
+    double x0, y0, z0, pitch;
+    int32_t nx, ny, nz, block;
+    float margin, guard;
+    int32_t reserved[2];
+} fb_geom; /* 64 bytes */
+
+/* One primitive: value = s * f(A x + t) - off, f canonical (type 0 sphere, 1 box, 2 cylinder, 3 cone,
+ * 4 halfspace, 5 rect_frustum, 6 capsule, 7 torus, 8 unbounded z cylinder).
+ * Primitive set of src/field_engine/ikarus_v1/expr.py:93-210 plus capsule/torus. */
+typedef struct fb_prim {
+    int32_t type, flags;
+    double p[12];
+    double A[12]; /* rows of the 3x4 world -> canonical map */
+    double s, off;
+} fb_prim; /* 216 bytes */
+
+/* Program instruction.  Chain form (mode 1): op 0 set, 1 set-negated, 2 union, 3 intersect,
+ * 4 subtract, 5 offset; arg = primitive (or -1), k = smooth radius or offset.  Postfix form
+ * (mode 0): op 0 push primitive arg, 1 union, 2 intersect, 3 subtract, 4 offset by k.
+ * Semantics of src/field_engine/ikarus_v1/expr.py:364-384. */
+typedef struct fb_insn {
+    int32_t op, arg;
+    double k;
+} fb_insn; /* 16 bytes */
+
+/* ------------------------------------------------------------------------------------------ runtime */
+
+int fb_abi_version(void);     /* no reference counterpart: ABI version of this library */
+int fb_device_arch(void);     /* no reference counterpart: compute capability x10 of the current device */
+int fb_sm_count_c(void);      /* no reference counterpart: SM count of the current device */
+/* No reference counterpart: float32 FMA throughput probe (roofline denominator); returns its flops. */
+int64_t fb_fp32_peak_launch(float* d_out, int blocks, int iters, void* stream);
+
+/* ------------------------------------------------------------------------------------------ EDT */
+
+/* Replaces edt_squared, src/field_engine/edt_native_v1/edt.cu:20 (<= 128 per axis, <= 262144 voxels).
+ * Squared distance of every voxel to the nearest zero byte of `mask` (host pointers). */
+int edt_squared(const uint8_t* mask, int nx, int ny, int nz, int32_t* output);
+
+/* Replaces edt_squared_large, src/field_engine/edt_native_large_v1/edt.cu:33 (<= 512 per axis; the
+ * reference's 2^20-voxel cap is lifted to 512^3). */
+int edt_squared_large(const uint8_t* mask, int nx, int ny, int nz, int32_t* output);
+
+/* Replace edt_pair_create / edt_pair_query / edt_pair_destroy,
+ * src/field_engine/edt_persistent_pair_v1/edt.cu:45-79 (persistent device buffers; signed float32
+ * distance, negative inside `mask`, and optionally both squared transforms, polarity-major). */
+void* edt_pair_create(int nx, int ny, int nz);
+int edt_pair_query(void* handle, const uint8_t* mask, double pitch, float* output, int32_t* squared);
+void edt_pair_destroy(void* handle);
+
+/* Device forms of the same transforms (src/field_engine/edt_persistent_pair_v1/edt.cu:12-42).
+ * fb_edt_squared_device: sites are the nonzero bytes when sites_nonzero, else the zero bytes.
+ * fb_edt_pair_device: polarity 0 to the nonzero voxels; d_squared (nullable) gets both.
+ * fb_edt_validate_device: status 1 when a byte is > 1 or only one class is present (synchronises). */
+int64_t fb_edt_scratch_bytes(int nx, int ny, int nz, int paired);
+int fb_edt_squared_device(const uint8_t* d_mask, int nx, int ny, int nz, int sites_nonzero, int32_t* d_out,
+                          void* d_scratch, int64_t scratch_len, void* stream);
+int fb_edt_pair_device(const uint8_t* d_mask, int nx, int ny, int nz, double pitch, float* d_signed,
+                       int32_t* d_squared, void* d_scratch, int64_t scratch_len, void* stream);
+int fb_edt_validate_device(const uint8_t* d_mask, int nx, int ny, int nz, void* d_scratch, int64_t scratch_len,
+                           void* stream);
+
+/* ------------------------------------------------------------------------------------------ field build */
+
+/* Replace the Warp kernels behind klassificera_och_evaluera_testfalt, src/field_engine/faltkarna_v1.py:
+ * k_classify_testfalt :129-164, host compaction np.where :277, k_eval_tile_testfalt :167-190 -- for any
+ * compiled recipe.  mode 1: d_chain is the culled chain form; mode 0: a postfix program (float64).
+ * Outputs: kind[n_blocks] (-1/0/+1), corner_min_abs[n_blocks], ascending active ids, count[0],
+ * tiles[count][block^3] (C order li, lj, lk).  fb_field_leaf_device reuses the lists that
+ * fb_field_classify_device left in d_scratch for the same recipe and grid. */
+int64_t fb_field_scratch_bytes(const fb_geom* g, int32_t n_prims, int32_t n_chain);
+int fb_field_classify_device(const fb_geom* g, const fb_prim* d_prims, int32_t n_prims, const fb_insn* d_chain,
+                             int32_t n_chain, int32_t mode, int32_t* d_kind, float* d_cma, int32_t* d_active,
+                             int32_t* d_count, void* d_scratch, int64_t scratch_len, void* stream);
+int fb_field_leaf_device(const fb_geom* g, const fb_prim* d_prims, int32_t n_prims, const fb_insn* d_chain,
+                         int32_t n_chain, int32_t mode, const int32_t* d_kind, const int32_t* d_active,
+                         const int32_t* d_count, float* d_tiles, int64_t capacity, void* d_scratch,
+                         int64_t scratch_len, void* stream);
+int fb_field_leaf_work_device(const fb_geom* g, const fb_prim* d_prims, int32_t n_prims, const fb_insn* d_chain,
+                              int32_t n_chain, int32_t mode, const int32_t* d_kind, const int32_t* d_active,
+                              const int32_t* d_count, float* d_tiles, int64_t capacity, void* d_scratch,
+                              int64_t scratch_len, uint64_t* d_work, void* stream);
+int fb_field_build_device(const fb_geom* g, const fb_prim* d_prims, int32_t n_prims, const fb_insn* d_chain,
+                          int32_t n_chain, int32_t mode, int32_t* d_kind, float* d_cma, int32_t* d_active,
+                          int32_t* d_count, float* d_tiles, int64_t capacity, void* d_scratch,
+                          int64_t scratch_len, void* stream);
+/* Status 6 when the last compaction's bounded look-back wait gave up (synchronises). */
+int fb_field_compact_error(const fb_geom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, void* stream);
+
+/* Replace meshsdf_classify_cpu / meshsdf_tiles_cpu, src/field_engine/mesh_sdf_native_v1/field.cpp:229,254,
+ * and k_classify_dense / k_eval_tile_dense, src/field_engine/faltkarna_v1_mesh_to_sdf.py:602-657. */
+int64_t fb_dense_scratch_bytes(int64_t nx, int64_t ny, int64_t nz, int32_t block);
+int fb_dense_classify_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, int32_t block, float margin,
+                             int32_t* d_kind, float* d_cma, int32_t* d_active, int32_t* d_count, float* d_tiles,
+                             int64_t capacity, void* d_scratch, int64_t scratch_len, void* stream);
+
+/* Replaces rekonstruera_tat_gpu (k_fill_background + k_scatter_tiles), src/field_engine/faltkarna_v1.py:193-236,328-350;
+ * output cropped to (nx, ny, nz).  d_slot: caller scratch of n_blocks int32. */
+int fb_field_reconstruct_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active,
+                                const float* d_tiles, int64_t nx, int64_t ny, int64_t nz, int32_t block, float big,
+                                int32_t* d_slot, float* d_out, void* stream);
+
+/* Replaces k_reduce_checksum_i64_safe, src/field_engine/faltkarna_v1.py:250-255 (accumulates into d_out[0]). */
+int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64_t* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FIELD_B200_H */
