@@ -27,6 +27,8 @@ SIGNATURES = {
     "fb_edt_squared_device": (I, [P, I, I, I, I, P, P, I64, P]),
     "fb_edt_pair_device": (I, [P, I, I, I, D, P, P, P, I64, P]),
     "fb_edt_validate_device": (I, [P, I, I, I, P, I64, P]),
+    "fb_edt_squared_device_noalloc": (I, [P, I, I, I, I, P, P]),
+    "fb_edt_noalloc_capacity": (I64, [P]),
     # EDT, host pointers (reference names)
     "edt_squared_large": (I, [P, I, I, I, P]),
     "edt_squared": (I, [P, I, I, I, P]),

@@ -11,6 +11,7 @@ enum {
     FB_INVALID = 1,
     FB_RUNTIME = 2,
     FB_TIMEOUT = 6,   // a bounded device-side wait gave up; the context stays usable
+    FB_NOALLOC_LIMIT = 7,  // the grid exceeds the fixed scratch of an allocation-free entry point
 };
 
 #define FB_CUDA(call)                                    \

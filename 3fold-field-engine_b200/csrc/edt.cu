@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 #include <new>
 
 namespace {
@@ -353,6 +354,81 @@ struct Pair {
 };
 
 }  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free EDT for callers that cannot allocate device memory.
+//
+// Some hosts own every byte of device memory themselves (an engine embedding this library behind
+// its own pool allocator, a real-time loop that must never hit the implicit synchronisation of
+// cudaMalloc/cudaFree, a plugin whose host forbids allocation calls); they can pass input and
+// output buffers but not scratch.  For them the squared EDT below keeps its scratch (bit words
+// and the int32 intermediate) in a fixed array compiled into this library.
+//
+// Limit: at most kNoAllocVoxels = 2^20 voxels and 512 per axis -- the reference's own EDT
+// contract (src/field_engine/edt_native_large_v1/edt.cu:34-37).  Every GPU that loads this
+// library holds the array (kNoAllocScratchBytes, about 5.1 MiB) until the process exits.
+// ---------------------------------------------------------------------------------------------
+constexpr int64_t kNoAllocVoxels = int64_t(1) << 20;
+// bit words: nx*ny*ceil(nz/32) <= voxels/32 + nx*ny <= 2^15 + 512*512; plus 256 B of counters and
+// one int32 intermediate per voxel
+constexpr int64_t kNoAllocBitBytes = ((kNoAllocVoxels / 32 + 512 * 512) * 4 + 255) / 256 * 256;
+constexpr int64_t kNoAllocScratchBytes = 256 + kNoAllocBitBytes + kNoAllocVoxels * 4;
+static __device__ __align__(256) unsigned char g_edt_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_lock;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the array on the current device, looked up once per device.  The name
+// g_edt_noalloc_scratch in host code is a host-side stand-in, not a device address, so kernels
+// get this pointer instead.
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return FB_RUNTIME;
+    std::lock_guard<std::mutex> guard(g_noalloc_lock);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_edt_noalloc_scratch) != cudaSuccess || !p) return FB_RUNTIME;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return FB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Squared EDT exactly as fb_edt_squared_device, with no allocation and no caller scratch: the
+// scratch is the library's fixed device array.  Inputs and outputs are the caller's device
+// buffers.  Status 0 ok, 1 invalid arguments, 2 CUDA failure, 7 grid larger than the fixed
+// scratch (more than 2^20 voxels) -- rejected before anything is enqueued.
+// The first call on each device looks the array up (cudaGetSymbolAddress) with that device
+// current; make that first call before any stream capture.  The array is shared by every call
+// and keeps the last call's contents (nothing in it needs to start at zero: every word a call
+// reads it writes first), so calls whose work overlaps on the GPU -- on different streams, or
+// from different threads -- race on it and must be serialised by the caller.
+int fb_edt_squared_device_noalloc(const uint8_t* d_mask, int nx, int ny, int nz, int sites_nonzero,
+                                  int32_t* d_out, void* stream) noexcept {
+    if (!d_mask || !d_out || !shape_ok(nx, ny, nz)) return FB_INVALID;
+    if ((int64_t)nx * ny * nz > kNoAllocVoxels) return FB_NOALLOC_LIMIT;
+    const int64_t need = scratch_bytes(nx, ny, nz, 1);
+    if (need > kNoAllocScratchBytes) return FB_NOALLOC_LIMIT;
+    void* scratch = nullptr;
+    if (int rc = noalloc_scratch(&scratch)) return rc;
+    return enqueue(d_mask, nx, ny, nz, 0, sites_nonzero, 1.0, d_out, nullptr, scratch, kNoAllocScratchBytes,
+                   static_cast<cudaStream_t>(stream), false);
+}
+
+// Size in bytes of the fixed scratch array and the largest voxel count it serves.
+int64_t fb_edt_noalloc_capacity(int64_t* max_voxels) noexcept {
+    if (max_voxels) *max_voxels = kNoAllocVoxels;
+    return kNoAllocScratchBytes;
+}
+
+}  // extern "C"
 
 extern "C" {
 

@@ -5,7 +5,8 @@
  * src/field_engine/csg_batch_native_v1/execute.cpp):
  *   - every entry point is extern "C" and noexcept; integer status: 0 ok, 1 invalid input,
  *     2 runtime / CUDA failure, 3-5 the CSG codes of execute.cpp/gather.cpp, 6 a bounded device
- *     wait gave up (the context stays usable);
+ *     wait gave up (the context stays usable), 7 a grid beyond an allocation-free entry point's
+ *     fixed scratch;
  *   - arguments are validated before any output is written;
  *   - handles are created and destroyed explicitly; a handle that failed stays failed;
  *   - *_device entry points take device pointers and a cudaStream_t (as void*), enqueue their
@@ -91,6 +92,17 @@ int fb_edt_pair_device(const uint8_t* d_mask, int nx, int ny, int nz, double pit
                        int32_t* d_squared, void* d_scratch, int64_t scratch_len, void* stream);
 int fb_edt_validate_device(const uint8_t* d_mask, int nx, int ny, int nz, void* d_scratch, int64_t scratch_len,
                            void* stream);
+
+/* No counterpart in the reference.  For callers that cannot allocate device memory (hosts that own
+ * every device byte through their own allocator, loops that must never meet cudaMalloc's implicit
+ * synchronisation): fb_edt_squared_device without caller scratch -- the scratch is a fixed
+ * ~5.1 MiB device array inside this library, so grids are limited to 2^20 voxels and 512 per axis
+ * (status 7 beyond that).  The first call on a device resolves the array's address and should come
+ * before any stream capture; calls that overlap on the GPU share the array and race.
+ * fb_edt_noalloc_capacity returns the array's size and writes the voxel limit. */
+int fb_edt_squared_device_noalloc(const uint8_t* d_mask, int nx, int ny, int nz, int sites_nonzero,
+                                  int32_t* d_out, void* stream);
+int64_t fb_edt_noalloc_capacity(int64_t* max_voxels);
 
 /* ------------------------------------------------------------------------------------------ field build */
 
