@@ -170,17 +170,35 @@ def classify_fixtures():
 
 
 def csg_fixtures():
-    """Programs and outputs of probes/field_engine/field_csg_batch_probe.py:41-51."""
+    """Programs and outputs of probes/field_engine/field_csg_batch_probe.py:41-51, inputs restated in
+    csg_inputs.py and checked here against the capture through the oracle; plus the packed-field
+    query capture of probes/field_engine/field_native_pack_probe.py:26-40 (rng 445, 4097 points per
+    field, origin 0, pitch 1)."""
+    sys.path.insert(0, str(REPO))
+    sys.path.insert(0, str(HERE))
+    import oracle
+    import csg_inputs
     w = Writer()
     with np.load(REF / "reports/field_csg_batch_arrays.npz") as z:
         for curved in (False, True):
-            program = [("union", 0, 1), ("difference", 3, 2)] if curved else \
-                [("union", 0, 1), ("union", 5, 2), ("union", 3, 4), ("difference", 6, 7)]
             for pitch in (.5, .25):
                 name = f"csg/{curved}/{pitch}"
                 out = z[f"{curved}_{pitch}_0"]
+                fields, origin, shape, program = csg_inputs.case(curved, pitch)
+                assert oracle.csg_execute(fields, program).tobytes() == out.tobytes(), name
                 w.meta[name] = dict(curved=curved, pitch=pitch, program=program, shape=list(out.shape))
                 w.expect(name, "output", out)
+    rng = np.random.default_rng(445)
+    with np.load(REF / "reports/field_csg_curved_arrays.npz") as data:
+        cases = [(name, data[name]) for name in data.files if name.endswith("_0_field")]
+    with np.load(REF / "reports/field_native_pack_arrays.npz") as cap:
+        for name, raw in cases:
+            points = rng.uniform(-1, np.array(raw.shape) + 1, (4097, 3))
+            key = f"query/{name}"
+            w.meta[key] = dict(field_sha256=digest(raw), shape=list(raw.shape))
+            w.arrays[f"{key}__points"] = points
+            w.arrays[f"{key}__values"] = cap[f"{name}_0"]
+            assert cap[f"{name}_0"].tobytes() == cap[f"{name}_1"].tobytes()
     w.save("csg_golden")
     print("csg cases:", len(w.meta))
 

@@ -2,6 +2,8 @@
 
 These pins make the oracle trustworthy before it is used to check the CUDA library.
 """
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -67,3 +69,31 @@ def test_pack_matches_compiled_reference():
         nodes, payload = oracle.pack(g.z[key], meta["threshold"])
         assert sha(nodes) == meta["nodes_sha256"], name
         assert sha(payload) == meta["payload_sha256"], name
+
+
+def test_csg_restated_inputs_reproduce_reference_captures():
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import csg_inputs
+    g = Golden("csg_golden")
+    for name in g.names("csg/"):
+        m = g.meta[name]
+        fields, origin, shape, program = csg_inputs.case(m["curved"], m["pitch"])
+        assert g.matches(name, "output", oracle.csg_execute(fields, program)), name
+
+
+def test_query_restatement_matches_reference_capture():
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import csg_inputs
+    g = Golden("csg_golden")
+    fields = {}
+    for name in g.names("csg/"):
+        m = g.meta[name]
+        f, origin, shape, program = csg_inputs.case(m["curved"], m["pitch"])
+        fields[sha(oracle.csg_execute(f, program))] = oracle.csg_execute(f, program)
+    for name in g.names("query/"):
+        raw = fields[g.meta[name]["field_sha256"]]
+        nodes, payload = oracle.pack(raw, 512)
+        got = oracle.query_trilinear(nodes, payload, raw.shape, np.zeros(3), 1.0, g.z[f"{name}__points"])
+        assert got.tobytes() == g.z[f"{name}__values"].tobytes(), name
