@@ -492,27 +492,6 @@ __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __r
 }
 
 // ------------------------------------------------------------------------------------ localisation
-// Block-local float32 record of one primitive: L = A * origin + t in float64, rounded once.
-__device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double ox, double oy, double oz, int op,
-                                         float k, LocalPrim& out) {
-    out.type = F.type;
-    out.op = op;
-    out.ident = F.ident;
-    out.k = k;
-    out.s = F.s;
-    out.off = F.off;
-    const double* A = D.A;
-    out.L[0] = (float)fma(A[0], ox, fma(A[1], oy, fma(A[2], oz, A[3])));
-    out.L[1] = (float)fma(A[4], ox, fma(A[5], oy, fma(A[6], oz, A[7])));
-    out.L[2] = (float)fma(A[8], ox, fma(A[9], oy, fma(A[10], oz, A[11])));
-    out.L[3] = 0.f;
-    out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
-    out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
-    out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
-#pragma unroll
-    for (int j = 0; j < 12; ++j) out.p[j] = F.p[j];
-}
-
 // ------------------------------------------------------------------------------------ classify
 // float64 value of a block list at a world point (guard-band recheck).
 __device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, int n, const FbInsn* __restrict__ chain,
@@ -1380,6 +1359,33 @@ int fb_field_reconstruct_device(const int32_t* d_kind, const int32_t* d_active, 
     k_reconstruct<<<fb_div_up(nx * ny * nz, 256), 256, 0, st>>>(d_kind, d_slot, d_tiles, nx, ny, nz, block, nby, nbz,
                                                                 big, d_out);
     FB_LAUNCH();
+    return FB_OK;
+}
+
+// float32 primitive mirror (128-byte records) for the point-query kernels.
+int fb_query_prepare(const FbPrim* d_prims, int32_t n_prims, void* d_primf, void* stream) noexcept {
+    if (!d_prims || !d_primf || n_prims < 1) return FB_INVALID;
+    k_prepare_prims<<<fb_div_up(n_prims, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        d_prims, n_prims, static_cast<PrimF*>(d_primf));
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+// Device addresses of a classification's superblock lists inside its scratch (for accelerated
+// point queries): pool base, per-superblock offsets and lengths.
+int fb_field_accel(const FbGeom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, const void** pool,
+                   const int64_t** sb_off, const int32_t** sb_len, const int32_t** blk_off, const int32_t** blk_len,
+                   const uint32_t** blk_pool) noexcept {
+    if (!g || !geom_ok(*g) || !d_scratch || n_prims < 1 || n_chain < 1) return FB_INVALID;
+    const Geo G = make_geo(*g);
+    const Plan P = make_plan(G, n_prims, n_chain);
+    const char* b = static_cast<const char*>(d_scratch);
+    if (pool) *pool = b + P.pool;
+    if (sb_off) *sb_off = reinterpret_cast<const int64_t*>(b + P.off) + G.ncoarse;
+    if (sb_len) *sb_len = reinterpret_cast<const int32_t*>(b + P.len) + G.ncoarse;
+    if (blk_off) *blk_off = reinterpret_cast<const int32_t*>(b + P.blk_off);
+    if (blk_len) *blk_len = reinterpret_cast<const int32_t*>(b + P.blk_len);
+    if (blk_pool) *blk_pool = reinterpret_cast<const uint32_t*>(b + P.blk_pool);
     return FB_OK;
 }
 

@@ -150,6 +150,27 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
     }
 }
 
+// Block-local float32 record of one primitive: L = A * origin + t in float64, rounded once.
+__device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double ox, double oy, double oz, int op,
+                                         float k, LocalPrim& out) {
+    out.type = F.type;
+    out.op = op;
+    out.ident = F.ident;
+    out.k = k;
+    out.s = F.s;
+    out.off = F.off;
+    const double* A = D.A;
+    out.L[0] = (float)fma(A[0], ox, fma(A[1], oy, fma(A[2], oz, A[3])));
+    out.L[1] = (float)fma(A[4], ox, fma(A[5], oy, fma(A[6], oz, A[7])));
+    out.L[2] = (float)fma(A[8], ox, fma(A[9], oy, fma(A[10], oz, A[11])));
+    out.L[3] = 0.f;
+    out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
+    out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
+    out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
+#pragma unroll
+    for (int j = 0; j < 12; ++j) out.p[j] = F.p[j];
+}
+
 // ------------------------------------------------------------------------------------ float64
 // Every operation rounds once, in the written order (no contraction), so the values equal the
 // CPU float64 evaluation of the same program bit for bit.

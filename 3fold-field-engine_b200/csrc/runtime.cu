@@ -63,3 +63,16 @@ int64_t fb_fp32_peak_launch(float* d_out, int blocks, int iters, void* stream) {
 int fb_sm_count_c() { return fb_sm_count(); }
 
 }  // extern "C"
+
+extern "C" {
+
+// Stream-ordered device-to-device copy between raw device addresses (e.g. out of a build's
+// scratch); synchronises the stream.
+int fb_copy_device(void* dst, const void* src, int64_t bytes, void* stream) {
+    if (!dst || !src || bytes < 0) return 1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 2;
+    return cudaStreamSynchronize(st) == cudaSuccess ? 0 : 2;
+}
+
+}  // extern "C"

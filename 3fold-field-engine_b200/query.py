@@ -1,0 +1,109 @@
+"""SDF value and gradient point queries of recipes on the GPU.
+
+Drop-in surfaces:
+
+* ``eval_batch(node, points_mm, device=...)`` -> float32 (N,) -- src/field_engine/ikarus_v1/eval_warp.py:478-488.
+* ``gradient_batch(node, points_mm, h=0.05, device=...)`` -> float32 (N, 3) central differences --
+  eval_warp.py:718-733.
+
+``RecipeQueries`` keeps a compiled recipe resident and, when given a FieldBuilder of the same
+recipe, answers points inside that grid from their superblock's culled list (exact) instead of
+the whole chain; it serves value and value+gradient queries of device tensors without host
+round trips.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _lib
+from .expr import Compiled, compile_recipe
+
+PRIMF_BYTES = 128
+
+
+class RecipeQueries:
+    """A compiled recipe resident on one device, with optional acceleration by a built field."""
+
+    def __init__(self, recipe, *, device="cuda", builder=None):
+        import torch
+        self.lib = _lib.lib()
+        self.device = torch.device(device)
+        self.compiled: Compiled = recipe if isinstance(recipe, Compiled) else compile_recipe(recipe)
+        c = self.compiled
+        self.mode = 1 if c.chain is not None else 0
+        insns = c.chain if self.mode == 1 else c.program
+        self.n_chain = len(insns)
+        self.prims = torch.from_numpy(np.ascontiguousarray(c.prims).view(np.uint8).copy()).to(self.device)
+        self.chain = torch.from_numpy(np.ascontiguousarray(insns).view(np.uint8).copy()).to(self.device)
+        self.primf = torch.empty(len(c.prims) * PRIMF_BYTES, dtype=torch.uint8, device=self.device)
+        _lib.check(self.lib.fb_query_prepare(self.prims.data_ptr(), len(c.prims), self.primf.data_ptr(),
+                                             _lib.stream_handle()), "query prepare")
+        self._accel = None
+        if builder is not None and self.mode == 1:
+            self.attach(builder)
+
+    def attach(self, builder):
+        """Use `builder`'s superblock lists (the builder must have classified this same recipe)."""
+        pool, off, ln = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        st = self.lib.fb_field_accel(ct.addressof(builder.geom), builder.n_prims, builder.n_chain,
+                                     builder.scratch.data_ptr(), ct.byref(pool), ct.byref(off), ct.byref(ln),
+                                     None, None, None)
+        _lib.check(st, "field accel")
+        m = builder.meta
+        self._accel = (pool.value, off.value, ln.value, np.array([m.x0, m.y0, m.z0, m.pitch], np.float64),
+                       np.array([m.nx, m.ny, m.nz, m.block], np.int32), builder)
+
+    def _run(self, pts, value, grad, h=0.05, stream=None):
+        a = self._accel
+        args = (a[0], a[1], a[2], a[3].ctypes.data, a[4].ctypes.data) if a else (None, None, None, None, None)
+        st = self.lib.fb_query_points_device(self.primf.data_ptr(), self.chain.data_ptr(), self.n_chain, self.mode,
+                                             *args, pts.data_ptr(), pts.shape[0], float(h),
+                                             value.data_ptr() if value is not None else None,
+                                             grad.data_ptr() if grad is not None else None,
+                                             _lib.stream_handle(stream))
+        _lib.check(st, "point query")
+
+    def values(self, points, *, stream=None):
+        """float32 (N,) values at a float32 (N, 3) CUDA tensor of points."""
+        import torch
+        pts = points.to(self.device, torch.float32).contiguous()
+        out = torch.empty(pts.shape[0], dtype=torch.float32, device=self.device)
+        self._run(pts, out, None, stream=stream)
+        return out
+
+    def values_and_gradients(self, points, h=0.05, *, stream=None):
+        """(float32 (N,), float32 (N, 3)) values and central-difference gradients."""
+        import torch
+        pts = points.to(self.device, torch.float32).contiguous()
+        val = torch.empty(pts.shape[0], dtype=torch.float32, device=self.device)
+        grad = torch.empty((pts.shape[0], 3), dtype=torch.float32, device=self.device)
+        self._run(pts, val, grad, h=h, stream=stream)
+        return val, grad
+
+
+def _points(points_mm):
+    pts = np.asarray(points_mm)
+    if pts.ndim != 2 or pts.shape[1] != 3:
+        raise ValueError("points must be an (N, 3) array")
+    return pts
+
+
+def eval_batch(node, points_mm, device="cuda"):
+    """(N,) float32 SDF values of `node` at (N, 3) points (eval_warp.py:478-488)."""
+    import torch
+    pts = _points(points_mm)
+    q = RecipeQueries(node, device=device)
+    return q.values(torch.from_numpy(pts.astype(np.float32))).cpu().numpy()
+
+
+def gradient_batch(node, points_mm, h=0.05, device="cuda"):
+    """(N, 3) float32 central-difference gradients with step h (eval_warp.py:718-733)."""
+    import torch
+    pts = _points(points_mm)
+    q = RecipeQueries(node, device=device)
+    pts_t = torch.from_numpy(np.asarray(pts, dtype=np.float32)).to(q.device)
+    grad = torch.empty((len(pts), 3), dtype=torch.float32, device=q.device)
+    q._run(pts_t, None, grad, h=h)
+    return grad.cpu().numpy()

@@ -63,6 +63,8 @@ int fb_device_arch(void);     /* no reference counterpart: compute capability x1
 int fb_sm_count_c(void);      /* no reference counterpart: SM count of the current device */
 /* No reference counterpart: float32 FMA throughput probe (roofline denominator); returns its flops. */
 int64_t fb_fp32_peak_launch(float* d_out, int blocks, int iters, void* stream);
+/* No reference counterpart: stream-ordered device-to-device copy between raw addresses (synchronises). */
+int fb_copy_device(void* dst, const void* src, int64_t bytes, void* stream);
 
 /* ------------------------------------------------------------------------------------------ EDT */
 
@@ -146,6 +148,59 @@ int fb_field_reconstruct_device(const int32_t* d_kind, const int32_t* d_active, 
 
 /* Replaces k_reduce_checksum_i64_safe, src/field_engine/faltkarna_v1.py:250-255 (accumulates into d_out[0]). */
 int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64_t* d_out, void* stream);
+
+/* ------------------------------------------------------------------------------------------ packed fields */
+
+/* Replace adaptive_pack / adaptive_nodes / adaptive_samples / adaptive_copy / adaptive_free,
+ * src/field_engine/adaptive_pack_native_v1/pack.cpp:57-79: host float32 samples, int32 shape[3],
+ * threshold 8..4096; NULL on invalid input; 52-byte nodes and float32 payload with the reference's
+ * split decisions and order.  fb_pack_device takes device samples (synchronises the stream);
+ * fb_pack_payload_device returns the handle's device payload. */
+void* adaptive_pack(const void* data, const int32_t* shape, int threshold);
+void* fb_pack_device(const float* d_data, const int32_t* shape, int threshold, void* stream);
+int64_t adaptive_nodes(const void* handle);
+int64_t adaptive_samples(const void* handle);
+int adaptive_copy(const void* handle, void* nodes, int64_t count, void* payload, int64_t samples);
+void adaptive_free(void* handle);
+const float* fb_pack_payload_device(const void* handle);
+
+/* Replaces csg_execute, src/field_engine/csg_batch_native_v1/execute.cpp:10-53 (24-byte instructions
+ * {op, left, right, pad, offset}; statuses 1-5; the output is written only on success). */
+int csg_execute(const void* const* nodes, const int64_t* counts, const void* const* payload, const int64_t* lengths,
+                int32_t fields, const int32_t* shape, const void* program, int32_t instructions, float* output);
+
+/* Replace AdaptiveSampleBlocks.samples_at / query, src/field_engine/adaptive_sample_blocks_v1.py:182-230. */
+int fb_packed_samples_at(const void* nodes, int64_t count, const float* payload, int64_t samples,
+                         const int64_t* indices, int64_t n, float* out);
+int fb_packed_query_device(const void* d_nodes, const float* d_payload, const int32_t* shape, const double* origin,
+                           double pitch, const double* d_points, int64_t n, float* d_out, void* stream);
+
+/* ------------------------------------------------------------------------------------------ point queries */
+
+/* Replace eval_batch / gradient_batch, src/field_engine/ikarus_v1/eval_warp.py:478-488,718-733.
+ * fb_query_prepare fills the 128-byte float32 primitive mirror; fb_field_accel exposes a
+ * classification's culling lists inside its scratch (superblock and per-block) so that points
+ * inside that grid walk only their superblock's list. */
+int fb_query_prepare(const fb_prim* d_prims, int32_t n_prims, void* d_primf, void* stream);
+int fb_field_accel(const fb_geom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, const void** pool,
+                   const int64_t** sb_off, const int32_t** sb_len, const int32_t** blk_off, const int32_t** blk_len,
+                   const uint32_t** blk_pool);
+int fb_query_points_device(const void* d_primf, const fb_insn* d_chain, int32_t n_chain, int32_t mode,
+                           const void* accel_pool, const int64_t* accel_off, const int32_t* accel_len,
+                           const double* accel_grid, const int32_t* accel_dims, const float* d_points, int64_t n,
+                           double h, float* d_value, float* d_grad, void* stream);
+
+/* Replace the per-block-pitch field's lattices and its avstand / gradient queries,
+ * src/field_engine/faltkarna_v1_multires.py:84-104,384-459 (lattices built from a recipe). */
+int fb_multires_tiles_device(const void* d_primf, const fb_insn* d_chain, int32_t n_chain, int32_t mode,
+                             const fb_prim* d_prims, const double* lo, double h, int32_t B, const int32_t* bshape,
+                             const int32_t* d_bricks, const int8_t* d_levels, const int64_t* d_offsets,
+                             int64_t nbricks, const int32_t* d_blk_off, const int32_t* d_blk_len,
+                             const uint32_t* d_blk_pool, float guard, float* d_pool, void* stream);
+int fb_multires_query_device(const double* lo, double h, int32_t B, const int32_t* bshape, double margin,
+                             const int8_t* d_kind, const int8_t* d_level, const int64_t* d_tile_off,
+                             const float* d_pool, const double* d_points, int64_t n, double* d_value, double* d_grad,
+                             void* stream);
 
 #ifdef __cplusplus
 }

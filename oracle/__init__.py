@@ -352,3 +352,68 @@ def ref_pack(samples, threshold=512):
     finally:
         L.adaptive_free(h)
     return nodes, payload
+
+
+# ----------------------------------------------------------------------------------------- multires
+def multires_brick(lo, L, brick_shape, kind, pts):
+    """Brick per point, preferring the active brick on a face (faltkarna_v1_multires.py:384-402)."""
+    rel = (np.asarray(pts, dtype=np.float64) - lo) / L
+    b = np.floor(rel).astype(np.int64)
+    shp = np.array(brick_shape, dtype=np.int64)
+    outside = np.any((b < 0) | (b >= shp), axis=1)
+    b = np.clip(b, 0, shp - 1)
+    inactive = kind[b[:, 0], b[:, 1], b[:, 2]] != 0
+    for ax in range(3):
+        on_plane = (rel[:, ax] == np.floor(rel[:, ax])) & (b[:, ax] > 0) & inactive & ~outside
+        if not on_plane.any():
+            continue
+        cand = b[on_plane].copy()
+        cand[:, ax] -= 1
+        ok = kind[cand[:, 0], cand[:, 1], cand[:, 2]] == 0
+        idx = np.where(on_plane)[0][ok]
+        b[idx, ax] -= 1
+        inactive = kind[b[:, 0], b[:, 1], b[:, 2]] != 0
+    return b, outside
+
+
+def multires_avstand(lo, h, block, brick_shape, kind, niva, tiles, margin, pts):
+    """faltkarna_v1_multires.py:405-434 restated: trilinear at the brick's own pitch, +-margin
+    elsewhere; float64 (N,)."""
+    from scipy import ndimage
+    pts = np.atleast_2d(np.asarray(pts, dtype=np.float64))
+    L = block * h
+    b, outside = multires_brick(lo, L, brick_shape, kind, pts)
+    n_by, n_bz = brick_shape[1], brick_shape[2]
+    lin = (b[:, 0] * n_by + b[:, 1]) * n_bz + b[:, 2]
+    kd = kind[b[:, 0], b[:, 1], b[:, 2]]
+    out = np.where(kd < 0, -margin, margin).astype(np.float64)
+    out[outside] = margin
+    act = (kd == 0) & ~outside
+    for i in np.where(act)[0]:
+        u = int(lin[i])
+        bi, bj, bk = u // (n_by * n_bz), (u // n_bz) % n_by, u % n_bz
+        lvl = int(niva[bi, bj, bk])
+        o = lo + np.array([bi, bj, bk], dtype=np.float64) * L
+        lok = (pts[i:i + 1] - o) / (h / float(1 << lvl))
+        out[i] = ndimage.map_coordinates(tiles[u], lok.T, order=1, mode="nearest")[0]
+    return out
+
+
+def multires_gradient(lo, h, block, brick_shape, kind, niva, tiles, margin, pts):
+    """faltkarna_v1_multires.py:437-459 restated; float64 (N, 3)."""
+    pts = np.atleast_2d(np.asarray(pts, dtype=np.float64))
+    L = block * h
+    b, _ = multires_brick(lo, L, brick_shape, kind, pts)
+    lvl = niva[b[:, 0], b[:, 1], b[:, 2]].astype(np.int64)
+    hh = h / np.power(2.0, np.maximum(lvl, 0))
+    o = lo + b.astype(np.float64) * L
+    g = np.zeros((len(pts), 3))
+    for ax in range(3):
+        d = np.zeros((len(pts), 3))
+        d[:, ax] = hh
+        pa = np.minimum(pts + 0.5 * d, o + L)
+        pb = np.maximum(pts - 0.5 * d, o)
+        step = pa[:, ax] - pb[:, ax]
+        g[:, ax] = (multires_avstand(lo, h, block, brick_shape, kind, niva, tiles, margin, pa) -
+                    multires_avstand(lo, h, block, brick_shape, kind, niva, tiles, margin, pb)) / np.maximum(step, 1e-12)
+    return g
