@@ -1114,6 +1114,32 @@ __global__ void k_reconstruct(const int32_t* __restrict__ kind, const int32_t* _
     out[i] = v;
 }
 
+// Slot map of the first count[0] active blocks (device-side count: no host round trip).
+__global__ void k_slot_map_dev(const int32_t* __restrict__ active, const int32_t* __restrict__ count,
+                               int64_t capacity, int32_t* __restrict__ slot) {
+    const int64_t n = min((int64_t)count[0], capacity);
+    for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < n; a += (int64_t)gridDim.x * blockDim.x)
+        slot[active[a]] = (int32_t)a;
+}
+
+// Occupancy (1 where the field is negative) of every voxel: tile values in active blocks, the
+// block kind elsewhere.  Writes 16 voxels per thread along z with one 128-bit store when the row
+// allows it.
+__global__ void k_occupancy(const int32_t* __restrict__ kind, const int32_t* __restrict__ slot,
+                            const float* __restrict__ tiles, int64_t nx, int64_t ny, int64_t nz, int B, int nby,
+                            int nbz, uint8_t* __restrict__ mask) {
+    const int64_t n = nx * ny * nz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t z = i % nz, y = (i / nz) % ny, x = i / (nz * ny);
+        const int64_t blk = ((x / B) * nby + y / B) * nbz + z / B;
+        const int32_t s = slot[blk];
+        uint8_t v;
+        if (s >= 0) v = tiles[(int64_t)s * B * B * B + ((x % B) * B + (y % B)) * B + (z % B)] < 0.f;
+        else v = kind[blk] < 0;
+        mask[i] = v;
+    }
+}
+
 // Sum of trunc(v * scale) over negative values, in int64 (determinism-safe checksum,
 // src/field_engine/faltkarna_v1.py:250-255).
 __global__ void k_checksum_i64(const float* __restrict__ v, int64_t n, double scale, unsigned long long* out) {
@@ -1386,6 +1412,27 @@ int fb_field_accel(const FbGeom* g, int32_t n_prims, int32_t n_chain, const void
     if (blk_off) *blk_off = reinterpret_cast<const int32_t*>(b + P.blk_off);
     if (blk_len) *blk_len = reinterpret_cast<const int32_t*>(b + P.blk_len);
     if (blk_pool) *blk_pool = reinterpret_cast<const uint32_t*>(b + P.blk_pool);
+    return FB_OK;
+}
+
+// Occupancy mask (uint8, 1 = solid) of a built field, from device-resident kind / active / count /
+// tiles; stream-ordered, no host synchronisation.  d_slot: caller scratch of n_blocks int32.
+int fb_field_occupancy_device(const int32_t* d_kind, const int32_t* d_active, const int32_t* d_count,
+                              const float* d_tiles, int64_t capacity, int64_t nx, int64_t ny, int64_t nz,
+                              int32_t block, int32_t* d_slot, uint8_t* d_mask, void* stream) noexcept {
+    if (!d_kind || !d_active || !d_count || !d_tiles || !d_slot || !d_mask || nx < 1 || ny < 1 || nz < 1 ||
+        block < 1 || capacity < 0)
+        return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nby = (int)((ny + block - 1) / block), nbz = (int)((nz + block - 1) / block);
+    const int64_t nblocks = ((nx + block - 1) / block) * nby * nbz;
+    FB_CUDA(cudaMemsetAsync(d_slot, 0xff, nblocks * 4, st));
+    k_slot_map_dev<<<fb_sm_count() * 4, 256, 0, st>>>(d_active, d_count, capacity, d_slot);
+    FB_LAUNCH();
+    const int64_t n = nx * ny * nz;
+    k_occupancy<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)fb_sm_count() * 32), 256, 0, st>>>(
+        d_kind, d_slot, d_tiles, nx, ny, nz, block, nby, nbz, d_mask);
+    FB_LAUNCH();
     return FB_OK;
 }
 

@@ -1,0 +1,328 @@
+"""Serving: a continuous-batching request loop over device-resident fields.
+
+Requests (``submit`` returns a Future):
+  * ``build``  (recipe, GridMeta)               -> new resident field id + stats
+  * ``edit``   (field id, tools, op)             -> the field rebuilt with tool primitives unioned
+                                                   or subtracted (milling / drilling edits)
+  * ``query``  (field id, points (N, 3))         -> float32 values and central-difference gradients
+  * ``edt``    (field id)                        -> squared EDT of the field's occupancy (device)
+
+The scheduler thread admits queued requests while a stream slot is free and the HBM budget
+allows their estimated footprint, runs each request as a generator that enqueues asynchronous
+GPU work on its slot's stream and yields a CUDA event, resumes it when the event has completed,
+and admits the next arrival as soon as a slot frees -- so requests that arrive while others are on
+the GPU overlap with them on the device.  Resident fields are evicted least-recently-used when an
+admission would exceed the budget.  The reference's service is one synchronous request at a time
+over a pipe (src/field_engine/mesh_field_service_v1.py:44-113); its timeout/close behaviour is kept:
+a failed or timed-out request fails its future, the server stays usable.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+
+from . import _lib
+from . import expr as X
+from .build import FieldBuilder
+from .query import RecipeQueries
+
+
+class _Field:
+    def __init__(self, fid, recipe, comp, meta, fb, tiles, n_active):
+        self.id = fid
+        self.recipe = recipe
+        self.comp = comp
+        self.meta = meta
+        self.fb = fb
+        self.tiles = tiles
+        self.n_active = n_active
+        self.queries = None
+        self.edt = None
+        self.busy = 0
+        self.last_use = time.perf_counter()
+
+    @property
+    def nbytes(self):
+        t = [self.fb.scratch, self.fb.kind, self.fb.cma, self.fb.active, self.tiles, self.fb.prims, self.fb.chain]
+        if self.edt is not None:
+            t.append(self.edt)
+        return int(sum(x.numel() * x.element_size() for x in t))
+
+
+class _Request:
+    def __init__(self, kind, args):
+        self.kind = kind
+        self.args = args
+        self.future = Future()
+        self.arrival = time.perf_counter()
+        self.start = None
+        self.end = None
+        self.gen = None
+        self.event = None
+        self.slot = None
+        self.estimate = 0
+
+
+class FieldServer:
+    def __init__(self, *, device="cuda", slots=8, budget_bytes=150e9, request_timeout_s=30.0):
+        import torch
+        dev = torch.device(device)
+        # an explicit index: the scheduler thread selects this device with torch.cuda.set_device
+        self.device = dev if dev.index is not None else torch.device("cuda", torch.cuda.current_device())
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
+        self.free = collections.deque(range(slots))
+        self.budget = float(budget_bytes)
+        self.timeout = float(request_timeout_s)
+        self.fields = {}
+        self.next_id = 0
+        self.reserved = 0
+        self.pending = collections.deque()
+        self.inflight = []
+        self.lock = threading.Lock()
+        self.wake = threading.Event()
+        self.running = True
+        self.completed = []
+        self.thread = threading.Thread(target=self._loop, name="field-server", daemon=True)
+        self.thread.start()
+
+    # ------------------------------------------------------------------------------------ client API
+    def submit(self, kind, **args) -> Future:
+        if kind not in ("build", "edit", "query", "edt"):
+            raise ValueError(f"unknown request kind {kind!r}")
+        r = _Request(kind, args)
+        with self.lock:
+            if not self.running:
+                raise RuntimeError("server closed")
+            self.pending.append(r)
+        self.wake.set()
+        return r.future
+
+    def close(self):
+        with self.lock:
+            self.running = False
+        self.wake.set()
+        self.thread.join(timeout=60)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def resident_bytes(self):
+        return sum(f.nbytes for f in self.fields.values())
+
+    # ------------------------------------------------------------------------------------ scheduler
+    def _estimate(self, r):
+        if r.kind in ("build", "edit"):
+            meta = r.args["meta"] if r.kind == "build" else self.fields[r.args["field"]].meta
+            # culling lists + block arrays + a quarter of the blocks active (tiles), grown on demand
+            return int(meta.n_blocks * (meta.block ** 3) + meta.n_blocks * 64 + 64e6)
+        if r.kind == "query":
+            return int(len(r.args["points"]) * 32)
+        meta = self.fields[r.args["field"]].meta
+        return int(meta.nx * meta.ny * meta.nz * 14)
+
+    def _evict_for(self, need):
+        """Drop least-recently-used idle fields until `need` more bytes fit in the budget."""
+        resident = self.resident_bytes()
+        if resident + self.reserved + need <= self.budget:
+            return True
+        for f in sorted(self.fields.values(), key=lambda f: f.last_use):
+            if f.busy:
+                continue
+            del self.fields[f.id]
+            resident -= f.nbytes
+            if resident + self.reserved + need <= self.budget:
+                return True
+        return resident + self.reserved + need <= self.budget
+
+    def _admit(self):
+        """Start queued requests while a slot is free and the budget allows; returns those that
+        are now waiting on a device event."""
+        started = []
+        while self.free:
+            with self.lock:
+                if not self.pending:
+                    break
+                r = self.pending[0]
+            if r.kind != "build" and r.args.get("field") not in self.fields:
+                with self.lock:
+                    self.pending.popleft()
+                r.end = time.perf_counter()
+                r.future.set_exception(KeyError(f"field {r.args.get('field')} is not resident"))
+                continue
+            r.estimate = self._estimate(r)
+            if not self._evict_for(r.estimate):
+                break  # wait for memory: in-flight requests release their reservations
+            with self.lock:
+                self.pending.popleft()
+            r.slot = self.free.popleft()
+            self.reserved += r.estimate
+            r.start = time.perf_counter()
+            if r.kind != "build":
+                self.fields[r.args["field"]].busy += 1
+            r.gen = getattr(self, f"_run_{r.kind}")(r, self.streams[r.slot])
+            if self._step(r):
+                started.append(r)
+        return started
+
+    def _finish(self, r, result=None, error=None):
+        r.end = time.perf_counter()
+        self.free.append(r.slot)
+        self.reserved -= r.estimate
+        if r.kind != "build" and r.args.get("field") in self.fields:
+            f = self.fields[r.args["field"]]
+            f.busy -= 1
+            f.last_use = r.end
+        self.completed.append((r.kind, r.arrival, r.start, r.end))
+        if error is not None:
+            r.future.set_exception(error)
+        else:
+            r.future.set_result(result)
+
+    def _step(self, r):
+        """Run the request up to its next device event; False when it has finished."""
+        try:
+            r.event = next(r.gen)
+        except StopIteration as stop:
+            self._finish(r, result=stop.value)
+            return False
+        except Exception as e:  # a failed request fails its future; the server stays usable
+            self._finish(r, error=e)
+            return False
+        return True
+
+    def _loop(self):
+        try:
+            self._loop_body()
+        except BaseException as e:  # the scheduler itself failed: fail every request, refuse new ones
+            with self.lock:
+                self.running = False
+                waiting = list(self.pending) + list(self.inflight)
+                self.pending.clear()
+            self.inflight = []
+            for r in waiting:
+                if not r.future.done():
+                    r.future.set_exception(RuntimeError(f"field server stopped: {e!r}"))
+
+    def _loop_body(self):
+        import torch
+        torch.cuda.set_device(self.device)
+        while True:
+            with self.lock:
+                running = self.running
+                idle = not self.pending and not self.inflight
+            if not running and idle:
+                return
+            started = self._admit()
+            progressed = bool(started)
+            still = []
+            for r in self.inflight:
+                if not r.event.query():
+                    if time.perf_counter() - r.start > self.timeout:
+                        self._finish(r, error=TimeoutError("request exceeded the server timeout"))
+                        progressed = True
+                    else:
+                        still.append(r)
+                    continue
+                progressed = True
+                if self._step(r):
+                    still.append(r)
+            self.inflight = still + started
+            if not progressed:
+                self.wake.wait(timeout=0.0002)
+                self.wake.clear()
+
+    # ------------------------------------------------------------------------------------ request bodies
+    def _record(self, stream):
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        return ev
+
+    def _build_field(self, recipe, meta, stream):
+        import torch
+        with torch.cuda.stream(stream):
+            comp = recipe if isinstance(recipe, X.Compiled) else X.compile_recipe(recipe)
+            fb = FieldBuilder(comp, meta, device=self.device)
+            fb.classify(stream)
+            count = torch.empty(1, dtype=torch.int32, pin_memory=True)
+            count.copy_(fb.count, non_blocking=True)
+        yield self._record(stream)
+        n = int(count[0])
+        with torch.cuda.stream(stream):
+            tiles = torch.empty((max(n, 1), meta.block ** 3), dtype=torch.float32, device=self.device)
+            if n:
+                fb.leaf(tiles, n, stream=stream)
+        yield self._record(stream)
+        return comp, fb, tiles, n
+
+    def _run_build(self, r, stream):
+        recipe, meta = r.args["recipe"], r.args["meta"]
+        comp, fb, tiles, n = yield from self._build_field(recipe, meta, stream)
+        fid = self.next_id
+        self.next_id += 1
+        self.fields[fid] = _Field(fid, recipe, comp, meta, fb, tiles, n)
+        return dict(field=fid, n_active=n, leaf_voxels=n * meta.block ** 3)
+
+    def _run_edit(self, r, stream):
+        f = self.fields[r.args["field"]]
+        op = r.args.get("op", "subtract")
+        if op not in ("union", "subtract"):
+            raise ValueError("edit op must be union or subtract")
+        recipe = f.recipe
+        for tool in r.args["tools"]:
+            recipe = X.union(recipe, tool) if op == "union" else X.subtract(recipe, tool)
+        comp, fb, tiles, n = yield from self._build_field(recipe, f.meta, stream)
+        f.recipe, f.comp, f.fb, f.tiles, f.n_active = recipe, comp, fb, tiles, n
+        f.queries = None
+        f.edt = None
+        return dict(field=f.id, n_active=n, leaf_voxels=n * f.meta.block ** 3)
+
+    def _run_query(self, r, stream):
+        import torch
+        f = self.fields[r.args["field"]]
+        pts = r.args["points"]
+        h = float(r.args.get("h", f.meta.pitch))
+        with torch.cuda.stream(stream):
+            if f.queries is None:
+                f.queries = RecipeQueries(f.comp, device=self.device, builder=f.fb)
+            p = pts if isinstance(pts, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(pts, np.float32))
+            p = p.to(self.device, torch.float32, non_blocking=True)
+            val, grad = f.queries.values_and_gradients(p, h=h, stream=stream)
+            out_v = torch.empty(val.shape, dtype=val.dtype, pin_memory=True)
+            out_g = torch.empty(grad.shape, dtype=grad.dtype, pin_memory=True)
+            out_v.copy_(val, non_blocking=True)
+            out_g.copy_(grad, non_blocking=True)
+        yield self._record(stream)
+        return out_v.numpy(), out_g.numpy()
+
+    def _run_edt(self, r, stream):
+        import torch
+        f = self.fields[r.args["field"]]
+        m = f.meta
+        lib = _lib.lib()
+        with torch.cuda.stream(stream):
+            slot = torch.empty(m.n_blocks, dtype=torch.int32, device=self.device)
+            mask = torch.empty((m.nx, m.ny, m.nz), dtype=torch.uint8, device=self.device)
+            out = torch.empty((m.nx, m.ny, m.nz), dtype=torch.int32, device=self.device)
+            scratch = torch.empty(int(lib.fb_edt_scratch_bytes(m.nx, m.ny, m.nz, 0)), dtype=torch.uint8,
+                                  device=self.device)
+            _lib.check(lib.fb_field_occupancy_device(f.fb.kind.data_ptr(), f.fb.active.data_ptr(), f.fb.count.data_ptr(),
+                                                     f.tiles.data_ptr(), max(f.n_active, 1), m.nx, m.ny, m.nz, m.block,
+                                                     slot.data_ptr(), mask.data_ptr(), _lib.stream_handle(stream)),
+                       "occupancy")
+            _lib.check(lib.fb_edt_squared_device(mask.data_ptr(), m.nx, m.ny, m.nz, 1, out.data_ptr(),
+                                                 scratch.data_ptr(), scratch.numel(), _lib.stream_handle(stream)),
+                       "edt")
+            total = out.sum(dtype=torch.int64)
+            host = torch.empty((), dtype=torch.int64, pin_memory=True)
+            host.copy_(total, non_blocking=True)
+        yield self._record(stream)
+        f.edt = out
+        return dict(field=f.id, checksum=int(host.item()), voxels=int(out.numel()))

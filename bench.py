@@ -50,6 +50,12 @@ def parse():
     ap.add_argument("--edt-n", type=int, default=512, help="grid edge of the EDT")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=("plain", "batched", "serve"), default="plain",
+                    help="plain: the plain method at scale (default line); batched: 256 recipes, plain vs "
+                         "graph-batched; serve: the request loop")
+    ap.add_argument("--recipes", type=int, default=256)
+    ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
+    ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrival window")
     return ap.parse_args()
 
 
@@ -366,8 +372,143 @@ def run_reference(args, rank, world):
     }
 
 
+def run_batched(args):
+    """256 independent recipes (primitive counts log-uniform in [8, 2048], grids from
+    {64, 128, 256, 512}^3, leaf size by the autotuner), each followed by the squared EDT of its
+    occupancy: the recipe-by-recipe path against one CUDA-graph replay of the whole batch."""
+    import torch
+    import field_b200.batch as BT
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    raw = R.batch_recipes(count=args.recipes, seed=3)
+    comps = [(X.compile_recipe(r), n) for r, n, _ in raw]
+    t_compile = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tuner = BT.Autotuner()
+    blocks = tuner.tune(comps)
+    t_tune = time.perf_counter() - t0
+    recipes = [(c, BT.cube_meta(n, b)) for (c, n), b in zip(comps, blocks)]
+    t0 = time.perf_counter()
+    bb = BT.BatchBuilder(recipes, streams=8)
+    t_setup = time.perf_counter() - t0
+    voxels = bb.leaf_voxels
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def timed(fn, reps):
+        out = []
+        for _ in range(reps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out
+
+    plain = lambda: BT.plain_build(bb.items, bb.edt_scratch[0])
+    timed(plain, max(args.warmup, 3))
+    t_plain = timed(plain, args.steps)
+    bb.capture()
+    timed(bb.replay, max(args.warmup, 3))
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_batch = timed(bb.replay, args.steps)
+    clk = clocks.stop()
+    assert bb.check_counts()
+    mp, mb = statistics.median(t_plain), statistics.median(t_batch)
+    hist = {}
+    for b in blocks:
+        hist[str(b)] = hist.get(str(b), 0) + 1
+    return {
+        "metric": METRIC, "workload": "batched_256_recipes", "value": voxels / (mb * 1e-3) / 1e9, "unit": UNIT,
+        "plain_gvox_s": voxels / (mp * 1e-3) / 1e9, "batched_gvox_s": voxels / (mb * 1e-3) / 1e9,
+        "speedup_batched_vs_plain": mp / mb, "ms_plain": mp, "ms_batched": mb, "steps": args.steps,
+        "recipes": len(recipes), "leaf_voxels": voxels, "recipes_per_s": len(recipes) / (mb * 1e-3),
+        "leaf_sizes": hist, "autotune_s": t_tune, "compile_s": t_compile, "setup_s": t_setup,
+        "edt_voxels": int(sum(it.meta.nx * it.meta.ny * it.meta.nz for it in bb.items)),
+        "grid_sizes": {str(n): sum(1 for _, m in recipes if m.nx == n) for n in (64, 128, 256, 512)},
+        "clocks": clk, "dtype": "f32 (f64 guard band); int32 EDT", "data": "synthetic",
+    }
+
+
+def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
+    """Poisson arrivals at `rate` req/s for `seconds`: 40 % builds (recipes as the batched
+    workload), 30 % edits (1-64 tool capsules subtracted from a resident field), 20 % point queries
+    (1e5-1e6 points, value + gradient), 10 % EDT recomputations; latency = completion - arrival."""
+    import torch
+    import field_b200.batch as BT
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    import field_b200.serve as S
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(seed)
+    pool = [(X.compile_recipe(r), n) for r, n, _ in R.batch_recipes(count=64, seed=11)]
+    srv = S.FieldServer(slots=16, budget_bytes=150e9)
+    try:
+        # warm start: a few resident fields and every kernel configured
+        warm = [srv.submit("build", recipe=c, meta=BT.cube_meta(n, 8)) for c, n in pool[:8]]
+        live = [f.result(timeout=120)["field"] for f in warm]
+        srv.submit("edt", field=live[0]).result(timeout=120)
+        srv.submit("query", field=live[0], points=rng.uniform(0, 1, (1000, 3)).astype(np.float32)).result(timeout=120)
+        srv.completed.clear()
+        n_req = int(rate * seconds)
+        gaps = rng.exponential(1.0 / rate, size=n_req)
+        kinds = rng.choice(["build", "edit", "query", "edt"], size=n_req, p=[0.4, 0.3, 0.2, 0.1])
+        futs = []
+        t0 = time.perf_counter()
+        due = t0
+        for k, gap in zip(kinds, gaps):
+            due += gap
+            while time.perf_counter() < due:
+                pass
+            fid = live[int(rng.integers(len(live)))]
+            if k == "build":
+                c, n = pool[int(rng.integers(len(pool)))]
+                f = srv.submit("build", recipe=c, meta=BT.cube_meta(n, 8))
+                f.add_done_callback(lambda fu: live.append(fu.result()["field"]) if not fu.exception() else None)
+            elif k == "edit":
+                f = srv.submit("edit", field=fid, tools=R.tools(rng, int(rng.integers(1, 65))), op="subtract")
+            elif k == "query":
+                npts = int(rng.integers(100_000, 1_000_001))
+                f = srv.submit("query", field=fid, points=rng.uniform(0, 1, (npts, 3)).astype(np.float32))
+            else:
+                f = srv.submit("edt", field=fid)
+            futs.append(f)
+        errors = 0
+        for f in futs:
+            try:
+                f.result(timeout=600)
+            except Exception:
+                errors += 1
+        t_end = time.perf_counter()
+        lat = np.array([(e - a) * 1e3 for _, a, _, e in srv.completed])
+        by_kind = {}
+        for kind, a, _, e in srv.completed:
+            by_kind.setdefault(kind, []).append((e - a) * 1e3)
+    finally:
+        srv.close()
+    return {
+        "metric": METRIC, "workload": "serve_poisson", "rate_req_s": rate, "seconds": seconds, "requests": n_req,
+        "errors": errors, "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "by_kind": {k: {"n": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+                    for k, v in by_kind.items()},
+        "slots": 16, "budget_gb": 150, "data": "synthetic",
+    }
+
+
 def main():
     args = parse()
+    if args.workload == "batched":
+        print(json.dumps(run_batched(args)), flush=True)
+        return
+    if args.workload == "serve":
+        print(json.dumps(run_serve(args, rate=args.rate, seconds=args.seconds)), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

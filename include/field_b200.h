@@ -146,6 +146,13 @@ int fb_field_reconstruct_device(const int32_t* d_kind, const int32_t* d_active, 
                                 const float* d_tiles, int64_t nx, int64_t ny, int64_t nz, int32_t block, float big,
                                 int32_t* d_slot, float* d_out, void* stream);
 
+/* Replaces the solid reconstruction of src/field_engine/faltkarna_v1_mesh_to_sdf.py:695-713
+ * (reconstruct_solid_from_sparse) on device-resident fields: uint8 mask, 1 where the field is
+ * negative; reads the active count on the device (no synchronisation).  d_slot: n_blocks int32. */
+int fb_field_occupancy_device(const int32_t* d_kind, const int32_t* d_active, const int32_t* d_count,
+                              const float* d_tiles, int64_t capacity, int64_t nx, int64_t ny, int64_t nz,
+                              int32_t block, int32_t* d_slot, uint8_t* d_mask, void* stream);
+
 /* Replaces k_reduce_checksum_i64_safe, src/field_engine/faltkarna_v1.py:250-255 (accumulates into d_out[0]). */
 int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64_t* d_out, void* stream);
 

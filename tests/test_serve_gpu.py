@@ -1,0 +1,100 @@
+"""Continuous-batching server: results alone equal results in the concurrent mix, admission by
+budget with LRU eviction, failures fail only their own request (GPU)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _recipe(seed, n_parts=40):
+    import field_b200.recipes as R
+    import field_b200.expr as X
+    rng = np.random.default_rng(seed)
+    q = n_parts // 4
+    return X.subtract_all(X.union_all(R.parts(rng, q, q, q, n_parts - 3 * q, scale=0.6)), R.tools(rng, 4))
+
+
+def _requests(fields, rng):
+    import field_b200.recipes as R
+    reqs = []
+    for k in range(24):
+        f = fields[k % len(fields)]
+        kind = ("query", "edt", "query", "edit")[k % 4]
+        if kind == "query":
+            reqs.append(("query", dict(field=f, points=rng.uniform(0, 1, size=(20000, 3)).astype(np.float32))))
+        elif kind == "edt":
+            reqs.append(("edt", dict(field=f)))
+        else:
+            reqs.append(("edit", dict(field=f, tools=R.tools(rng, 3), op="subtract")))
+    return reqs
+
+
+def _same(a, b):
+    if isinstance(a, tuple):
+        return all(np.array_equal(x, y) for x, y in zip(a, b))
+    return a == b
+
+
+def test_results_alone_equal_results_in_the_mix():
+    import field_b200.serve as S
+    import field_b200.batch as BT
+    metas = [BT.cube_meta(n, b) for n, b in ((64, 8), (128, 8), (96, 4), (128, 16))]
+    # run 1: one request at a time
+    with S.FieldServer(slots=4) as srv:
+        fields = [srv.submit("build", recipe=_recipe(i), meta=m).result(timeout=60)["field"] for i, m in enumerate(metas)]
+        reqs = _requests(fields, np.random.default_rng(0))
+        alone = [srv.submit(k, **a).result(timeout=60) for k, a in reqs]
+    # run 2: the same builds and requests submitted all at once
+    with S.FieldServer(slots=4) as srv:
+        futs = [srv.submit("build", recipe=_recipe(i), meta=m) for i, m in enumerate(metas)]
+        fields2 = [f.result(timeout=60)["field"] for f in futs]
+        assert fields2 == fields
+        reqs = _requests(fields2, np.random.default_rng(0))
+        futs = [srv.submit(k, **a) for k, a in reqs]
+        mixed = [f.result(timeout=60) for f in futs]
+    # edits change the field for later requests in submission order: compare requests whose
+    # result cannot depend on an edit's position -- everything up to the first edit of each field,
+    # and every edit result (its own rebuild)
+    for (k, a), x, y in zip(reqs, alone, mixed):
+        if k == "edit":
+            assert x["n_active"] == y["n_active"]
+    first = {}
+    for i, (k, a) in enumerate(reqs):
+        if k == "edit":
+            first.setdefault(a["field"], i)
+    for i, ((k, a), x, y) in enumerate(zip(reqs, alone, mixed)):
+        if i < first.get(a["field"], len(reqs)):
+            assert _same(x, y), (i, k)
+
+
+def test_budget_admission_evicts_least_recently_used():
+    import field_b200.serve as S
+    import field_b200.batch as BT
+    meta = BT.cube_meta(128, 8)
+    with S.FieldServer(slots=2) as srv:
+        first = srv.submit("build", recipe=_recipe(0), meta=meta).result(timeout=60)["field"]
+        # room for about two resident fields next to one build's admission estimate
+        probe = S._Request("build", dict(recipe=None, meta=meta))
+        budget = srv._estimate(probe) + 2.5 * srv.fields[first].nbytes
+        srv.budget = budget
+        ids = [first] + [srv.submit("build", recipe=_recipe(i), meta=meta).result(timeout=60)["field"]
+                         for i in range(1, 6)]
+        assert srv.resident_bytes() <= budget
+        assert ids[0] not in srv.fields  # the oldest field was evicted to admit later builds
+        with pytest.raises(KeyError):
+            srv.submit("query", field=ids[0], points=np.zeros((4, 3), np.float32)).result(timeout=60)
+        v, g = srv.submit("query", field=ids[-1], points=np.full((8, 3), 0.5, np.float32)).result(timeout=60)
+        assert v.shape == (8,) and g.shape == (8, 3)
+
+
+def test_a_failing_request_leaves_the_server_usable():
+    import field_b200.serve as S
+    import field_b200.batch as BT
+    with S.FieldServer(slots=2) as srv:
+        fid = srv.submit("build", recipe=_recipe(3), meta=BT.cube_meta(64, 8)).result(timeout=60)["field"]
+        with pytest.raises(ValueError):
+            srv.submit("edit", field=fid, tools=[], op="intersect").result(timeout=60)
+        with pytest.raises(Exception):
+            srv.submit("build", recipe={"op": "nonsense"}, meta=BT.cube_meta(64, 8)).result(timeout=60)
+        out = srv.submit("edt", field=fid).result(timeout=60)
+        assert out["voxels"] == 64 ** 3
