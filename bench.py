@@ -22,7 +22,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -61,55 +60,62 @@ def parse():
 
 # ------------------------------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML (read-only queries) every `period_s`
+    while the timed region runs.  The device is found by the UUID torch reports for `cuda_index`,
+    so CUDA_VISIBLE_DEVICES remapping cannot pick the wrong board."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("hw_power_brake_slowdown", 0x80), ("sw_power_cap", 0x4))
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index, period_s=0.004):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.samples = []
+        self.error = None
+        self.thread = None
+        self.stop_flag = threading.Event()
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except OSError:
-            self.proc = None
+            self.nvml, self.h = self._handle()
+            self.max_mhz = self.nvml.nvmlDeviceGetMaxClockInfo(self.h, self.nvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: the line says so
+            self.error = f"nvml unavailable: {e!r}"[:120]
+            return
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        n = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append((n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM),
+                                     n.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception as e:
+                self.error = f"nvml query failed: {e!r}"[:120]
+                return
+            self.stop_flag.wait(self.period)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not sampled"], "samples": 0}
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        sm = [c for c, _ in self.samples]
+        reasons = sorted({name for _, mask in self.samples for name, bit in self.REASONS if mask & bit})
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+               "reasons": reasons, "samples": len(sm), "source": "nvml"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 # ------------------------------------------------------------------------------------------ workload
