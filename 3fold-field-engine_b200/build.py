@@ -61,6 +61,32 @@ class DeviceField:
                            corner_min_abs=self.corner_min_abs.cpu().numpy(), stats=stats_of(self.meta, kind, n))
 
 
+def device_tables(comp: Compiled, device, stream):
+    """(primitive table, instruction table) of a compiled recipe as uint8 device tensors, validated
+    and uploaded once per device and kept on the Compiled object; `stream` is made to wait for the
+    upload, so builds on any stream may share the tables (the kernels only read them)."""
+    import torch
+    cache = comp.__dict__.setdefault("_device_tables", {})
+    key = str(device)
+    if key not in cache:
+        mode = 1 if comp.chain is not None else 0
+        insns = comp.chain if mode == 1 else comp.program
+        if len(comp.prims) < 1:
+            raise ValueError("recipe has no primitive")
+        _validate_program(comp.prims, insns, mode)
+        with torch.cuda.stream(stream):
+            prims = torch.from_numpy(np.ascontiguousarray(comp.prims).view(np.uint8).copy()).pin_memory()
+            chain = torch.from_numpy(np.ascontiguousarray(insns).view(np.uint8).copy()).pin_memory()
+            dprims = prims.to(device, non_blocking=True)
+            dchain = chain.to(device, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(stream)
+        cache[key] = (dprims, dchain, done, (prims, chain))
+    dprims, dchain, done, _ = cache[key]
+    stream.wait_event(done)
+    return dprims, dchain
+
+
 class FieldBuilder:
     """Compiled recipe + scratch + outputs for one grid, resident on one device.
 
@@ -82,9 +108,7 @@ class FieldBuilder:
         if self.n_prims < 1:
             raise ValueError("recipe has no primitive")
         self.geom = geom_of(meta, guard)
-        _validate_program(c.prims, insns, self.mode)
-        self.prims = torch.from_numpy(np.ascontiguousarray(c.prims).view(np.uint8).copy()).to(self.device)
-        self.chain = torch.from_numpy(np.ascontiguousarray(insns).view(np.uint8).copy()).to(self.device)
+        self.prims, self.chain = device_tables(c, self.device, torch.cuda.current_stream(self.device))
         nbytes = self.lib.fb_field_scratch_bytes(ct.addressof(self.geom), self.n_prims, self.n_chain)
         if nbytes < 0:
             raise ValueError("grid outside the build contract")

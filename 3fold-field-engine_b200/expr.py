@@ -495,6 +495,41 @@ def compile_recipe(node) -> Compiled:
     return Compiled(prims, _records(prog), None)
 
 
+def compile_tools(tools):
+    """PRIM records of edit tools, one primitive each (a leaf under transforms / scale / offset)."""
+    recs = []
+    for tool in tools:
+        c = _Compiler()
+        ch = c.chain(tool, np.eye(4), 1.0)
+        if ch is None or len(ch) != 1 or ch[0][0] != CH_SET:
+            raise ValueError("an edit tool must be a single primitive")
+        recs.append(c.prims[ch[0][1]])
+    return np.array(recs, dtype=PRIM) if recs else np.zeros(0, PRIM)
+
+
+def extend(comp: Compiled, tool_prims, op="subtract") -> Compiled:
+    """``comp`` with each tool primitive subtracted from (op "subtract") or unioned to (op "union")
+    the result in order -- the compiled form of subtract(...subtract(recipe, t1)..., tn) -- without
+    recompiling the recipe: the tools' records are appended to the table, one chain entry each
+    (or push + operator in the postfix program of a recipe that has no chain)."""
+    if op not in ("union", "subtract"):
+        raise ValueError("edit op must be union or subtract")
+    tool_prims = np.asarray(tool_prims, dtype=PRIM)
+    base = len(comp.prims)
+    prims = np.concatenate([comp.prims, tool_prims])
+    idx = range(base, base + len(tool_prims))
+    if comp.chain is not None:
+        code = CH_SUBTRACT if op == "subtract" else CH_UNION
+        chain = np.concatenate([comp.chain, _records([(code, i, 0.0) for i in idx])])
+        return Compiled(prims, _records(_chain_to_program([(int(r["op"]), int(r["arg"]), float(r["k"]))
+                                                            for r in chain])), chain)
+    code = OP_SUBTRACT if op == "subtract" else OP_UNION
+    rows = []
+    for i in idx:
+        rows += [(OP_PUSH, i, 0.0), (code, -1, 0.0)]
+    return Compiled(prims, np.concatenate([comp.program, _records(rows)]), None)
+
+
 def eval_sdf_py(node, p):
     """Pure-Python float64 evaluation of a tree (the reference's ground truth, for small checks;
     src/field_engine/ikarus_v1/expr.py:263-385).  Uses the compiled form on one point."""

@@ -19,6 +19,7 @@ import numpy as np
 
 from . import _lib
 from .expr import Compiled, compile_recipe
+from .build import device_tables
 
 PRIMF_BYTES = 128
 
@@ -35,8 +36,7 @@ class RecipeQueries:
         self.mode = 1 if c.chain is not None else 0
         insns = c.chain if self.mode == 1 else c.program
         self.n_chain = len(insns)
-        self.prims = torch.from_numpy(np.ascontiguousarray(c.prims).view(np.uint8).copy()).to(self.device)
-        self.chain = torch.from_numpy(np.ascontiguousarray(insns).view(np.uint8).copy()).to(self.device)
+        self.prims, self.chain = device_tables(c, self.device, torch.cuda.current_stream(self.device))
         self.primf = torch.empty(len(c.prims) * PRIMF_BYTES, dtype=torch.uint8, device=self.device)
         _lib.check(self.lib.fb_query_prepare(self.prims.data_ptr(), len(c.prims), self.primf.data_ptr(),
                                              _lib.stream_handle()), "query prepare")

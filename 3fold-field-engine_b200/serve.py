@@ -7,14 +7,21 @@ Requests (``submit`` returns a Future):
   * ``query``  (field id, points (N, 3))         -> float32 values and central-difference gradients
   * ``edt``    (field id)                        -> squared EDT of the field's occupancy (device)
 
-The scheduler thread admits queued requests while a stream slot is free and the HBM budget
-allows their estimated footprint, runs each request as a generator that enqueues asynchronous
-GPU work on its slot's stream and yields a CUDA event, resumes it when the event has completed,
-and admits the next arrival as soon as a slot frees -- so requests that arrive while others are on
-the GPU overlap with them on the device.  Resident fields are evicted least-recently-used when an
-admission would exceed the budget.  The reference's service is one synchronous request at a time
-over a pipe (src/field_engine/mesh_field_service_v1.py:44-113); its timeout/close behaviour is kept:
-a failed or timed-out request fails its future, the server stays usable.
+Request preparation (compiling a recipe, compiling edit tools to primitive records, staging query
+points in pinned host memory) runs on the submitting thread.  The scheduler thread admits queued
+requests while a stream slot is free and the HBM budget allows their estimated footprint, runs
+each request as a generator that enqueues asynchronous GPU work on its slot's stream and yields a
+CUDA event, resumes it when the event has completed, and admits the next arrival as soon as a slot
+frees -- so requests that arrive while others are on the GPU overlap with them on the device.
+
+Per field, requests take effect in submission order: a request waits while an earlier request on
+the same field is still queued or an earlier edit of it is still running, so every result is the
+one the same requests give one at a time.  An edit appends the compiled tools to the field's chain
+(no recompilation of the recipe) and rebuilds into new buffers; requests already running keep
+reading the previous version.  Resident fields are evicted least-recently-used when an admission
+would exceed the budget.  The reference's service is one synchronous request at a time over a pipe
+(src/field_engine/mesh_field_service_v1.py:44-113); its timeout/close behaviour is kept: a failed or
+timed-out request fails its future, the server stays usable.
 """
 from __future__ import annotations
 
@@ -32,17 +39,17 @@ from .query import RecipeQueries
 
 
 class _Field:
-    def __init__(self, fid, recipe, comp, meta, fb, tiles, n_active):
+    def __init__(self, fid, comp, meta, fb, tiles, n_active):
         self.id = fid
-        self.recipe = recipe
         self.comp = comp
         self.meta = meta
         self.fb = fb
         self.tiles = tiles
         self.n_active = n_active
-        self.queries = None
+        self.queries = None  # (RecipeQueries, CUDA event marking its tables ready)
         self.edt = None
         self.busy = 0
+        self.editing = False
         self.last_use = time.perf_counter()
 
     @property
@@ -66,6 +73,37 @@ class _Request:
         self.slot = None
         self.estimate = 0
 
+    @property
+    def field(self):
+        return self.args.get("field")
+
+
+def _prepare(kind, args):
+    """Caller-thread preparation: compiled recipes and tools, pinned float32 points."""
+    import torch
+    if kind == "build":
+        r = args["recipe"]
+        args["recipe"] = r if isinstance(r, X.Compiled) else X.compile_recipe(r)
+    elif kind == "edit":
+        op = args.get("op", "subtract")
+        if op not in ("union", "subtract"):
+            raise ValueError("edit op must be union or subtract")
+        tools = args["tools"]
+        args["tool_prims"] = tools if isinstance(tools, np.ndarray) else X.compile_tools(tools)
+        args["op"] = op
+    elif kind == "query":
+        p = args["points"]
+        if isinstance(p, torch.Tensor):
+            if p.dim() != 2 or p.shape[1] != 3:
+                raise ValueError("points must be an (N, 3) array")
+            p = p.to(torch.float32).contiguous()
+            args["points"] = p if p.is_cuda or p.is_pinned() else p.pin_memory()
+        else:
+            a = np.ascontiguousarray(p, dtype=np.float32)
+            if a.ndim != 2 or a.shape[1] != 3:
+                raise ValueError("points must be an (N, 3) array")
+            args["points"] = torch.from_numpy(a).pin_memory()
+
 
 class FieldServer:
     def __init__(self, *, device="cuda", slots=8, budget_bytes=150e9, request_timeout_s=30.0):
@@ -80,7 +118,7 @@ class FieldServer:
         self.fields = {}
         self.next_id = 0
         self.reserved = 0
-        self.pending = collections.deque()
+        self.pending = []
         self.inflight = []
         self.lock = threading.Lock()
         self.wake = threading.Event()
@@ -94,6 +132,12 @@ class FieldServer:
         if kind not in ("build", "edit", "query", "edt"):
             raise ValueError(f"unknown request kind {kind!r}")
         r = _Request(kind, args)
+        try:
+            _prepare(kind, args)
+        except Exception as e:  # an unusable request fails its own future
+            r.end = time.perf_counter()
+            r.future.set_exception(e)
+            return r.future
         with self.lock:
             if not self.running:
                 raise RuntimeError("server closed")
@@ -119,12 +163,12 @@ class FieldServer:
     # ------------------------------------------------------------------------------------ scheduler
     def _estimate(self, r):
         if r.kind in ("build", "edit"):
-            meta = r.args["meta"] if r.kind == "build" else self.fields[r.args["field"]].meta
+            meta = r.args["meta"] if r.kind == "build" else self.fields[r.field].meta
             # culling lists + block arrays + a quarter of the blocks active (tiles), grown on demand
             return int(meta.n_blocks * (meta.block ** 3) + meta.n_blocks * 64 + 64e6)
         if r.kind == "query":
             return int(len(r.args["points"]) * 32)
-        meta = self.fields[r.args["field"]].meta
+        meta = self.fields[r.field].meta
         return int(meta.nx * meta.ny * meta.nz * 14)
 
     def _evict_for(self, need):
@@ -133,7 +177,7 @@ class FieldServer:
         if resident + self.reserved + need <= self.budget:
             return True
         for f in sorted(self.fields.values(), key=lambda f: f.last_use):
-            if f.busy:
+            if f.busy or f.editing:
                 continue
             del self.fields[f.id]
             resident -= f.nbytes
@@ -142,43 +186,61 @@ class FieldServer:
         return resident + self.reserved + need <= self.budget
 
     def _admit(self):
-        """Start queued requests while a slot is free and the budget allows; returns those that
-        are now waiting on a device event."""
+        """Start queued requests, oldest first, while a slot is free and the budget allows; a
+        request whose field has an earlier request still queued, or an edit still running, waits
+        without holding back requests on other fields.  Returns the requests now waiting on a
+        device event."""
         started = []
-        while self.free:
-            with self.lock:
-                if not self.pending:
-                    break
-                r = self.pending[0]
-            if r.kind != "build" and r.args.get("field") not in self.fields:
-                with self.lock:
-                    self.pending.popleft()
-                r.end = time.perf_counter()
-                r.future.set_exception(KeyError(f"field {r.args.get('field')} is not resident"))
-                continue
+        with self.lock:
+            queue = list(self.pending)
+        if not queue:
+            return started
+        taken = set()
+        held = set()  # fields with an earlier request still queued
+        for r in queue:
+            if not self.free:
+                break
+            if r.kind != "build":
+                f = self.fields.get(r.field)
+                if f is None:
+                    if r.field in held:
+                        continue
+                    taken.add(id(r))
+                    r.end = time.perf_counter()
+                    r.future.set_exception(KeyError(f"field {r.field} is not resident"))
+                    continue
+                if r.field in held or f.editing:
+                    held.add(r.field)
+                    continue
             r.estimate = self._estimate(r)
             if not self._evict_for(r.estimate):
-                break  # wait for memory: in-flight requests release their reservations
-            with self.lock:
-                self.pending.popleft()
+                break  # wait for memory, oldest first: in-flight requests release their reservations
+            taken.add(id(r))
             r.slot = self.free.popleft()
             self.reserved += r.estimate
             r.start = time.perf_counter()
             if r.kind != "build":
-                self.fields[r.args["field"]].busy += 1
+                f = self.fields[r.field]
+                f.busy += 1
+                f.editing = r.kind == "edit"
             r.gen = getattr(self, f"_run_{r.kind}")(r, self.streams[r.slot])
             if self._step(r):
                 started.append(r)
+        if taken:
+            with self.lock:
+                self.pending = [r for r in self.pending if id(r) not in taken]
         return started
 
     def _finish(self, r, result=None, error=None):
         r.end = time.perf_counter()
         self.free.append(r.slot)
         self.reserved -= r.estimate
-        if r.kind != "build" and r.args.get("field") in self.fields:
-            f = self.fields[r.args["field"]]
+        if r.kind != "build" and r.field in self.fields:
+            f = self.fields[r.field]
             f.busy -= 1
             f.last_use = r.end
+            if r.kind == "edit":
+                f.editing = False
         self.completed.append((r.kind, r.arrival, r.start, r.end))
         if error is not None:
             r.future.set_exception(error)
@@ -204,7 +266,7 @@ class FieldServer:
             with self.lock:
                 self.running = False
                 waiting = list(self.pending) + list(self.inflight)
-                self.pending.clear()
+                self.pending = []
             self.inflight = []
             for r in waiting:
                 if not r.future.done():
@@ -219,8 +281,8 @@ class FieldServer:
                 idle = not self.pending and not self.inflight
             if not running and idle:
                 return
-            started = self._admit()
-            progressed = bool(started)
+            self.wake.clear()
+            progressed = False
             still = []
             for r in self.inflight:
                 if not r.event.query():
@@ -233,10 +295,12 @@ class FieldServer:
                 progressed = True
                 if self._step(r):
                     still.append(r)
-            self.inflight = still + started
-            if not progressed:
-                self.wake.wait(timeout=0.0002)
-                self.wake.clear()
+            self.inflight = still
+            started = self._admit()
+            self.inflight += started
+            if not progressed and not started:
+                # new submissions set `wake`; device completions are polled
+                self.wake.wait(timeout=0.0001 if self.inflight else 0.01)
 
     # ------------------------------------------------------------------------------------ request bodies
     def _record(self, stream):
@@ -245,10 +309,9 @@ class FieldServer:
         ev.record(stream)
         return ev
 
-    def _build_field(self, recipe, meta, stream):
+    def _build_field(self, comp, meta, stream):
         import torch
         with torch.cuda.stream(stream):
-            comp = recipe if isinstance(recipe, X.Compiled) else X.compile_recipe(recipe)
             fb = FieldBuilder(comp, meta, device=self.device)
             fb.classify(stream)
             count = torch.empty(1, dtype=torch.int32, pin_memory=True)
@@ -260,41 +323,38 @@ class FieldServer:
             if n:
                 fb.leaf(tiles, n, stream=stream)
         yield self._record(stream)
-        return comp, fb, tiles, n
+        return fb, tiles, n
 
     def _run_build(self, r, stream):
-        recipe, meta = r.args["recipe"], r.args["meta"]
-        comp, fb, tiles, n = yield from self._build_field(recipe, meta, stream)
+        comp, meta = r.args["recipe"], r.args["meta"]
+        fb, tiles, n = yield from self._build_field(comp, meta, stream)
         fid = self.next_id
         self.next_id += 1
-        self.fields[fid] = _Field(fid, recipe, comp, meta, fb, tiles, n)
+        self.fields[fid] = _Field(fid, comp, meta, fb, tiles, n)
         return dict(field=fid, n_active=n, leaf_voxels=n * meta.block ** 3)
 
     def _run_edit(self, r, stream):
-        f = self.fields[r.args["field"]]
-        op = r.args.get("op", "subtract")
-        if op not in ("union", "subtract"):
-            raise ValueError("edit op must be union or subtract")
-        recipe = f.recipe
-        for tool in r.args["tools"]:
-            recipe = X.union(recipe, tool) if op == "union" else X.subtract(recipe, tool)
-        comp, fb, tiles, n = yield from self._build_field(recipe, f.meta, stream)
-        f.recipe, f.comp, f.fb, f.tiles, f.n_active = recipe, comp, fb, tiles, n
+        f = self.fields[r.field]
+        comp = X.extend(f.comp, r.args["tool_prims"], r.args["op"])
+        fb, tiles, n = yield from self._build_field(comp, f.meta, stream)
+        f.comp, f.fb, f.tiles, f.n_active = comp, fb, tiles, n
         f.queries = None
         f.edt = None
         return dict(field=f.id, n_active=n, leaf_voxels=n * f.meta.block ** 3)
 
     def _run_query(self, r, stream):
         import torch
-        f = self.fields[r.args["field"]]
+        f = self.fields[r.field]
         pts = r.args["points"]
         h = float(r.args.get("h", f.meta.pitch))
         with torch.cuda.stream(stream):
             if f.queries is None:
-                f.queries = RecipeQueries(f.comp, device=self.device, builder=f.fb)
-            p = pts if isinstance(pts, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(pts, np.float32))
-            p = p.to(self.device, torch.float32, non_blocking=True)
-            val, grad = f.queries.values_and_gradients(p, h=h, stream=stream)
+                # tables prepared on this stream; later queries on other streams wait for them
+                f.queries = (RecipeQueries(f.comp, device=self.device, builder=f.fb), self._record(stream))
+            q, ready = f.queries
+            stream.wait_event(ready)
+            p = pts.to(self.device, non_blocking=True)
+            val, grad = q.values_and_gradients(p, h=h, stream=stream)
             out_v = torch.empty(val.shape, dtype=val.dtype, pin_memory=True)
             out_g = torch.empty(grad.shape, dtype=grad.dtype, pin_memory=True)
             out_v.copy_(val, non_blocking=True)
@@ -304,17 +364,18 @@ class FieldServer:
 
     def _run_edt(self, r, stream):
         import torch
-        f = self.fields[r.args["field"]]
+        f = self.fields[r.field]
         m = f.meta
         lib = _lib.lib()
+        fb, tiles, n_active = f.fb, f.tiles, f.n_active
         with torch.cuda.stream(stream):
             slot = torch.empty(m.n_blocks, dtype=torch.int32, device=self.device)
             mask = torch.empty((m.nx, m.ny, m.nz), dtype=torch.uint8, device=self.device)
             out = torch.empty((m.nx, m.ny, m.nz), dtype=torch.int32, device=self.device)
             scratch = torch.empty(int(lib.fb_edt_scratch_bytes(m.nx, m.ny, m.nz, 0)), dtype=torch.uint8,
                                   device=self.device)
-            _lib.check(lib.fb_field_occupancy_device(f.fb.kind.data_ptr(), f.fb.active.data_ptr(), f.fb.count.data_ptr(),
-                                                     f.tiles.data_ptr(), max(f.n_active, 1), m.nx, m.ny, m.nz, m.block,
+            _lib.check(lib.fb_field_occupancy_device(fb.kind.data_ptr(), fb.active.data_ptr(), fb.count.data_ptr(),
+                                                     tiles.data_ptr(), max(n_active, 1), m.nx, m.ny, m.nz, m.block,
                                                      slot.data_ptr(), mask.data_ptr(), _lib.stream_handle(stream)),
                        "occupancy")
             _lib.check(lib.fb_edt_squared_device(mask.data_ptr(), m.nx, m.ny, m.nz, 1, out.data_ptr(),
@@ -324,5 +385,6 @@ class FieldServer:
             host = torch.empty((), dtype=torch.int64, pin_memory=True)
             host.copy_(total, non_blocking=True)
         yield self._record(stream)
-        f.edt = out
+        if f.fb is fb:
+            f.edt = out
         return dict(field=f.id, checksum=int(host.item()), voxels=int(out.numel()))

@@ -444,7 +444,9 @@ def run_batched(args):
 def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
     """Poisson arrivals at `rate` req/s for `seconds`: 40 % builds (recipes as the batched
     workload), 30 % edits (1-64 tool capsules subtracted from a resident field), 20 % point queries
-    (1e5-1e6 points, value + gradient), 10 % EDT recomputations; latency = completion - arrival."""
+    (1e5-1e6 points, value + gradient), 10 % EDT recomputations; latency = completion - arrival.
+    Request payloads (recipes, tool lists, point sets) are generated before the arrival window, as
+    a client would hold them; the submitting thread sleeps between arrivals."""
     import torch
     import field_b200.batch as BT
     import field_b200.expr as X
@@ -453,55 +455,64 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
     torch.cuda.set_device(0)
     rng = np.random.default_rng(seed)
     pool = [(X.compile_recipe(r), n) for r, n, _ in R.batch_recipes(count=64, seed=11)]
+    n_req = int(rate * seconds)
+    gaps = rng.exponential(1.0 / rate, size=n_req)
+    kinds = rng.choice(["build", "edit", "query", "edt"], size=n_req, p=[0.4, 0.3, 0.2, 0.1])
+    point_sets = [rng.uniform(0, 1, (int(m), 3)).astype(np.float32)
+                  for m in np.geomspace(100_000, 1_000_000, 8)]
+    tool_sets = [X.compile_tools(R.tools(rng, int(k))) for k in rng.integers(1, 65, size=32)]
+    working_set = 64  # requests on fields pick among the most recently built ones
     srv = S.FieldServer(slots=16, budget_bytes=150e9)
     try:
         # warm start: a few resident fields and every kernel configured
         warm = [srv.submit("build", recipe=c, meta=BT.cube_meta(n, 8)) for c, n in pool[:8]]
         live = [f.result(timeout=120)["field"] for f in warm]
         srv.submit("edt", field=live[0]).result(timeout=120)
-        srv.submit("query", field=live[0], points=rng.uniform(0, 1, (1000, 3)).astype(np.float32)).result(timeout=120)
+        srv.submit("query", field=live[0], points=point_sets[0][:1000]).result(timeout=120)
+        srv.submit("edit", field=live[1], tools=tool_sets[0]).result(timeout=120)
         srv.completed.clear()
-        n_req = int(rate * seconds)
-        gaps = rng.exponential(1.0 / rate, size=n_req)
-        kinds = rng.choice(["build", "edit", "query", "edt"], size=n_req, p=[0.4, 0.3, 0.2, 0.1])
         futs = []
         t0 = time.perf_counter()
         due = t0
         for k, gap in zip(kinds, gaps):
             due += gap
-            while time.perf_counter() < due:
-                pass
-            fid = live[int(rng.integers(len(live)))]
+            wait = due - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            fid = live[-working_set:][int(rng.integers(min(len(live), working_set)))]
             if k == "build":
                 c, n = pool[int(rng.integers(len(pool)))]
                 f = srv.submit("build", recipe=c, meta=BT.cube_meta(n, 8))
                 f.add_done_callback(lambda fu: live.append(fu.result()["field"]) if not fu.exception() else None)
             elif k == "edit":
-                f = srv.submit("edit", field=fid, tools=R.tools(rng, int(rng.integers(1, 65))), op="subtract")
+                f = srv.submit("edit", field=fid, tools=tool_sets[int(rng.integers(len(tool_sets)))], op="subtract")
             elif k == "query":
-                npts = int(rng.integers(100_000, 1_000_001))
-                f = srv.submit("query", field=fid, points=rng.uniform(0, 1, (npts, 3)).astype(np.float32))
+                f = srv.submit("query", field=fid, points=point_sets[int(rng.integers(len(point_sets)))])
             else:
                 f = srv.submit("edt", field=fid)
             futs.append(f)
-        errors = 0
+        t_submitted = time.perf_counter()
+        errors = {}
         for f in futs:
             try:
                 f.result(timeout=600)
-            except Exception:
-                errors += 1
+            except Exception as e:
+                errors[type(e).__name__] = errors.get(type(e).__name__, 0) + 1
         t_end = time.perf_counter()
         lat = np.array([(e - a) * 1e3 for _, a, _, e in srv.completed])
         by_kind = {}
-        for kind, a, _, e in srv.completed:
-            by_kind.setdefault(kind, []).append((e - a) * 1e3)
+        for kind, a, st, e in srv.completed:
+            by_kind.setdefault(kind, []).append(((e - a) * 1e3, (st - a) * 1e3))
     finally:
         srv.close()
     return {
         "metric": METRIC, "workload": "serve_poisson", "rate_req_s": rate, "seconds": seconds, "requests": n_req,
-        "errors": errors, "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": float(np.percentile(lat, 50)),
+        "errors": errors, "offered_req_s": n_req / (t_submitted - t0),
+        "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": float(np.percentile(lat, 50)),
         "p99_ms": float(np.percentile(lat, 99)),
-        "by_kind": {k: {"n": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+        "by_kind": {k: {"n": len(v), "p50_ms": float(np.percentile([x for x, _ in v], 50)),
+                        "p99_ms": float(np.percentile([x for x, _ in v], 99)),
+                        "queue_p50_ms": float(np.percentile([q for _, q in v], 50))}
                     for k, v in by_kind.items()},
         "slots": 16, "budget_gb": 150, "data": "synthetic",
     }

@@ -52,19 +52,28 @@ def test_results_alone_equal_results_in_the_mix():
         reqs = _requests(fields2, np.random.default_rng(0))
         futs = [srv.submit(k, **a) for k, a in reqs]
         mixed = [f.result(timeout=60) for f in futs]
-    # edits change the field for later requests in submission order: compare requests whose
-    # result cannot depend on an edit's position -- everything up to the first edit of each field,
-    # and every edit result (its own rebuild)
-    for (k, a), x, y in zip(reqs, alone, mixed):
-        if k == "edit":
-            assert x["n_active"] == y["n_active"]
-    first = {}
-    for i, (k, a) in enumerate(reqs):
-        if k == "edit":
-            first.setdefault(a["field"], i)
+    # per field, requests take effect in submission order: every result equals its result alone
     for i, ((k, a), x, y) in enumerate(zip(reqs, alone, mixed)):
-        if i < first.get(a["field"], len(reqs)):
-            assert _same(x, y), (i, k)
+        assert _same(x, y), (i, k)
+
+
+def test_edit_appends_tools_like_a_recompiled_recipe():
+    import field_b200.serve as S
+    import field_b200.batch as BT
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    meta = BT.cube_meta(96, 8)
+    rng = np.random.default_rng(5)
+    tools = R.tools(rng, 6)
+    pts = rng.uniform(0, 1, size=(5000, 3)).astype(np.float32)
+    with S.FieldServer(slots=2) as srv:
+        a = srv.submit("build", recipe=_recipe(7), meta=meta).result(timeout=60)["field"]
+        srv.submit("edit", field=a, tools=tools, op="subtract").result(timeout=60)
+        edited = srv.submit("query", field=a, points=pts).result(timeout=60)
+        b = srv.submit("build", recipe=X.subtract_all(_recipe(7), tools), meta=meta).result(timeout=60)["field"]
+        direct = srv.submit("query", field=b, points=pts).result(timeout=60)
+        assert srv.fields[a].n_active == srv.fields[b].n_active
+    assert _same(edited, direct)
 
 
 def test_budget_admission_evicts_least_recently_used():
