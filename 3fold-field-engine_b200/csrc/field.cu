@@ -36,9 +36,12 @@ static_assert(sizeof(FbGeom) == 64, "fb_geom layout");
 namespace {
 
 constexpr float kBig = 1.0e6f;  // background of interior (-) and exterior (+) blocks, faltkarna_v1.py:46
-constexpr int kCapCoarse = 1024;
-constexpr int kCapSuper = 256;
-constexpr int kCapBlock = 48;
+constexpr int kCapCoarse = 1024;           // least list capacity of a coarse region
+constexpr int kCapSuper = 256;             // least list capacity of a superblock
+constexpr int64_t kCapBudget = 8 << 20;    // list entries per level beyond which capacities stop growing
+constexpr int kCapBlock = 48;              // per-block list of the thread-per-block cull; leaf staging chunk
+constexpr int kCapBlockWarp = 96;          // per-block list of the warp-per-block cull
+constexpr int64_t kWarpCullBlocks = 1 << 17;  // grids up to this many blocks cull each block with a warp
 constexpr int kSuperEdge = 32;    // voxels per superblock edge
 constexpr int kCoarseDiv = 2;     // superblocks per coarse-region edge
 constexpr int kTile = 2048;       // compaction tile (256 threads x 8)
@@ -98,7 +101,16 @@ struct Plan {
     int64_t blk_off, blk_len, blk_pool, blk_cap;  // per-block culled lists of active blocks
     int64_t pool_full, pool_coarse, pool_super;  // element offsets inside pool
     int64_t ntiles;
+    int cap_coarse, cap_super;  // list capacities per coarse region / superblock
+    bool warp_blocks;           // per-block lists culled by one warp each, at blk_pool + b * kCapBlockWarp
 };
+
+// List capacity of a level: grows while the level's lists stay within kCapBudget entries, never
+// beyond the chain length (a list is a subsequence of the chain, so that capacity never overflows).
+int level_cap(int64_t nregions, int base, int n_chain) {
+    const int64_t grown = std::max<int64_t>(base, kCapBudget / std::max<int64_t>(nregions, 1));
+    return (int)std::min<int64_t>(grown, std::max(n_chain, 1));
+}
 
 int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
 
@@ -106,10 +118,13 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     Plan p{};
     int64_t at = 0;
     p.primf = at; at += align256((int64_t)std::max(n_prims, 1) * sizeof(PrimF));
+    p.cap_coarse = level_cap(G.ncoarse, kCapCoarse, n_chain);
+    p.cap_super = level_cap(G.nsuper, kCapSuper, n_chain);
+    p.warp_blocks = G.nblocks <= kWarpCullBlocks;
     p.pool_full = 0;
     p.pool_coarse = n_chain;
-    p.pool_super = p.pool_coarse + G.ncoarse * kCapCoarse;
-    const int64_t pool_elems = p.pool_super + G.nsuper * kCapSuper;
+    p.pool_super = p.pool_coarse + G.ncoarse * p.cap_coarse;
+    const int64_t pool_elems = p.pool_super + G.nsuper * p.cap_super;
     p.pool = at; at += align256(pool_elems * 4);
     p.off = at; at += align256((G.ncoarse + G.nsuper) * 8);
     p.len = at; at += align256((G.ncoarse + G.nsuper) * 4);
@@ -118,7 +133,7 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     p.misc = at; at += 256;  // [0] ticket, [1] error flag, [2] block-list pool cursor
     p.blk_off = at; at += align256(G.nblocks * 4);
     p.blk_len = at; at += align256(G.nblocks * 4);
-    p.blk_cap = std::max<int64_t>(G.nblocks * 12, 4096);
+    p.blk_cap = p.warp_blocks ? G.nblocks * kCapBlockWarp : std::max<int64_t>(G.nblocks * 12, 4096);
     p.blk_pool = at; at += align256(p.blk_cap * 4);
     p.total = at;
     return p;
@@ -491,6 +506,32 @@ __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __r
     }
 }
 
+// Block-level cull with one warp per block, for grids of few blocks (where one thread per block
+// would leave most of the GPU idle): the superblock list culled to the block's own list, stored at
+// blk_pool + b * cap.  blk_len[b] = -1 when it does not fit; that block then uses the superblock list
+// (exact, only slower).
+__global__ void __launch_bounds__(128) k_cull_blocks(Geo G, const FbInsn* __restrict__ chain,
+                                                     const PrimF* __restrict__ primf, const uint32_t* __restrict__ pool,
+                                                     const int64_t* __restrict__ sb_off,
+                                                     const int32_t* __restrict__ sb_len, int32_t* __restrict__ blk_off,
+                                                     int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool,
+                                                     int cap) {
+    const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (b >= G.nblocks) return;
+    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
+    const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
+    const float half = 0.5f * G.B;
+    const float cx = G.fx0 + (bi * G.B + half) * G.fpitch;
+    const float cy = G.fy0 + (bj * G.B + half) * G.fpitch;
+    const float cz = G.fz0 + (bk * G.B + half) * G.fpitch;
+    const float R = 1.7320509f * half * G.fpitch;
+    const int n = warp_walk(pool + sb_off[s], sb_len[s], chain, primf, cx, cy, cz, R, G.eps, blk_pool + b * cap, cap);
+    if ((threadIdx.x & 31) == 0) {
+        blk_off[b] = (int32_t)(b * cap);
+        blk_len[b] = n <= cap ? n : -1;
+    }
+}
+
 // ------------------------------------------------------------------------------------ localisation
 // ------------------------------------------------------------------------------------ classify
 // float64 value of a block list at a world point (guard-band recheck).
@@ -511,7 +552,8 @@ __device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, in
 // mode), so the walk over the superblock's list runs in lockstep with broadcast loads.
 __host__ __device__ __forceinline__ int threads_per_super(int S) { return ((S * S * S + 31) / 32) * 32; }
 
-template <bool kChain>
+// kListed: the per-block lists are already in blk_pool (k_cull_blocks); read them instead of culling.
+template <bool kChain, bool kListed>
 __global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restrict__ prims,
                                                   const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
                                                   int n_chain, const uint32_t* __restrict__ pool,
@@ -539,16 +581,24 @@ __global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restric
     if (kChain) {
         const uint32_t* plist = pool + sb_off[s_id];
         const int plen = sb_len[s_id];
-        // block-level cull of the superblock list
-        const float half = 0.5f * B;
-        const float cx = G.fx0 + (bi * B + half) * G.fpitch;
-        const float cy = G.fy0 + (bj * B + half) * G.fpitch;
-        const float cz = G.fz0 + (bk * B + half) * G.fpitch;
-        const float R = 1.7320509f * half * G.fpitch;
-        const int n = seq_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, blist, kCapBlock);
-        nblist = n;
-        const uint32_t* list = n <= kCapBlock ? blist : plist;
-        const int len = n <= kCapBlock ? n : plen;
+        const uint32_t* list;
+        int len;
+        if (kListed) {
+            const int n = blk_len[b];
+            list = n >= 0 ? blk_pool + blk_off[b] : plist;
+            len = n >= 0 ? n : plen;
+        } else {
+            // block-level cull of the superblock list
+            const float half = 0.5f * B;
+            const float cx = G.fx0 + (bi * B + half) * G.fpitch;
+            const float cy = G.fy0 + (bj * B + half) * G.fpitch;
+            const float cz = G.fz0 + (bk * B + half) * G.fpitch;
+            const float R = 1.7320509f * half * G.fpitch;
+            const int n = seq_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, blist, kCapBlock);
+            nblist = n;
+            list = n <= kCapBlock ? blist : plist;
+            len = n <= kCapBlock ? n : plen;
+        }
         const double ox = G.x0 + (double)(bi * B) * G.pitch;
         const double oy = G.y0 + (double)(bj * B) * G.pitch;
         const double oz = G.z0 + (double)(bk * B) * G.pitch;
@@ -617,7 +667,7 @@ __global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restric
         cma[b] = mn;
     }
     kind[b] = kd;
-    if (kChain && kd == 0) {  // keep the culled list for the leaf pass
+    if (kChain && !kListed && kd == 0) {  // keep the culled list for the leaf pass
         int len = -1;
         if (nblist >= 0 && nblist <= kCapBlock) {
             const int slot = atomicAdd(blk_cursor, nblist);
@@ -842,46 +892,19 @@ __device__ __forceinline__ void store_group(float* out, int group, const float* 
     }
 }
 
-// Leaf tile of one block whose culled list is longer than the shared staging: every primitive is
-// localised on the fly (rare; kept out of line so the fast loop stays small).
-template <int B, int VG>
-__device__ __noinline__ void leaf_block_slow(const Geo& G, const FbPrim* __restrict__ prims,
-                                             const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
-                                             const uint32_t* __restrict__ list, int len, int bi, int bj, int bk,
-                                             float* __restrict__ out) {
-    constexpr int kVox = B * B * B;
-    constexpr int kGroups = kVox / (32 * VG);
-    const int lane = threadIdx.x & 31;
-    const double ox = G.x0 + (double)(bi * B) * G.pitch;
-    const double oy = G.y0 + (double)(bj * B) * G.pitch;
-    const double oz = G.z0 + (double)(bk * B) * G.pitch;
-    for (int g = 0; g < kGroups; ++g) {
-        const int v0 = (g * 32 + lane) * VG;
-        const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
-        const float dx = li * G.fpitch, dy = lj * G.fpitch;
-        float dz[VG], acc[VG], v[VG];
-        for (int k = 0; k < VG; ++k) {
-            dz[k] = (lk0 + k) * G.fpitch;
-            acc[k] = 0.f;
-        }
-        for (int i = 0; i < len; ++i) {
-            const uint32_t e = list[i];
-            const FbInsn I = chain[e >> 2];
-            const int op = effective_op(e, I.op);
-            if (op == CH_OFFSET) {
-                for (int k = 0; k < VG; ++k) acc[k] -= (float)I.k;
-                continue;
-            }
-            LocalPrim P;
-            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, P);
-            eval_group<VG>(P, dx, dy, dz, v);
-            combine_group<VG>(op, P.k, acc, v);
-        }
-        for (int k = 0; k < VG; ++k)
-            if (!(fabsf(acc[k]) >= G.guard))
-                acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li, (int64_t)bj * B + lj,
-                                            (int64_t)bk * B + lk0 + k);
-        store_group<VG>(out, g * 32 + lane, acc);
+template <int VG>
+__device__ __forceinline__ void load_group(const float* out, int group, float* acc) {
+    if (VG == 8) {
+        const float4* o = reinterpret_cast<const float4*>(out) + 2 * group;
+        const float4 a = o[0], b = o[1];
+        acc[0] = a.x; acc[1] = a.y; acc[2] = a.z; acc[3] = a.w;
+        acc[4] = b.x; acc[5] = b.y; acc[6] = b.z; acc[7] = b.w;
+    } else if (VG == 4) {
+        const float4 a = reinterpret_cast<const float4*>(out)[group];
+        acc[0] = a.x; acc[1] = a.y; acc[2] = a.z; acc[3] = a.w;
+    } else {
+        const float2 a = reinterpret_cast<const float2*>(out)[group];
+        acc[0] = a.x; acc[1] = a.y;
     }
 }
 
@@ -930,7 +953,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim
         bool fits = true;
         int stored = kind[blk] == 0 ? blk_len[blk] : -1;
         const int64_t soff = stored >= 0 ? (int64_t)blk_off[blk] : 0;
-        if (stored < 0 || stored > kCapBlock || soff < 0 || soff + stored > blk_cap) stored = -1;
+        if (stored < 0 || soff < 0 || soff + stored > blk_cap) stored = -1;
         if (stored >= 0) {
             list = blk_pool + soff;
             len = stored;
@@ -968,54 +991,63 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim
                 atomicAdd(&work[1], flops * kVox);
             }
         }
-        if (!fits) {
-            leaf_block_slow<B, VG>(G, prims, primf, chain, list, len, bi, bj, bk, out);
-            continue;
-        }
-        for (int i = lane; i < len; i += 32) {
-            const uint32_t e = list[i];
-            const FbInsn I = chain[e >> 2];
-            const int op = effective_op(e, I.op);
-            if (op == CH_OFFSET) {
-                sp[i].op = op;
-                sp[i].k = (float)I.k;
-            } else {
-                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
-            }
-        }
-        __syncwarp();
-        for (int g = 0; g < kGroups; ++g) {
-            const int v0 = (g * 32 + lane) * VG;
-            const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
-            const float dx = li * G.fpitch, dy = lj * G.fpitch;
-            float dz[VG], acc[VG], v[VG];
-#pragma unroll
-            for (int k = 0; k < VG; ++k) {
-                dz[k] = (lk0 + k) * G.fpitch;
-                acc[k] = 0.f;
-            }
-            for (int i = 0; i < len; ++i) {
-                const LocalPrim& P = sp[i];
-                const int op = P.op;
+        (void)fits;
+        // the list in chunks of kCapBlock localised primitives; between chunks each lane keeps its
+        // partial fold in its own part of the tile (the same float operations in the same order)
+        for (int c0 = 0; c0 == 0 || c0 < len; c0 += kCapBlock) {  // one pass even for an empty list
+            const int clen = max(0, min(kCapBlock, len - c0));
+            const bool first = c0 == 0, last = c0 + clen >= len;
+            __syncwarp();
+            for (int i = lane; i < clen; i += 32) {
+                const uint32_t e = list[c0 + i];
+                const FbInsn I = chain[e >> 2];
+                const int op = effective_op(e, I.op);
                 if (op == CH_OFFSET) {
-#pragma unroll
-                    for (int k = 0; k < VG; ++k) acc[k] -= P.k;
-                    continue;
+                    sp[i].op = op;
+                    sp[i].k = (float)I.k;
+                } else {
+                    localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
                 }
-                eval_group<VG>(P, dx, dy, dz, v);
-                combine_group<VG>(op, P.k, acc, v);
             }
-            // guard band: float64 recheck so the sign never disagrees with the float64 value
-            bool near = false;
+            __syncwarp();
+            for (int g = 0; g < kGroups; ++g) {
+                const int v0 = (g * 32 + lane) * VG;
+                const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
+                const float dx = li * G.fpitch, dy = lj * G.fpitch;
+                float dz[VG], acc[VG], v[VG];
 #pragma unroll
-            for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
-            if (near) {
-                for (int k = 0; k < VG; ++k)
-                    if (!(fabsf(acc[k]) >= G.guard))
-                        acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
-                                                    (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
+                for (int k = 0; k < VG; ++k) dz[k] = (lk0 + k) * G.fpitch;
+                if (first) {
+#pragma unroll
+                    for (int k = 0; k < VG; ++k) acc[k] = 0.f;
+                } else {
+                    load_group<VG>(out, g * 32 + lane, acc);
+                }
+                for (int i = 0; i < clen; ++i) {
+                    const LocalPrim& P = sp[i];
+                    const int op = P.op;
+                    if (op == CH_OFFSET) {
+#pragma unroll
+                        for (int k = 0; k < VG; ++k) acc[k] -= P.k;
+                        continue;
+                    }
+                    eval_group<VG>(P, dx, dy, dz, v);
+                    combine_group<VG>(op, P.k, acc, v);
+                }
+                if (last) {
+                    // guard band: float64 recheck so the sign never disagrees with the float64 value
+                    bool near = false;
+#pragma unroll
+                    for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
+                    if (near) {
+                        for (int k = 0; k < VG; ++k)
+                            if (!(fabsf(acc[k]) >= G.guard))
+                                acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
+                                                            (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
+                    }
+                }
+                store_group<VG>(out, g * 32 + lane, acc);
             }
-            store_group<VG>(out, g * 32 + lane, acc);
         }
     }
 }
@@ -1123,20 +1155,58 @@ __global__ void k_slot_map_dev(const int32_t* __restrict__ active, const int32_t
 }
 
 // Occupancy (1 where the field is negative) of every voxel: tile values in active blocks, the
-// block kind elsewhere.  Writes 16 voxels per thread along z with one 128-bit store when the row
-// allows it.
-__global__ void k_occupancy(const int32_t* __restrict__ kind, const int32_t* __restrict__ slot,
-                            const float* __restrict__ tiles, int64_t nx, int64_t ny, int64_t nz, int B, int nby,
-                            int nbz, uint8_t* __restrict__ mask) {
-    const int64_t n = nx * ny * nz;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t z = i % nz, y = (i / nz) % ny, x = i / (nz * ny);
-        const int64_t blk = ((x / B) * nby + y / B) * nbz + z / B;
-        const int32_t s = slot[blk];
-        uint8_t v;
-        if (s >= 0) v = tiles[(int64_t)s * B * B * B + ((x % B) * B + (y % B)) * B + (z % B)] < 0.f;
-        else v = kind[blk] < 0;
-        mask[i] = v;
+// block kind elsewhere.  One thread per 16 consecutive z voxels of an (x, y) row: the row's block
+// runs are read as float4 from the tiles (a tile row of B floats is contiguous along z) and the 16
+// bytes leave in one 128-bit store when rows are 16-byte aligned (nz % 16 == 0).
+template <int B>
+__global__ void __launch_bounds__(256) k_occupancy(const int32_t* __restrict__ kind, const int32_t* __restrict__ slot,
+                                                   const float* __restrict__ tiles, int nx, int ny, int nz, int nby,
+                                                   int nbz, uint8_t* __restrict__ mask) {
+    constexpr int kB3 = B * B * B;
+    const int chunks = (nz + 15) >> 4;
+    const int64_t total = (int64_t)nx * ny * chunks;
+    const bool vec = (nz & 15) == 0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / chunks;
+        const int c = (int)(t - row * chunks);
+        const int x = (int)(row / ny), y = (int)(row - (int64_t)x * ny);
+        const int z0 = c << 4;
+        const int64_t blk_row = ((int64_t)(x / B) * nby + y / B) * nbz;
+        const int lxy = ((x % B) * B + (y % B)) * B;
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int seg = 0; seg < 16; seg += (B < 16 ? B : 16)) {
+            const int z = z0 + seg;
+            if (z >= nz) continue;  // (not break: the loop stays fully unrolled, w[] in registers)
+            const int64_t blk = blk_row + z / B;
+            const int32_t s = slot[blk];
+            constexpr int kRun = B < 16 ? B : 16;
+            if (s >= 0) {
+                const float4* src = reinterpret_cast<const float4*>(tiles + (int64_t)s * kB3 + lxy + (z % B));
+#pragma unroll
+                for (int q = 0; q < kRun / 4; ++q) {
+                    const float4 v = src[q];
+                    const int k = seg + 4 * q;  // byte index within the 16
+                    const uint32_t bits = (uint32_t)(v.x < 0.f) | ((uint32_t)(v.y < 0.f) << 8) |
+                                          ((uint32_t)(v.z < 0.f) << 16) | ((uint32_t)(v.w < 0.f) << 24);
+                    w[k >> 2] = bits;
+                }
+            } else {
+                const uint32_t fill = kind[blk] < 0 ? 0x01010101u : 0u;
+#pragma unroll
+                for (int q = 0; q < kRun / 4; ++q) w[(seg >> 2) + q] = fill;
+            }
+        }
+        uint8_t* dst = mask + row * nz + z0;
+        if (vec) {
+            *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        } else {
+            const int n = min(16, nz - z0);
+            for (int k = 0; k < n; ++k) {
+                const uint32_t wk = k < 8 ? (k < 4 ? w[0] : w[1]) : (k < 12 ? w[2] : w[3]);
+                dst[k] = (uint8_t)(wk >> (8 * (k & 3)));
+            }
+        }
     }
 }
 
@@ -1209,21 +1279,31 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
         const int coarse_edge = kSuperEdge * kCoarseDiv;
         // coarse regions from the full chain
         k_cull<<<fb_div_up(G.ncoarse * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, nullptr, nullptr, n_chain, 1,
-                                                               1, 1, S.off, S.len, P.pool_coarse, kCapCoarse,
+                                                               1, 1, S.off, S.len, P.pool_coarse, P.cap_coarse,
                                                                G.S * G.B * kCoarseDiv, G.ncx, G.ncy, G.ncz);
         FB_LAUNCH();
         (void)coarse_edge;
         // superblocks from their coarse region
         k_cull<<<fb_div_up(G.nsuper * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off, S.len, 0, kCoarseDiv,
                                                               G.ncy, G.ncz, S.off + G.ncoarse, S.len + G.ncoarse,
-                                                              P.pool_super, kCapSuper, G.S * G.B, G.nsx, G.nsy, G.nsz);
+                                                              P.pool_super, P.cap_super, G.S * G.B, G.nsx, G.nsy, G.nsz);
         FB_LAUNCH();
         FB_CUDA(cudaMemsetAsync(S.misc, 0, 256, st));
-        k_classify<true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
-            G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
-            S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
+        if (P.warp_blocks) {
+            k_cull_blocks<<<fb_div_up(G.nblocks * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off + G.ncoarse,
+                                                                         S.len + G.ncoarse, S.blk_off, S.blk_len,
+                                                                         S.blk_pool, kCapBlockWarp);
+            FB_LAUNCH();
+            k_classify<true, true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+                G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
+                S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
+        } else {
+            k_classify<true, false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+                G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
+                S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
+        }
     } else {
-        k_classify<false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+        k_classify<false, false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
             G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
             S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
     }
@@ -1421,7 +1501,8 @@ int fb_field_occupancy_device(const int32_t* d_kind, const int32_t* d_active, co
                               const float* d_tiles, int64_t capacity, int64_t nx, int64_t ny, int64_t nz,
                               int32_t block, int32_t* d_slot, uint8_t* d_mask, void* stream) noexcept {
     if (!d_kind || !d_active || !d_count || !d_tiles || !d_slot || !d_mask || nx < 1 || ny < 1 || nz < 1 ||
-        block < 1 || capacity < 0)
+        (block != 4 && block != 8 && block != 16) || capacity < 0 || nx > INT32_MAX || ny > INT32_MAX ||
+        nz > INT32_MAX || (reinterpret_cast<uintptr_t>(d_tiles) & 15) || (reinterpret_cast<uintptr_t>(d_mask) & 15))
         return FB_INVALID;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nby = (int)((ny + block - 1) / block), nbz = (int)((nz + block - 1) / block);
@@ -1429,9 +1510,13 @@ int fb_field_occupancy_device(const int32_t* d_kind, const int32_t* d_active, co
     FB_CUDA(cudaMemsetAsync(d_slot, 0xff, nblocks * 4, st));
     k_slot_map_dev<<<fb_sm_count() * 4, 256, 0, st>>>(d_active, d_count, capacity, d_slot);
     FB_LAUNCH();
-    const int64_t n = nx * ny * nz;
-    k_occupancy<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)fb_sm_count() * 32), 256, 0, st>>>(
-        d_kind, d_slot, d_tiles, nx, ny, nz, block, nby, nbz, d_mask);
+    const int64_t items = nx * ny * ((nz + 15) / 16);
+    const int grid = (int)std::min<int64_t>((items + 255) / 256, (int64_t)fb_sm_count() * 16);
+    switch (block) {
+        case 4: k_occupancy<4><<<grid, 256, 0, st>>>(d_kind, d_slot, d_tiles, (int)nx, (int)ny, (int)nz, nby, nbz, d_mask); break;
+        case 8: k_occupancy<8><<<grid, 256, 0, st>>>(d_kind, d_slot, d_tiles, (int)nx, (int)ny, (int)nz, nby, nbz, d_mask); break;
+        default: k_occupancy<16><<<grid, 256, 0, st>>>(d_kind, d_slot, d_tiles, (int)nx, (int)ny, (int)nz, nby, nbz, d_mask); break;
+    }
     FB_LAUNCH();
     return FB_OK;
 }

@@ -148,7 +148,8 @@ int fb_field_reconstruct_device(const int32_t* d_kind, const int32_t* d_active, 
 
 /* Replaces the solid reconstruction of src/field_engine/faltkarna_v1_mesh_to_sdf.py:695-713
  * (reconstruct_solid_from_sparse) on device-resident fields: uint8 mask, 1 where the field is
- * negative; reads the active count on the device (no synchronisation).  d_slot: n_blocks int32. */
+ * negative; reads the active count on the device (no synchronisation).  d_slot: n_blocks int32.
+ * block is 4, 8 or 16; d_tiles and d_mask are 16-byte aligned (status 1 otherwise). */
 int fb_field_occupancy_device(const int32_t* d_kind, const int32_t* d_active, const int32_t* d_count,
                               const float* d_tiles, int64_t capacity, int64_t nx, int64_t ny, int64_t nz,
                               int32_t block, int32_t* d_slot, uint8_t* d_mask, void* stream);

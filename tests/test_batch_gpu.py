@@ -72,3 +72,37 @@ def test_autotuner_times_each_bucket(tmp_path):
         assert entry["block"] == min((int(b) for b in entry["ms"]), key=lambda b: entry["ms"][str(b)])
     again = BT.Autotuner(tmp_path / "tune.json")
     assert again.table == tuner.table
+
+
+@pytest.mark.parametrize("block,shape", [(4, (37, 41, 45)), (8, (64, 72, 80)), (16, (50, 33, 96)), (8, (40, 40, 29))])
+def test_occupancy_matches_the_host_layout(block, shape):
+    """The device occupancy mask equals the one read off the host SparseField: tile values < 0 in
+    active blocks, kind == -1 elsewhere; ragged grids (rows not a multiple of 16) included."""
+    import torch
+    import field_b200._lib as L
+    import field_b200.build as FB
+    import field_b200.recipes as R
+    import field_b200.expr as X
+    from field_b200.grid import GridMeta
+    rng = np.random.default_rng(block + shape[2])
+    nx, ny, nz = shape
+    meta = GridMeta(0.0, 0.0, 0.0, 1.0 / max(shape), nx, ny, nz, block)
+    comp = X.compile_recipe(X.union_all(R.parts(rng, 6, 6, 4, 4, scale=0.8)))
+    fb = FB.FieldBuilder(comp, meta)
+    field = fb.build()
+    slot = torch.empty(meta.n_blocks, dtype=torch.int32, device="cuda")
+    mask = torch.empty(shape, dtype=torch.uint8, device="cuda")
+    L.check(L.lib().fb_field_occupancy_device(field.kind.data_ptr(), field.active.data_ptr(), field.count.data_ptr(),
+                                              field.tiles.data_ptr(), max(field.n_active, 1), nx, ny, nz, block,
+                                              slot.data_ptr(), mask.data_ptr(), L.stream_handle()), "occupancy")
+    sf = field.to_host()
+    nbx, nby, nbz = meta.n_bx, meta.n_by, meta.n_bz
+    pad = np.repeat(np.repeat(np.repeat((sf.kind.reshape(nbx, nby, nbz) < 0).astype(np.uint8), block, 0), block, 1),
+                    block, 2)
+    for t, blk in enumerate(sf.active_ids):
+        bi, rem = divmod(int(blk), nby * nbz)
+        bj, bk = divmod(rem, nbz)
+        pad[bi * block:(bi + 1) * block, bj * block:(bj + 1) * block, bk * block:(bk + 1) * block] = sf.tiles[t] < 0
+    want = pad[:nx, :ny, :nz]
+    assert 0 < want.sum() < want.size
+    assert np.array_equal(mask.cpu().numpy(), want)
