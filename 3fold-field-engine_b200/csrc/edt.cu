@@ -4,15 +4,15 @@
 //   1. k_edt_bits  : the uint8 mask becomes one 32-bit word per 32 z-samples of every (x, y) line
 //                    (1 B read + 1/8 B written per voxel); the same pass validates the mask
 //                    (values 0/1, both classes present) with warp-aggregated counters.
-//   2. k_edt_zy    : one CTA per (32-wide z chunk, x plane, polarity).  For every y line it finds
-//                    the nearest site along z from the line's bit words (clz/ffs over the chunk's
-//                    own word, a ballot over the other words), stages dz^2 for the chunk in shared
-//                    memory, then runs the y pass there: g(y,z) = min_y' dz(y',z)^2 + (y-y')^2 by a
-//                    window search that stops once t^2 >= best.  Writes int32 g (4 B/voxel).
-//   3. k_edt_x     : one CTA per (z chunk, y row, polarity): stages the nx x 32 column block of g
-//                    in shared memory with coalesced 128 B rows, runs the same window search along
-//                    x and writes the final int32 (4 B/voxel) -- or, in the paired form, both
-//                    polarities at once plus the correctly rounded signed float32 distance.
+//   2. k_edt_zy    : one CTA per (32-wide z chunk, x plane, polarity), lanes = z columns.  For every
+//                    y line it finds the nearest site along z from the line's bit words (clz/ffs over
+//                    the chunk's own word, a ballot over the other words) and runs the y pass
+//                    g(y,z) = min_y' dz(y',z)^2 + (y-y')^2 as an exact lower envelope (below), banded
+//                    over the CTA's warps.  Writes int32 g (4 B/voxel).
+//   3. k_edt_x     : one CTA per (z chunk, y row, polarity): streams the nx x 32 column block of g
+//                    with coalesced 128 B rows into the same envelope along x and writes the final
+//                    int32 (4 B/voxel); the paired form runs both polarities, then k_edt_signed
+//                    turns the two squared distances into the correctly rounded signed float32.
 // Global traffic per voxel and polarity: 1 (mask) + 4 + 4 (g round trip) + 4 (output) + 1/4 (bit
 // words, mostly L2) bytes -- the 13 B/voxel algorithmic figure.
 //
@@ -28,8 +28,7 @@
 
 namespace {
 
-constexpr int kMaxAxis = 512;            // shared-memory staging holds 512 x 32 int32 per polarity
-constexpr int kThreads = 512;
+constexpr int kMaxAxis = 512;            // hull entries pack a site index < 2^11 and c < 2^21; smem holds 512 x 32
 
 struct Counters {
     unsigned long long ones;     // mask bytes equal to 1
@@ -87,104 +86,264 @@ __global__ void __launch_bounds__(256) k_edt_bits(const uint8_t* __restrict__ ma
 }
 
 // ------------------------------------------------------------------------------------------
-// Exact 1-D min-plus along a staged column, out(q) = min_s col(s) + (q - s)^2.
+// Exact 1-D min-plus along a column, out(q) = min_s f(s) + (q - s)^2, by lower envelopes.
 //
-// The smallest minimiser s*(q) is non-decreasing in q (for q1 < q2 a smaller minimiser of q2
-// would contradict the minimality of s*(q1); the squares' cross terms decide it).  So:
-//   step A: every kSample-th target q gets (value, smallest minimiser) by a window search that
-//           stops once t^2 exceeds the best value (no farther source can tie or win);
-//   step B: every other target scans only [s*(q_a), s*(q_b)] between its two sampled neighbours,
-//           all targets of an interval sharing each loaded source.
-// Both steps are exact; the cost is ~window/kSample + interval width per target instead of
-// ~2*window per target.
+// Site s contributes the parabola P_s(q) = c_s - 2 q s + q^2 with c_s = f(s) + s^2, so out(q) is the
+// lower envelope of lines c_s - 2 q s plus q^2: the sites that matter are the vertices of the lower
+// convex hull of the points (s, c_s), and site b between a and u is never strictly lowest exactly
+// when (c_b - c_a)(u - b) >= (c_u - c_b)(b - a) -- an integer test, no division (the reference's
+// envelope intersects parabolas with floor division instead, edt_persistent_pair_v1/edt.cu:12-29).
+// Sites with no finite value (the sentinel) never win against a finite one and are left out.
+//
+// A CTA owns 32 adjacent columns (lanes) over the whole axis; its kBandWarps warps split the axis
+// into bands:
+//   1. build : each warp runs the hull stack over its band's sites, one stack per lane, in shared
+//              memory at the band's own rows (a band never holds more entries than rows);
+//   2. merge : pairwise joins of band groups in log2(kBandWarps) rounds -- the bridge between two
+//              x-separated lower hulls trims a suffix of the left one and a prefix of the right one --
+//              leaving each band a contiguous surviving range [lo, hi];
+//   3. output: each warp finds the hull vertex covering its first target (band scan + binary search)
+//              and walks the hull forward over its targets, one compare per step.
+// Values are exact integers: c < 2^20 and |products| < 2^29 for axes up to 512.
 // ------------------------------------------------------------------------------------------
-constexpr int kSample = 8;
+constexpr int kBandWarps = 8;
+constexpr int kBandThreads = 32 * kBandWarps;
 
-// (value, smallest minimiser) at q; col is this lane's column (stride 32 in shared memory).
-__device__ __forceinline__ int32_t window_argmin(const int32_t* col, int q, int len, int& arg) {
-    int32_t best = col[q * 32];
-    int bi = q;
-    for (int t = 1; t < len; ++t) {
-        const int32_t tt = t * t;
-        if (tt > best) break;
-        const int lo = q - t, hi = q + t;
-        if (lo < 0 && hi >= len) break;
-        if (hi < len) {  // a larger index wins only when strictly better
-            const int32_t v = col[hi * 32] + tt;
-            if (v < best) { best = v; bi = hi; }
-        }
-        if (lo >= 0) {   // a smaller index wins ties
-            const int32_t v = col[lo * 32] + tt;
-            if (v <= best) { best = v; bi = lo; }
-        }
-    }
-    arg = bi;
-    return best;
+__device__ __forceinline__ uint32_t pack_site(int v, int c) { return ((uint32_t)v << 21) | (uint32_t)c; }
+__device__ __forceinline__ int site_v(uint32_t e) { return (int)(e >> 21); }
+__device__ __forceinline__ int site_c(uint32_t e) { return (int)(e & 0x1fffffu); }
+
+// Middle site b of a < b < u is never strictly below both neighbours' parabolas.
+__device__ __forceinline__ bool hidden(uint32_t a, uint32_t b, uint32_t u) {
+    const int va = site_v(a), vb = site_v(b), vu = site_v(u);
+    const int ca = site_c(a), cb = site_c(b), cu = site_c(u);
+    return (cb - ca) * (vu - vb) >= (cu - cb) * (vb - va);
 }
 
-// One column pass over a shared-memory block col[len][32]; lanes are columns, warps split the
-// targets.  `sidx` is shared scratch of ceil(len / kSample) * 32 int16.  `store(q, v)` receives
-// every result.  Contains a __syncthreads(): every thread of the CTA must call it.
-template <typename Store>
-__device__ __forceinline__ void column_pass(const int32_t* col, int16_t* sidx, int len, Store store) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int nsamp = (len + kSample - 1) / kSample;
-    for (int m = warp; m < nsamp; m += nwarps) {
-        int arg;
-        const int32_t v = window_argmin(col + lane, m * kSample, len, arg);
-        sidx[m * 32 + lane] = (int16_t)arg;
-        store(m * kSample, v);
+// P_next(q) <= P_cur(q) for sites cur < next: the hull walk moves on.
+__device__ __forceinline__ bool next_wins(uint32_t cur, uint32_t nxt, int q) {
+    return site_c(nxt) - site_c(cur) <= 2 * q * (site_v(nxt) - site_v(cur));
+}
+
+// Shared layout of a band pass over an axis of length n: hull[n][32] entries, then per band and
+// lane the entry count and the surviving range.
+struct BandSmem {
+    uint32_t* hull;
+    int* cnt;
+    int* lo;
+    int* hi;
+};
+
+__device__ __forceinline__ BandSmem band_smem(void* base, int n) {
+    BandSmem b;
+    b.hull = static_cast<uint32_t*>(base);
+    b.cnt = reinterpret_cast<int*>(b.hull + n * 32);
+    b.lo = b.cnt + kBandWarps * 32;
+    b.hi = b.lo + kBandWarps * 32;
+    return b;
+}
+
+__host__ __device__ __forceinline__ int band_rows(int n) { return (n + kBandWarps - 1) / kBandWarps; }
+
+int band_smem_bytes(int n) { return n * 32 * 4 + 3 * kBandWarps * 32 * 4; }
+
+// Hull stack of one lane over the rows of one band: entries in shared memory at the band's rows,
+// the top two also unpacked in registers.
+struct HullStack {
+    uint32_t* base;  // &hull[row0 * 32 + lane]
+    int top;         // index of the top entry, -1 when empty
+    int v0, c0, v1, c1;  // second and top entry
+
+    __device__ __forceinline__ HullStack(uint32_t* hull, int row0, int lane)
+        : base(hull + row0 * 32 + lane), top(-1), v0(0), c0(0), v1(0), c1(0) {}
+
+    // push site (v, c); sites arrive in increasing v
+    __device__ __forceinline__ void push(int v, int c) {
+        while (top >= 1 && (c1 - c0) * (v - v1) >= (c - c1) * (v1 - v0)) {
+            --top;
+            v1 = v0;
+            c1 = c0;
+            if (top >= 1) {
+                const uint32_t e = base[(top - 1) * 32];
+                v0 = site_v(e);
+                c0 = site_c(e);
+            }
+        }
+        ++top;
+        base[top * 32] = pack_site(v, c);
+        v0 = v1;
+        c0 = c1;
+        v1 = v;
+        c1 = c;
+    }
+};
+
+__device__ __forceinline__ bool band_live(const BandSmem& sm, int b, int lane) {
+    return sm.hi[b * 32 + lane] >= sm.lo[b * 32 + lane];
+}
+
+// Phase 2: pairwise joins of band groups in log2(kBandWarps) rounds (warp j joins group j of the
+// round), each the bridge between two x-separated lower hulls: trim the left group's suffix and the
+// right group's prefix until the junction is convex.  Every band ends with a surviving range [lo, hi]
+// (empty when hi < lo); the ranges in band order are the column's lower hull.  Contains
+// __syncthreads(): every thread of the CTA calls it.
+__device__ void hull_merge(const BandSmem& sm, int n) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rows = band_rows(n);
+    sm.lo[warp * 32 + lane] = 0;
+    sm.hi[warp * 32 + lane] = sm.cnt[warp * 32 + lane] - 1;
+    for (int half = 1; half < kBandWarps; half *= 2) {
+        __syncthreads();
+        const int a = warp * 2 * half, m = a + half, e = min(kBandWarps, a + 2 * half);
+        if (m < kBandWarps) {
+            int L = m - 1;
+            while (L >= a && !band_live(sm, L, lane)) --L;
+            int R = m;
+            while (R < e && !band_live(sm, R, lane)) ++R;
+            if (L >= a && R < e) {
+                // every step removes one entry: the loop ends within n steps
+                for (int step = 0; step <= n; ++step) {
+                    const int hiL = sm.hi[L * 32 + lane], loR = sm.lo[R * 32 + lane];
+                    const uint32_t e1 = sm.hull[(L * rows + hiL) * 32 + lane];
+                    const uint32_t r0 = sm.hull[(R * rows + loR) * 32 + lane];
+                    int pb = L, pi = hiL - 1;
+                    if (pi < sm.lo[L * 32 + lane]) {
+                        pb = L - 1;
+                        while (pb >= a && !band_live(sm, pb, lane)) --pb;
+                        pi = pb >= a ? sm.hi[pb * 32 + lane] : -1;
+                    }
+                    if (pb >= a && hidden(sm.hull[(pb * rows + pi) * 32 + lane], e1, r0)) {
+                        sm.hi[L * 32 + lane] = hiL - 1;
+                        if (hiL - 1 < sm.lo[L * 32 + lane]) L = pb;
+                        continue;
+                    }
+                    int sb = R, si = loR + 1;
+                    if (si > sm.hi[R * 32 + lane]) {
+                        sb = R + 1;
+                        while (sb < e && !band_live(sm, sb, lane)) ++sb;
+                        si = sb < e ? sm.lo[sb * 32 + lane] : -1;
+                    }
+                    if (sb < e && hidden(e1, r0, sm.hull[(sb * rows + si) * 32 + lane])) {
+                        sm.lo[R * 32 + lane] = loR + 1;
+                        if (loR + 1 > sm.hi[R * 32 + lane]) R = sb;
+                        continue;
+                    }
+                    break;
+                }
+            }
+        }
     }
     __syncthreads();
-    for (int m = warp; m < nsamp; m += nwarps) {
-        const int q0 = m * kSample;
-        const int nt = min(kSample - 1, len - 1 - q0);  // targets q0+1 .. q0+nt
-        if (nt <= 0) continue;
-        const int lo = sidx[m * 32 + lane];
-        const int hi = m + 1 < nsamp ? sidx[(m + 1) * 32 + lane] : len - 1;
-        int32_t best[kSample - 1];
-#pragma unroll
-        for (int i = 0; i < kSample - 1; ++i) best[i] = 0x7fffffff;
-        for (int s = lo; s <= hi; ++s) {
-            const int32_t f = col[s * 32 + lane];
-            const int d = q0 + 1 - s;
-#pragma unroll
-            for (int i = 0; i < kSample - 1; ++i) best[i] = min(best[i], f + (d + i) * (d + i));
+}
+
+// Phase 3 for targets [q0, q1) of one warp: store(q, value) for each; lanes whose column has no site
+// store `sentinel`.
+template <typename Store>
+__device__ __forceinline__ void hull_output(const BandSmem& sm, int n, int q0, int q1, int32_t sentinel, Store store) {
+    const int lane = threadIdx.x & 31;
+    const int rows = band_rows(n);
+    if (q0 >= q1) return;
+    int b = 0;
+    while (b < kBandWarps && !band_live(sm, b, lane)) ++b;
+    if (b == kBandWarps) {
+        for (int q = q0; q < q1; ++q) store(q, sentinel);
+        return;
+    }
+    // band holding the vertex that covers q0: the first band whose last surviving entry is not
+    // beaten at q0 by the next surviving band's first one
+    for (;;) {
+        int nb = b + 1;
+        while (nb < kBandWarps && !band_live(sm, nb, lane)) ++nb;
+        if (nb == kBandWarps) break;
+        if (!next_wins(sm.hull[(b * rows + sm.hi[b * 32 + lane]) * 32 + lane],
+                       sm.hull[(nb * rows + sm.lo[nb * 32 + lane]) * 32 + lane], q0))
+            break;
+        b = nb;
+    }
+    // binary search inside band b: the first index whose successor does not win at q0
+    int lo = sm.lo[b * 32 + lane], hi = sm.hi[b * 32 + lane];
+    const uint32_t* band = sm.hull + b * rows * 32 + lane;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (next_wins(band[mid * 32], band[(mid + 1) * 32], q0)) lo = mid + 1;
+        else hi = mid;
+    }
+    // walk: cur = (vc, cc); successor (vn, cn) at index i of band b (has == false past the end)
+    const uint32_t e = band[lo * 32];
+    int vc = site_v(e), cc = site_c(e);
+    int i = lo, bhi = sm.hi[b * 32 + lane];
+    int vn = 0, cn = 0;
+    bool has = true;
+    auto load_next = [&]() {
+        if (i < bhi) {
+            ++i;
+        } else {
+            int k = b + 1;
+            while (k < kBandWarps && !band_live(sm, k, lane)) ++k;
+            if (k == kBandWarps) { has = false; return; }
+            b = k;
+            band = sm.hull + b * rows * 32 + lane;
+            i = sm.lo[b * 32 + lane];
+            bhi = sm.hi[b * 32 + lane];
         }
-#pragma unroll
-        for (int i = 0; i < kSample - 1; ++i)
-            if (i < nt) store(q0 + 1 + i, best[i]);
+        const uint32_t x = band[i * 32];
+        vn = site_v(x);
+        cn = site_c(x);
+    };
+    load_next();
+    for (int q = q0; q < q1; ++q) {
+        while (has && cn - cc <= 2 * q * (vn - vc)) {
+            vc = vn;
+            cc = cn;
+            load_next();
+        }
+        store(q, cc + q * (q - 2 * vc));
     }
 }
 
-// z pass (from bit words) + y pass.  grid = (W, nx, polarities); dynamic smem = ny * 32 * 4 bytes.
-// Polarity p measures to set bits when (p ^ invert) == 0, to clear bits otherwise.
-__global__ void __launch_bounds__(kThreads) k_edt_zy(const uint32_t* __restrict__ bits, int32_t* __restrict__ g,
-                                                     int nx, int ny, int nz, int W, int invert, int32_t sentinel) {
-    extern __shared__ int32_t col[];  // [ny][32]
+// z pass (nearest set bit along z from the bit words) + y pass.  grid = (W, nx, polarities),
+// block = kBandThreads, dynamic smem = band_smem_bytes(ny).  Polarity p measures to set bits when
+// (p ^ invert) == 0, to clear bits otherwise.
+__global__ void __launch_bounds__(kBandThreads) k_edt_zy(const uint32_t* __restrict__ bits, int32_t* __restrict__ g,
+                                                         int nx, int ny, int nz, int W, int invert, int32_t sentinel) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BandSmem sm = band_smem(smem_raw, ny);
     const int w = blockIdx.x, x = blockIdx.y, pol = blockIdx.z;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool flip = (pol ^ invert) != 0;
     const int tail = nz & 31;
     const uint32_t last_valid = tail ? ((1u << tail) - 1u) : 0xffffffffu;
     const int z = 32 * w + lane;
-    for (int y = warp; y < ny; y += nwarps) {
-        uint32_t word = 0;
-        if (lane < W) {
-            word = bits[((int64_t)x * ny + y) * W + lane];
-            if (flip) word = ~word;
-            if (lane == W - 1) word &= last_valid;
-        }
-        const uint32_t nonzero = __ballot_sync(0xffffffffu, word != 0);
-        const uint32_t own = __shfl_sync(0xffffffffu, word, w);
-        const uint32_t below = nonzero & ((1u << w) - 1u);
-        const uint32_t above = nonzero & ~((2u << w) - 1u);
-        const int pw = below ? 31 - __clz(below) : 0;
-        const int nw = above ? __ffs(above) - 1 : 0;
-        const uint32_t prev_word = __shfl_sync(0xffffffffu, word, pw);
-        const uint32_t next_word = __shfl_sync(0xffffffffu, word, nw);
-        int32_t value = sentinel;
-        if (nonzero) {
+    const int rows = band_rows(ny);
+    const int y0 = warp * rows, y1 = min(ny, y0 + rows);
+    // 1. nearest site along z for each row of the band, pushed onto the lane's hull stack
+    HullStack st(sm.hull, y0, lane);
+    const uint32_t* line = bits + ((int64_t)x * ny + y0) * W + lane;  // row y0's words, one per lane < W
+    const bool loads = lane < W;
+    constexpr int kAhead = 4;  // rows of bit words in flight ahead of the stack work
+    uint32_t ring[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) ring[k] = (loads && y0 + k < y1) ? line[k * W] : 0u;
+    for (int yb = y0; yb < y1; yb += kAhead) {
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+            const int y = yb + k;
+            uint32_t word = ring[k];
+            ring[k] = (loads && y + kAhead < y1) ? line[(y + kAhead - y0) * W] : 0u;
+            if (y >= y1) break;
+            if (loads) {
+                if (flip) word = ~word;
+                if (lane == W - 1) word &= last_valid;
+            }
+            const uint32_t nonzero = __ballot_sync(0xffffffffu, word != 0);
+            if (!nonzero) continue;  // no site on this line (uniform across the warp)
+            const uint32_t own = __shfl_sync(0xffffffffu, word, w);
+            const uint32_t below = nonzero & ((1u << w) - 1u);
+            const uint32_t above = nonzero & ~((2u << w) - 1u);
+            const int pw = below ? 31 - __clz(below) : 0;
+            const int nw = above ? __ffs(above) - 1 : 0;
+            const uint32_t prev_word = __shfl_sync(0xffffffffu, word, pw);
+            const uint32_t next_word = __shfl_sync(0xffffffffu, word, nw);
             const uint32_t low = own & (0xffffffffu >> (31 - lane));
             const uint32_t high = own & (0xffffffffu << lane);
             int prev = -(1 << 20), next = 1 << 20;
@@ -193,17 +352,52 @@ __global__ void __launch_bounds__(kThreads) k_edt_zy(const uint32_t* __restrict_
             if (high) next = 32 * w + __ffs(high) - 1;
             else if (above) next = 32 * nw + __ffs(next_word) - 1;
             const int d = min(z - prev, next - z);
-            value = d * d;
+            st.push(y, d * d + y * y);
         }
-        col[y * 32 + lane] = value;
     }
-    __syncthreads();
-    int32_t* out = g + (int64_t)pol * nx * ny * nz;
-    int16_t* sidx = reinterpret_cast<int16_t*>(col + ny * 32);
+    sm.cnt[warp * 32 + lane] = st.top + 1;
+    hull_merge(sm, ny);
+    if (z >= nz) return;
+    int32_t* out = g + (int64_t)pol * nx * ny * nz + ((int64_t)x * ny) * nz + z;
+    hull_output(sm, ny, y0, y1, sentinel, [&](int y, int32_t v) { out[(int64_t)y * nz] = v; });
+}
+
+// x pass.  grid = (W, ny, polarities), block = kBandThreads, dynamic smem = band_smem_bytes(nx).
+// Reads g (polarity-major, `size` voxels each) and writes out with the same layout; out may be g
+// itself (each CTA reads its whole column block before it writes any of it).
+__global__ void __launch_bounds__(kBandThreads) k_edt_x(const int32_t* g, int32_t* out, int nx, int ny, int nz,
+                                                        int32_t sentinel) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BandSmem sm = band_smem(smem_raw, nx);
+    const int w = blockIdx.x, y = blockIdx.y, pol = blockIdx.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int z = 32 * w + lane;
     const bool live = z < nz;
-    column_pass(col, sidx, ny, [&](int y, int32_t v) {
-        if (live) out[((int64_t)x * ny + y) * nz + z] = v;
-    });
+    const int64_t size = (int64_t)nx * ny * nz;
+    const int64_t col = (int64_t)pol * size + (int64_t)y * nz + z;
+    const int64_t stride = (int64_t)ny * nz;
+    const int rows = band_rows(nx);
+    const int x0 = warp * rows, x1 = min(nx, x0 + rows);
+    HullStack st(sm.hull, x0, lane);
+    constexpr int kAhead = 8;  // loads in flight ahead of the stack work
+    int32_t buf[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) buf[k] = (live && x0 + k < x1) ? g[col + (int64_t)(x0 + k) * stride] : sentinel;
+    for (int xb = x0; xb < x1; xb += kAhead) {
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+            const int xx = xb + k;
+            const int32_t f = buf[k];
+            const int xn = xx + kAhead;
+            buf[k] = (live && xn < x1) ? g[col + (int64_t)xn * stride] : sentinel;
+            if (xx < x1 && f < sentinel) st.push(xx, f + xx * xx);
+        }
+    }
+    sm.cnt[warp * 32 + lane] = st.top + 1;
+    hull_merge(sm, nx);
+    if (!live) return;
+    int32_t* dst = out + col;
+    hull_output(sm, nx, x0, x1, sentinel, [&](int x, int32_t v) { dst[(int64_t)x * stride] = v; });
 }
 
 // Correctly rounded signed distance of one voxel from its two squared distances, the reference's
@@ -216,48 +410,12 @@ __device__ __forceinline__ float signed_from_pair(int32_t sq_out, int32_t sq_in,
     return __fsub_rn(delta, __fmul_rn(sign, half));
 }
 
-// x pass.  grid = (W, ny, npol_launch); dynamic smem = npol_stage * nx * 32 * 4 bytes.
-// paired == 0: one polarity per CTA (blockIdx.z), writes int32 squared distances to out.
-// paired == 1: both polarities in one CTA; writes the signed float32 distance and, if squared is
-//              non-null, both squared arrays (polarity-major).
-__global__ void __launch_bounds__(kThreads) k_edt_x(const int32_t* __restrict__ g, int32_t* __restrict__ out,
-                                                    float* __restrict__ signed_out, int nx, int ny, int nz,
-                                                    int paired, double pitch, float half) {
-    // shared: col[npol][nx][32], then (paired) res0[nx][32], then sidx
-    extern __shared__ int32_t col[];
-    const int w = blockIdx.x, y = blockIdx.y;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int z = 32 * w + lane;
-    const bool live = z < nz;
-    const int64_t size = (int64_t)nx * ny * nz;
-    const int npol = paired ? 2 : 1;
-    const int pol0 = paired ? 0 : blockIdx.z;
-    for (int p = 0; p < npol; ++p) {
-        const int32_t* src = g + (int64_t)(pol0 + p) * size;
-        for (int x = warp; x < nx; x += nwarps)
-            col[(p * nx + x) * 32 + lane] = live ? src[((int64_t)x * ny + y) * nz + z] : 0;
-    }
-    int32_t* res0 = col + npol * nx * 32;
-    int16_t* sidx = reinterpret_cast<int16_t*>(res0 + (paired ? nx * 32 : 0));
-    __syncthreads();
-    if (!paired) {
-        int32_t* dst = out + (int64_t)pol0 * size;
-        column_pass(col, sidx, nx, [&](int x, int32_t v) {
-            if (live) dst[((int64_t)x * ny + y) * nz + z] = v;
-        });
-        return;
-    }
-    column_pass(col, sidx, nx, [&](int x, int32_t v) {
-        res0[x * 32 + lane] = v;
-        if (live && out) out[((int64_t)x * ny + y) * nz + z] = v;
-    });
-    __syncthreads();
-    column_pass(col + nx * 32, sidx, nx, [&](int x, int32_t v) {
-        if (!live) return;
-        const int64_t i = ((int64_t)x * ny + y) * nz + z;
-        signed_out[i] = signed_from_pair(res0[x * 32 + lane], v, pitch, half);
-        if (out) out[size + i] = v;
-    });
+// Signed float32 distance of every voxel from the two polarities' squared distances (sq[0]: to the
+// nonzero voxels, sq[1]: to the zero voxels).
+__global__ void __launch_bounds__(256) k_edt_signed(const int32_t* __restrict__ sq, float* __restrict__ out,
+                                                    int64_t size, double pitch, float half) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < size; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = signed_from_pair(sq[i], sq[size + i], pitch, half);
 }
 
 bool shape_ok(int nx, int ny, int nz) {
@@ -277,15 +435,11 @@ int64_t scratch_bytes(int nx, int ny, int nz, int npol) {
     return 256 + bits + (int64_t)npol * size * 4;
 }
 
-int sidx_bytes(int len) { return (len + kSample - 1) / kSample * 32 * 2; }
-
 int configure_once() {
     static int done = 0;
     if (done) return FB_OK;
-    FB_CUDA(cudaFuncSetAttribute(k_edt_zy, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kMaxAxis * 32 * 4 + sidx_bytes(kMaxAxis)));
-    FB_CUDA(cudaFuncSetAttribute(k_edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 3 * kMaxAxis * 32 * 4 + sidx_bytes(kMaxAxis)));
+    FB_CUDA(cudaFuncSetAttribute(k_edt_zy, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes(kMaxAxis)));
+    FB_CUDA(cudaFuncSetAttribute(k_edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes(kMaxAxis)));
     done = 1;
     return FB_OK;
 }
@@ -315,16 +469,17 @@ int enqueue(const uint8_t* d_mask, int nx, int ny, int nz, int paired, int sites
     const int32_t sentinel = sentinel_of(nx, ny, nz);
     // Single polarity measuring to zero bytes = the set bits flipped.
     const int invert = paired ? 0 : (sites_nonzero ? 0 : 1);
-    k_edt_zy<<<dim3(W, nx, npol), kThreads, ny * 32 * 4 + sidx_bytes(ny), stream>>>(bits, g, nx, ny, nz, W, invert,
-                                                                                     sentinel);
+    k_edt_zy<<<dim3(W, nx, npol), kBandThreads, band_smem_bytes(ny), stream>>>(bits, g, nx, ny, nz, W, invert, sentinel);
     FB_LAUNCH();
-    const float half = (float)(0.5 * pitch);
     if (paired) {
-        k_edt_x<<<dim3(W, ny, 1), kThreads, 3 * nx * 32 * 4 + sidx_bytes(nx), stream>>>(g, out_sq, out_signed, nx, ny,
-                                                                                         nz, 1, pitch, half);
+        // both polarities' x passes into the squared output (or in place), then the signed values
+        int32_t* sq = out_sq ? out_sq : g;
+        k_edt_x<<<dim3(W, ny, 2), kBandThreads, band_smem_bytes(nx), stream>>>(g, sq, nx, ny, nz, sentinel);
+        FB_LAUNCH();
+        const int grid = (int)std::min<int64_t>((size + 255) / 256, (int64_t)sms * 16);
+        k_edt_signed<<<grid, 256, 0, stream>>>(sq, out_signed, size, pitch, (float)(0.5 * pitch));
     } else {
-        k_edt_x<<<dim3(W, ny, 1), kThreads, nx * 32 * 4 + sidx_bytes(nx), stream>>>(g, out_sq, nullptr, nx, ny, nz, 0,
-                                                                                     pitch, half);
+        k_edt_x<<<dim3(W, ny, 1), kBandThreads, band_smem_bytes(nx), stream>>>(g, out_sq, nx, ny, nz, sentinel);
     }
     FB_LAUNCH();
     (void)size;
