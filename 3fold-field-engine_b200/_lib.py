@@ -52,8 +52,8 @@ SIGNATURES = {
     "fb_copy_device": (I, [P, P, I64, P]),
     # queries
     "fb_query_prepare": (I, [P, I, P, P]),
-    "fb_field_accel": (I, [P, I, I, P, P, P, P, P, P, P]),
-    "fb_query_points_device": (I, [P, P, I, I, P, P, P, P, P, P, I64, D, P, P, P]),
+    "fb_field_accel": (I, [P, I, I, P, P, P, P, P, P, P, P, P]),
+    "fb_query_points_device": (I, [P, P, I, I, P, P, P, P, P, P, P, P, P, I64, I, P, I64, D, P, P, P]),
     "fb_multires_tiles_device": (I, [P, P, I, I, P, P, D, I, P, P, P, P, I64, P, P, P, F, P, P]),
     "fb_multires_query_device": (I, [P, D, I, P, D, P, P, P, P, P, I64, P, P, P]),
 }

@@ -112,12 +112,21 @@ class FieldBuilder:
         nbytes = self.lib.fb_field_scratch_bytes(ct.addressof(self.geom), self.n_prims, self.n_chain)
         if nbytes < 0:
             raise ValueError("grid outside the build contract")
-        self.scratch = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+        # one device allocation carved into the outputs and the scratch (256-byte aligned parts);
+        # count[0] is written by every classification, so nothing needs clearing here
         nb = meta.n_blocks
-        self.kind = torch.empty(nb, dtype=torch.int32, device=self.device)
-        self.cma = torch.empty(nb, dtype=torch.float32, device=self.device)
-        self.active = torch.empty(nb, dtype=torch.int32, device=self.device)
-        self.count = torch.zeros(1, dtype=torch.int32, device=self.device)
+        part = lambda n: (n + 255) // 256 * 256
+        sizes = (part(nb * 4), part(nb * 4), part(nb * 4), 256, part(int(nbytes)))
+        self.slab = torch.empty(sum(sizes), dtype=torch.uint8, device=self.device)
+        views, at = [], 0
+        for size in sizes:
+            views.append(self.slab[at:at + size])
+            at += size
+        self.kind = views[0][:nb * 4].view(torch.int32)
+        self.cma = views[1][:nb * 4].view(torch.float32)
+        self.active = views[2][:nb * 4].view(torch.int32)
+        self.count = views[3][:4].view(torch.int32)
+        self.scratch = views[4][:int(nbytes)]
 
     def _args(self):
         return (ct.addressof(self.geom), self.prims.data_ptr(), self.n_prims, self.chain.data_ptr(), self.n_chain,

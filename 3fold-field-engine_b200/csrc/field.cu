@@ -1477,11 +1477,12 @@ int fb_query_prepare(const FbPrim* d_prims, int32_t n_prims, void* d_primf, void
     return FB_OK;
 }
 
-// Device addresses of a classification's superblock lists inside its scratch (for accelerated
-// point queries): pool base, per-superblock offsets and lengths.
+// Device addresses of a classification's culling lists inside its scratch (for accelerated point
+// queries): superblock pool base, offsets and lengths; per-block offsets, lengths and pool, the
+// pool's capacity, and whether every block has a list (else only blocks of kind 0).
 int fb_field_accel(const FbGeom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, const void** pool,
                    const int64_t** sb_off, const int32_t** sb_len, const int32_t** blk_off, const int32_t** blk_len,
-                   const uint32_t** blk_pool) noexcept {
+                   const uint32_t** blk_pool, int64_t* blk_cap, int32_t* blk_all) noexcept {
     if (!g || !geom_ok(*g) || !d_scratch || n_prims < 1 || n_chain < 1) return FB_INVALID;
     const Geo G = make_geo(*g);
     const Plan P = make_plan(G, n_prims, n_chain);
@@ -1492,6 +1493,8 @@ int fb_field_accel(const FbGeom* g, int32_t n_prims, int32_t n_chain, const void
     if (blk_off) *blk_off = reinterpret_cast<const int32_t*>(b + P.blk_off);
     if (blk_len) *blk_len = reinterpret_cast<const int32_t*>(b + P.blk_len);
     if (blk_pool) *blk_pool = reinterpret_cast<const uint32_t*>(b + P.blk_pool);
+    if (blk_cap) *blk_cap = P.blk_cap;
+    if (blk_all) *blk_all = P.warp_blocks ? 1 : 0;  // every block has a list (else only kind == 0 blocks)
     return FB_OK;
 }
 

@@ -2,9 +2,10 @@
 //
 // Recipes (src/field_engine/ikarus_v1/eval_warp.py:478-488 eval_batch, :718-733 gradient_batch):
 //   k_eval_points evaluates the compiled program at float32 points (thread per point).  With a
-//   built field's culling lists (the superblock lists a classification left in its scratch) each
-//   point inside the grid walks only its superblock's list -- exact for every point of that
-//   superblock, by the same strict-domination argument as the build -- instead of the whole chain.
+//   built field's culling lists (the lists a classification left in its scratch) each point inside
+//   the grid walks only its block's list where the classification kept one, else its superblock's
+//   -- exact for every point of that region, by the same strict-domination argument as the build --
+//   instead of the whole chain.
 //   k_gradient_points: central differences with step h along each axis, the six offset points
 //   formed in float64 and rounded to float32 as the reference does.
 // Per-block pitch fields (src/field_engine/faltkarna_v1_multires.py:84-104, :384-459):
@@ -51,10 +52,17 @@ __device__ float eval_point(const PrimF* __restrict__ primf, const FbInsn* __res
     return sp == 1 ? st[0] : __int_as_float(0x7fc00000);
 }
 
-struct Accel {  // a built field's superblock lists (nullptr pool: walk the whole chain)
+struct Accel {  // a built field's culling lists (nullptr pool: walk the whole chain)
     const uint32_t* pool;
     const int64_t* sb_off;
     const int32_t* sb_len;
+    // per-block lists (nullable): used where kind == 0, or for every block when blk_all
+    const int32_t* kind;
+    const int32_t* blk_off;
+    const int32_t* blk_len;
+    const uint32_t* blk_pool;
+    int64_t blk_cap;
+    int blk_all;
     double x0, y0, z0, pitch;
     int nx, ny, nz, B, S, nsy, nsz, nbx, nby, nbz;
 };
@@ -69,6 +77,15 @@ __device__ __forceinline__ float eval_accel(const PrimF* primf, const FbInsn* ch
         if (fx >= 0 && fy >= 0 && fz >= 0 && fx <= ex && fy <= ey && fz <= ez) {
             const int bi = min((int)(fx / A.B), A.nbx - 1), bj = min((int)(fy / A.B), A.nby - 1),
                       bk = min((int)(fz / A.B), A.nbz - 1);
+            if (A.blk_len) {  // the block's own list: culled for a region holding the whole block
+                const int64_t b = ((int64_t)bi * A.nby + bj) * A.nbz + bk;
+                if (A.blk_all || A.kind[b] == 0) {
+                    const int len = A.blk_len[b];
+                    const int64_t off = len >= 0 ? (int64_t)A.blk_off[b] : -1;
+                    if (len >= 0 && off >= 0 && off + len <= A.blk_cap)
+                        return eval_point(primf, chain, n_chain, 1, A.blk_pool + off, len, x, y, z);
+                }
+            }
             const int64_t s = ((int64_t)(bi / A.S) * A.nsy + bj / A.S) * A.nsz + bk / A.S;
             return eval_point(primf, chain, n_chain, 1, A.pool + A.sb_off[s], A.sb_len[s], x, y, z);
         }
@@ -336,8 +353,9 @@ int fb_query_prepare(const FbPrim* d_prims, int32_t n_prims, void* d_primf, void
 int fb_query_points_device(const void* d_primf, const FbInsn* d_chain, int32_t n_chain, int32_t mode,
                            const void* accel_pool, const int64_t* accel_off, const int32_t* accel_len,
                            const double* accel_grid /* x0,y0,z0,pitch */, const int32_t* accel_dims /* nx,ny,nz,B */,
-                           const float* d_points, int64_t n, double h, float* d_value, float* d_grad,
-                           void* stream) noexcept {
+                           const int32_t* d_kind, const int32_t* blk_off, const int32_t* blk_len,
+                           const uint32_t* blk_pool, int64_t blk_cap, int32_t blk_all, const float* d_points, int64_t n,
+                           double h, float* d_value, float* d_grad, void* stream) noexcept {
     if (!d_primf || !d_chain || n_chain < 1 || !d_points || n < 0 || (!d_value && !d_grad)) return FB_INVALID;
     if (n == 0) return FB_OK;
     Accel A{};
@@ -351,6 +369,14 @@ int fb_query_points_device(const void* d_primf, const FbInsn* d_chain, int32_t n
         A.S = std::max(1, 32 / A.B);
         A.nsy = (A.nby + A.S - 1) / A.S;
         A.nsz = (A.nbz + A.S - 1) / A.S;
+        if (blk_off && blk_len && blk_pool && blk_cap > 0 && (blk_all || d_kind)) {
+            A.kind = d_kind;
+            A.blk_off = blk_off;
+            A.blk_len = blk_len;
+            A.blk_pool = blk_pool;
+            A.blk_cap = blk_cap;
+            A.blk_all = blk_all ? 1 : 0;
+        }
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)fb_sm_count() * 16);

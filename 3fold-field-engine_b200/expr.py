@@ -518,16 +518,17 @@ def extend(comp: Compiled, tool_prims, op="subtract") -> Compiled:
     base = len(comp.prims)
     prims = np.concatenate([comp.prims, tool_prims])
     idx = range(base, base + len(tool_prims))
-    if comp.chain is not None:
-        code = CH_SUBTRACT if op == "subtract" else CH_UNION
-        chain = np.concatenate([comp.chain, _records([(code, i, 0.0) for i in idx])])
-        return Compiled(prims, _records(_chain_to_program([(int(r["op"]), int(r["arg"]), float(r["k"]))
-                                                            for r in chain])), chain)
+    # the program of a chain ends with push + operator per hard chain entry, so the tools' part is
+    # appended to the existing program in both forms
     code = OP_SUBTRACT if op == "subtract" else OP_UNION
     rows = []
     for i in idx:
         rows += [(OP_PUSH, i, 0.0), (code, -1, 0.0)]
-    return Compiled(prims, np.concatenate([comp.program, _records(rows)]), None)
+    program = np.concatenate([comp.program, _records(rows)])
+    if comp.chain is not None:
+        ch = CH_SUBTRACT if op == "subtract" else CH_UNION
+        return Compiled(prims, program, np.concatenate([comp.chain, _records([(ch, i, 0.0) for i in idx])]))
+    return Compiled(prims, program, None)
 
 
 def eval_sdf_py(node, p):

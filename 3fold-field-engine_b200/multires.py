@@ -76,7 +76,8 @@ def _accel(builder):
     pool, off, ln = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
     boff, blen, bpool = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
     st = L.fb_field_accel(ct.addressof(builder.geom), builder.n_prims, builder.n_chain, builder.scratch.data_ptr(),
-                          ct.byref(pool), ct.byref(off), ct.byref(ln), ct.byref(boff), ct.byref(blen), ct.byref(bpool))
+                          ct.byref(pool), ct.byref(off), ct.byref(ln), ct.byref(boff), ct.byref(blen), ct.byref(bpool),
+                          None, None)
     _lib.check(st, "field accel")
     return pool.value, off.value, ln.value, boff.value, blen.value, bpool.value
 

@@ -47,17 +47,21 @@ class RecipeQueries:
     def attach(self, builder):
         """Use `builder`'s superblock lists (the builder must have classified this same recipe)."""
         pool, off, ln = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        boff, blen, bpool = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        bcap, ball = ct.c_int64(), ct.c_int32()
         st = self.lib.fb_field_accel(ct.addressof(builder.geom), builder.n_prims, builder.n_chain,
                                      builder.scratch.data_ptr(), ct.byref(pool), ct.byref(off), ct.byref(ln),
-                                     None, None, None)
+                                     ct.byref(boff), ct.byref(blen), ct.byref(bpool), ct.byref(bcap), ct.byref(ball))
         _lib.check(st, "field accel")
         m = builder.meta
         self._accel = (pool.value, off.value, ln.value, np.array([m.x0, m.y0, m.z0, m.pitch], np.float64),
-                       np.array([m.nx, m.ny, m.nz, m.block], np.int32), builder)
+                       np.array([m.nx, m.ny, m.nz, m.block], np.int32),
+                       (builder.kind.data_ptr(), boff.value, blen.value, bpool.value, bcap.value, ball.value), builder)
 
     def _run(self, pts, value, grad, h=0.05, stream=None):
         a = self._accel
-        args = (a[0], a[1], a[2], a[3].ctypes.data, a[4].ctypes.data) if a else (None, None, None, None, None)
+        args = (a[0], a[1], a[2], a[3].ctypes.data, a[4].ctypes.data, *a[5]) if a else (None,) * 5 + (None, None,
+                                                                                                     None, None, 0, 0)
         st = self.lib.fb_query_points_device(self.primf.data_ptr(), self.chain.data_ptr(), self.n_chain, self.mode,
                                              *args, pts.data_ptr(), pts.shape[0], float(h),
                                              value.data_ptr() if value is not None else None,

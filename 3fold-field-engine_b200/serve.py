@@ -51,10 +51,12 @@ class _Field:
         self.busy = 0
         self.editing = False
         self.last_use = time.perf_counter()
+        self.accounted = 0  # bytes of this field in the server's resident total
 
     @property
     def nbytes(self):
-        t = [self.fb.scratch, self.fb.kind, self.fb.cma, self.fb.active, self.tiles, self.fb.prims, self.fb.chain]
+        """Device bytes the field holds: the build's slab (block arrays + scratch), tiles, EDT."""
+        t = [self.fb.slab, self.tiles]
         if self.edt is not None:
             t.append(self.edt)
         return int(sum(x.numel() * x.element_size() for x in t))
@@ -116,6 +118,7 @@ class FieldServer:
         self.budget = float(budget_bytes)
         self.timeout = float(request_timeout_s)
         self.fields = {}
+        self.resident = 0  # sum of the resident fields' bytes, kept up to date on every change
         self.next_id = 0
         self.reserved = 0
         self.pending = []
@@ -158,7 +161,13 @@ class FieldServer:
         self.close()
 
     def resident_bytes(self):
-        return sum(f.nbytes for f in self.fields.values())
+        return self.resident
+
+    def _account(self, f):
+        """Bring the resident total up to date after field `f` changed its buffers."""
+        now = f.nbytes
+        self.resident += now - f.accounted
+        f.accounted = now
 
     # ------------------------------------------------------------------------------------ scheduler
     def _estimate(self, r):
@@ -180,7 +189,8 @@ class FieldServer:
             if f.busy or f.editing:
                 continue
             del self.fields[f.id]
-            resident -= f.nbytes
+            self.resident -= f.accounted
+            resident -= f.accounted
             if resident + self.reserved + need <= self.budget:
                 return True
         return resident + self.reserved + need <= self.budget
@@ -331,6 +341,7 @@ class FieldServer:
         fid = self.next_id
         self.next_id += 1
         self.fields[fid] = _Field(fid, comp, meta, fb, tiles, n)
+        self._account(self.fields[fid])
         return dict(field=fid, n_active=n, leaf_voxels=n * meta.block ** 3)
 
     def _run_edit(self, r, stream):
@@ -340,6 +351,8 @@ class FieldServer:
         f.comp, f.fb, f.tiles, f.n_active = comp, fb, tiles, n
         f.queries = None
         f.edt = None
+        if f.id in self.fields:
+            self._account(f)
         return dict(field=f.id, n_active=n, leaf_voxels=n * f.meta.block ** 3)
 
     def _run_query(self, r, stream):
@@ -387,4 +400,6 @@ class FieldServer:
         yield self._record(stream)
         if f.fb is fb:
             f.edt = out
+            if f.id in self.fields:
+                self._account(f)
         return dict(field=f.id, checksum=int(host.item()), voxels=int(out.numel()))

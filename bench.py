@@ -471,6 +471,7 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
         srv.submit("query", field=live[0], points=point_sets[0][:1000]).result(timeout=120)
         srv.submit("edit", field=live[1], tools=tool_sets[0]).result(timeout=120)
         srv.completed.clear()
+        alloc0 = torch.cuda.memory_stats()
         futs = []
         t0 = time.perf_counter()
         due = t0
@@ -499,7 +500,13 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
             except Exception as e:
                 errors[type(e).__name__] = errors.get(type(e).__name__, 0) + 1
         t_end = time.perf_counter()
+        alloc1 = torch.cuda.memory_stats()
         lat = np.array([(e - a) * 1e3 for _, a, _, e in srv.completed])
+        # worst latency of the requests arriving in each half second: a stall shows as one window
+        windows = {}
+        for _, a, _, e in srv.completed:
+            k = int((a - t0) / 0.5)
+            windows[k] = max(windows.get(k, 0.0), (e - a) * 1e3)
         by_kind = {}
         for kind, a, st, e in srv.completed:
             by_kind.setdefault(kind, []).append(((e - a) * 1e3, (st - a) * 1e3))
@@ -514,6 +521,13 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
                         "p99_ms": float(np.percentile([x for x, _ in v], 99)),
                         "queue_p50_ms": float(np.percentile([q for _, q in v], 50))}
                     for k, v in by_kind.items()},
+        "slowest": [{"kind": k, "arrival_s": round(a - t0, 3), "queue_ms": round((st - a) * 1e3, 1),
+                     "service_ms": round((e - st) * 1e3, 1)}
+                    for k, a, st, e in sorted(srv.completed, key=lambda c: c[1] - c[3])[:5]],
+        "worst_ms_per_half_second": [round(windows.get(k, 0.0), 1) for k in range(max(windows) + 1)] if windows else [],
+        "allocator": {k: int(alloc1.get(k, 0) - alloc0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
+                                                                           "num_alloc_retries")},
+        "resident_gb": round(srv.resident_bytes() / 1e9, 2),
         "slots": 16, "budget_gb": 150, "data": "synthetic",
     }
 

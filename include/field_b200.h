@@ -188,15 +188,18 @@ int fb_packed_query_device(const void* d_nodes, const float* d_payload, const in
 /* Replace eval_batch / gradient_batch, src/field_engine/ikarus_v1/eval_warp.py:478-488,718-733.
  * fb_query_prepare fills the 128-byte float32 primitive mirror; fb_field_accel exposes a
  * classification's culling lists inside its scratch (superblock and per-block) so that points
- * inside that grid walk only their superblock's list. */
+ * inside that grid walk only their block's list (where the classification kept one; blk_all = 1:
+ * every block, else blocks of kind 0) or their superblock's list. */
 int fb_query_prepare(const fb_prim* d_prims, int32_t n_prims, void* d_primf, void* stream);
 int fb_field_accel(const fb_geom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, const void** pool,
                    const int64_t** sb_off, const int32_t** sb_len, const int32_t** blk_off, const int32_t** blk_len,
-                   const uint32_t** blk_pool);
+                   const uint32_t** blk_pool, int64_t* blk_cap, int32_t* blk_all);
 int fb_query_points_device(const void* d_primf, const fb_insn* d_chain, int32_t n_chain, int32_t mode,
                            const void* accel_pool, const int64_t* accel_off, const int32_t* accel_len,
-                           const double* accel_grid, const int32_t* accel_dims, const float* d_points, int64_t n,
-                           double h, float* d_value, float* d_grad, void* stream);
+                           const double* accel_grid, const int32_t* accel_dims, const int32_t* d_kind,
+                           const int32_t* blk_off, const int32_t* blk_len, const uint32_t* blk_pool, int64_t blk_cap,
+                           int32_t blk_all, const float* d_points, int64_t n, double h, float* d_value, float* d_grad,
+                           void* stream);
 
 /* Replace the per-block-pitch field's lattices and its avstand / gradient queries,
  * src/field_engine/faltkarna_v1_multires.py:84-104,384-459 (lattices built from a recipe). */

@@ -1,0 +1,62 @@
+"""Host-side recipe logic without a GPU: edits appended to a compiled recipe equal the recompiled
+edited recipe byte for byte, and edit tools must be single primitives."""
+import numpy as np
+import pytest
+
+
+def _base(seed):
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    rng = np.random.default_rng(seed)
+    return X.union_all(R.parts(rng, 4, 3, 3, 2, scale=0.6)), rng
+
+
+@pytest.mark.parametrize("op", ["subtract", "union"])
+def test_extend_equals_recompiled_recipe(op):
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    base, rng = _base(1)
+    tools = R.tools(rng, 7)
+    edited = base
+    for t in tools:
+        edited = X.subtract(edited, t) if op == "subtract" else X.union(edited, t)
+    want = X.compile_recipe(edited)
+    got = X.extend(X.compile_recipe(base), X.compile_tools(tools), op)
+    for key in ("prims", "chain", "program"):
+        assert np.array_equal(getattr(want, key).view(np.uint8), getattr(got, key).view(np.uint8)), key
+
+
+def test_extend_twice_equals_one_recompile():
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    base, rng = _base(2)
+    t1, t2 = R.tools(rng, 3), R.tools(rng, 4)
+    got = X.extend(X.extend(X.compile_recipe(base), X.compile_tools(t1)), X.compile_tools(t2))
+    want = X.compile_recipe(X.subtract_all(X.subtract_all(base, t1), t2))
+    for key in ("prims", "chain", "program"):
+        assert np.array_equal(getattr(want, key).view(np.uint8), getattr(got, key).view(np.uint8)), key
+
+
+def test_extend_keeps_non_chain_recipes_as_programs():
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    base, rng = _base(3)
+    # a smooth union whose right operand is itself a union has no chain form
+    smooth = X.union(base, X.union(X.sphere(0.1, (0.5, 0.5, 0.5)), X.sphere(0.05, (0.3, 0.5, 0.5))), k=0.02)
+    comp = X.compile_recipe(smooth)
+    assert comp.chain is None
+    tools = R.tools(rng, 2)
+    got = X.extend(comp, X.compile_tools(tools))
+    want = X.compile_recipe(X.subtract_all(smooth, tools))
+    assert got.chain is None
+    assert np.array_equal(want.program.view(np.uint8), got.program.view(np.uint8))
+    assert np.array_equal(want.prims.view(np.uint8), got.prims.view(np.uint8))
+
+
+def test_composite_tools_and_bad_ops_are_rejected():
+    import field_b200.expr as X
+    base, _ = _base(4)
+    with pytest.raises(ValueError):
+        X.compile_tools([X.union(X.sphere(0.1), X.sphere(0.2, (0.3, 0.0, 0.0)))])
+    with pytest.raises(ValueError):
+        X.extend(X.compile_recipe(base), X.compile_tools([X.sphere(0.1)]), "intersect")

@@ -45,12 +45,14 @@ def test_gradient_batch_matches_float64_central_difference():
         assert np.abs(got - want).max() < 2e-3, name
 
 
-def test_accelerated_queries_equal_full_chain():
+# 256^3 / B8: every block keeps a culled list (warp-per-block cull); 512^3 / B8: only surface blocks do
+@pytest.mark.parametrize("n", [256, 512])
+def test_accelerated_queries_equal_full_chain(n):
     import torch
     import field_b200.build as B
     import field_b200.query as Q
     import field_b200.recipes as R
-    recipe, meta = R.milled_part(seed=3, n=256, block=8, n_parts=512, n_tools=64)
+    recipe, meta = R.milled_part(seed=3, n=n, block=8, n_parts=512, n_tools=64)
     fb = B.FieldBuilder(recipe, meta)
     fb.classify()
     plain = Q.RecipeQueries(fb.compiled)
