@@ -104,6 +104,8 @@ def bygg_multires_fran_recept(recipe, lo, h_grov, brick_shape, block=8, levels=N
         lengths_all = torch.empty(meta.n_blocks, dtype=torch.int32, device=fb.device)
         _copy_device(lengths_all, blk_len, meta.n_blocks * 4)
         lens_host = lengths_all[torch.from_numpy(active).to(fb.device)].cpu().numpy()
+    # a block whose culled list overflowed its capacity (length -1) counts as longer than any threshold
+    lens_host = np.where(lens_host < 0, np.iinfo(np.int32).max, lens_host)
     if levels is None:
         lv = np.zeros(n_active, np.int8)
     elif isinstance(levels, (int, np.integer)):

@@ -49,9 +49,10 @@ def parse():
     ap.add_argument("--edt-n", type=int, default=512, help="grid edge of the EDT")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=("plain", "batched", "serve"), default="plain",
+    ap.add_argument("--check-bricks", type=int, default=24, help="precision: bricks checked per level")
+    ap.add_argument("--workload", choices=("plain", "batched", "serve", "precision"), default="plain",
                     help="plain: the plain method at scale (default line); batched: 256 recipes, plain vs "
-                         "graph-batched; serve: the request loop")
+                         "graph-batched; serve: the request loop; precision: float32 vs float64 at mixed pitch")
     ap.add_argument("--recipes", type=int, default=256)
     ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
     ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrival window")
@@ -320,7 +321,25 @@ def run_ours(args, rank, world, local_rank):
         secs, desc, cores, _ = cpu_sample(comp, meta, mask_np, n_active=n_active)
         result["cpu_baseline"] = {"value": leaf_voxels / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
                                   "sample": desc, "seconds_per_step": secs}
+        # the float64 oracle, as the checker, on a sample of the timed run's leaf tiles
+        result["accuracy"] = leaf_accuracy(comp, meta, builder, tiles, n_active)
     return result
+
+
+def leaf_accuracy(comp, meta, builder, tiles, n_active, n_blocks=48, seed=5):
+    """Max |d_f32 - d_f64| / pitch over a seeded sample of active blocks (all their voxels, and
+    inside the 3-voxel band), and sign disagreements, against the float64 oracle."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(n_active, size=min(n_blocks, n_active), replace=False))
+    ids = builder.active[:n_active].cpu().numpy()[pick].astype(np.int32)
+    got = tiles[pick].cpu().numpy().astype(np.float64).reshape(len(pick), -1)
+    want = oracle.tiles_program(comp.prims, comp.program, meta, ids).reshape(len(pick), -1)
+    err = np.abs(got - want) / meta.pitch
+    band = np.abs(want) <= 3 * meta.pitch
+    return {"blocks": int(len(pick)), "voxels": int(got.size), "max_err_pitch": float(err.max()),
+            "max_err_pitch_band": float(err[band].max()) if band.any() else 0.0,
+            "sign_disagreements": int(np.count_nonzero((got >= 0) != (want >= 0))), "checker": "float64 oracle"}
 
 
 def e2e_leg(comp, meta, mask_np, dev, steps=2):
@@ -429,7 +448,23 @@ def run_batched(args):
     hist = {}
     for b in blocks:
         hist[str(b)] = hist.get(str(b), 0) + 1
+    accuracy = None
+    if not args.no_cpu:  # the float64 oracle, as the checker, on sampled blocks of sampled recipes
+        rng = np.random.default_rng(8)
+        worst, worst_band, sign, nblk = 0.0, 0.0, 0, 0
+        by_grid = {}
+        for i in sorted(rng.choice(len(bb.items), size=min(24, len(bb.items)), replace=False)):
+            it, (comp, _) = bb.items[int(i)], comps[int(i)]
+            a = leaf_accuracy(comp, it.meta, it.fb, it.tiles, it.capacity, n_blocks=8, seed=int(i))
+            worst, worst_band = max(worst, a["max_err_pitch"]), max(worst_band, a["max_err_pitch_band"])
+            sign += a["sign_disagreements"]
+            nblk += a["blocks"]
+            g = by_grid.setdefault(str(it.meta.nx), 0.0)
+            by_grid[str(it.meta.nx)] = max(g, a["max_err_pitch_band"])
+        accuracy = {"recipes": 24, "blocks": nblk, "max_err_pitch": worst, "max_err_pitch_band": worst_band,
+                    "max_err_pitch_band_by_grid": by_grid, "sign_disagreements": sign, "checker": "float64 oracle"}
     return {
+        "accuracy": accuracy,
         "metric": METRIC, "workload": "batched_256_recipes", "value": voxels / (mb * 1e-3) / 1e9, "unit": UNIT,
         "plain_gvox_s": voxels / (mp * 1e-3) / 1e9, "batched_gvox_s": voxels / (mb * 1e-3) / 1e9,
         "speedup_batched_vs_plain": mp / mb, "ms_plain": mp, "ms_batched": mb, "steps": args.steps,
@@ -532,10 +567,87 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
     }
 
 
+def run_precision(args):
+    """Precision stress: 1000 near-tangent sphere pairs (gap U[0, 0.5] fine pitches) and 64 walls half
+    a fine voxel thick, as a per-block-pitch field mixing pitch 1/128 (level 0) and 1/512 (level 2)
+    over the unit cube (512^3-equivalent).  The GPU builds every brick lattice; the float64 oracle
+    (the CPU leg, timed) evaluates a seeded sample of bricks of both levels; the line reports the
+    worst per-block |d_f32 - d_f64| in units of the brick's pitch and the sign disagreements."""
+    import torch
+    import field_b200.multires as M
+    import field_b200.recipes as R
+    import field_b200.expr as X
+    import oracle
+    torch.cuda.set_device(0)
+    recipe = R.tangent_pairs(seed=4, n_pairs=1000, pitch=1.0 / 512, walls=64)
+    comp = X.compile_recipe(recipe)
+    # the fine pitch where a brick's culled list is at least the median length (the crowded bricks)
+    fine = lambda lens: np.where(np.asarray(lens) >= np.median(lens), 2, 0)
+    build = lambda: M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 128, (16, 16, 16), block=8, levels=fine)
+    build()  # warm-up: kernels configured
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    F = build()
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    tiles = F.tiles
+    rng = np.random.default_rng(1)
+    per_level = {}
+    for u in sorted(tiles):
+        bi, bj, bk = np.unravel_index(int(u), F.brick_shape)
+        per_level.setdefault(int(F.niva[bi, bj, bk]), []).append(int(u))
+    checked, block_max, sign, rel = {}, [], 0, 0.0
+    t_cpu = 0.0
+    for lvl, ids in sorted(per_level.items()):
+        pick = rng.choice(ids, size=min(args.check_bricks, len(ids)), replace=False)
+        checked[str(lvl)] = int(len(pick))
+        pitch = F.h_grov / (1 << lvl)
+        for u in pick:
+            bi, bj, bk = np.unravel_index(int(u), F.brick_shape)
+            m = tiles[int(u)].shape[0]
+            pts = F.lo + np.array([bi, bj, bk]) * F.L + np.indices((m, m, m)).reshape(3, -1).T * pitch
+            c0 = time.perf_counter()
+            want = oracle.eval_points(comp.prims, comp.program, pts)
+            t_cpu += time.perf_counter() - c0
+            got = tiles[int(u)].reshape(-1).astype(np.float64)
+            err = np.abs(got - want)
+            band = np.abs(want) <= 3 * pitch
+            block_max.append(float(err[band].max() / pitch) if band.any() else 0.0)
+            rel = max(rel, float((err / np.maximum(np.abs(want), pitch)).max()))
+            sign += int(np.count_nonzero((got >= 0) != (want >= 0)))
+    samples = int(sum(t.size for t in tiles.values()))
+    worst = max(block_max) if block_max else 0.0
+    # the plain single build (64 primitives, 256^3, B = 8): its leaf tiles against the same checker
+    import field_b200.build as B
+    c0_recipe, c0_meta = R.plain_union(seed=0, n=256, block=8)
+    c0_comp = X.compile_recipe(c0_recipe)
+    c0_fb = B.FieldBuilder(c0_comp, c0_meta)
+    c0 = c0_fb.build()
+    c0_acc = leaf_accuracy(c0_comp, c0_meta, c0_fb, c0.tiles, c0.n_active, n_blocks=256)
+    return {
+        "metric": METRIC, "workload": "precision_stress_tangent_pairs_mixed_pitch", "value": worst,
+        "unit": "pitch (max per-block |d_f32 - d_f64| within 3 pitches of the surface)", "higher_is_better": False,
+        "sign_disagreements": sign, "max_rel_err": rel,
+        "per_block_max_err_pitch": {"p50": float(np.percentile(block_max, 50)), "max": worst,
+                                    "blocks": len(block_max)},
+        "plain_single_build_256": dict(c0_acc, n_active=int(c0.n_active)),
+        "bricks_checked_by_level": checked, "bricks_by_level": {str(k): len(v) for k, v in per_level.items()},
+        "pitches": {"0": 1.0 / 128, "2": 1.0 / 512}, "lattice_samples": samples, "build_s": build_s,
+        "cpu_baseline": {"value": t_cpu, "unit": "s (float64 oracle over the checked bricks)", "cores": oracle.threads(),
+                         "kind": "port", "sample": f"{len(block_max)} bricks, all lattice points"},
+        "config": {"workload": "1000 near-tangent pairs + 64 half-voxel walls, pitch 1/128 and 1/512",
+                   "primitives": int(len(comp.prims))},
+        "dtype": "f32 (f64 guard band)", "data": "synthetic",
+    }
+
+
 def main():
     args = parse()
     if args.workload == "batched":
         print(json.dumps(run_batched(args)), flush=True)
+        return
+    if args.workload == "precision":
+        print(json.dumps(run_precision(args)), flush=True)
         return
     if args.workload == "serve":
         print(json.dumps(run_serve(args, rate=args.rate, seconds=args.seconds)), flush=True)
