@@ -806,6 +806,21 @@ __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float
     }
 }
 
+// The five kinds the milling recipes rarely use, out of line and one voxel per call (scalar
+// arguments stay in registers): the hot loop keeps only the four common kinds inlined, small enough
+// to stay in the instruction cache.
+__device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float dy, float dz) {
+    float x, y, z;
+    if (P.ident) {
+        x = P.L[0] + dx; y = P.L[1] + dy; z = P.L[2] + dz;
+    } else {
+        x = fmaf(P.A[2], dz, fmaf(P.A[0], dx, fmaf(P.A[1], dy, P.L[0])));
+        y = fmaf(P.A[5], dz, fmaf(P.A[3], dx, fmaf(P.A[4], dy, P.L[1])));
+        z = fmaf(P.A[8], dz, fmaf(P.A[6], dx, fmaf(P.A[7], dy, P.L[2])));
+    }
+    return fmaf(P.s, canon_f(P.type, P.p, x, y, z), -P.off);
+}
+
 template <int VG>
 __device__ __forceinline__ void eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
     switch (P.type) {
@@ -813,11 +828,9 @@ __device__ __forceinline__ void eval_group(const LocalPrim& P, float dx, float d
     case P_BOX: eval_group_t<VG, P_BOX>(P, dx, dy, dz, v); break;
     case P_CAPSULE: eval_group_t<VG, P_CAPSULE>(P, dx, dy, dz, v); break;
     case P_TORUS: eval_group_t<VG, P_TORUS>(P, dx, dy, dz, v); break;
-    case P_CYLINDER: eval_group_t<VG, P_CYLINDER>(P, dx, dy, dz, v); break;
-    case P_CONE: eval_group_t<VG, P_CONE>(P, dx, dy, dz, v); break;
-    case P_HALFSPACE: eval_group_t<VG, P_HALFSPACE>(P, dx, dy, dz, v); break;
-    case P_FRUSTUM: eval_group_t<VG, P_FRUSTUM>(P, dx, dy, dz, v); break;
-    default: eval_group_t<VG, P_CYL_INF>(P, dx, dy, dz, v);
+    default:
+#pragma unroll
+        for (int k = 0; k < VG; ++k) v[k] = eval_one_rare(P, dx, dy, dz[k]);
     }
 }
 
@@ -911,7 +924,7 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
 // voxels along z (VG = 4, or 2 for 4^3 blocks) and stores each group with one vector store.
 template <int B>
-__global__ void __launch_bounds__(32 * kLeafWarps, 5) k_leaf(Geo G, const FbPrim* __restrict__ prims,
+__global__ void __launch_bounds__(32 * kLeafWarps, 4) k_leaf(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
                                                              const FbInsn* __restrict__ chain,
                                                              const uint32_t* __restrict__ pool,
