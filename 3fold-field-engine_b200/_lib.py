@@ -53,7 +53,8 @@ SIGNATURES = {
     # queries
     "fb_query_prepare": (I, [P, I, P, P]),
     "fb_field_accel": (I, [P, I, I, P, P, P, P, P, P, P, P, P]),
-    "fb_query_points_device": (I, [P, P, I, I, P, P, P, P, P, P, P, P, P, I64, I, P, I64, D, P, P, P]),
+    "fb_query_points_device": (I, [P, P, I, I, P, P, P, P, P, P, P, P, P, I64, I, P, I64, D, P, P, P, I64, P]),
+    "fb_query_scratch_bytes": (I64, [P, I64, I]),
     "fb_multires_tiles_device": (I, [P, P, I, I, P, P, D, I, P, P, P, P, I64, P, P, P, F, P, P]),
     "fb_multires_query_device": (I, [P, D, I, P, D, P, P, P, P, P, I64, P, P, P]),
 }

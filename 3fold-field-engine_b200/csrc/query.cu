@@ -67,9 +67,14 @@ struct Accel {  // a built field's culling lists (nullptr pool: walk the whole c
     int nx, ny, nz, B, S, nsy, nsz, nbx, nby, nbz;
 };
 
-__device__ __forceinline__ float eval_accel(const PrimF* primf, const FbInsn* chain, int n_chain, int chain_mode,
-                                            const Accel& A, float x, float y, float z) {
-    if (chain_mode && A.pool) {
+// The list a point at (x, y, z) walks and its key: block b (0 <= b < nblocks) where the
+// classification kept the block's list, nblocks + superblock for other points inside the grid,
+// nblocks + nsuper (nullptr list) for the whole chain.
+__device__ __forceinline__ int64_t accel_list(const Accel& A, int n_chain, float x, float y, float z,
+                                              const uint32_t*& list, int& len) {
+    const int64_t nblocks = (int64_t)A.nbx * A.nby * A.nbz;
+    const int64_t nsuper = (int64_t)((A.nbx + A.S - 1) / A.S) * A.nsy * A.nsz;
+    if (A.pool) {
         // the voxel cell containing the point, inside the grid's block range
         const double fx = ((double)x - A.x0) / A.pitch, fy = ((double)y - A.y0) / A.pitch,
                      fz = ((double)z - A.z0) / A.pitch;
@@ -80,15 +85,33 @@ __device__ __forceinline__ float eval_accel(const PrimF* primf, const FbInsn* ch
             if (A.blk_len) {  // the block's own list: culled for a region holding the whole block
                 const int64_t b = ((int64_t)bi * A.nby + bj) * A.nbz + bk;
                 if (A.blk_all || A.kind[b] == 0) {
-                    const int len = A.blk_len[b];
-                    const int64_t off = len >= 0 ? (int64_t)A.blk_off[b] : -1;
-                    if (len >= 0 && off >= 0 && off + len <= A.blk_cap)
-                        return eval_point(primf, chain, n_chain, 1, A.blk_pool + off, len, x, y, z);
+                    const int n = A.blk_len[b];
+                    const int64_t off = n >= 0 ? (int64_t)A.blk_off[b] : -1;
+                    if (n >= 0 && off >= 0 && off + n <= A.blk_cap) {
+                        list = A.blk_pool + off;
+                        len = n;
+                        return b;
+                    }
                 }
             }
             const int64_t s = ((int64_t)(bi / A.S) * A.nsy + bj / A.S) * A.nsz + bk / A.S;
-            return eval_point(primf, chain, n_chain, 1, A.pool + A.sb_off[s], A.sb_len[s], x, y, z);
+            list = A.pool + A.sb_off[s];
+            len = A.sb_len[s];
+            return nblocks + s;
         }
+    }
+    list = nullptr;
+    len = n_chain;
+    return nblocks + nsuper;
+}
+
+__device__ __forceinline__ float eval_accel(const PrimF* primf, const FbInsn* chain, int n_chain, int chain_mode,
+                                            const Accel& A, float x, float y, float z) {
+    if (chain_mode) {
+        const uint32_t* list;
+        int len;
+        accel_list(A, n_chain, x, y, z, list, len);
+        return eval_point(primf, chain, n_chain, 1, list, len, x, y, z);
     }
     return eval_point(primf, chain, n_chain, chain_mode, nullptr, n_chain, x, y, z);
 }
@@ -120,6 +143,179 @@ __global__ void k_gradient_points(const PrimF* __restrict__ primf, const FbInsn*
         if (value) value[i] = eval_accel(primf, chain, n_chain, chain_mode, A, (float)p[0], (float)p[1], (float)p[2]);
     }
 }
+
+// ------------------------------------------------------------------------------------ binned queries
+// Evaluation points sorted by the list they walk, so that the lanes of a warp share one list
+// (broadcast loads, one primitive kind at a time) instead of each lane walking its own.  Point e of
+// a query with `nvar` variants is point e / nvar at variant e % nvar: 0 the point itself, 1 + 2a + s
+// the offset along axis a (s = 0: +h, 1: -h), formed in float64 and rounded to float32 exactly as
+// k_gradient_points forms them, and every value is computed by the same eval_point -- so the
+// results are bit-identical to the unsorted kernels.
+__device__ __forceinline__ void variant_point(const float* __restrict__ pts, int64_t e, int nvar, double h, float& x,
+                                              float& y, float& z) {
+    const int64_t i = e / nvar;
+    const int v = (int)(e - i * nvar);
+    const double p[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+    float q[3];
+    for (int c = 0; c < 3; ++c) q[c] = (float)p[c];
+    if (v > 0) {
+        const int a = (v - 1) >> 1, s = (v - 1) & 1;
+        q[a] = (float)(p[a] + (s ? -h : h));
+    }
+    x = q[0];
+    y = q[1];
+    z = q[2];
+}
+
+__global__ void k_query_keys(Accel A, int n_chain, const float* __restrict__ pts, int64_t ne, int nvar, double h,
+                             int32_t* __restrict__ keys, int32_t* __restrict__ count) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
+        float x, y, z;
+        variant_point(pts, e, nvar, h, x, y, z);
+        const uint32_t* list;
+        int len;
+        const int32_t key = (int32_t)accel_list(A, n_chain, x, y, z, list, len);
+        keys[e] = key;
+        atomicAdd(&count[key], 1);
+    }
+}
+
+// Exclusive scan of count[0, n) in place: tiles of kScanTile per CTA, then the tile sums, then the
+// tile offsets added back.
+constexpr int kScanThreads = 1024, kScanItems = 4, kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int32_t block_exclusive_scan(int32_t v, int32_t* warp_sums, int32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    total = warp_sums[(blockDim.x >> 5) - 1];
+    const int32_t before = warp > 0 ? warp_sums[warp - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __restrict__ data, int64_t n,
+                                                             int32_t* __restrict__ tile_sums) {
+    __shared__ int32_t warp_sums[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? data[base + k] : 0;
+        sum += v[k];
+    }
+    int32_t total;
+    int32_t run = block_exclusive_scan(sum, warp_sums, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) data[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// One CTA scans the tile sums (at most kScanTile of them) in place.
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int32_t* __restrict__ tile_sums, int ntiles) {
+    __shared__ int32_t warp_sums[32];
+    const int base = threadIdx.x * kScanItems;
+    int32_t v[kScanItems], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < ntiles ? tile_sums[base + k] : 0;
+        sum += v[k];
+    }
+    int32_t total;
+    int32_t run = block_exclusive_scan(sum, warp_sums, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < ntiles) tile_sums[base + k] = run;
+        run += v[k];
+    }
+}
+
+__global__ void k_scan_add(int32_t* __restrict__ data, int64_t n, const int32_t* __restrict__ tile_sums) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        data[i] += tile_sums[i / kScanTile];
+}
+
+// cursor[key] starts at the key's first sorted position and ends past its last.
+__global__ void k_query_scatter(const int32_t* __restrict__ keys, int64_t ne, int32_t* __restrict__ cursor,
+                                int32_t* __restrict__ order) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
+        order[atomicAdd(&cursor[keys[e]], 1)] = (int32_t)e;
+}
+
+__global__ void k_query_eval_sorted(const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain, int n_chain,
+                                    Accel A, const float* __restrict__ pts, int64_t ne, int nvar, double h,
+                                    const int32_t* __restrict__ order, float* __restrict__ vals) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ne; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = order[t];
+        float x, y, z;
+        variant_point(pts, e, nvar, h, x, y, z);
+        const uint32_t* list;
+        int len;
+        accel_list(A, n_chain, x, y, z, list, len);
+        vals[e] = eval_point(primf, chain, n_chain, 1, list, len, x, y, z);
+    }
+}
+
+// value = variant 0, gradient component a = (v(1 + 2a) - v(2 + 2a)) / (2h), k_gradient_points' arithmetic.
+__global__ void k_query_combine(const float* __restrict__ vals, int64_t n, double h, float* __restrict__ grad,
+                                float* __restrict__ value) {
+    const float inv = (float)(2.0 * h);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float* v = vals + 7 * i;
+        for (int a = 0; a < 3; ++a) grad[3 * i + a] = (v[1 + 2 * a] - v[2 + 2 * a]) / inv;
+        if (value) value[i] = v[0];
+    }
+}
+
+struct BinnedPlan {
+    int64_t ne, nbins, ntiles;
+    int64_t keys, order, vals, count, tiles, total;
+};
+
+BinnedPlan binned_plan(int64_t n, int nvar, int64_t nbins) {
+    BinnedPlan p{};
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    p.ne = n * nvar;
+    p.nbins = nbins;
+    p.ntiles = (nbins + kScanTile - 1) / kScanTile;
+    int64_t at = 0;
+    p.keys = at; at += al(p.ne * 4);
+    p.order = at; at += al(p.ne * 4);
+    p.vals = at; at += al(p.ne * 4);
+    p.count = at; at += al(nbins * 4);
+    p.tiles = at; at += al(p.ntiles * 4);
+    p.total = at;
+    return p;
+}
+
+int64_t accel_bins(const int32_t* dims) {
+    const int B = dims[3];
+    if (B < 1) return -1;
+    const int64_t nbx = (dims[0] + B - 1) / B, nby = (dims[1] + B - 1) / B, nbz = (dims[2] + B - 1) / B;
+    const int64_t S = std::max(1, 32 / B);
+    const int64_t ns = ((nbx + S - 1) / S) * ((nby + S - 1) / S) * ((nbz + S - 1) / S);
+    return nbx * nby * nbz + ns + 1;
+}
+
+constexpr int64_t kMaxBins = int64_t(kScanTile) * kScanTile;  // one tile-sum CTA covers them
+constexpr int64_t kMaxBinnedPoints = int64_t(1) << 31;          // sorted positions are int32
 
 // ------------------------------------------------------------------------------------ multires
 struct Multi {
@@ -350,12 +546,23 @@ extern "C" {
 // whole chain / program.
 int fb_query_prepare(const FbPrim* d_prims, int32_t n_prims, void* d_primf, void* stream) noexcept;
 
+// Scratch bytes of the sorted query path for n points (with_grad: value + gradient, 7 evaluations
+// per point) on an accelerated grid of dims (nx, ny, nz, B); -1 when that grid takes the unsorted path.
+int64_t fb_query_scratch_bytes(const int32_t* accel_dims, int64_t n, int32_t with_grad) noexcept {
+    if (!accel_dims || n < 0) return -1;
+    const int64_t nbins = accel_bins(accel_dims);
+    const int nvar = with_grad ? 7 : 1;
+    if (nbins <= 0 || nbins > kMaxBins || n * nvar >= kMaxBinnedPoints) return -1;
+    return binned_plan(n, nvar, nbins).total;
+}
+
 int fb_query_points_device(const void* d_primf, const FbInsn* d_chain, int32_t n_chain, int32_t mode,
                            const void* accel_pool, const int64_t* accel_off, const int32_t* accel_len,
                            const double* accel_grid /* x0,y0,z0,pitch */, const int32_t* accel_dims /* nx,ny,nz,B */,
                            const int32_t* d_kind, const int32_t* blk_off, const int32_t* blk_len,
                            const uint32_t* blk_pool, int64_t blk_cap, int32_t blk_all, const float* d_points, int64_t n,
-                           double h, float* d_value, float* d_grad, void* stream) noexcept {
+                           double h, float* d_value, float* d_grad, void* d_scratch, int64_t scratch_len,
+                           void* stream) noexcept {
     if (!d_primf || !d_chain || n_chain < 1 || !d_points || n < 0 || (!d_value && !d_grad)) return FB_INVALID;
     if (n == 0) return FB_OK;
     Accel A{};
@@ -381,6 +588,38 @@ int fb_query_points_device(const void* d_primf, const FbInsn* d_chain, int32_t n
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)fb_sm_count() * 16);
     const PrimF* primf = static_cast<const PrimF*>(d_primf);
+    const int nvar = d_grad ? 7 : 1;
+    const int64_t nbins = A.pool ? accel_bins(accel_dims) : -1;
+    if (d_scratch && A.pool && nbins > 0 && nbins <= kMaxBins && n * nvar < kMaxBinnedPoints) {
+        const BinnedPlan P = binned_plan(n, nvar, nbins);
+        if (scratch_len < P.total) return FB_INVALID;
+        char* b = static_cast<char*>(d_scratch);
+        int32_t* keys = reinterpret_cast<int32_t*>(b + P.keys);
+        int32_t* order = reinterpret_cast<int32_t*>(b + P.order);
+        float* vals = d_grad ? reinterpret_cast<float*>(b + P.vals) : d_value;
+        int32_t* count = reinterpret_cast<int32_t*>(b + P.count);
+        int32_t* tiles = reinterpret_cast<int32_t*>(b + P.tiles);
+        const int ge = (int)std::min<int64_t>((P.ne + 255) / 256, (int64_t)fb_sm_count() * 16);
+        FB_CUDA(cudaMemsetAsync(count, 0, nbins * 4, st));
+        k_query_keys<<<ge, 256, 0, st>>>(A, n_chain, d_points, P.ne, nvar, h, keys, count);
+        FB_LAUNCH();
+        k_scan_tiles<<<(unsigned)P.ntiles, kScanThreads, 0, st>>>(count, nbins, tiles);
+        FB_LAUNCH();
+        k_scan_sums<<<1, kScanThreads, 0, st>>>(tiles, (int)P.ntiles);
+        FB_LAUNCH();
+        k_scan_add<<<(int)std::min<int64_t>((nbins + 255) / 256, (int64_t)fb_sm_count() * 16), 256, 0, st>>>(
+            count, nbins, tiles);
+        FB_LAUNCH();
+        k_query_scatter<<<ge, 256, 0, st>>>(keys, P.ne, count, order);
+        FB_LAUNCH();
+        k_query_eval_sorted<<<ge, 256, 0, st>>>(primf, d_chain, n_chain, A, d_points, P.ne, nvar, h, order, vals);
+        FB_LAUNCH();
+        if (d_grad) {
+            k_query_combine<<<grid, 128, 0, st>>>(vals, n, h, d_grad, d_value);
+            FB_LAUNCH();
+        }
+        return FB_OK;
+    }
     if (d_grad) {
         k_gradient_points<<<grid, 128, 0, st>>>(primf, d_chain, n_chain, mode, A, d_points, n, h, d_grad, d_value);
     } else {

@@ -59,13 +59,23 @@ class RecipeQueries:
                        (builder.kind.data_ptr(), boff.value, blen.value, bpool.value, bcap.value, ball.value), builder)
 
     def _run(self, pts, value, grad, h=0.05, stream=None):
+        import torch
         a = self._accel
+        scratch, nscratch = None, 0
+        if a is not None and pts.shape[0] > 0:
+            nbytes = int(self.lib.fb_query_scratch_bytes(a[4].ctypes.data, pts.shape[0], 1 if grad is not None else 0))
+            if nbytes > 0:
+                scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+                nscratch = nbytes
+                if isinstance(stream, torch.cuda.Stream):  # freed only after that stream's kernels
+                    scratch.record_stream(stream)
         args = (a[0], a[1], a[2], a[3].ctypes.data, a[4].ctypes.data, *a[5]) if a else (None,) * 5 + (None, None,
                                                                                                      None, None, 0, 0)
         st = self.lib.fb_query_points_device(self.primf.data_ptr(), self.chain.data_ptr(), self.n_chain, self.mode,
                                              *args, pts.data_ptr(), pts.shape[0], float(h),
                                              value.data_ptr() if value is not None else None,
                                              grad.data_ptr() if grad is not None else None,
+                                             scratch.data_ptr() if scratch is not None else None, nscratch,
                                              _lib.stream_handle(stream))
         _lib.check(st, "point query")
 

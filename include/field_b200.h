@@ -199,7 +199,11 @@ int fb_query_points_device(const void* d_primf, const fb_insn* d_chain, int32_t 
                            const double* accel_grid, const int32_t* accel_dims, const int32_t* d_kind,
                            const int32_t* blk_off, const int32_t* blk_len, const uint32_t* blk_pool, int64_t blk_cap,
                            int32_t blk_all, const float* d_points, int64_t n, double h, float* d_value, float* d_grad,
-                           void* stream);
+                           void* d_scratch, int64_t scratch_len, void* stream);
+/* Scratch of the sorted query path (evaluation points sorted by the culled list they walk, so a
+ * warp's lanes share one list); -1 when the grid takes the unsorted path.  No reference
+ * counterpart: an execution strategy of fb_query_points_device, same results bit for bit. */
+int64_t fb_query_scratch_bytes(const int32_t* accel_dims, int64_t n, int32_t with_grad);
 
 /* Replace the per-block-pitch field's lattices and its avstand / gradient queries,
  * src/field_engine/faltkarna_v1_multires.py:84-104,384-459 (lattices built from a recipe). */
