@@ -40,7 +40,9 @@ constexpr int kCapCoarse = 1024;           // least list capacity of a coarse re
 constexpr int kCapSuper = 256;             // least list capacity of a superblock
 constexpr int64_t kCapBudget = 8 << 20;    // list entries per level beyond which capacities stop growing
 constexpr int kCapBlock = 48;              // per-block list of the thread-per-block cull; leaf staging chunk
-constexpr int kCapBlockWarp = 96;          // per-block list of the warp-per-block cull
+constexpr int kCapBlockWarp = 96;          // least per-block list of the warp-per-block cull
+constexpr int kCapBlockWarpMax = 1024;     // ... grown while the lists stay within kCapBlockBudget
+constexpr int64_t kCapBlockBudget = 4 << 20;
 constexpr int64_t kWarpCullBlocks = 1 << 17;  // grids up to this many blocks cull each block with a warp
 constexpr int kSuperEdge = 32;    // voxels per superblock edge
 constexpr int kCoarseDiv = 2;     // superblocks per coarse-region edge
@@ -102,7 +104,8 @@ struct Plan {
     int64_t pool_full, pool_coarse, pool_super;  // element offsets inside pool
     int64_t ntiles;
     int cap_coarse, cap_super;  // list capacities per coarse region / superblock
-    bool warp_blocks;           // per-block lists culled by one warp each, at blk_pool + b * kCapBlockWarp
+    bool warp_blocks;           // per-block lists culled by one warp each, at blk_pool + b * cap_block
+    int cap_block;              // their capacity
 };
 
 // List capacity of a level: grows while the level's lists stay within kCapBudget entries, never
@@ -121,6 +124,8 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     p.cap_coarse = level_cap(G.ncoarse, kCapCoarse, n_chain);
     p.cap_super = level_cap(G.nsuper, kCapSuper, n_chain);
     p.warp_blocks = G.nblocks <= kWarpCullBlocks;
+    p.cap_block = (int)std::min<int64_t>(
+        kCapBlockWarpMax, std::max<int64_t>(kCapBlockWarp, kCapBlockBudget / std::max<int64_t>(G.nblocks, 1)));
     p.pool_full = 0;
     p.pool_coarse = n_chain;
     p.pool_super = p.pool_coarse + G.ncoarse * p.cap_coarse;
@@ -133,7 +138,7 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     p.misc = at; at += 256;  // [0] ticket, [1] error flag, [2] block-list pool cursor
     p.blk_off = at; at += align256(G.nblocks * 4);
     p.blk_len = at; at += align256(G.nblocks * 4);
-    p.blk_cap = p.warp_blocks ? G.nblocks * kCapBlockWarp : std::max<int64_t>(G.nblocks * 12, 4096);
+    p.blk_cap = p.warp_blocks ? G.nblocks * p.cap_block : std::max<int64_t>(G.nblocks * 12, 4096);
     p.blk_pool = at; at += align256(p.blk_cap * 4);
     p.total = at;
     return p;
@@ -340,27 +345,24 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
             continue;
         }
         const int op = head.op;
-        // end of the run
-        int j = i + 1;
-        while (j < n_in) {
-            const int e = j + lane;
-            bool same = false;
-            if (e < n_in) {
-                const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, false);
-                same = E.op == op && runnable(E.op, E.k);
-            }
-            const unsigned stop = __ballot_sync(0xffffffffu, !same);
-            if (stop) { j += __ffs(stop) - 1; break; }
-            j += 32;
-        }
-        j = min(j, n_in);
-        // pass 1: aggregate bound of the run
+        // pass 1, 32 elements at a time: the run's end (the first element of another kind) and the
+        // aggregate bound of the elements before it
         float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
-        for (int b = i; b < j; b += 32) {
+        int j = n_in;
+        for (int b = i; b < n_in; b += 32) {
             const int e = b + lane;
-            if (e < j) {
-                const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
-                agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+            bool same = false;
+            Elem E;
+            if (e < n_in) {
+                E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+                same = e == i || (E.op == op && runnable(E.op, E.k));
+            }
+            const unsigned stop = __ballot_sync(0xffffffffu, e < n_in && !same);
+            const int end = stop ? b + __ffs(stop) - 1 : min(b + 32, n_in);
+            if (e < end) agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+            if (stop) {
+                j = end;
+                break;
             }
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -432,16 +434,14 @@ __device__ int seq_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn*
             continue;
         }
         const int op = head.op;
-        int j = i + 1;
-        while (j < n_in) {
-            const Elem E = load_elem(in, j, chain, primf, cx, cy, cz, R, eps, false);
-            if (!(E.op == op && runnable(E.op, E.k))) break;
-            ++j;
-        }
+        // pass 1: the run's end and its aggregate bound in one traversal
         float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
-        for (int e = i; e < j; ++e) {
-            const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+        int j = i;
+        while (j < n_in) {
+            const Elem E = load_elem(in, j, chain, primf, cx, cy, cz, R, eps, true);
+            if (j > i && !(E.op == op && runnable(E.op, E.k))) break;
             agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+            ++j;
         }
         const RunState rs = run_decide(op, agg, alo, ahi);
         if (rs.reset) n = 0;
@@ -1305,7 +1305,7 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
         if (P.warp_blocks) {
             k_cull_blocks<<<fb_div_up(G.nblocks * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off + G.ncoarse,
                                                                          S.len + G.ncoarse, S.blk_off, S.blk_len,
-                                                                         S.blk_pool, kCapBlockWarp);
+                                                                         S.blk_pool, P.cap_block);
             FB_LAUNCH();
             k_classify<true, true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
                 G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
