@@ -92,9 +92,10 @@ class FieldBuilder:
 
     ``build()`` returns a DeviceField sized exactly (one 4-byte count read between the classify and
     leaf launches); ``enqueue(capacity_tiles)`` runs the whole build stream-ordered into a fixed
-    tile buffer (CUDA-graph capturable)."""
+    tile buffer (CUDA-graph capturable).  ``alloc`` (optional) supplies the one device allocation
+    the builder makes (outputs + scratch), e.g. from a server's memory pool."""
 
-    def __init__(self, recipe, meta: GridMeta, *, device="cuda", guard=None, library=None):
+    def __init__(self, recipe, meta: GridMeta, *, device="cuda", guard=None, library=None, alloc=None):
         import torch
         self.lib = _lib.lib(library)
         self.meta = meta
@@ -117,7 +118,9 @@ class FieldBuilder:
         nb = meta.n_blocks
         part = lambda n: (n + 255) // 256 * 256
         sizes = (part(nb * 4), part(nb * 4), part(nb * 4), 256, part(int(nbytes)))
-        self.slab = torch.empty(sum(sizes), dtype=torch.uint8, device=self.device)
+        # `alloc(nbytes) -> uint8 device tensor` lets a caller place the slab in its own memory pool
+        self.slab = (alloc(sum(sizes)) if alloc is not None
+                     else torch.empty(sum(sizes), dtype=torch.uint8, device=self.device))
         views, at = [], 0
         for size in sizes:
             views.append(self.slab[at:at + size])

@@ -25,9 +25,11 @@ timed-out request fails its future, the server stays usable.
 """
 from __future__ import annotations
 
+import bisect
 import collections
 import threading
 import time
+import weakref
 from concurrent.futures import Future
 
 import numpy as np
@@ -36,6 +38,58 @@ from . import _lib
 from . import expr as X
 from .build import FieldBuilder
 from .query import RecipeQueries
+
+
+class DeviceArena:
+    """One device allocation handed out by first fit, so that resident fields do not each cost a
+    cudaMalloc (which can stall the whole process for tens of milliseconds on large sizes).
+
+    ``alloc(nbytes)`` returns a uint8 view of the arena, or None when no free range fits.  The range
+    returns to the free list when that view object is garbage collected: keep it referenced for as
+    long as any tensor derived from it is in use (derived views do not keep it alive).  In the server
+    a field's buffers die only after every request that used them has seen its GPU work complete, so
+    a returned range is never still being written."""
+
+    ALIGN = 512
+
+    def __init__(self, nbytes, device):
+        import torch
+        self.nbytes = int(nbytes) // self.ALIGN * self.ALIGN
+        self.base = torch.empty(self.nbytes, dtype=torch.uint8, device=device)
+        self.free = [(0, self.nbytes)]  # (offset, size), sorted by offset, coalesced
+        self.used = 0
+        self.lock = threading.Lock()
+
+    def alloc(self, nbytes):
+        n = max(self.ALIGN, (int(nbytes) + self.ALIGN - 1) // self.ALIGN * self.ALIGN)
+        with self.lock:
+            for i, (off, size) in enumerate(self.free):
+                if size >= n:
+                    if size == n:
+                        del self.free[i]
+                    else:
+                        self.free[i] = (off + n, size - n)
+                    self.used += n
+                    break
+            else:
+                return None
+        view = self.base[off:off + int(nbytes)]
+        weakref.finalize(view, self._release, off, n)
+        return view
+
+    def _release(self, off, n):
+        with self.lock:
+            self.used -= n
+            i = bisect.bisect_left(self.free, (off, 0))
+            # merge with the following and the preceding free range
+            if i < len(self.free) and self.free[i][0] == off + n:
+                n += self.free[i][1]
+                del self.free[i]
+            if i > 0 and self.free[i - 1][0] + self.free[i - 1][1] == off:
+                off, n = self.free[i - 1][0], self.free[i - 1][1] + n
+                del self.free[i - 1]
+                i -= 1
+            self.free.insert(i, (off, n))
 
 
 class _Field:
@@ -48,6 +102,7 @@ class _Field:
         self.n_active = n_active
         self.queries = None  # (RecipeQueries, CUDA event marking its tables ready)
         self.edt = None
+        self.owners = []  # arena blocks behind tiles / edt (they must outlive those views)
         self.busy = 0
         self.editing = False
         self.last_use = time.perf_counter()
@@ -108,11 +163,14 @@ def _prepare(kind, args):
 
 
 class FieldServer:
-    def __init__(self, *, device="cuda", slots=8, budget_bytes=150e9, request_timeout_s=30.0):
+    def __init__(self, *, device="cuda", slots=8, budget_bytes=150e9, request_timeout_s=30.0, arena_bytes=0):
+        """arena_bytes > 0: resident field buffers come from one DeviceArena of that size (requests
+        that do not fit fall back to the caching allocator)."""
         import torch
         dev = torch.device(device)
         # an explicit index: the scheduler thread selects this device with torch.cuda.set_device
         self.device = dev if dev.index is not None else torch.device("cuda", torch.cuda.current_device())
+        self.arena = DeviceArena(arena_bytes, self.device) if arena_bytes else None
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
         self.free = collections.deque(range(slots))
         self.budget = float(budget_bytes)
@@ -162,6 +220,12 @@ class FieldServer:
 
     def resident_bytes(self):
         return self.resident
+
+    def _alloc(self, nbytes):
+        """uint8 device block for a resident buffer: from the arena when it fits."""
+        import torch
+        blk = self.arena.alloc(nbytes) if self.arena is not None else None
+        return blk if blk is not None else torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
 
     def _account(self, f):
         """Bring the resident total up to date after field `f` changed its buffers."""
@@ -322,35 +386,39 @@ class FieldServer:
     def _build_field(self, comp, meta, stream):
         import torch
         with torch.cuda.stream(stream):
-            fb = FieldBuilder(comp, meta, device=self.device)
+            fb = FieldBuilder(comp, meta, device=self.device, alloc=self._alloc)
             fb.classify(stream)
             count = torch.empty(1, dtype=torch.int32, pin_memory=True)
             count.copy_(fb.count, non_blocking=True)
         yield self._record(stream)
         n = int(count[0])
         with torch.cuda.stream(stream):
-            tiles = torch.empty((max(n, 1), meta.block ** 3), dtype=torch.float32, device=self.device)
+            b3 = meta.block ** 3
+            owner = self._alloc(max(n, 1) * b3 * 4)
+            tiles = owner.view(torch.float32).view(max(n, 1), b3)
             if n:
                 fb.leaf(tiles, n, stream=stream)
         yield self._record(stream)
-        return fb, tiles, n
+        return fb, tiles, owner, n
 
     def _run_build(self, r, stream):
         comp, meta = r.args["recipe"], r.args["meta"]
-        fb, tiles, n = yield from self._build_field(comp, meta, stream)
+        fb, tiles, owner, n = yield from self._build_field(comp, meta, stream)
         fid = self.next_id
         self.next_id += 1
         self.fields[fid] = _Field(fid, comp, meta, fb, tiles, n)
+        self.fields[fid].owners = [owner]
         self._account(self.fields[fid])
         return dict(field=fid, n_active=n, leaf_voxels=n * meta.block ** 3)
 
     def _run_edit(self, r, stream):
         f = self.fields[r.field]
         comp = X.extend(f.comp, r.args["tool_prims"], r.args["op"])
-        fb, tiles, n = yield from self._build_field(comp, f.meta, stream)
+        fb, tiles, owner, n = yield from self._build_field(comp, f.meta, stream)
         f.comp, f.fb, f.tiles, f.n_active = comp, fb, tiles, n
         f.queries = None
         f.edt = None
+        f.owners = [owner]
         if f.id in self.fields:
             self._account(f)
         return dict(field=f.id, n_active=n, leaf_voxels=n * f.meta.block ** 3)
@@ -380,11 +448,12 @@ class FieldServer:
         f = self.fields[r.field]
         m = f.meta
         lib = _lib.lib()
-        fb, tiles, n_active = f.fb, f.tiles, f.n_active
+        fb, tiles, n_active, owners = f.fb, f.tiles, f.n_active, list(f.owners)  # held until the GPU is done
         with torch.cuda.stream(stream):
             slot = torch.empty(m.n_blocks, dtype=torch.int32, device=self.device)
             mask = torch.empty((m.nx, m.ny, m.nz), dtype=torch.uint8, device=self.device)
-            out = torch.empty((m.nx, m.ny, m.nz), dtype=torch.int32, device=self.device)
+            out_owner = self._alloc(m.nx * m.ny * m.nz * 4)
+            out = out_owner.view(torch.int32).view(m.nx, m.ny, m.nz)
             scratch = torch.empty(int(lib.fb_edt_scratch_bytes(m.nx, m.ny, m.nz, 0)), dtype=torch.uint8,
                                   device=self.device)
             _lib.check(lib.fb_field_occupancy_device(fb.kind.data_ptr(), fb.active.data_ptr(), fb.count.data_ptr(),
@@ -400,6 +469,7 @@ class FieldServer:
         yield self._record(stream)
         if f.fb is fb:
             f.edt = out
+            f.owners = owners + [out_owner]
             if f.id in self.fields:
                 self._account(f)
         return dict(field=f.id, checksum=int(host.item()), voxels=int(out.numel()))

@@ -35,7 +35,8 @@ def _same(a, b):
     return a == b
 
 
-def test_results_alone_equal_results_in_the_mix():
+@pytest.mark.parametrize("arena", [0, 2e9])  # the caching allocator, or resident buffers from an arena
+def test_results_alone_equal_results_in_the_mix(arena):
     import field_b200.serve as S
     import field_b200.batch as BT
     metas = [BT.cube_meta(n, b) for n, b in ((64, 8), (128, 8), (96, 4), (128, 16))]
@@ -45,7 +46,7 @@ def test_results_alone_equal_results_in_the_mix():
         reqs = _requests(fields, np.random.default_rng(0))
         alone = [srv.submit(k, **a).result(timeout=60) for k, a in reqs]
     # run 2: the same builds and requests submitted all at once
-    with S.FieldServer(slots=4) as srv:
+    with S.FieldServer(slots=4, arena_bytes=arena) as srv:
         futs = [srv.submit("build", recipe=_recipe(i), meta=m) for i, m in enumerate(metas)]
         fields2 = [f.result(timeout=60)["field"] for f in futs]
         assert fields2 == fields
@@ -107,3 +108,18 @@ def test_a_failing_request_leaves_the_server_usable():
             srv.submit("build", recipe={"op": "nonsense"}, meta=BT.cube_meta(64, 8)).result(timeout=60)
         out = srv.submit("edt", field=fid).result(timeout=60)
         assert out["voxels"] == 64 ** 3
+
+
+def test_arena_ranges_return_when_fields_go():
+    import gc
+    import field_b200.serve as S
+    import field_b200.batch as BT
+    with S.FieldServer(slots=2, arena_bytes=1e9) as srv:
+        ids = [srv.submit("build", recipe=_recipe(i), meta=BT.cube_meta(96, 8)).result(timeout=60)["field"]
+               for i in range(3)]
+        srv.submit("edt", field=ids[0]).result(timeout=60)
+        srv.submit("edit", field=ids[1], tools=[], op="subtract").result(timeout=60)
+        assert srv.arena.used > 0
+        srv.fields.clear()
+    gc.collect()
+    assert srv.arena.used == 0 and srv.arena.free == [(0, srv.arena.nbytes)]
