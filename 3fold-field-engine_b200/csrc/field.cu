@@ -924,7 +924,7 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
 // voxels along z (VG = 4, or 2 for 4^3 blocks) and stores each group with one vector store.
 template <int B>
-__global__ void __launch_bounds__(32 * kLeafWarps, 4) k_leaf(Geo G, const FbPrim* __restrict__ prims,
+__global__ void __launch_bounds__(32 * kLeafWarps, 6) k_leaf(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
                                                              const FbInsn* __restrict__ chain,
                                                              const uint32_t* __restrict__ pool,
@@ -939,7 +939,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4) k_leaf(Geo G, const FbPrim
                                                              const int32_t* __restrict__ blk_len,
                                                              const uint32_t* __restrict__ blk_pool, int64_t blk_cap) {
     constexpr int kVox = B * B * B;
-    constexpr int VG = B == 4 ? 2 : 8;
+    constexpr int VG = B == 4 ? 2 : 4;
     constexpr int kGroups = kVox / (32 * VG);
     __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
     __shared__ uint32_t s_list[kLeafWarps][kCapBlock];

@@ -93,6 +93,10 @@ class ClockSampler:
         except Exception as e:  # no NVML: the line says so
             self.error = f"nvml unavailable: {e!r}"[:120]
             return
+        # the timing loop holds the interpreter lock between its launches; a short switch interval lets
+        # the sampler run every few milliseconds (device timing is by CUDA events, unaffected)
+        self.switch = sys.getswitchinterval()
+        sys.setswitchinterval(0.0005)
         self.thread = threading.Thread(target=self._run, daemon=True)
         self.thread.start()
 
@@ -112,6 +116,7 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not sampled"], "samples": 0}
         self.stop_flag.set()
         self.thread.join(timeout=5)
+        sys.setswitchinterval(self.switch)
         sm = [c for c, _ in self.samples]
         reasons = sorted({name for _, mask in self.samples for name, bit in self.REASONS if mask & bit})
         out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
