@@ -156,7 +156,7 @@ __global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* 
     F.type = P.type;
     F.s = (float)P.s;
     F.off = (float)P.off;
-    F.pad0 = F.pad1 = F.pad2 = 0.f;
+    F.ball = F.ball_k = F.pad = 0.f;
     bool ident = true;
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) ident &= P.A[r * 4 + c] == (r == c ? 1.0 : 0.0);
@@ -201,6 +201,45 @@ __global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* 
         for (int j = 0; j < 12; ++j) F.p[j] = (float)p[j];
     }
     F.lip = (float)(fabs(P.s) * sqrt(row) * canon * (1.0 + 1e-6));
+    // Bounding ball, for kinds whose canonical value is the exact Euclidean distance, of the
+    // canonical solid (centre cc, radius rc).  When the frame map is a similarity (A_lin^T A_lin =
+    // a^2 I) and s > 0, value(x) = s a d_world(x) - off with d_world the exact distance to the world
+    // solid, which lies in the ball of centre A_lin^-1 (cc - t), radius rc / a: so
+    //   s a (|x - c| - r) - off <= value(x) <= s a (|x - c| + r) - off.
+    // Stored in the spare slots p[8..11] (these kinds read p[0..4] only), flagged by ball = 1.
+    double cc[3] = {0.0, 0.0, 0.0}, rc = -1.0;
+    switch (P.type) {
+    case P_SPHERE: rc = p[0]; break;
+    case P_BOX: rc = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]); break;
+    case P_CYLINDER: rc = sqrt(p[0] * p[0] + p[1] * p[1]); break;
+    case P_CAPSULE: {
+        const double len = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+        for (int c = 0; c < 3; ++c) cc[c] = 0.5 * p[c];
+        rc = 0.5 * len + p[3];
+        break;
+    }
+    case P_TORUS: rc = p[0] + p[1]; break;
+    default: break;
+    }
+    const double a2 = (G[0][0] + G[1][1] + G[2][2]) / 3.0;
+    bool similar = rc >= 0.0 && a2 > 0.0 && P.s > 0.0;
+    for (int r = 0; r < 3 && similar; ++r)
+        for (int c = 0; c < 3; ++c) similar &= fabs(G[r][c] - (r == c ? a2 : 0.0)) <= 1e-9 * a2;
+    if (similar) {
+        const double a = sqrt(a2);
+        double cw[3];
+        for (int c = 0; c < 3; ++c) {  // A_lin^-1 = A_lin^T / a^2 for a similarity
+            double v = 0.0;
+            for (int r = 0; r < 3; ++r) v += P.A[r * 4 + c] * (cc[r] - P.A[r * 4 + 3]);
+            cw[c] = v / a2;
+        }
+        const double rw = rc / a;
+        const double mag = fmax(fabs(cw[0]), fmax(fabs(cw[1]), fabs(cw[2])));
+        F.ball = 1.f;
+        F.ball_k = (float)(P.s * a);
+        for (int c = 0; c < 3; ++c) F.p[8 + c] = (float)cw[c];
+        F.p[11] = (float)(rw * (1.0 + 1e-6) + 1e-6 * mag);  // covers rounding the centre to float32
+    }
     out[i] = F;
 }
 
@@ -271,9 +310,21 @@ struct Elem {
     float lo, hi;  // bounds of the value the combine sees (-p for a subtraction)
 };
 
+// The same enclosure from the primitive's bounding ball (PrimF.ball == 1): no evaluation of the
+// primitive, a few loads -- looser by up to the ball's diameter.
+__device__ __forceinline__ void element_interval_ball(const PrimF& P, float cx, float cy, float cz, float R, float eps,
+                                                      float& lo, float& hi) {
+    const float dx = cx - P.p[8], dy = cy - P.p[9], dz = cz - P.p[10];
+    const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    const float k = P.ball_k, rw = P.p[11];
+    const float m = eps + 1e-6f * (k * (d + R + rw) + fabsf(P.off));
+    lo = fmaf(k, d - R - rw, -P.off) - m;
+    hi = fmaf(k, d + R + rw, -P.off) + m;
+}
+
 __device__ __forceinline__ Elem load_elem(const uint32_t* __restrict__ in, int e, const FbInsn* __restrict__ chain,
                                           const PrimF* __restrict__ primf, float cx, float cy, float cz, float R,
-                                          float eps, bool with_bounds) {
+                                          float eps, bool with_bounds, bool ball = false) {
     Elem E;
     E.ent = in ? in[e] : (uint32_t)e << 2;  // a null list is the whole chain in order
     const FbInsn I = chain[E.ent >> 2];
@@ -282,7 +333,9 @@ __device__ __forceinline__ Elem load_elem(const uint32_t* __restrict__ in, int e
     E.lo = E.hi = 0.f;
     if (with_bounds && E.op != CH_OFFSET) {
         float lo, hi;
-        element_interval(primf[I.arg], cx, cy, cz, R, eps, lo, hi);
+        const PrimF& P = primf[I.arg];
+        if (ball && P.ball != 0.f) element_interval_ball(P, cx, cy, cz, R, eps, lo, hi);
+        else element_interval(P, cx, cy, cz, R, eps, lo, hi);
         if (E.op == CH_SUBTRACT || E.op == CH_SETNEG) { E.lo = -hi; E.hi = -lo; }
         else { E.lo = lo; E.hi = hi; }
     }
@@ -319,6 +372,9 @@ __device__ __forceinline__ bool run_keep(int op, const Elem& E, float bound) {
 // Hard runs are decided with two warp-parallel passes (aggregate bound, then keep/drop with
 // ballot compaction); other elements (offsets, smooth booleans, sets) step one at a time.
 // Returns the kept count (may exceed cap: then the output is incomplete and must not be used).
+// kBall: bound primitives by their bounding balls where they have one (the coarse level, where
+// every region walks the whole chain).
+template <bool kBall = false>
 __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn* __restrict__ chain,
                          const PrimF* __restrict__ primf, float cx, float cy, float cz, float R, float eps,
                          uint32_t* __restrict__ out, int cap) {
@@ -354,7 +410,7 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
             bool same = false;
             Elem E;
             if (e < n_in) {
-                E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+                E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true, kBall);
                 same = e == i || (E.op == op && runnable(E.op, E.k));
             }
             const unsigned stop = __ballot_sync(0xffffffffu, e < n_in && !same);
@@ -369,29 +425,88 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
             const float t = __shfl_xor_sync(0xffffffffu, agg, o);
             agg = op == CH_UNION ? fminf(agg, t) : fmaxf(agg, t);
         }
-        const RunState rs = run_decide(op, agg, alo, ahi);
-        if (rs.reset) n = 0;
-        bool first = rs.reset;
+        RunState rs = run_decide(op, agg, alo, ahi);
         float klo = 3.0e38f, khi = -3.0e38f;
-        // pass 2: keep / drop, ballot compaction in chain order
-        for (int b = i; b < j; b += 32) {
-            const int e = b + lane;
-            bool keep = false;
-            Elem E;
-            if (e < j) {
-                E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
-                keep = run_keep(op, E, rs.bound);
-                if (keep) { klo = fminf(klo, E.lo); khi = fmaxf(khi, E.hi); }
+        if (kBall) {
+            // the ball bounds pick candidates (every other element of the run provably loses, so the
+            // run's result is the candidates' result); the exact bounds of the candidates alone then
+            // give the run's decision, and the candidates are compacted in place with it
+            const int n0 = n;
+            for (int b = i; b < j; b += 32) {
+                const int e = b + lane;
+                bool keep = false;
+                Elem E;
+                if (e < j) {
+                    E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true, true);
+                    keep = run_keep(op, E, rs.bound);
+                }
+                const unsigned kept = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = n + __popc(kept & below);
+                    if (pos < cap) out[pos] = E.ent;
+                }
+                n += __popc(kept);
             }
-            const unsigned kept = __ballot_sync(0xffffffffu, keep);
-            if (keep) {
-                const int pos = n + __popc(kept & below);
-                uint32_t rec = E.ent;
-                if (first && pos == 0) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
-                if (pos < cap) out[pos] = rec;
+            const int nc = n - n0;  // candidates at out[n0, n)
+            if (n > cap) {          // overflowed: the region falls back to its parent's list anyway
+                i = j;
+                continue;
             }
-            if (kept) first = false;
-            n += __popc(kept);
+            float agg2 = op == CH_UNION ? 3.0e38f : -3.0e38f;
+            for (int b = 0; b < nc; b += 32) {
+                if (b + lane < nc) {
+                    const Elem E = load_elem(out + n0, b + lane, chain, primf, cx, cy, cz, R, eps, true);
+                    agg2 = op == CH_UNION ? fminf(agg2, E.hi) : fmaxf(agg2, E.lo);
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float t = __shfl_xor_sync(0xffffffffu, agg2, o);
+                agg2 = op == CH_UNION ? fminf(agg2, t) : fmaxf(agg2, t);
+            }
+            rs = run_decide(op, agg2, alo, ahi);
+            n = rs.reset ? 0 : n0;  // compaction target: positions never above the ones being read
+            bool first = rs.reset;
+            for (int b = 0; b < nc; b += 32) {
+                bool keep = false;
+                Elem E;
+                if (b + lane < nc) {
+                    E = load_elem(out + n0, b + lane, chain, primf, cx, cy, cz, R, eps, true);
+                    keep = run_keep(op, E, rs.bound);
+                    if (keep) { klo = fminf(klo, E.lo); khi = fmaxf(khi, E.hi); }
+                }
+                const unsigned kept = __ballot_sync(0xffffffffu, keep);  // every read precedes the writes
+                if (keep) {
+                    const int pos = n + __popc(kept & below);
+                    uint32_t rec = E.ent;
+                    if (first && pos == 0) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
+                    out[pos] = rec;
+                }
+                if (kept) first = false;
+                n += __popc(kept);
+            }
+        } else {
+            if (rs.reset) n = 0;
+            bool first = rs.reset;
+            // pass 2: keep / drop, ballot compaction in chain order
+            for (int b = i; b < j; b += 32) {
+                const int e = b + lane;
+                bool keep = false;
+                Elem E;
+                if (e < j) {
+                    E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+                    keep = run_keep(op, E, rs.bound);
+                    if (keep) { klo = fminf(klo, E.lo); khi = fmaxf(khi, E.hi); }
+                }
+                const unsigned kept = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = n + __popc(kept & below);
+                    uint32_t rec = E.ent;
+                    if (first && pos == 0) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
+                    if (pos < cap) out[pos] = rec;
+                }
+                if (kept) first = false;
+                n += __popc(kept);
+            }
         }
         for (int o = 16; o > 0; o >>= 1) {
             klo = fminf(klo, __shfl_xor_sync(0xffffffffu, klo, o));
@@ -472,6 +587,7 @@ __device__ int seq_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn*
 
 // Level cull.  Regions of `edge` voxels on a (rnx, rny, rnz) grid; parent region = coords / div
 // on a (pnx, pny, pnz) grid (parent_off == nullptr: the single full list [0, n_full)).
+template <bool kBall>
 __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
                        uint32_t* __restrict__ pool, const int64_t* __restrict__ parent_off,
                        const int32_t* __restrict__ parent_len, int n_full, int div, int pny, int pnz,
@@ -494,7 +610,8 @@ __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __r
     const float cz = G.fz0 + (rz * edge + half) * G.fpitch;
     const float R = 1.7320509f * half * G.fpitch;
     uint32_t* dst = pool + pool_base + r * cap;
-    const int n = warp_walk(parent_off ? pool + poff : nullptr, plen, chain, primf, cx, cy, cz, R, G.eps, dst, cap);
+    const int n = warp_walk<kBall>(parent_off ? pool + poff : nullptr, plen, chain, primf, cx, cy, cz, R, G.eps, dst,
+                                   cap);
     if ((threadIdx.x & 31) == 0) {
         if (n <= cap) {
             off[r] = pool_base + r * cap;
@@ -1291,13 +1408,13 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
         FB_LAUNCH();
         const int coarse_edge = kSuperEdge * kCoarseDiv;
         // coarse regions from the full chain
-        k_cull<<<fb_div_up(G.ncoarse * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, nullptr, nullptr, n_chain, 1,
+        k_cull<true><<<fb_div_up(G.ncoarse * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, nullptr, nullptr, n_chain, 1,
                                                                1, 1, S.off, S.len, P.pool_coarse, P.cap_coarse,
                                                                G.S * G.B * kCoarseDiv, G.ncx, G.ncy, G.ncz);
         FB_LAUNCH();
         (void)coarse_edge;
         // superblocks from their coarse region
-        k_cull<<<fb_div_up(G.nsuper * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off, S.len, 0, kCoarseDiv,
+        k_cull<false><<<fb_div_up(G.nsuper * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off, S.len, 0, kCoarseDiv,
                                                               G.ncy, G.ncz, S.off + G.ncoarse, S.len + G.ncoarse,
                                                               P.pool_super, P.cap_super, G.S * G.B, G.nsx, G.nsy, G.nsz);
         FB_LAUNCH();

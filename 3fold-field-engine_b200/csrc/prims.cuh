@@ -32,7 +32,8 @@ static_assert(sizeof(FbInsn) == 16, "fb_insn layout");
 // float32 mirror used for interval culling in world coordinates (128 bytes).
 struct __align__(16) PrimF {
     int32_t type, ident;
-    float s, off, lip, pad0, pad1, pad2;
+    float s, off, lip;
+    float ball, ball_k, pad;  // bounding ball present (1) and its value scale; centre, radius in p[8..11]
     float A[12];
     float p[12];
 };
