@@ -402,9 +402,12 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
         }
         const int op = head.op;
         // pass 1, 32 elements at a time: the run's end (the first element of another kind) and the
-        // aggregate bound of the elements before it
+        // aggregate bound of the elements before it.  With ball bounds the same pass also writes the
+        // candidates: elements not beaten by the bound so far (the minimum over everything up to and
+        // including their chunk) -- a superset of those the final bound keeps.
         float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
         int j = n_in;
+        const int n0 = n;
         for (int b = i; b < n_in; b += 32) {
             const int e = b + lane;
             bool same = false;
@@ -416,6 +419,20 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
             const unsigned stop = __ballot_sync(0xffffffffu, e < n_in && !same);
             const int end = stop ? b + __ffs(stop) - 1 : min(b + 32, n_in);
             if (e < end) agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+            if (kBall) {
+                float run = agg;
+                for (int o = 16; o > 0; o >>= 1) {
+                    const float t = __shfl_xor_sync(0xffffffffu, run, o);
+                    run = op == CH_UNION ? fminf(run, t) : fmaxf(run, t);
+                }
+                const bool keep = e < end && run_keep(op, E, run);
+                const unsigned kept = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = n + __popc(kept & below);
+                    if (pos < cap) out[pos] = E.ent;
+                }
+                n += __popc(kept);
+            }
             if (stop) {
                 j = end;
                 break;
@@ -428,25 +445,9 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
         RunState rs = run_decide(op, agg, alo, ahi);
         float klo = 3.0e38f, khi = -3.0e38f;
         if (kBall) {
-            // the ball bounds pick candidates (every other element of the run provably loses, so the
-            // run's result is the candidates' result); the exact bounds of the candidates alone then
-            // give the run's decision, and the candidates are compacted in place with it
-            const int n0 = n;
-            for (int b = i; b < j; b += 32) {
-                const int e = b + lane;
-                bool keep = false;
-                Elem E;
-                if (e < j) {
-                    E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true, true);
-                    keep = run_keep(op, E, rs.bound);
-                }
-                const unsigned kept = __ballot_sync(0xffffffffu, keep);
-                if (keep) {
-                    const int pos = n + __popc(kept & below);
-                    if (pos < cap) out[pos] = E.ent;
-                }
-                n += __popc(kept);
-            }
+            // pass 1 wrote the candidates (every other element of the run provably loses, so the run's
+            // result is the candidates' result); the exact bounds of the candidates alone give the
+            // run's decision, and the candidates are compacted in place with it
             const int nc = n - n0;  // candidates at out[n0, n)
             if (n > cap) {          // overflowed: the region falls back to its parent's list anyway
                 i = j;
