@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=1024, help="grid edge of the field build")
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=1024,
+                    help="grid edge of the field build (--grid under torchrun, whose parser takes --n for its own)")
     ap.add_argument("--edt-n", type=int, default=512, help="grid edge of the EDT")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -124,6 +125,24 @@ class ClockSampler:
         if self.error:
             out["error"] = self.error
         return out
+
+
+# ------------------------------------------------------------------------------------------ ranks
+def max_over_ranks(x, world, device="cpu"):
+    """The largest value of `x` over all ranks (the job's time is its slowest rank's)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, steps, total_ms):
+    """Whole-job throughput in G units/s: every rank processes `units_per_rank` per step (replicas,
+    weak scaling) and the job takes the slowest rank's `total_ms` for `steps` steps."""
+    return units_per_rank * world * steps / (total_ms * 1e-3) / 1e9
 
 
 # ------------------------------------------------------------------------------------------ workload
@@ -251,13 +270,9 @@ def run_ours(args, rank, world, local_rank):
     t_leaf = [e[1].elapsed_time(e[2]) for e in events]
     t_edt = [e[2].elapsed_time(e[3]) for e in events]
     t_step = [e[0].elapsed_time(e[3]) for e in events]
-    total_ms = float(sum(t_step))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(sum(t_step)), world, dev)
     leaf_voxels = n_active * b3
-    value = leaf_voxels * world * args.steps / (total_ms * 1e-3) / 1e9
+    value = job_rate(leaf_voxels, world, args.steps, total_ms)
 
     # executed work of the leaf kernel and the float32 peak (untimed)
     work = torch.zeros(2, dtype=torch.int64, device=dev)
@@ -681,7 +696,8 @@ def main():
         if backend == "nccl":
             import torch
             torch.cuda.set_device(local_rank)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        # short: ranks that wait for a lost peer end with an error instead of hanging
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
     try:
         if args.impl == "reference":
             res = run_reference(args, rank, world)
