@@ -671,8 +671,10 @@ __device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, in
 __host__ __device__ __forceinline__ int threads_per_super(int S) { return ((S * S * S + 31) / 32) * 32; }
 
 // kListed: the per-block lists are already in blk_pool (k_cull_blocks); read them instead of culling.
+// 10 CTAs per SM (48 registers): the walk and the corner folds wait on loads and on the instruction
+// cache, and more resident warps hide that better than the few spills cost.
 template <bool kChain, bool kListed>
-__global__ void __launch_bounds__(128) k_classify(Geo G, const FbPrim* __restrict__ prims,
+__global__ void __launch_bounds__(128, 10) k_classify(Geo G, const FbPrim* __restrict__ prims,
                                                   const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
                                                   int n_chain, const uint32_t* __restrict__ pool,
                                                   const int64_t* __restrict__ sb_off,
