@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
     ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrival window")
     ap.add_argument("--arena-gb", type=float, default=120.0, help="serve: device arena for resident fields (0: none)")
+    ap.add_argument("--slots", type=int, default=16, help="serve: concurrent request slots (one stream each)")
     return ap.parse_args()
 
 
@@ -520,7 +521,8 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
     tool_sets = [X.compile_tools(R.tools(rng, int(k))) for k in rng.integers(1, 65, size=32)]
     working_set = 64  # requests on fields pick among the most recently built ones
     # resident field buffers from one 120 GB arena: no cudaMalloc per build once it is taken
-    srv = S.FieldServer(slots=16, budget_bytes=150e9, arena_bytes=getattr(args, "arena_gb", 120.0) * 1e9)
+    slots = int(getattr(args, "slots", 16))
+    srv = S.FieldServer(slots=slots, budget_bytes=150e9, arena_bytes=getattr(args, "arena_gb", 120.0) * 1e9)
     try:
         # warm start: a resident field of every grid size, every kernel configured, one EDT per
         # grid size and one query per point-set size (pinned staging of each size allocated once)
@@ -597,7 +599,7 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
         "allocator": {k: int(alloc1.get(k, 0) - alloc0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
                                                                            "num_alloc_retries")},
         "resident_gb": round(srv.resident_bytes() / 1e9, 2),
-        "slots": 16, "budget_gb": 150, "arena_gb": getattr(args, "arena_gb", 120.0), "data": "synthetic",
+        "slots": slots, "budget_gb": 150, "arena_gb": getattr(args, "arena_gb", 120.0), "data": "synthetic",
     }
 
 
