@@ -2,17 +2,19 @@
 //
 // Algorithm (a from-scratch design, not the reference's one-thread-per-line envelope):
 //   1. k_edt_bits  : the uint8 mask becomes one 32-bit word per 32 z-samples of every (x, y) line
-//                    (1 B read + 1/8 B written per voxel); the same pass validates the mask
-//                    (values 0/1, both classes present) with warp-aggregated counters.
+//                    (1 B read + 1/8 B written per voxel, four bytes per SWAR step); the validating
+//                    form also checks the mask (values 0/1, both classes present) with
+//                    warp-aggregated counters.
 //   2. k_edt_zy    : one CTA per (32-wide z chunk, x plane, polarity), lanes = z columns.  For every
 //                    y line it finds the nearest site along z from the line's bit words (clz/ffs over
-//                    the chunk's own word, a ballot over the other words) and runs the y pass
-//                    g(y,z) = min_y' dz(y',z)^2 + (y-y')^2 as an exact lower envelope (below), banded
-//                    over the CTA's warps.  Writes int32 g (4 B/voxel).
-//   3. k_edt_x     : one CTA per (z chunk, y row, polarity): streams the nx x 32 column block of g
-//                    with coalesced 128 B rows into the same envelope along x and writes the final
-//                    int32 (4 B/voxel); the paired form runs both polarities, then k_edt_signed
-//                    turns the two squared distances into the correctly rounded signed float32.
+//                    the chunk's own word, a ballot over the other words) into shared memory, then
+//                    runs the y pass g(y,z) = min_y' dz(y',z)^2 + (y-y')^2 as an exact lower
+//                    envelope (below), banded over the CTA's warps.  Writes int32 g (4 B/voxel).
+//   3. k_edt_x     : one CTA per (z chunk, y row, polarity): stages the nx x 32 column block of g in
+//                    shared memory with cp.async (coalesced 128 B rows, every load in flight at
+//                    once), runs the same envelope along x in place and writes the final int32
+//                    (4 B/voxel); the paired form runs both polarities, then k_edt_signed turns the
+//                    two squared distances into the correctly rounded signed float32.
 // Global traffic per voxel and polarity: 1 (mask) + 4 + 4 (g round trip) + 4 (output) + 1/4 (bit
 // words, mostly L2) bytes -- the 13 B/voxel algorithmic figure.
 //
@@ -35,9 +37,23 @@ struct Counters {
     unsigned long long invalid;  // mask bytes greater than 1
 };
 
+// Nonzero flags of the four bytes of q as bits 0..3 (byte i -> bit i).  The byte-wise OR folds
+// every bit of a byte onto its bit 0; the multiply then gathers the four bit-0s: byte i's bit lands
+// at bit 24 + i of the product and no partial products overlap, so nothing carries.
+__device__ __forceinline__ uint32_t nonzero4(uint32_t q) {
+    uint32_t t = q | (q >> 4);
+    t |= t >> 2;
+    t |= t >> 1;
+    t &= 0x01010101u;
+    return (t * 0x01020408u) >> 24;
+}
+
+// kCount: also count the mask bytes equal to 1 and flag bytes greater than 1.
+template <bool kCount>
 __global__ void __launch_bounds__(256) k_edt_bits(const uint8_t* __restrict__ mask, uint32_t* __restrict__ bits,
                                                   int64_t lines, int nz, int W, Counters* counters) {
-    unsigned long long ones = 0, invalid = 0;
+    unsigned long long ones = 0;
+    uint32_t bad = 0;
     const int64_t total = lines * W;
     const bool vec = (nz & 15) == 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
@@ -48,32 +64,34 @@ __global__ void __launch_bounds__(256) k_edt_bits(const uint8_t* __restrict__ ma
         const uint8_t* src = mask + line * nz + z0;
         uint32_t word = 0;
         if (vec) {
-            // 16-byte aligned: line*nz and z0 are multiples of 16.
+            // 16-byte aligned: line*nz and z0 are multiples of 16; n is 16 or 32.
             for (int h = 0; h < n; h += 16) {
-                uint4 v = *reinterpret_cast<const uint4*>(src + h);
-                uint32_t q[4] = {v.x, v.y, v.z, v.w};
+                const uint4 v = *reinterpret_cast<const uint4*>(src + h);
+                const uint32_t q[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        uint32_t byte = (q[j] >> (8 * b)) & 0xffu;
-                        word |= (uint32_t)(byte != 0) << (h + 4 * j + b);
-                        ones += byte == 1;
-                        invalid += byte > 1;
+                    word |= nonzero4(q[j]) << (h + 4 * j);
+                    if (kCount) {
+                        ones += __popc(q[j] & 0x01010101u);
+                        bad |= q[j] & 0xfefefefeu;
                     }
                 }
             }
         } else {
             for (int b = 0; b < n; ++b) {
-                uint32_t byte = src[b];
+                const uint32_t byte = src[b];
                 word |= (uint32_t)(byte != 0) << b;
-                ones += byte == 1;
-                invalid += byte > 1;
+                if (kCount) {
+                    ones += byte & 1u;
+                    bad |= byte & 0xfeu;
+                }
             }
         }
         bits[i] = word;
     }
-    if (counters) {
+    if (kCount) {
+        // a byte > 1 makes the mask invalid whatever `ones` says, so `ones` may count its low bit
+        unsigned long long invalid = bad != 0;
         for (int o = 16; o > 0; o >>= 1) {
             ones += __shfl_xor_sync(0xffffffffu, ones, o);
             invalid += __shfl_xor_sync(0xffffffffu, invalid, o);
@@ -83,6 +101,12 @@ __global__ void __launch_bounds__(256) k_edt_bits(const uint8_t* __restrict__ ma
             if (invalid) atomicAdd(&counters->invalid, invalid);
         }
     }
+}
+
+void launch_bits(int grid, cudaStream_t stream, const uint8_t* mask, uint32_t* bits, int64_t lines, int nz, int W,
+                 Counters* counters) {
+    if (counters) k_edt_bits<true><<<grid, 256, 0, stream>>>(mask, bits, lines, nz, W, counters);
+    else k_edt_bits<false><<<grid, 256, 0, stream>>>(mask, bits, lines, nz, W, nullptr);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -95,19 +119,23 @@ __global__ void __launch_bounds__(256) k_edt_bits(const uint8_t* __restrict__ ma
 // envelope intersects parabolas with floor division instead, edt_persistent_pair_v1/edt.cu:12-29).
 // Sites with no finite value (the sentinel) never win against a finite one and are left out.
 //
-// A CTA owns 32 adjacent columns (lanes) over the whole axis; its kBandWarps warps split the axis
-// into bands:
-//   1. build : each warp runs the hull stack over its band's sites, one stack per lane, in shared
-//              memory at the band's own rows (a band never holds more entries than rows);
-//   2. merge : pairwise joins of band groups in log2(kBandWarps) rounds -- the bridge between two
+// A CTA owns 32 adjacent columns (lanes) over the whole axis, staged in shared memory as rows of
+// 32 words (row r holds f(r) of the 32 columns: 128 B, conflict-free per lane); its kBandWarps
+// warps split the axis into bands:
+//   1. stage : f of the band's rows lands in the band's own rows of the array (cp.async from global
+//              memory in the x pass; computed from the bit words in the zy pass);
+//   2. build : each warp runs the hull stack over its band's rows, one stack per lane, in place --
+//              stack entry k overwrites row r0 + k, never beyond the row being read;
+//   3. merge : pairwise joins of band groups in log2(kBandWarps) rounds -- the bridge between two
 //              x-separated lower hulls trims a suffix of the left one and a prefix of the right one --
 //              leaving each band a contiguous surviving range [lo, hi];
-//   3. output: each warp finds the hull vertex covering its first target (band scan + binary search)
+//   4. output: each warp finds the hull vertex covering its first target (band scan + binary search)
 //              and walks the hull forward over its targets, one compare per step.
-// Values are exact integers: c < 2^20 and |products| < 2^29 for axes up to 512.
+// Values are exact integers: c < 2^21 and |products| < 2^31 for axes up to 512.
 // ------------------------------------------------------------------------------------------
 constexpr int kBandWarps = 8;
 constexpr int kBandThreads = 32 * kBandWarps;
+constexpr int kNever = 1 << 30;  // c of a successor that never wins (every real c is < 2^21)
 
 __device__ __forceinline__ uint32_t pack_site(int v, int c) { return ((uint32_t)v << 21) | (uint32_t)c; }
 __device__ __forceinline__ int site_v(uint32_t e) { return (int)(e >> 21); }
@@ -147,34 +175,47 @@ __host__ __device__ __forceinline__ int band_rows(int n) { return (n + kBandWarp
 
 int band_smem_bytes(int n) { return n * 32 * 4 + 3 * kBandWarps * 32 * 4; }
 
-// Hull stack of one lane over the rows of one band: entries in shared memory at the band's rows,
-// the top two also unpacked in registers.
-struct HullStack {
-    uint32_t* base;  // &hull[row0 * 32 + lane]
-    int top;         // index of the top entry, -1 when empty
-    int v0, c0, v1, c1;  // second and top entry
+// Hull stack of one lane over rows r0, r0 + 1, ... whose f values sit in the lane's column of
+// the staged rows; entries overwrite the rows from r0 on (entry k at row r0 + k).  Registers hold
+// the top entry (v1, c1) and its edge from the entry below (dv, dc), so the convexity test is one
+// multiply-compare and a pop needs one shared-memory load.
+struct InPlaceHull {
+    uint32_t* base;  // &hull[r0 * 32 + lane]
+    int r0;
+    int top;             // index of the top entry, -1 when empty
+    int v1, c1, dv, dc;  // top entry; top minus the entry below (valid when top >= 1)
 
-    __device__ __forceinline__ HullStack(uint32_t* hull, int row0, int lane)
-        : base(hull + row0 * 32 + lane), top(-1), v0(0), c0(0), v1(0), c1(0) {}
+    __device__ __forceinline__ InPlaceHull(uint32_t* hull, int r0_, int lane)
+        : base(hull + r0_ * 32 + lane), r0(r0_), top(-1), v1(0), c1(0), dv(1), dc(0) {}
 
-    // push site (v, c); sites arrive in increasing v
-    __device__ __forceinline__ void push(int v, int c) {
-        while (top >= 1 && (c1 - c0) * (v - v1) >= (c - c1) * (v1 - v0)) {
-            --top;
-            v1 = v0;
-            c1 = c0;
-            if (top >= 1) {
-                const uint32_t e = base[(top - 1) * 32];
-                v0 = site_v(e);
-                c0 = site_c(e);
+    // rows [ra, rb) in increasing order; f >= sentinel is no site
+    __device__ __forceinline__ void rows(int ra, int rb, int32_t sentinel) {
+#pragma unroll 4
+        for (int v = ra; v < rb; ++v) {
+            const int f = (int)base[(v - r0) * 32];
+            if (f >= sentinel) continue;
+            const int c = f + v * v;
+            int ev = v - v1, ec = c - c1;
+            // the top is hidden between the entry below it and the new site
+            while (top >= 1 && dc * ev >= ec * dv) {
+                --top;
+                v1 -= dv;
+                c1 -= dc;
+                if (top >= 1) {
+                    const uint32_t e = base[(top - 1) * 32];
+                    dv = v1 - site_v(e);
+                    dc = c1 - site_c(e);
+                }
+                ev = v - v1;
+                ec = c - c1;
             }
+            ++top;
+            base[top * 32] = pack_site(v, c);
+            v1 = v;
+            c1 = c;
+            dv = ev;
+            dc = ec;
         }
-        ++top;
-        base[top * 32] = pack_site(v, c);
-        v0 = v1;
-        c0 = c1;
-        v1 = v;
-        c1 = c;
     }
 };
 
@@ -182,7 +223,7 @@ __device__ __forceinline__ bool band_live(const BandSmem& sm, int b, int lane) {
     return sm.hi[b * 32 + lane] >= sm.lo[b * 32 + lane];
 }
 
-// Phase 2: pairwise joins of band groups in log2(kBandWarps) rounds (warp j joins group j of the
+// Phase 3: pairwise joins of band groups in log2(kBandWarps) rounds (warp j joins group j of the
 // round), each the bridge between two x-separated lower hulls: trim the left group's suffix and the
 // right group's prefix until the junction is convex.  Every band ends with a surviving range [lo, hi]
 // (empty when hi < lo); the ranges in band order are the column's lower hull.  Contains
@@ -236,8 +277,8 @@ __device__ void hull_merge(const BandSmem& sm, int n) {
     __syncthreads();
 }
 
-// Phase 3 for targets [q0, q1) of one warp: store(q, value) for each; lanes whose column has no site
-// store `sentinel`.
+// Phase 4 for targets [q0, q1) of one warp: store(value) for q = q0, q0 + 1, ... in order; lanes
+// whose column has no site store `sentinel`.
 template <typename Store>
 __device__ __forceinline__ void hull_output(const BandSmem& sm, int n, int q0, int q1, int32_t sentinel, Store store) {
     const int lane = threadIdx.x & 31;
@@ -246,7 +287,7 @@ __device__ __forceinline__ void hull_output(const BandSmem& sm, int n, int q0, i
     int b = 0;
     while (b < kBandWarps && !band_live(sm, b, lane)) ++b;
     if (b == kBandWarps) {
-        for (int q = q0; q < q1; ++q) store(q, sentinel);
+        for (int q = q0; q < q1; ++q) store(sentinel);
         return;
     }
     // band holding the vertex that covers q0: the first band whose last surviving entry is not
@@ -262,44 +303,61 @@ __device__ __forceinline__ void hull_output(const BandSmem& sm, int n, int q0, i
     }
     // binary search inside band b: the first index whose successor does not win at q0
     int lo = sm.lo[b * 32 + lane], hi = sm.hi[b * 32 + lane];
-    const uint32_t* band = sm.hull + b * rows * 32 + lane;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (next_wins(band[mid * 32], band[(mid + 1) * 32], q0)) lo = mid + 1;
-        else hi = mid;
+    {
+        const uint32_t* band = sm.hull + b * rows * 32 + lane;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (next_wins(band[mid * 32], band[(mid + 1) * 32], q0)) lo = mid + 1;
+            else hi = mid;
+        }
     }
-    // walk: cur = (vc, cc); successor (vn, cn) at index i of band b (has == false past the end)
-    const uint32_t e = band[lo * 32];
+    // walk: p points at the successor of the current vertex (vc, cc), dn = its v - vc and cn its
+    // c - cc; pend is the last surviving entry of p's band.  Past the last vertex the successor
+    // never wins (dn = 0, cn = kNever).
+    const uint32_t* p = sm.hull + (b * rows + lo) * 32 + lane;
+    const uint32_t* pend = sm.hull + (b * rows + sm.hi[b * 32 + lane]) * 32 + lane;
+    const uint32_t e = *p;
     int vc = site_v(e), cc = site_c(e);
-    int i = lo, bhi = sm.hi[b * 32 + lane];
-    int vn = 0, cn = 0;
-    bool has = true;
-    auto load_next = [&]() {
-        if (i < bhi) {
-            ++i;
+    int dn = 0, cn = kNever;
+    auto fetch = [&]() {
+        if (p < pend) {
+            p += 32;
         } else {
             int k = b + 1;
             while (k < kBandWarps && !band_live(sm, k, lane)) ++k;
-            if (k == kBandWarps) { has = false; return; }
+            if (k == kBandWarps) {
+                dn = 0;
+                cn = kNever;
+                return;
+            }
             b = k;
-            band = sm.hull + b * rows * 32 + lane;
-            i = sm.lo[b * 32 + lane];
-            bhi = sm.hi[b * 32 + lane];
+            p = sm.hull + (k * rows + sm.lo[k * 32 + lane]) * 32 + lane;
+            pend = sm.hull + (k * rows + sm.hi[k * 32 + lane]) * 32 + lane;
         }
-        const uint32_t x = band[i * 32];
-        vn = site_v(x);
-        cn = site_c(x);
+        const uint32_t x = *p;
+        dn = site_v(x) - vc;
+        cn = site_c(x) - cc;
     };
-    load_next();
+    fetch();
+#pragma unroll 4
     for (int q = q0; q < q1; ++q) {
-        while (has && cn - cc <= 2 * q * (vn - vc)) {
-            vc = vn;
-            cc = cn;
-            load_next();
+        const int q2 = 2 * q;
+        while (cn <= q2 * dn) {
+            vc += dn;
+            cc += cn;
+            fetch();
         }
-        store(q, cc + q * (q - 2 * vc));
+        store(cc + q * (q - 2 * vc));
     }
 }
+
+__device__ __forceinline__ void cp_async4(uint32_t* smem_dst, const int32_t* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // z pass (nearest set bit along z from the bit words) + y pass.  grid = (W, nx, polarities),
 // block = kBandThreads, dynamic smem = band_smem_bytes(ny).  Polarity p measures to set bits when
@@ -316,11 +374,14 @@ __global__ void __launch_bounds__(kBandThreads) k_edt_zy(const uint32_t* __restr
     const int z = 32 * w + lane;
     const int rows = band_rows(ny);
     const int y0 = warp * rows, y1 = min(ny, y0 + rows);
-    // 1. nearest site along z for each row of the band, pushed onto the lane's hull stack
-    HullStack st(sm.hull, y0, lane);
+    // 1. f(y) = squared distance to the nearest site along z, for each row of the band, into the
+    //    band's rows (sentinel where the row has no site)
+    uint32_t* const mine = sm.hull + y0 * 32 + lane;
     const uint32_t* line = bits + ((int64_t)x * ny + y0) * W + lane;  // row y0's words, one per lane < W
     const bool loads = lane < W;
-    constexpr int kAhead = 4;  // rows of bit words in flight ahead of the stack work
+    const uint32_t below_mask = (1u << w) - 1u, above_mask = ~((2u << w) - 1u);
+    const uint32_t low_mask = 0xffffffffu >> (31 - lane), high_mask = 0xffffffffu << lane;
+    constexpr int kAhead = 8;  // rows of bit words in flight
     uint32_t ring[kAhead];
 #pragma unroll
     for (int k = 0; k < kAhead; ++k) ring[k] = (loads && y0 + k < y1) ? line[k * W] : 0u;
@@ -336,30 +397,39 @@ __global__ void __launch_bounds__(kBandThreads) k_edt_zy(const uint32_t* __restr
                 if (lane == W - 1) word &= last_valid;
             }
             const uint32_t nonzero = __ballot_sync(0xffffffffu, word != 0);
-            if (!nonzero) continue;  // no site on this line (uniform across the warp)
-            const uint32_t own = __shfl_sync(0xffffffffu, word, w);
-            const uint32_t below = nonzero & ((1u << w) - 1u);
-            const uint32_t above = nonzero & ~((2u << w) - 1u);
-            const int pw = below ? 31 - __clz(below) : 0;
-            const int nw = above ? __ffs(above) - 1 : 0;
-            const uint32_t prev_word = __shfl_sync(0xffffffffu, word, pw);
-            const uint32_t next_word = __shfl_sync(0xffffffffu, word, nw);
-            const uint32_t low = own & (0xffffffffu >> (31 - lane));
-            const uint32_t high = own & (0xffffffffu << lane);
-            int prev = -(1 << 20), next = 1 << 20;
-            if (low) prev = 32 * w + 31 - __clz(low);
-            else if (below) prev = 32 * pw + 31 - __clz(prev_word);
-            if (high) next = 32 * w + __ffs(high) - 1;
-            else if (above) next = 32 * nw + __ffs(next_word) - 1;
-            const int d = min(z - prev, next - z);
-            st.push(y, d * d + y * y);
+            int f = sentinel;
+            if (nonzero) {  // uniform across the warp
+                const uint32_t own = __shfl_sync(0xffffffffu, word, w);
+                const uint32_t below = nonzero & below_mask;
+                const uint32_t above = nonzero & above_mask;
+                const int pw = below ? 31 - __clz(below) : 0;
+                const int nw = above ? __ffs(above) - 1 : 0;
+                const uint32_t prev_word = __shfl_sync(0xffffffffu, word, pw);
+                const uint32_t next_word = __shfl_sync(0xffffffffu, word, nw);
+                const uint32_t low = own & low_mask;
+                const uint32_t high = own & high_mask;
+                int prev = -(1 << 20), next = 1 << 20;
+                if (low) prev = 32 * w + 31 - __clz(low);
+                else if (below) prev = 32 * pw + 31 - __clz(prev_word);
+                if (high) next = 32 * w + __ffs(high) - 1;
+                else if (above) next = 32 * nw + __ffs(next_word) - 1;
+                const int d = min(z - prev, next - z);
+                f = d * d;
+            }
+            mine[(y - y0) * 32] = (uint32_t)f;
         }
     }
+    // 2. hull stack over the band, in place
+    InPlaceHull st(sm.hull, y0, lane);
+    st.rows(y0, y1, sentinel);
     sm.cnt[warp * 32 + lane] = st.top + 1;
     hull_merge(sm, ny);
     if (z >= nz) return;
-    int32_t* out = g + (int64_t)pol * nx * ny * nz + ((int64_t)x * ny) * nz + z;
-    hull_output(sm, ny, y0, y1, sentinel, [&](int y, int32_t v) { out[(int64_t)y * nz] = v; });
+    int32_t* out = g + (int64_t)pol * nx * ny * nz + ((int64_t)x * ny + y0) * nz + z;
+    hull_output(sm, ny, y0, y1, sentinel, [&](int32_t v) {
+        *out = v;
+        out += nz;
+    });
 }
 
 // x pass.  grid = (W, ny, polarities), block = kBandThreads, dynamic smem = band_smem_bytes(nx).
@@ -378,26 +448,38 @@ __global__ void __launch_bounds__(kBandThreads) k_edt_x(const int32_t* g, int32_
     const int64_t stride = (int64_t)ny * nz;
     const int rows = band_rows(nx);
     const int x0 = warp * rows, x1 = min(nx, x0 + rows);
-    HullStack st(sm.hull, x0, lane);
-    constexpr int kAhead = 8;  // loads in flight ahead of the stack work
-    int32_t buf[kAhead];
+    // 1. stage the band's column values into its rows, in four commit groups so that the hull
+    //    starts on the first quarter while the rest is in flight
+    constexpr int kGroups = 4;
+    const int chunk = (rows + kGroups - 1) / kGroups;
+    uint32_t* const mine = sm.hull + x0 * 32 + lane;
+    InPlaceHull st(sm.hull, x0, lane);
+    if (live) {
+        const int32_t* src = g + col + (int64_t)x0 * stride;
 #pragma unroll
-    for (int k = 0; k < kAhead; ++k) buf[k] = (live && x0 + k < x1) ? g[col + (int64_t)(x0 + k) * stride] : sentinel;
-    for (int xb = x0; xb < x1; xb += kAhead) {
-#pragma unroll
-        for (int k = 0; k < kAhead; ++k) {
-            const int xx = xb + k;
-            const int32_t f = buf[k];
-            const int xn = xx + kAhead;
-            buf[k] = (live && xn < x1) ? g[col + (int64_t)xn * stride] : sentinel;
-            if (xx < x1 && f < sentinel) st.push(xx, f + xx * xx);
+        for (int j = 0; j < kGroups; ++j) {
+            const int ka = j * chunk, kb = min(x1 - x0, ka + chunk);
+            for (int k = ka; k < kb; ++k) cp_async4(mine + k * 32, src + (int64_t)k * stride);
+            cp_async_commit();
         }
+        // 2. hull stack over the band, in place, one commit group at a time
+        cp_async_wait<kGroups - 1>();
+        st.rows(x0, min(x1, x0 + chunk), sentinel);
+        cp_async_wait<kGroups - 2>();
+        st.rows(min(x1, x0 + chunk), min(x1, x0 + 2 * chunk), sentinel);
+        cp_async_wait<kGroups - 3>();
+        st.rows(min(x1, x0 + 2 * chunk), min(x1, x0 + 3 * chunk), sentinel);
+        cp_async_wait<0>();
+        st.rows(min(x1, x0 + 3 * chunk), x1, sentinel);
     }
     sm.cnt[warp * 32 + lane] = st.top + 1;
     hull_merge(sm, nx);
     if (!live) return;
-    int32_t* dst = out + col;
-    hull_output(sm, nx, x0, x1, sentinel, [&](int x, int32_t v) { dst[(int64_t)x * stride] = v; });
+    int32_t* dst = out + col + (int64_t)x0 * stride;
+    hull_output(sm, nx, x0, x1, sentinel, [&](int32_t v) {
+        *dst = v;
+        dst += stride;
+    });
 }
 
 // Correctly rounded signed distance of one voxel from its two squared distances, the reference's
@@ -464,7 +546,7 @@ int enqueue(const uint8_t* d_mask, int nx, int ny, int nz, int paired, int sites
     const int sms = fb_sm_count();
     const int64_t words = lines * W;
     int grid0 = (int)std::min<int64_t>((words + 255) / 256, (int64_t)sms * 8);
-    k_edt_bits<<<grid0, 256, 0, stream>>>(d_mask, bits, lines, nz, W, count ? counters : nullptr);
+    launch_bits(grid0, stream, d_mask, bits, lines, nz, W, count ? counters : nullptr);
     FB_LAUNCH();
     const int32_t sentinel = sentinel_of(nx, ny, nz);
     // Single polarity measuring to zero bytes = the set bits flipped.
@@ -622,8 +704,8 @@ int fb_edt_validate_device(const uint8_t* d_mask, int nx, int ny, int nz, void* 
     char* base = static_cast<char*>(d_scratch);
     FB_CUDA(cudaMemsetAsync(base, 0, sizeof(Counters), s));
     int grid0 = (int)std::min<int64_t>((lines * W + 255) / 256, (int64_t)fb_sm_count() * 8);
-    k_edt_bits<<<grid0, 256, 0, s>>>(d_mask, reinterpret_cast<uint32_t*>(base + 256), lines, nz, W,
-                                     reinterpret_cast<Counters*>(base));
+    launch_bits(grid0, s, d_mask, reinterpret_cast<uint32_t*>(base + 256), lines, nz, W,
+                reinterpret_cast<Counters*>(base));
     FB_LAUNCH();
     return read_validity(base, lines * nz, s);
 }
