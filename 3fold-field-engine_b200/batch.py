@@ -1,15 +1,16 @@
 """Batched builds of many independent recipes: one CUDA graph, several streams, an autotuner.
 
 ``BatchBuilder(recipes)`` prepares every recipe once (compiled tables, scratch, fixed-capacity
-tile buffers, occupancy masks, EDT outputs) and records the whole batch -- per recipe: culling,
-classification, compaction, fused leaf evaluation, occupancy rasterisation and the squared EDT of
-that occupancy -- into one CUDA graph whose branches are spread over ``streams`` streams.  A
-replay launches everything with one host call and no host synchronisation in between; the
-recipes' kernels overlap on the device.
+tile buffers and, with ``edt=True``, occupancy masks and EDT outputs) and records the whole batch
+-- per recipe: culling, classification, compaction and fused leaf evaluation (the field build),
+optionally followed by occupancy rasterisation and the squared EDT of that occupancy -- into one
+CUDA graph whose branches are spread over ``streams`` streams.  A replay launches everything with
+one host call and no host synchronisation in between; the recipes' kernels overlap on the device.
 
 ``plain_build(...)`` is the same work done recipe by recipe through the public single-build path
-(classification, a host read of the active count, leaf evaluation, occupancy, EDT), the
-reference's own orchestration (src/field_engine/faltkarna_v1_g7_fix.py:56-112).
+(classification, a host read of the active count, leaf evaluation, then occupancy and EDT when
+asked), the reference's own orchestration (src/field_engine/faltkarna_v1_g7_fix.py:56-112: classify,
+host read of the kinds, compaction, tile evaluation).
 
 ``Autotuner`` chooses the leaf size (4, 8 or 16) per recipe: it times the three sizes on one
 representative recipe of each (grid size, primitive-count octave) bucket and keeps the fastest
@@ -87,24 +88,29 @@ class Autotuner:
 class _Item:
     """One recipe's resident state."""
 
-    def __init__(self, comp, meta, device):
+    def __init__(self, comp, meta, device, edt=True):
         import torch
         self.meta = meta
         self.fb = FieldBuilder(comp, meta, device=device)
         self.fb.classify()
         self.capacity = max(int(self.fb.count.item()), 1)
         self.tiles = torch.empty((self.capacity, meta.block ** 3), dtype=torch.float32, device=self.fb.device)
-        self.slot = torch.empty(meta.n_blocks, dtype=torch.int32, device=self.fb.device)
-        self.mask = torch.empty((meta.nx, meta.ny, meta.nz), dtype=torch.uint8, device=self.fb.device)
-        self.edt = torch.empty((meta.nx, meta.ny, meta.nz), dtype=torch.int32, device=self.fb.device)
+        self.slot = self.mask = self.edt = None
+        if edt:
+            self.slot = torch.empty(meta.n_blocks, dtype=torch.int32, device=self.fb.device)
+            self.mask = torch.empty((meta.nx, meta.ny, meta.nz), dtype=torch.uint8, device=self.fb.device)
+            self.edt = torch.empty((meta.nx, meta.ny, meta.nz), dtype=torch.int32, device=self.fb.device)
 
     @property
     def leaf_voxels(self):
         return self.capacity * self.meta.block ** 3
 
     def enqueue(self, edt_scratch, stream=None):
+        """The field build; then occupancy and EDT when edt_scratch is given."""
         lib = self.fb.lib
         self.fb.enqueue(self.tiles, self.capacity, stream=stream)
+        if edt_scratch is None:
+            return
         m = self.meta
         st = lib.fb_field_occupancy_device(self.fb.kind.data_ptr(), self.fb.active.data_ptr(), self.fb.count.data_ptr(),
                                            self.tiles.data_ptr(), self.capacity, m.nx, m.ny, m.nz, m.block,
@@ -119,15 +125,19 @@ class _Item:
 class BatchBuilder:
     """Many recipes, one CUDA graph.  recipes: list of (recipe or Compiled, GridMeta)."""
 
-    def __init__(self, recipes, *, device="cuda", streams=8):
+    def __init__(self, recipes, *, device="cuda", streams=8, edt=True):
         import torch
         self.device = torch.device(device)
-        self.items = [_Item(r if isinstance(r, Compiled) else compile_recipe(r), meta, self.device)
+        self.has_edt = bool(edt)
+        self.items = [_Item(r if isinstance(r, Compiled) else compile_recipe(r), meta, self.device, edt=self.has_edt)
                       for r, meta in recipes]
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, streams))]
-        edt_max = max(int(_lib.lib().fb_edt_scratch_bytes(it.meta.nx, it.meta.ny, it.meta.nz, 0)) for it in self.items)
-        self.edt_scratch = [torch.empty(edt_max, dtype=torch.uint8, device=self.device) for _ in self.streams]
-        self.graph = None
+        self.edt_scratch = []
+        if self.has_edt:
+            edt_max = max(int(_lib.lib().fb_edt_scratch_bytes(it.meta.nx, it.meta.ny, it.meta.nz, 0))
+                          for it in self.items)
+            self.edt_scratch = [torch.empty(edt_max, dtype=torch.uint8, device=self.device) for _ in self.streams]
+        self.graphs = {}
         # largest recipes first, dealt round-robin: the streams finish close together
         self.order = sorted(range(len(self.items)), key=lambda i: -self.items[i].meta.n_blocks)
 
@@ -135,44 +145,60 @@ class BatchBuilder:
     def leaf_voxels(self):
         return sum(it.leaf_voxels for it in self.items)
 
-    def enqueue(self):
-        """All recipes, stream-ordered on the side streams, joined back on the current stream."""
+    def _with_edt(self, edt):
+        edt = self.has_edt if edt is None else bool(edt)
+        if edt and not self.has_edt:
+            raise ValueError("this BatchBuilder was made with edt=False")
+        return edt
+
+    def enqueue(self, edt=None):
+        """All recipes, stream-ordered on the side streams, joined back on the current stream.
+        edt: also occupancy + EDT per recipe (default: when the builder holds their buffers)."""
         import torch
+        edt = self._with_edt(edt)
         main = torch.cuda.current_stream(self.device)
         for s in self.streams:
             s.wait_stream(main)
         for k, i in enumerate(self.order):
             j = k % len(self.streams)
             with torch.cuda.stream(self.streams[j]):
-                self.items[i].enqueue(self.edt_scratch[j], stream=self.streams[j])
+                self.items[i].enqueue(self.edt_scratch[j] if edt else None, stream=self.streams[j])
         for s in self.streams:
             main.wait_stream(s)
 
-    def capture(self):
-        """Record the batch into one CUDA graph (after one eager run has configured every kernel)."""
+    def capture(self, edt=None):
+        """Record the batch into one CUDA graph (after one eager run has configured every kernel);
+        one graph per form (build only, build + EDT)."""
         import torch
-        self.enqueue()
+        edt = self._with_edt(edt)
+        self.enqueue(edt)
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            self.enqueue()
+            self.enqueue(edt)
         torch.cuda.synchronize(self.device)
-        self.graph = g
+        self.graphs[edt] = g
         return g
 
-    def replay(self):
-        if self.graph is None:
-            self.capture()
-        self.graph.replay()
+    @property
+    def graph(self):
+        return self.graphs.get(self.has_edt)
+
+    def replay(self, edt=None):
+        edt = self._with_edt(edt)
+        if edt not in self.graphs:
+            self.capture(edt)
+        self.graphs[edt].replay()
 
     def check_counts(self):
         """True when every recipe still has the active count its tiles were sized for."""
         return all(int(it.fb.count.item()) == it.capacity for it in self.items)
 
 
-def plain_build(items, edt_scratch):
+def plain_build(items, edt_scratch=None):
     """The same work recipe by recipe on the current stream, with the single-build path's host
-    synchronisation (the active count is read before each leaf pass)."""
+    synchronisation (the active count is read before each leaf pass); occupancy + EDT per recipe
+    when edt_scratch is given."""
     import torch
     lib = _lib.lib()
     for it in items:
@@ -181,6 +207,9 @@ def plain_build(items, edt_scratch):
         n = int(fb.count.item())
         if n:
             fb.leaf(it.tiles, min(n, it.capacity))
+        if edt_scratch is None:
+            torch.cuda.current_stream().synchronize()
+            continue
         m = it.meta
         _lib.check(lib.fb_field_occupancy_device(fb.kind.data_ptr(), fb.active.data_ptr(), fb.count.data_ptr(),
                                                  it.tiles.data_ptr(), it.capacity, m.nx, m.ny, m.nz, m.block,

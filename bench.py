@@ -56,6 +56,7 @@ def parse():
                     help="plain: the plain method at scale (default line); batched: 256 recipes, plain vs "
                          "graph-batched; serve: the request loop; precision: float32 vs float64 at mixed pitch")
     ap.add_argument("--recipes", type=int, default=256)
+    ap.add_argument("--streams", type=int, default=16, help="batched: streams the graph's branches spread over")
     ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
     ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrival window")
     ap.add_argument("--arena-gb", type=float, default=120.0, help="serve: device arena for resident fields (0: none)")
@@ -422,8 +423,10 @@ def run_reference(args, rank, world):
 
 def run_batched(args):
     """256 independent recipes (primitive counts log-uniform in [8, 2048], grids from
-    {64, 128, 256, 512}^3, leaf size by the autotuner), each followed by the squared EDT of its
-    occupancy: the recipe-by-recipe path against one CUDA-graph replay of the whole batch."""
+    {64, 128, 256, 512}^3, leaf size by the autotuner): the recipe-by-recipe build path against one
+    CUDA-graph replay of the whole batch.  The headline is the field build (culling,
+    classification, compaction, leaf evaluation); the same pair is also timed with each build
+    followed by occupancy rasterisation and the squared EDT of that occupancy."""
     import torch
     import field_b200.batch as BT
     import field_b200.expr as X
@@ -439,7 +442,7 @@ def run_batched(args):
     t_tune = time.perf_counter() - t0
     recipes = [(c, BT.cube_meta(n, b)) for (c, n), b in zip(comps, blocks)]
     t0 = time.perf_counter()
-    bb = BT.BatchBuilder(recipes, streams=8)
+    bb = BT.BatchBuilder(recipes, streams=args.streams)
     t_setup = time.perf_counter() - t0
     voxels = bb.leaf_voxels
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -457,17 +460,26 @@ def run_batched(args):
             out.append(e0.elapsed_time(e1))
         return out
 
-    plain = lambda: BT.plain_build(bb.items, bb.edt_scratch[0])
+    plain = lambda: BT.plain_build(bb.items)
     timed(plain, max(args.warmup, 3))
     t_plain = timed(plain, args.steps)
-    bb.capture()
-    timed(bb.replay, max(args.warmup, 3))
+    bb.capture(edt=False)
+    replay = lambda: bb.replay(edt=False)
+    timed(replay, max(args.warmup, 3))
     clocks = ClockSampler(0)
     clocks.start()
-    t_batch = timed(bb.replay, args.steps)
+    t_batch = timed(replay, args.steps)
     clk = clocks.stop()
     assert bb.check_counts()
     mp, mb = statistics.median(t_plain), statistics.median(t_batch)
+    # the same builds, each followed by occupancy + squared EDT
+    plain_edt = lambda: BT.plain_build(bb.items, bb.edt_scratch[0])
+    timed(plain_edt, max(args.warmup, 3))
+    mpe = statistics.median(timed(plain_edt, args.steps))
+    bb.capture(edt=True)
+    replay_edt = lambda: bb.replay(edt=True)
+    timed(replay_edt, max(args.warmup, 3))
+    mbe = statistics.median(timed(replay_edt, args.steps))
     hist = {}
     for b in blocks:
         hist[str(b)] = hist.get(str(b), 0) + 1
@@ -491,9 +503,12 @@ def run_batched(args):
         "metric": METRIC, "workload": "batched_256_recipes", "value": voxels / (mb * 1e-3) / 1e9, "unit": UNIT,
         "plain_gvox_s": voxels / (mp * 1e-3) / 1e9, "batched_gvox_s": voxels / (mb * 1e-3) / 1e9,
         "speedup_batched_vs_plain": mp / mb, "ms_plain": mp, "ms_batched": mb, "steps": args.steps,
-        "recipes": len(recipes), "leaf_voxels": voxels, "recipes_per_s": len(recipes) / (mb * 1e-3),
+        "recipes": len(recipes), "streams": args.streams, "leaf_voxels": voxels, "recipes_per_s": len(recipes) / (mb * 1e-3),
         "leaf_sizes": hist, "autotune_s": t_tune, "compile_s": t_compile, "setup_s": t_setup,
-        "edt_voxels": int(sum(it.meta.nx * it.meta.ny * it.meta.nz for it in bb.items)),
+        "with_edt": {"ms_plain": mpe, "ms_batched": mbe, "plain_gvox_s": voxels / (mpe * 1e-3) / 1e9,
+                     "batched_gvox_s": voxels / (mbe * 1e-3) / 1e9, "speedup_batched_vs_plain": mpe / mbe,
+                     "edt_voxels": int(sum(it.meta.nx * it.meta.ny * it.meta.nz for it in bb.items)),
+                     "note": "each build followed by occupancy rasterisation + squared EDT of the occupancy"},
         "grid_sizes": {str(n): sum(1 for _, m in recipes if m.nx == n) for n in (64, 128, 256, 512)},
         "clocks": clk, "dtype": "f32 (f64 guard band); int32 EDT", "data": "synthetic",
     }

@@ -48,6 +48,28 @@ def test_graph_batch_equals_plain_builds():
         assert (it.edt.cpu().numpy() == oracle.edt_squared(1 - m)).all()
 
 
+def test_build_only_graph_equals_plain_builds():
+    """The build-only graph (no occupancy / EDT) gives the same kinds and tiles as the plain
+    build-only path, and a builder made without EDT buffers refuses the EDT form."""
+    import torch
+    import field_b200.batch as BT
+    recipes = _recipes(9, seed=17)
+    bb = BT.BatchBuilder(recipes, streams=3, edt=False)
+    assert all(it.edt is None for it in bb.items)
+    bb.replay(edt=False)
+    torch.cuda.synchronize()
+    assert bb.check_counts()
+    got = [(it.fb.kind.clone(), it.tiles.clone()) for it in bb.items]
+    for it in bb.items:
+        it.tiles.zero_()
+    BT.plain_build(bb.items)
+    for (kind, tiles), it in zip(got, bb.items):
+        assert torch.equal(kind, it.fb.kind)
+        assert torch.equal(tiles, it.tiles)
+    with pytest.raises(ValueError):
+        bb.capture(edt=True)
+
+
 def test_replays_are_deterministic():
     import torch
     import field_b200.batch as BT
