@@ -58,17 +58,23 @@ class RecipeQueries:
                        np.array([m.nx, m.ny, m.nz, m.block], np.int32),
                        (builder.kind.data_ptr(), boff.value, blen.value, bpool.value, bcap.value, ball.value), builder)
 
-    def _run(self, pts, value, grad, h=0.05, stream=None):
+    def _run(self, pts, value, grad, h=0.05, stream=None, alloc=None):
+        """alloc(nbytes) -> uint8 device tensor for the sorted path's scratch, which the alloc's
+        owner keeps alive until the query's kernels have completed (default: torch's allocator,
+        with the block tied to `stream`)."""
         import torch
         a = self._accel
         scratch, nscratch = None, 0
         if a is not None and pts.shape[0] > 0:
             nbytes = int(self.lib.fb_query_scratch_bytes(a[4].ctypes.data, pts.shape[0], 1 if grad is not None else 0))
             if nbytes > 0:
-                scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
                 nscratch = nbytes
-                if isinstance(stream, torch.cuda.Stream):  # freed only after that stream's kernels
-                    scratch.record_stream(stream)
+                if alloc is not None:
+                    scratch = alloc(nbytes)
+                else:
+                    scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+                    if isinstance(stream, torch.cuda.Stream):  # freed only after that stream's kernels
+                        scratch.record_stream(stream)
         args = (a[0], a[1], a[2], a[3].ctypes.data, a[4].ctypes.data, *a[5]) if a else (None,) * 5 + (None, None,
                                                                                                      None, None, 0, 0)
         st = self.lib.fb_query_points_device(self.primf.data_ptr(), self.chain.data_ptr(), self.n_chain, self.mode,
@@ -87,13 +93,19 @@ class RecipeQueries:
         self._run(pts, out, None, stream=stream)
         return out
 
-    def values_and_gradients(self, points, h=0.05, *, stream=None):
-        """(float32 (N,), float32 (N, 3)) values and central-difference gradients."""
+    def values_and_gradients(self, points, h=0.05, *, stream=None, alloc=None):
+        """(float32 (N,), float32 (N, 3)) values and central-difference gradients.  alloc: as in
+        _run, also used for the two outputs (whose blocks the alloc's owner keeps alive)."""
         import torch
         pts = points.to(self.device, torch.float32).contiguous()
-        val = torch.empty(pts.shape[0], dtype=torch.float32, device=self.device)
-        grad = torch.empty((pts.shape[0], 3), dtype=torch.float32, device=self.device)
-        self._run(pts, val, grad, h=h, stream=stream)
+        n = pts.shape[0]
+        if alloc is not None:
+            val = alloc(max(n, 1) * 4).view(torch.float32)[:n]
+            grad = alloc(max(n, 1) * 12).view(torch.float32)[:3 * n].view(n, 3)
+        else:
+            val = torch.empty(n, dtype=torch.float32, device=self.device)
+            grad = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        self._run(pts, val, grad, h=h, stream=stream, alloc=alloc)
         return val, grad
 
 

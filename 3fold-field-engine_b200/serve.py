@@ -92,6 +92,45 @@ class DeviceArena:
             self.free.insert(i, (off, n))
 
 
+class PinnedPool:
+    """Pinned host blocks handed out by power-of-two size class and recycled, so that a request's
+    host staging costs no pinned allocation once the pool has warmed up (a fresh pinned allocation
+    is a driver call that can take milliseconds and holds the caller).
+
+    ``take(nbytes)`` returns (uint8 pinned view, handle).  ``bind(obj, handle)`` returns the block
+    to the pool when `obj` -- the numpy array handed to a client, say -- is garbage collected;
+    ``give_back(handle)`` returns it at once."""
+
+    MIN = 1 << 16
+
+    def __init__(self):
+        self.free = collections.defaultdict(list)  # size class -> pinned uint8 tensors
+        self.lock = threading.Lock()
+        self.allocated = 0
+
+    def _new(self, cls):
+        import torch
+        return torch.empty(cls, dtype=torch.uint8, pin_memory=True)
+
+    def take(self, nbytes):
+        cls = max(self.MIN, 1 << max(0, int(nbytes) - 1).bit_length())
+        with self.lock:
+            lst = self.free[cls]
+            blk = lst.pop() if lst else None
+        if blk is None:
+            blk = self._new(cls)
+            self.allocated += cls
+        return blk[:int(nbytes)], (cls, blk)
+
+    def bind(self, obj, handle):
+        weakref.finalize(obj, self.give_back, handle)
+
+    def give_back(self, handle):
+        cls, blk = handle
+        with self.lock:
+            self.free[cls].append(blk)
+
+
 class _Field:
     def __init__(self, fid, comp, meta, fb, tiles, n_active):
         self.id = fid
@@ -172,6 +211,10 @@ class FieldServer:
         self.device = dev if dev.index is not None else torch.device("cuda", torch.cuda.current_device())
         self.arena = DeviceArena(arena_bytes, self.device) if arena_bytes else None
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
+        # per slot: a pinned word area for the scalars its request reads back (active count, EDT
+        # checksum); a slot runs one request at a time, so it is never shared
+        self.slot_host = [torch.zeros(8, dtype=torch.int64, pin_memory=True) for _ in range(slots)]
+        self.pinned = PinnedPool()
         self.free = collections.deque(range(slots))
         self.budget = float(budget_bytes)
         self.timeout = float(request_timeout_s)
@@ -226,6 +269,16 @@ class FieldServer:
         import torch
         blk = self.arena.alloc(nbytes) if self.arena is not None else None
         return blk if blk is not None else torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+
+    def _keeper(self, keep):
+        """alloc(nbytes) for a request's device temporaries: blocks from _alloc, each appended to
+        `keep`, the request's list that lives until its last device event has completed (a derived
+        tensor does not keep an arena block alive; the block object itself must)."""
+        def alloc(nbytes):
+            blk = self._alloc(nbytes)
+            keep.append(blk)
+            return blk
+        return alloc
 
     def _account(self, f):
         """Bring the resident total up to date after field `f` changed its buffers."""
@@ -383,12 +436,12 @@ class FieldServer:
         ev.record(stream)
         return ev
 
-    def _build_field(self, comp, meta, stream):
+    def _build_field(self, comp, meta, stream, slot):
         import torch
         with torch.cuda.stream(stream):
             fb = FieldBuilder(comp, meta, device=self.device, alloc=self._alloc)
             fb.classify(stream)
-            count = torch.empty(1, dtype=torch.int32, pin_memory=True)
+            count = self.slot_host[slot].view(torch.int32)[:1]
             count.copy_(fb.count, non_blocking=True)
         yield self._record(stream)
         n = int(count[0])
@@ -403,7 +456,7 @@ class FieldServer:
 
     def _run_build(self, r, stream):
         comp, meta = r.args["recipe"], r.args["meta"]
-        fb, tiles, owner, n = yield from self._build_field(comp, meta, stream)
+        fb, tiles, owner, n = yield from self._build_field(comp, meta, stream, r.slot)
         fid = self.next_id
         self.next_id += 1
         self.fields[fid] = _Field(fid, comp, meta, fb, tiles, n)
@@ -414,7 +467,7 @@ class FieldServer:
     def _run_edit(self, r, stream):
         f = self.fields[r.field]
         comp = X.extend(f.comp, r.args["tool_prims"], r.args["op"])
-        fb, tiles, owner, n = yield from self._build_field(comp, f.meta, stream)
+        fb, tiles, owner, n = yield from self._build_field(comp, f.meta, stream, r.slot)
         f.comp, f.fb, f.tiles, f.n_active = comp, fb, tiles, n
         f.queries = None
         f.edt = None
@@ -428,20 +481,39 @@ class FieldServer:
         f = self.fields[r.field]
         pts = r.args["points"]
         h = float(r.args.get("h", f.meta.pitch))
+        keep = []  # device temporaries, alive until the request's device work has completed
+        alloc = self._keeper(keep)
         with torch.cuda.stream(stream):
             if f.queries is None:
                 # tables prepared on this stream; later queries on other streams wait for them
                 f.queries = (RecipeQueries(f.comp, device=self.device, builder=f.fb), self._record(stream))
             q, ready = f.queries
             stream.wait_event(ready)
-            p = pts.to(self.device, non_blocking=True)
-            val, grad = q.values_and_gradients(p, h=h, stream=stream)
-            out_v = torch.empty(val.shape, dtype=val.dtype, pin_memory=True)
-            out_g = torch.empty(grad.shape, dtype=grad.dtype, pin_memory=True)
+            n = pts.shape[0]
+            if pts.is_cuda:
+                p = pts
+            else:
+                p = alloc(max(n, 1) * 12).view(torch.float32)[:3 * n].view(n, 3)
+                p.copy_(pts, non_blocking=True)
+            val, grad = q.values_and_gradients(p, h=h, stream=stream, alloc=alloc)
+            hv, tok_v = self.pinned.take(max(n, 1) * 4)
+            hg, tok_g = self.pinned.take(max(n, 1) * 12)
+            out_v = hv.view(torch.float32)[:n]
+            out_g = hg.view(torch.float32)[:3 * n].view(n, 3)
             out_v.copy_(val, non_blocking=True)
             out_g.copy_(grad, non_blocking=True)
-        yield self._record(stream)
-        return out_v.numpy(), out_g.numpy()
+        try:
+            yield self._record(stream)
+        except BaseException:
+            self.pinned.give_back(tok_v)
+            self.pinned.give_back(tok_g)
+            raise
+        arr_v, arr_g = out_v.numpy(), out_g.numpy()
+        # the pinned blocks go back to the pool when the client drops these arrays
+        self.pinned.bind(arr_v, tok_v)
+        self.pinned.bind(arr_g, tok_g)
+        del keep
+        return arr_v, arr_g
 
     def _run_edt(self, r, stream):
         import torch
@@ -449,13 +521,14 @@ class FieldServer:
         m = f.meta
         lib = _lib.lib()
         fb, tiles, n_active, owners = f.fb, f.tiles, f.n_active, list(f.owners)  # held until the GPU is done
+        keep = []  # device temporaries, alive until the request's device work has completed
+        alloc = self._keeper(keep)
         with torch.cuda.stream(stream):
-            slot = torch.empty(m.n_blocks, dtype=torch.int32, device=self.device)
-            mask = torch.empty((m.nx, m.ny, m.nz), dtype=torch.uint8, device=self.device)
+            slot = alloc(m.n_blocks * 4).view(torch.int32)
+            mask = alloc(m.nx * m.ny * m.nz).view(m.nx, m.ny, m.nz)
             out_owner = self._alloc(m.nx * m.ny * m.nz * 4)
             out = out_owner.view(torch.int32).view(m.nx, m.ny, m.nz)
-            scratch = torch.empty(int(lib.fb_edt_scratch_bytes(m.nx, m.ny, m.nz, 0)), dtype=torch.uint8,
-                                  device=self.device)
+            scratch = alloc(int(lib.fb_edt_scratch_bytes(m.nx, m.ny, m.nz, 0)))
             _lib.check(lib.fb_field_occupancy_device(fb.kind.data_ptr(), fb.active.data_ptr(), fb.count.data_ptr(),
                                                      tiles.data_ptr(), max(n_active, 1), m.nx, m.ny, m.nz, m.block,
                                                      slot.data_ptr(), mask.data_ptr(), _lib.stream_handle(stream)),
@@ -464,9 +537,10 @@ class FieldServer:
                                                  scratch.data_ptr(), scratch.numel(), _lib.stream_handle(stream)),
                        "edt")
             total = out.sum(dtype=torch.int64)
-            host = torch.empty((), dtype=torch.int64, pin_memory=True)
+            host = self.slot_host[r.slot][1]
             host.copy_(total, non_blocking=True)
         yield self._record(stream)
+        del keep
         if f.fb is fb:
             f.edt = out
             f.owners = owners + [out_owner]

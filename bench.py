@@ -531,7 +531,8 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
     n_req = int(rate * seconds)
     gaps = rng.exponential(1.0 / rate, size=n_req)
     kinds = rng.choice(["build", "edit", "query", "edt"], size=n_req, p=[0.4, 0.3, 0.2, 0.1])
-    point_sets = [rng.uniform(0, 1, (int(m), 3)).astype(np.float32)
+    # the client keeps its point sets in pinned host memory, which the server takes without a copy
+    point_sets = [torch.from_numpy(rng.uniform(0, 1, (int(m), 3)).astype(np.float32)).pin_memory()
                   for m in np.geomspace(100_000, 1_000_000, 8)]
     tool_sets = [X.compile_tools(R.tools(rng, int(k))) for k in rng.integers(1, 65, size=32)]
     working_set = 64  # requests on fields pick among the most recently built ones

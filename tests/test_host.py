@@ -1,5 +1,6 @@
-"""Host-side recipe logic without a GPU: edits appended to a compiled recipe equal the recompiled
-edited recipe byte for byte, and edit tools must be single primitives."""
+"""Host-side logic without a GPU: edits appended to a compiled recipe equal the recompiled edited
+recipe byte for byte, edit tools must be single primitives, and the server's pinned staging pool
+recycles a block only once its result array is gone."""
 import numpy as np
 import pytest
 
@@ -60,3 +61,32 @@ def test_composite_tools_and_bad_ops_are_rejected():
         X.compile_tools([X.union(X.sphere(0.1), X.sphere(0.2, (0.3, 0.0, 0.0)))])
     with pytest.raises(ValueError):
         X.extend(X.compile_recipe(base), X.compile_tools([X.sphere(0.1)]), "intersect")
+
+
+def test_pinned_pool_recycles_a_block_when_its_array_is_dropped():
+    """Query results are numpy views of pooled pinned blocks: a block stays out of the pool while
+    the array (or any slice of it) lives, and the next request of that size class reuses it."""
+    import gc
+    import torch
+    import field_b200.serve as S
+
+    class HostPool(S.PinnedPool):  # plain host memory: the recycling rule needs no GPU
+        def _new(self, cls):
+            return torch.empty(cls, dtype=torch.uint8)
+
+    pool = HostPool()
+    view, handle = pool.take(1000)
+    arr = view.view(torch.float32).numpy()
+    pool.bind(arr, handle)
+    part = arr[10:]
+    del arr, view
+    gc.collect()
+    assert sum(len(v) for v in pool.free.values()) == 0  # the slice still holds it
+    del part
+    gc.collect()
+    assert sum(len(v) for v in pool.free.values()) == 1
+    _, again = pool.take(900)
+    assert again[1].data_ptr() == handle[1].data_ptr()
+    assert pool.allocated == S.PinnedPool.MIN
+    _, other = pool.take(S.PinnedPool.MIN + 1)  # the next size class: a new block
+    assert other[0] == 2 * S.PinnedPool.MIN and pool.allocated == 3 * S.PinnedPool.MIN
