@@ -45,6 +45,7 @@ SIGNATURES = {
     "fb_dense_classify_device": (I, [P, I64, I64, I64, I, F, P, P, P, P, P, I64, P, I64, P]),
     "fb_field_reconstruct_device": (I, [P, P, I64, P, I64, I64, I64, I, F, P, P, P]),
     "fb_checksum_i64_device": (I, [P, I64, D, P, P]),
+    "fb_sum_i32_device": (I, [P, I64, P, P]),
     "fb_field_occupancy_device": (I, [P, P, P, P, I64, I64, I64, I64, I, P, P, P]),
     "fb_field_leaf_work_device": (I, [P, P, I, P, I, I, P, P, P, P, I64, P, I64, P, P]),
     "fb_fp32_peak_launch": (I64, [P, I, I, P]),

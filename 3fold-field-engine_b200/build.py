@@ -18,6 +18,8 @@ from __future__ import annotations
 import ctypes as ct
 import math
 
+import weakref
+
 import numpy as np
 
 from . import _lib
@@ -61,10 +63,15 @@ class DeviceField:
                            corner_min_abs=self.corner_min_abs.cpu().numpy(), stats=stats_of(self.meta, kind, n))
 
 
-def device_tables(comp: Compiled, device, stream):
+def device_tables(comp: Compiled, device, stream, *, alloc=None, pinned=None):
     """(primitive table, instruction table) of a compiled recipe as uint8 device tensors, validated
     and uploaded once per device and kept on the Compiled object; `stream` is made to wait for the
-    upload, so builds on any stream may share the tables (the kernels only read them)."""
+    upload, so builds on any stream may share the tables (the kernels only read them).
+
+    alloc(nbytes) -> uint8 device tensor places the tables in the caller's device pool (the
+    returned blocks are kept with the tables); pinned (a serve.PinnedPool) supplies the host
+    staging, whose blocks go back to it through release_staging once the upload has completed
+    (at the latest when the Compiled object goes away)."""
     import torch
     cache = comp.__dict__.setdefault("_device_tables", {})
     key = str(device)
@@ -74,17 +81,46 @@ def device_tables(comp: Compiled, device, stream):
         if len(comp.prims) < 1:
             raise ValueError("recipe has no primitive")
         _validate_program(comp.prims, insns, mode)
+        host = [np.ascontiguousarray(comp.prims).view(np.uint8).reshape(-1),
+                np.ascontiguousarray(insns).view(np.uint8).reshape(-1)]
+        handles = []
         with torch.cuda.stream(stream):
-            prims = torch.from_numpy(np.ascontiguousarray(comp.prims).view(np.uint8).copy()).pin_memory()
-            chain = torch.from_numpy(np.ascontiguousarray(insns).view(np.uint8).copy()).pin_memory()
-            dprims = prims.to(device, non_blocking=True)
-            dchain = chain.to(device, non_blocking=True)
+            staged, out = [], []
+            for h in host:
+                if pinned is not None:
+                    view, handle = pinned.take(h.nbytes)
+                    view.numpy()[:] = h
+                    handles.append(handle)
+                else:
+                    view = torch.from_numpy(h.copy()).pin_memory()
+                staged.append(view)
+                if alloc is not None:
+                    d = alloc(h.nbytes)
+                    d.copy_(view, non_blocking=True)
+                else:
+                    d = view.to(device, non_blocking=True)
+                out.append(d)
             done = torch.cuda.Event()
             done.record(stream)
-        cache[key] = (dprims, dchain, done, (prims, chain))
-    dprims, dchain, done, _ = cache[key]
+        if handles:
+            weakref.finalize(comp, _give_back_all, pinned, handles)
+        cache[key] = (out[0], out[1], done, tuple(staged), handles)
+    dprims, dchain, done = cache[key][:3]
     stream.wait_event(done)
     return dprims, dchain
+
+
+def _give_back_all(pinned, handles):
+    while handles:
+        pinned.give_back(handles.pop())
+
+
+def release_staging(comp: Compiled, device, pinned):
+    """Return the pinned staging blocks of comp's table upload to `pinned`; call it once that
+    upload has completed (after an event recorded on the upload stream behind it)."""
+    entry = comp.__dict__.get("_device_tables", {}).get(str(device))
+    if entry is not None and entry[4]:
+        _give_back_all(pinned, entry[4])
 
 
 class FieldBuilder:
@@ -93,9 +129,11 @@ class FieldBuilder:
     ``build()`` returns a DeviceField sized exactly (one 4-byte count read between the classify and
     leaf launches); ``enqueue(capacity_tiles)`` runs the whole build stream-ordered into a fixed
     tile buffer (CUDA-graph capturable).  ``alloc`` (optional) supplies the one device allocation
-    the builder makes (outputs + scratch), e.g. from a server's memory pool."""
+    the builder makes (outputs + scratch), e.g. from a server's memory pool, and -- with
+    ``pinned`` -- the recipe's tables when they are first uploaded (see device_tables)."""
 
-    def __init__(self, recipe, meta: GridMeta, *, device="cuda", guard=None, library=None, alloc=None):
+    def __init__(self, recipe, meta: GridMeta, *, device="cuda", guard=None, library=None, alloc=None,
+                 pinned=None):
         import torch
         self.lib = _lib.lib(library)
         self.meta = meta
@@ -109,7 +147,8 @@ class FieldBuilder:
         if self.n_prims < 1:
             raise ValueError("recipe has no primitive")
         self.geom = geom_of(meta, guard)
-        self.prims, self.chain = device_tables(c, self.device, torch.cuda.current_stream(self.device))
+        self.prims, self.chain = device_tables(c, self.device, torch.cuda.current_stream(self.device),
+                                               alloc=alloc, pinned=pinned)
         nbytes = self.lib.fb_field_scratch_bytes(ct.addressof(self.geom), self.n_prims, self.n_chain)
         if nbytes < 0:
             raise ValueError("grid outside the build contract")

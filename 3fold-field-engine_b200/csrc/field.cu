@@ -1355,6 +1355,16 @@ __global__ void k_checksum_i64(const float* __restrict__ v, int64_t n, double sc
     if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, (unsigned long long)acc);
 }
 
+// Exact sum of int32 values into one int64 word: per-thread partial sums, a warp reduction, one
+// 64-bit atomic per warp (wraps modulo 2^64 like the signed sum).
+__global__ void __launch_bounds__(256) k_sum_i32(const int32_t* __restrict__ v, int64_t n, unsigned long long* out) {
+    long long acc = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += v[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, (unsigned long long)acc);
+}
+
 // ------------------------------------------------------------------------------------ host side
 struct Scratch {
     int32_t* blk_off;
@@ -1664,6 +1674,18 @@ int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64
     if (n == 0) return FB_OK;
     k_checksum_i64<<<std::min<int64_t>(fb_div_up(n, 256), fb_sm_count() * 8), 256, 0, st>>>(
         d_values, n, scale, reinterpret_cast<unsigned long long*>(d_out));
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+// Sum of n int32 values into d_out[0] (set to zero first, on the stream).
+int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* stream) noexcept {
+    if (!d_out || n < 0 || (n > 0 && !d_values)) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    FB_CUDA(cudaMemsetAsync(d_out, 0, sizeof(int64_t), st));
+    if (n == 0) return FB_OK;
+    k_sum_i32<<<std::min<int64_t>(fb_div_up(n, 256), fb_sm_count() * 8), 256, 0, st>>>(
+        d_values, n, reinterpret_cast<unsigned long long*>(d_out));
     FB_LAUNCH();
     return FB_OK;
 }

@@ -7,8 +7,10 @@ Requests (``submit`` returns a Future):
   * ``query``  (field id, points (N, 3))         -> float32 values and central-difference gradients
   * ``edt``    (field id)                        -> squared EDT of the field's occupancy (device)
 
-Request preparation (compiling a recipe, compiling edit tools to primitive records, staging query
-points in pinned host memory) runs on the submitting thread.  The scheduler thread admits queued
+Request preparation (compiling a recipe, compiling edit tools to primitive records, copying query
+points given as numpy arrays into pinned host memory) runs on the submitting thread; points given as
+pinned host or device tensors are used without a host copy.  Query results are numpy arrays over
+pooled pinned blocks, which return to the pool when the client drops them.  The scheduler thread admits queued
 requests while a stream slot is free and the HBM budget allows their estimated footprint, runs
 each request as a generator that enqueues asynchronous GPU work on its slot's stream and yields a
 CUDA event, resumes it when the event has completed, and admits the next arrival as soon as a slot
@@ -36,7 +38,7 @@ import numpy as np
 
 from . import _lib
 from . import expr as X
-from .build import FieldBuilder
+from .build import FieldBuilder, release_staging
 from .query import RecipeQueries
 
 
@@ -112,18 +114,42 @@ class PinnedPool:
         import torch
         return torch.empty(cls, dtype=torch.uint8, pin_memory=True)
 
+    SPAN = 2  # a request may take a free block up to 2^SPAN times its own size class
+
+    @classmethod
+    def size_class(cls, nbytes):
+        return max(cls.MIN, 1 << max(0, int(nbytes) - 1).bit_length())
+
     def take(self, nbytes):
-        cls = max(self.MIN, 1 << max(0, int(nbytes) - 1).bit_length())
+        """A free block of nbytes' size class, else of one of the next SPAN classes up (so small
+        requests do not drain the blocks kept for large ones); a new block of the class only when
+        none of those is free."""
+        cls = self.size_class(nbytes)
+        blk, got = None, cls
         with self.lock:
-            lst = self.free[cls]
-            blk = lst.pop() if lst else None
+            for k in range(self.SPAN + 1):
+                lst = self.free.get(cls << k)
+                if lst:
+                    blk, got = lst.pop(), cls << k
+                    break
         if blk is None:
             blk = self._new(cls)
             self.allocated += cls
-        return blk[:int(nbytes)], (cls, blk)
+        return blk[:int(nbytes)], (got, blk)
 
     def bind(self, obj, handle):
         weakref.finalize(obj, self.give_back, handle)
+
+    def reserve(self, nbytes, count):
+        """Make sure at least `count` blocks of nbytes' own size class are free (allocating ahead
+        of need)."""
+        cls = self.size_class(nbytes)
+        with self.lock:
+            missing = count - len(self.free[cls])
+        for _ in range(max(0, missing)):
+            blk = self._new(cls)
+            self.allocated += cls
+            self.give_back((cls, blk))
 
     def give_back(self, handle):
         cls, blk = handle
@@ -190,10 +216,11 @@ def _prepare(kind, args):
     elif kind == "query":
         p = args["points"]
         if isinstance(p, torch.Tensor):
+            # taken as given: pinned or device tensors are staged asynchronously; a pageable host
+            # tensor is copied synchronously when the request runs
             if p.dim() != 2 or p.shape[1] != 3:
                 raise ValueError("points must be an (N, 3) array")
-            p = p.to(torch.float32).contiguous()
-            args["points"] = p if p.is_cuda or p.is_pinned() else p.pin_memory()
+            args["points"] = p.to(torch.float32).contiguous()
         else:
             a = np.ascontiguousarray(p, dtype=np.float32)
             if a.ndim != 2 or a.shape[1] != 3:
@@ -214,11 +241,12 @@ class FieldServer:
         # per slot: a pinned word area for the scalars its request reads back (active count, EDT
         # checksum); a slot runs one request at a time, so it is never shared
         self.slot_host = [torch.zeros(8, dtype=torch.int64, pin_memory=True) for _ in range(slots)]
+        self.slot_dev = torch.zeros((slots, 8), dtype=torch.int64, device=self.device)
         self.pinned = PinnedPool()
         self.free = collections.deque(range(slots))
         self.budget = float(budget_bytes)
         self.timeout = float(request_timeout_s)
-        self.fields = {}
+        self.fields = collections.OrderedDict()  # least recently used first
         self.resident = 0  # sum of the resident fields' bytes, kept up to date on every change
         self.next_id = 0
         self.reserved = 0
@@ -264,11 +292,24 @@ class FieldServer:
     def resident_bytes(self):
         return self.resident
 
+    def reserve_pinned(self, nbytes, count):
+        """Pre-allocate `count` pinned staging blocks for results of up to nbytes (e.g. query
+        outputs: 4 B per point for values, 12 B for gradients), so the first bursts of requests
+        of that size meet no pinned allocation."""
+        self.pinned.reserve(nbytes, count)
+
     def _alloc(self, nbytes):
-        """uint8 device block for a resident buffer: from the arena when it fits."""
+        """uint8 device block for a resident buffer or a request's temporaries: from the arena,
+        evicting least-recently-used idle fields while it is full; torch's allocator only when
+        nothing more can be evicted."""
         import torch
-        blk = self.arena.alloc(nbytes) if self.arena is not None else None
-        return blk if blk is not None else torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+        if self.arena is not None:
+            blk = self.arena.alloc(nbytes)
+            while blk is None and self._evict_lru():
+                blk = self.arena.alloc(nbytes)
+            if blk is not None:
+                return blk
+        return torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
 
     def _keeper(self, keep):
         """alloc(nbytes) for a request's device temporaries: blocks from _alloc, each appended to
@@ -299,18 +340,25 @@ class FieldServer:
 
     def _evict_for(self, need):
         """Drop least-recently-used idle fields until `need` more bytes fit in the budget."""
-        resident = self.resident_bytes()
-        if resident + self.reserved + need <= self.budget:
-            return True
-        for f in sorted(self.fields.values(), key=lambda f: f.last_use):
-            if f.busy or f.editing:
-                continue
-            del self.fields[f.id]
-            self.resident -= f.accounted
-            resident -= f.accounted
-            if resident + self.reserved + need <= self.budget:
+        while self.resident + self.reserved + need > self.budget:
+            if not self._evict_lru():
+                return False
+        return True
+
+    def _evict_lru(self):
+        """Drop the least-recently-used idle resident field (its buffers return to the arena once
+        nothing holds them); False when every resident field is in use."""
+        for f in self.fields.values():  # oldest use first
+            if not f.busy and not f.editing:
+                del self.fields[f.id]
+                self.resident -= f.accounted
                 return True
-        return resident + self.reserved + need <= self.budget
+        return False
+
+    def _touch(self, f):
+        f.last_use = time.perf_counter()
+        if f.id in self.fields:
+            self.fields.move_to_end(f.id)
 
     def _admit(self):
         """Start queued requests, oldest first, while a slot is free and the budget allows; a
@@ -365,7 +413,7 @@ class FieldServer:
         if r.kind != "build" and r.field in self.fields:
             f = self.fields[r.field]
             f.busy -= 1
-            f.last_use = r.end
+            self._touch(f)
             if r.kind == "edit":
                 f.editing = False
         self.completed.append((r.kind, r.arrival, r.start, r.end))
@@ -439,11 +487,13 @@ class FieldServer:
     def _build_field(self, comp, meta, stream, slot):
         import torch
         with torch.cuda.stream(stream):
-            fb = FieldBuilder(comp, meta, device=self.device, alloc=self._alloc)
+            fb = FieldBuilder(comp, meta, device=self.device, alloc=self._alloc, pinned=self.pinned)
             fb.classify(stream)
             count = self.slot_host[slot].view(torch.int32)[:1]
             count.copy_(fb.count, non_blocking=True)
         yield self._record(stream)
+        # the tables' upload (if this build made it) ran on this stream ahead of the classification
+        release_staging(comp, self.device, self.pinned)
         n = int(count[0])
         with torch.cuda.stream(stream):
             b3 = meta.block ** 3
@@ -536,8 +586,10 @@ class FieldServer:
             _lib.check(lib.fb_edt_squared_device(mask.data_ptr(), m.nx, m.ny, m.nz, 1, out.data_ptr(),
                                                  scratch.data_ptr(), scratch.numel(), _lib.stream_handle(stream)),
                        "edt")
-            total = out.sum(dtype=torch.int64)
-            host = self.slot_host[r.slot][1]
+            total = self.slot_dev[r.slot, 0:1]
+            _lib.check(lib.fb_sum_i32_device(out.data_ptr(), out.numel(), total.data_ptr(),
+                                             _lib.stream_handle(stream)), "edt checksum")
+            host = self.slot_host[r.slot][1:2]
             host.copy_(total, non_blocking=True)
         yield self._record(stream)
         del keep

@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--streams", type=int, default=16, help="batched: streams the graph's branches spread over")
     ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
     ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrival window")
-    ap.add_argument("--arena-gb", type=float, default=120.0, help="serve: device arena for resident fields (0: none)")
+    ap.add_argument("--arena-gb", type=float, default=150.0, help="serve: device arena for resident fields and request temporaries (0: none)")
     ap.add_argument("--slots", type=int, default=16, help="serve: concurrent request slots (one stream each)")
     return ap.parse_args()
 
@@ -536,9 +536,10 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
                   for m in np.geomspace(100_000, 1_000_000, 8)]
     tool_sets = [X.compile_tools(R.tools(rng, int(k))) for k in rng.integers(1, 65, size=32)]
     working_set = 64  # requests on fields pick among the most recently built ones
-    # resident field buffers from one 120 GB arena: no cudaMalloc per build once it is taken
+    # resident field buffers and request temporaries from one arena the size of the budget: no
+    # cudaMalloc (or cudaFree, which synchronises the device) on the request path once it is taken
     slots = int(getattr(args, "slots", 16))
-    srv = S.FieldServer(slots=slots, budget_bytes=150e9, arena_bytes=getattr(args, "arena_gb", 120.0) * 1e9)
+    srv = S.FieldServer(slots=slots, budget_bytes=150e9, arena_bytes=getattr(args, "arena_gb", 150.0) * 1e9)
     try:
         # warm start: a resident field of every grid size, every kernel configured, one EDT per
         # grid size and one query per point-set size (pinned staging of each size allocated once)
@@ -551,13 +552,38 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
         for ps in point_sets:
             srv.submit("query", field=live[0], points=ps).result(timeout=120)
         srv.submit("edit", field=live[1], tools=tool_sets[0]).result(timeout=120)
+        # pinned staging for as many concurrent results of each query size as there are slots, and
+        # for the recipe tables that builds and edits upload
+        for ps in point_sets:
+            srv.reserve_pinned(len(ps) * 4, slots)
+            srv.reserve_pinned(len(ps) * 12, slots)
+        for c in range(16, 21):  # recipe tables of 64 KB to 1 MB
+            srv.reserve_pinned(1 << c, 2 * slots)
         srv.completed.clear()
         # the collector's full passes over the request objects would pause both threads mid-window
         gc.collect()
         gc.freeze()
         gc.disable()
         alloc0 = torch.cuda.memory_stats()
-        futs = []
+        # the client takes each result as it completes and drops it (result arrays are views of
+        # the server's pooled pinned blocks, which return to the pool when dropped)
+        errors = {}
+        outstanding = [0]
+        count_lock = threading.Lock()
+        all_done = threading.Event()
+        submitted = [False]
+
+        def on_done(fu, kind):
+            e = fu.exception()
+            if e is not None:
+                errors[type(e).__name__] = errors.get(type(e).__name__, 0) + 1
+            elif kind == "build":
+                live.append(fu.result()["field"])
+            with count_lock:
+                outstanding[0] -= 1
+                if submitted[0] and outstanding[0] == 0:
+                    all_done.set()
+
         t0 = time.perf_counter()
         due = t0
         for k, gap in zip(kinds, gaps):
@@ -566,24 +592,25 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
             if wait > 0:
                 time.sleep(wait)
             fid = live[-working_set:][int(rng.integers(min(len(live), working_set)))]
+            with count_lock:
+                outstanding[0] += 1
             if k == "build":
                 c, n = pool[int(rng.integers(len(pool)))]
                 f = srv.submit("build", recipe=c, meta=BT.cube_meta(n, 8))
-                f.add_done_callback(lambda fu: live.append(fu.result()["field"]) if not fu.exception() else None)
             elif k == "edit":
                 f = srv.submit("edit", field=fid, tools=tool_sets[int(rng.integers(len(tool_sets)))], op="subtract")
             elif k == "query":
                 f = srv.submit("query", field=fid, points=point_sets[int(rng.integers(len(point_sets)))])
             else:
                 f = srv.submit("edt", field=fid)
-            futs.append(f)
+            f.add_done_callback(lambda fu, kind=str(k): on_done(fu, kind))
         t_submitted = time.perf_counter()
-        errors = {}
-        for f in futs:
-            try:
-                f.result(timeout=600)
-            except Exception as e:
-                errors[type(e).__name__] = errors.get(type(e).__name__, 0) + 1
+        with count_lock:
+            submitted[0] = True
+            if outstanding[0] == 0:
+                all_done.set()
+        if not all_done.wait(timeout=600):
+            errors["ClientTimeout"] = outstanding[0]
         t_end = time.perf_counter()
         gc.enable()
         gc.unfreeze()
@@ -615,7 +642,7 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
         "allocator": {k: int(alloc1.get(k, 0) - alloc0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
                                                                            "num_alloc_retries")},
         "resident_gb": round(srv.resident_bytes() / 1e9, 2),
-        "slots": slots, "budget_gb": 150, "arena_gb": getattr(args, "arena_gb", 120.0), "data": "synthetic",
+        "slots": slots, "budget_gb": 150, "arena_gb": getattr(args, "arena_gb", 150.0), "data": "synthetic",
     }
 
 

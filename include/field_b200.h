@@ -156,6 +156,9 @@ int fb_field_occupancy_device(const int32_t* d_kind, const int32_t* d_active, co
 
 /* Replaces k_reduce_checksum_i64_safe, src/field_engine/faltkarna_v1.py:250-255 (accumulates into d_out[0]). */
 int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64_t* d_out, void* stream);
+/* Exact sum of n int32 values into d_out[0] (zeroed first, stream-ordered); the served EDT
+ * request's result summary.  No counterpart in the reference, which sums on the host. */
+int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------ packed fields */
 

@@ -90,3 +90,11 @@ def test_pinned_pool_recycles_a_block_when_its_array_is_dropped():
     assert pool.allocated == S.PinnedPool.MIN
     _, other = pool.take(S.PinnedPool.MIN + 1)  # the next size class: a new block
     assert other[0] == 2 * S.PinnedPool.MIN and pool.allocated == 3 * S.PinnedPool.MIN
+    pool.give_back(other)
+    _, small = pool.take(10)  # its own class is empty: the next class's free block serves it
+    assert small[0] == 2 * S.PinnedPool.MIN and pool.allocated == 3 * S.PinnedPool.MIN
+    pool.give_back(small)
+    pool.reserve(S.PinnedPool.MIN * 64, 2)  # reserve allocates blocks of its own class
+    assert len(pool.free[S.PinnedPool.MIN * 64]) == 2
+    _, tiny = pool.take(10)  # 64 classes up is beyond the span: the 2*MIN block, not a reserved one
+    assert tiny[0] == 2 * S.PinnedPool.MIN and len(pool.free[S.PinnedPool.MIN * 64]) == 2

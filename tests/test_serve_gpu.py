@@ -123,3 +123,27 @@ def test_arena_ranges_return_when_fields_go():
         srv.fields.clear()
     gc.collect()
     assert srv.arena.used == 0 and srv.arena.free == [(0, srv.arena.nbytes)]
+
+
+def test_a_full_arena_evicts_idle_fields_instead_of_leaving_it():
+    """With the arena full, a build evicts least-recently-used idle fields until its buffers fit;
+    every resident buffer stays inside the arena (no device allocation on the request path), and
+    the newest field still answers."""
+    import gc
+    import field_b200.serve as S
+    import field_b200.batch as BT
+    meta = BT.cube_meta(96, 8)
+    with S.FieldServer(slots=2, arena_bytes=2e9) as probe:
+        probe.submit("build", recipe=_recipe(0), meta=meta).result(timeout=60)
+        per_field = probe.arena.used
+    gc.collect()
+    with S.FieldServer(slots=2, arena_bytes=int(2.5 * per_field)) as srv:
+        base, end = srv.arena.base.data_ptr(), srv.arena.base.data_ptr() + srv.arena.nbytes
+        ids = [srv.submit("build", recipe=_recipe(i), meta=meta).result(timeout=60)["field"] for i in range(6)]
+        assert ids[0] not in srv.fields and ids[-1] in srv.fields
+        assert len(srv.fields) <= 2
+        for f in srv.fields.values():
+            for t in [f.fb.slab, f.tiles]:
+                assert base <= t.data_ptr() and t.data_ptr() + t.numel() * t.element_size() <= end
+        v, g = srv.submit("query", field=ids[-1], points=np.full((8, 3), 0.5, np.float32)).result(timeout=60)
+        assert v.shape == (8,) and np.isfinite(v).all()
