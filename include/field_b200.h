@@ -160,6 +160,34 @@ int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64
  * request's result summary.  No counterpart in the reference, which sums on the host. */
 int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* stream);
 
+/* Packed adaptive block tree (the reference's AdaptiveBlocks, src/field_engine/field_adaptive_blocks_v1.py):
+ * build(), :113-147, one level at a time from the dense classifications at sides 8, 4, 2, 1
+ * (fb_dense_classify_device), then packing and rank checkpoints; sample(), :53-82.
+ * fb_tree_codes_device: codes of one level's n nodes and the exclusive rank of its ranked code
+ * (2 at sides 8/4/2, 3 at side 1), the level total in *d_total; d_coords = NULL for the root level
+ * (rx x ry x rz root blocks in C order).  fb_tree_expand_device: 8 child corners per branch at
+ * 8 * rank + child.  fb_tree_values_device: dense samples of the side-1 value leaves by rank.
+ * fb_tree_pack_device: 2-bit codes four per byte (d_packed 4-byte aligned, sized to a multiple of
+ * 4 bytes) and the checkpoints every 64 bytes (floor(bytes / 64) + 1 entries each).
+ * fb_tree_sample_device: values at int64 grid indices [n][3]; *d_status OR-ed with 1 (index outside
+ * the grid), 2 (branch below side 1), 4 (rank outside the arrays), those outputs NaN. */
+int64_t fb_tree_scan_bytes(int64_t n);
+int fb_tree_codes_device(const int32_t* d_kind, int32_t side, int64_t nbx, int64_t nby, int64_t nbz, int64_t nx,
+                         int64_t ny, int64_t nz, const int32_t* d_coords, int64_t rx, int64_t ry, int64_t rz,
+                         int64_t n, uint8_t* d_codes, int32_t* d_rank, int32_t* d_total, void* d_scratch,
+                         int64_t scratch_len, void* stream);
+int fb_tree_expand_device(const uint8_t* d_codes, const int32_t* d_rank, const int32_t* d_coords, int64_t rx,
+                          int64_t ry, int64_t rz, int64_t n, int32_t side, int32_t* d_child, void* stream);
+int fb_tree_values_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, const uint8_t* d_codes,
+                          const int32_t* d_rank, const int32_t* d_coords, int64_t n, float* d_values, void* stream);
+int64_t fb_tree_pack_scratch_bytes(int64_t node_count);
+int fb_tree_pack_device(const uint8_t* d_codes, int64_t node_count, uint8_t* d_packed, int32_t* d_branch_prefix,
+                        int32_t* d_value_prefix, void* d_scratch, int64_t scratch_len, void* stream);
+int fb_tree_sample_device(const uint8_t* d_packed, int64_t node_count, const int32_t* d_branch_prefix,
+                          const int32_t* d_value_prefix, const float* d_values, int64_t n_values, int64_t root_count,
+                          int64_t r0, int64_t r1, int64_t r2, int64_t nx, int64_t ny, int64_t nz, double pitch,
+                          const int64_t* d_ijk, int64_t n, float* d_out, int32_t* d_status, void* stream);
+
 /* ------------------------------------------------------------------------------------------ packed fields */
 
 /* Replace adaptive_pack / adaptive_nodes / adaptive_samples / adaptive_copy / adaptive_free,

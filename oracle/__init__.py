@@ -417,3 +417,82 @@ def multires_gradient(lo, h, block, brick_shape, kind, niva, tiles, margin, pts)
         g[:, ax] = (multires_avstand(lo, h, block, brick_shape, kind, niva, tiles, margin, pa) -
                     multires_avstand(lo, h, block, brick_shape, kind, niva, tiles, margin, pb)) / np.maximum(step, 1e-12)
     return g
+
+
+# ----------------------------------------------------------------------------------------- adaptive block tree
+TREE_SIDES = (8, 4, 2, 1)
+
+
+def tree_build(dense, pitch):
+    """The packed adaptive block tree of src/field_engine/field_adaptive_blocks_v1.py:113-147,
+    restated level by level: dict(shape, root_shape, root_count, node_count, packed,
+    branch_prefix, value_prefix, values, histogram).  Block kinds from classify_dense at sides 8,
+    4, 2, 1; a node at corner (x, y, z) is 0 outside the grid or for kind > 0, 1 for kind < 0, 3
+    (with dense[x, y, z] appended to the values) for kind 0 at side 1, else 2 with its 8 children
+    (x + i h, y + j h, z + k h), i, j, k in C order, appended in breadth-first order."""
+    d = np.ascontiguousarray(dense, dtype=np.float32)
+    shape = d.shape
+    kinds = {}
+    for side in TREE_SIDES:
+        nb = tuple(-(-n // side) for n in shape)
+        kinds[side] = classify_dense(d, pitch, side)["kind"].reshape(nb)
+    root_shape = kinds[8].shape
+    coords = (np.indices(root_shape).reshape(3, -1).T * 8).astype(np.int64)
+    offsets = np.array([(i, j, k) for i in (0, 1) for j in (0, 1) for k in (0, 1)], np.int64)
+    codes, values, hist = [], np.zeros(0, np.float32), {}
+    for side in TREE_SIDES:
+        if len(coords) == 0:
+            break
+        x, y, z = coords.T
+        inside = (x < shape[0]) & (y < shape[1]) & (z < shape[2])
+        k = np.ones(len(coords), np.int64)
+        k[inside] = kinds[side][x[inside] // side, y[inside] // side, z[inside] // side]
+        code = np.zeros(len(coords), np.uint8)
+        code[inside & (k < 0)] = 1
+        code[inside & (k == 0)] = 3 if side == 1 else 2
+        codes.append(code)
+        for c in (0, 1, 3):
+            cnt = int(np.count_nonzero(code == c))
+            if cnt:
+                hist[f"side{side}_kind{c}"] = cnt
+        if side == 1:
+            values = d[x[code == 3], y[code == 3], z[code == 3]].astype(np.float32)
+        coords = (coords[code == 2][:, None, :] + offsets[None] * (side // 2)).reshape(-1, 3)
+    code = np.concatenate(codes)
+    padded = np.pad(code, (0, (-len(code)) % 4))
+    packed = (padded.reshape(-1, 4).astype(np.uint32) << np.array([0, 2, 4, 6], np.uint32)).sum(axis=1).astype(np.uint8)
+    prefixes = []
+    for c in (2, 3):
+        per_byte = ((packed[:, None] >> np.array([0, 2, 4, 6], np.uint8)) & 3 == c).sum(axis=1)
+        cumulative = np.concatenate(([0], np.cumsum(per_byte)))
+        prefixes.append(cumulative[0:len(packed) + 1:64].astype(np.int32))
+    return dict(shape=shape, root_shape=root_shape, root_count=int(np.prod(root_shape)), node_count=len(code),
+                packed=packed, branch_prefix=prefixes[0], value_prefix=prefixes[1], values=values,
+                histogram=dict(sorted(hist.items())))
+
+
+def tree_sample(tree, indices, pitch):
+    """float32 values of a tree_build dict at integer grid coordinates [N, 3]
+    (field_adaptive_blocks_v1.py:53-82): descend by child octant, ranking with full prefix counts."""
+    ijk = np.asarray(indices, dtype=np.int64)
+    codes = ((tree["packed"][:, None] >> np.array([0, 2, 4, 6], np.uint8)) & 3).reshape(-1)
+    before = {c: np.concatenate(([0], np.cumsum(codes == c))) for c in (2, 3)}
+    rs = tree["root_shape"]
+    node = ((ijk[:, 0] // 8) * rs[1] + ijk[:, 1] // 8) * rs[2] + ijk[:, 2] // 8
+    size = np.full(len(ijk), 8, np.int64)
+    out = np.full(len(ijk), np.nan, np.float32)
+    todo = np.arange(len(ijk))
+    while len(todo):
+        c = codes[node[todo]]
+        leaf = todo[c < 2]
+        sign = np.where(c[c < 2] == 0, 1.0, -1.0)
+        out[leaf] = sign * np.sqrt(3.0) * size[leaf] * pitch
+        val = todo[c == 3]
+        out[val] = tree["values"][before[3][node[val]]]
+        br = todo[c == 2]
+        half = size[br] // 2
+        octant = (ijk[br] // half[:, None]) % 2
+        node[br] = tree["root_count"] + 8 * before[2][node[br]] + 4 * octant[:, 0] + 2 * octant[:, 1] + octant[:, 2]
+        size[br] = half
+        todo = br
+    return out
