@@ -48,7 +48,7 @@ SIGNATURES = {
     "fb_sum_i32_device": (I, [P, I64, P, P]),
     # packed adaptive block tree
     "fb_tree_scan_bytes": (I64, [I64]),
-    "fb_tree_codes_device": (I, [P, I, I64, I64, I64, I64, I64, I64, P, I64, I64, I64, I64, P, P, P, P, I64, P]),
+    "fb_tree_codes_device": (I, [P, I64, I64, I64, I, F, P, I64, I64, I64, I64, P, P, P, P, I64, P]),
     "fb_tree_expand_device": (I, [P, P, P, I64, I64, I64, I64, I, P, P]),
     "fb_tree_values_device": (I, [P, I64, I64, I64, P, P, P, I64, P, P]),
     "fb_tree_pack_scratch_bytes": (I64, [I64]),

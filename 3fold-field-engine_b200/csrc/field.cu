@@ -20,6 +20,7 @@
 // (classification rule), :167-190 (tile order), :277 (ascending compaction); dense input
 // src/field_engine/faltkarna_v1_mesh_to_sdf.py:602-657.
 #include "common.cuh"
+#include "dense.cuh"
 #include "prims.cuh"
 #include <algorithm>
 #include <cmath>
@@ -1222,19 +1223,10 @@ __global__ void k_classify_dense(const float* __restrict__ dense, int64_t nx, in
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= nblocks) return;
     const int64_t bk = t % nbz, bj = (t / nbz) % nby, bi = t / ((int64_t)nbz * nby);
-    float mn = 1.0e30f;
-    bool pos = false, neg = false;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int64_t cx = min(bi * B + (c & 1) * B, nx - 1);
-        const int64_t cy = min(bj * B + ((c >> 1) & 1) * B, ny - 1);
-        const int64_t cz = min(bk * B + ((c >> 2) & 1) * B, nz - 1);
-        const float v = dense[(cx * ny + cy) * nz + cz];
-        mn = fminf(mn, fabsf(v));
-        if (v >= 0.0f) pos = true; else neg = true;
-    }
+    float mn;
+    const int k = dense_block_kind(dense, nx, ny, nz, B, bi * B, bj * B, bk * B, margin, &mn);
     if (cma) cma[t] = mn;
-    kind[t] = (pos && neg) ? 0 : ((mn <= margin) ? 0 : (neg ? -1 : 1));
+    kind[t] = k;
 }
 
 // Warp per active block; each lane copies voxels with the index clamped to n-1.

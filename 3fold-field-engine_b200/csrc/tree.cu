@@ -4,9 +4,11 @@
 // value leaves in node order.
 //
 // Build, level by level (sides 8, 4, 2, 1; field_adaptive_blocks_v1.py:113-147):
-//   k_tree_codes  : code of every node of the level from the dense block classification of its
-//                   side (outside the grid 0, kind > 0 -> 0, kind < 0 -> 1, kind 0 -> 3 at side 1
-//                   else 2) and the flag the level's exclusive scan ranks (2 at sides > 1, 3 at 1);
+//   k_tree_codes  : code of every node of the level from the dense classification rule of its
+//                   block (dense_block_kind, evaluated for the level's nodes only -- not for every
+//                   block of the grid at that side): outside the grid 0, kind > 0 -> 0, kind < 0
+//                   -> 1, kind 0 -> 3 at side 1 else 2; and the flag the level's exclusive scan
+//                   ranks (2 at sides > 1, 3 at 1);
 //   k_tree_expand : each branch of rank b writes its 8 children at 8b + (4i + 2j + k) of the next
 //                   level -- the breadth-first order in which the children of the b-th branch of
 //                   the whole tree start at root_count + 8b;
@@ -15,6 +17,7 @@
 // checkpoints.  k_tree_sample walks the tree for grid indices the way AdaptiveBlocks.sample does
 // (field_adaptive_blocks_v1.py:35-82), counting codes 16 nodes per 32-bit word with popc.
 #include "common.cuh"
+#include "dense.cuh"
 #include <algorithm>
 
 namespace {
@@ -121,17 +124,16 @@ __device__ __forceinline__ void node_corner(const Level& L, int64_t i, int64_t& 
     }
 }
 
-__global__ void k_tree_codes(const int32_t* __restrict__ kind, int side, int64_t nbx, int64_t nby, int64_t nbz,
-                             int64_t nx, int64_t ny, int64_t nz, Level L, int64_t n, uint8_t* __restrict__ codes,
-                             int32_t* __restrict__ flag) {
+__global__ void k_tree_codes(const float* __restrict__ dense, int side, float margin, int64_t nx, int64_t ny,
+                             int64_t nz, Level L, int64_t n, uint8_t* __restrict__ codes, int32_t* __restrict__ flag) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t x, y, z;
     node_corner(L, i, x, y, z);
     int code = 0;
-    if (x < nx && y < ny && z < nz) {
-        const int64_t b = ((x / side) * nby + y / side) * nbz + z / side;
-        const int k = (b >= 0 && b < nbx * nby * nbz) ? kind[b] : 1;
+    if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) {
+        float mn;
+        const int k = dense_block_kind(dense, nx, ny, nz, side, x, y, z, margin, &mn);
         code = k > 0 ? 0 : (k < 0 ? 1 : (side == 1 ? 3 : 2));
     }
     codes[i] = (uint8_t)code;
@@ -270,22 +272,23 @@ int64_t fb_tree_scan_bytes(int64_t n) noexcept {
 }
 
 // One level of the tree: codes[n] and rank[n] (exclusive count of the level's ranked code: 2 at
-// sides 8/4/2, 3 at side 1) with the level total in *d_total.  d_kind: the dense block
-// classification at this side (nbx x nby x nbz blocks); d_coords: the level's node corners [n][3],
-// or nullptr for the root level (C order over rx x ry x rz root blocks of side 8).
-int fb_tree_codes_device(const int32_t* d_kind, int32_t side, int64_t nbx, int64_t nby, int64_t nbz, int64_t nx,
-                         int64_t ny, int64_t nz, const int32_t* d_coords, int64_t rx, int64_t ry, int64_t rz,
-                         int64_t n, uint8_t* d_codes, int32_t* d_rank, int32_t* d_total, void* d_scratch,
-                         int64_t scratch_len, void* stream) noexcept {
-    if (!d_kind || !d_codes || !d_rank || !d_total || n < 0 || (side != 8 && side != 4 && side != 2 && side != 1))
+// sides 8/4/2, 3 at side 1) with the level total in *d_total.  Each node is classified from the
+// dense field by the block rule with this side's margin (float32 of sqrt(3) * side * pitch);
+// d_coords: the level's node corners [n][3], or nullptr for the root level (C order over
+// rx x ry x rz root blocks of side 8).
+int fb_tree_codes_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, int32_t side, float margin,
+                         const int32_t* d_coords, int64_t rx, int64_t ry, int64_t rz, int64_t n, uint8_t* d_codes,
+                         int32_t* d_rank, int32_t* d_total, void* d_scratch, int64_t scratch_len,
+                         void* stream) noexcept {
+    if (!d_dense || !d_codes || !d_rank || !d_total || n < 0 || (side != 8 && side != 4 && side != 2 && side != 1))
         return FB_INVALID;
-    if (nx < 1 || ny < 1 || nz < 1 || nbx < 1 || nby < 1 || nbz < 1 || n >= (int64_t(1) << 31)) return FB_INVALID;
+    if (nx < 1 || ny < 1 || nz < 1 || n >= (int64_t(1) << 31)) return FB_INVALID;
     if (!d_coords && (side != 8 || rx < 1 || ry < 1 || rz < 1 || rx * ry * rz != n)) return FB_INVALID;
     if (n > 0 && (!d_scratch || scratch_len < fb_tree_scan_bytes(n))) return FB_INVALID;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Level L{d_coords, rx, ry, rz};
     if (n > 0) {
-        k_tree_codes<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_kind, side, nbx, nby, nbz, nx, ny, nz, L, n, d_codes,
+        k_tree_codes<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_dense, side, margin, nx, ny, nz, L, n, d_codes,
                                                                  d_rank);
         FB_LAUNCH();
     }

@@ -13,7 +13,8 @@ The format: one 2-bit code per node -- 0 a leaf outside the surface (its value i
 dense sample -- packed four per byte in breadth-first order; the children of the b-th branch are
 nodes root_count + 8b ... + 7, so ranks replace pointers; rank checkpoints every 64 bytes (256
 nodes) for codes 2 and 3.  The tree is decided by the dense block classification at sides 8, 4, 2
-and 1 (the 8-corner rule with the full block-diagonal margin, ``fb_dense_classify_device``).
+and 1 (the 8-corner rule with the full block-diagonal margin of ``fb_dense_classify_device``),
+evaluated for the tree's nodes only.
 """
 from __future__ import annotations
 
@@ -149,31 +150,18 @@ def build_device(dense, pitch, *, stream=None):
     nx, ny, nz = (int(v) for v in dense.shape)
     dense = dense.to(torch.float32).contiguous()
     sh = _lib.stream_handle(stream)
-    kinds = {}
-    for side in SIDES:
-        nb = tuple(-(-n // side) for n in (nx, ny, nz))
-        n_blocks = nb[0] * nb[1] * nb[2]
-        kind = torch.empty(n_blocks, dtype=torch.int32, device=dev)
-        active = torch.empty(n_blocks, dtype=torch.int32, device=dev)
-        count = torch.empty(1, dtype=torch.int32, device=dev)
-        scratch = torch.empty(int(lib.fb_dense_scratch_bytes(nx, ny, nz, side)), dtype=torch.uint8, device=dev)
-        margin = float(np.float32(math.sqrt(3.0) * side * pitch))
-        _check(lib.fb_dense_classify_device(dense.data_ptr(), nx, ny, nz, side, margin, kind.data_ptr(), None,
-                                            active.data_ptr(), count.data_ptr(), None, 0, scratch.data_ptr(),
-                                            scratch.numel(), sh), "dense classify")
-        kinds[side] = (kind, nb)
-    root_shape = kinds[8][1]
+    root_shape = tuple(-(-v // 8) for v in (nx, ny, nz))
     n = root_shape[0] * root_shape[1] * root_shape[2]
     coords = None
     level_codes, level_sizes = [], []
     values = torch.empty(0, dtype=torch.float32, device=dev)
     total = torch.empty(1, dtype=torch.int32, device=dev)
     for side in SIDES:
-        kind, nb = kinds[side]
+        margin = float(np.float32(math.sqrt(3.0) * side * pitch))  # the dense classification's margin
         codes = torch.empty(n, dtype=torch.uint8, device=dev)
         rank = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
         scratch = torch.empty(int(lib.fb_tree_scan_bytes(n)), dtype=torch.uint8, device=dev)
-        _check(lib.fb_tree_codes_device(kind.data_ptr(), side, *nb, nx, ny, nz,
+        _check(lib.fb_tree_codes_device(dense.data_ptr(), nx, ny, nz, side, margin,
                                         coords.data_ptr() if coords is not None else None, *root_shape, n,
                                         codes.data_ptr(), rank.data_ptr(), total.data_ptr(), scratch.data_ptr(),
                                         scratch.numel(), sh), "tree codes")

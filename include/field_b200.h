@@ -161,8 +161,8 @@ int fb_checksum_i64_device(const float* d_values, int64_t n, double scale, int64
 int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* stream);
 
 /* Packed adaptive block tree (the reference's AdaptiveBlocks, src/field_engine/field_adaptive_blocks_v1.py):
- * build(), :113-147, one level at a time from the dense classifications at sides 8, 4, 2, 1
- * (fb_dense_classify_device), then packing and rank checkpoints; sample(), :53-82.
+ * build(), :113-147, one level at a time, each node classified from the dense field by the rule of
+ * fb_dense_classify_device at its side, then packing and rank checkpoints; sample(), :53-82.
  * fb_tree_codes_device: codes of one level's n nodes and the exclusive rank of its ranked code
  * (2 at sides 8/4/2, 3 at side 1), the level total in *d_total; d_coords = NULL for the root level
  * (rx x ry x rz root blocks in C order).  fb_tree_expand_device: 8 child corners per branch at
@@ -172,10 +172,9 @@ int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* 
  * fb_tree_sample_device: values at int64 grid indices [n][3]; *d_status OR-ed with 1 (index outside
  * the grid), 2 (branch below side 1), 4 (rank outside the arrays), those outputs NaN. */
 int64_t fb_tree_scan_bytes(int64_t n);
-int fb_tree_codes_device(const int32_t* d_kind, int32_t side, int64_t nbx, int64_t nby, int64_t nbz, int64_t nx,
-                         int64_t ny, int64_t nz, const int32_t* d_coords, int64_t rx, int64_t ry, int64_t rz,
-                         int64_t n, uint8_t* d_codes, int32_t* d_rank, int32_t* d_total, void* d_scratch,
-                         int64_t scratch_len, void* stream);
+int fb_tree_codes_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, int32_t side, float margin,
+                         const int32_t* d_coords, int64_t rx, int64_t ry, int64_t rz, int64_t n, uint8_t* d_codes,
+                         int32_t* d_rank, int32_t* d_total, void* d_scratch, int64_t scratch_len, void* stream);
 int fb_tree_expand_device(const uint8_t* d_codes, const int32_t* d_rank, const int32_t* d_coords, int64_t rx,
                           int64_t ry, int64_t rz, int64_t n, int32_t side, int32_t* d_child, void* stream);
 int fb_tree_values_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, const uint8_t* d_codes,
