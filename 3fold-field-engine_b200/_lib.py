@@ -46,6 +46,8 @@ SIGNATURES = {
     "fb_field_reconstruct_device": (I, [P, P, I64, P, I64, I64, I64, I, F, P, P, P]),
     "fb_checksum_i64_device": (I, [P, I64, D, P, P]),
     "fb_sum_i32_device": (I, [P, I64, P, P]),
+    # mesh -> field stage (host pointers)
+    "meshsdf_field_cpu": (I, [P, I64, P, I64, D, D, D, D, D, D, I64, I64, I64, I, I, P, P, P, P, P]),
     # packed adaptive block tree
     "fb_tree_scan_bytes": (I64, [I64]),
     "fb_tree_codes_device": (I, [P, I64, I64, I64, I, F, P, I64, I64, I64, I64, P, P, P, P, I64, P]),

@@ -1,0 +1,397 @@
+// Mesh -> signed distance field stage on the GPU: the reference's ray-parity winding rule and the
+// paired exact EDT (src/field_engine/mesh_sdf_native_v1/field.cpp:19-226, the native form of
+// faltkarna_v1_mesh_to_sdf's raypar_vindning path).
+//
+//   1. k_mesh_tri_count / k_mesh_tri_fill : for every triangle, the vertical rays of the (x, y)
+//      columns inside its bounding box that it crosses, each hit's z and the triangle's xy
+//      orientation; count, scan, fill.  Float64 with the reference's operation order and no
+//      contraction (every product and sum an explicit _rn operation), so each hit is the same bits.
+//   2. k_mesh_col_count / scan / k_mesh_col_scatter : hits grouped by column (the winding sum does
+//      not depend on their order within a column); the global z range by order-preserving atomics.
+//   3. k_mesh_winding : a voxel is solid when the oriented hits above it (by the reference's
+//      normalised key comparison) do not cancel; the voxels where winding and ray parity disagree
+//      are counted.
+//   4. the paired exact squared EDT of the solid mask (fb_edt_pair_device), then k_mesh_finish:
+//      sd = float32(sqrt(sq_out) pitch) - float32(sqrt(sq_in) pitch) with the optional half-pitch
+//      correction, and the surface layer (solid voxels on the boundary or next to a non-solid one).
+//
+// Bit-exact against the reference for the solid mask, the surface layer and the statistics.  The
+// reference forms each distance from its nearest feature's offsets, sqrt((dx p)^2 + (dy p)^2 +
+// (dz p)^2); here from the exact squared distance, sqrt(n) p -- the same number up to float64
+// rounding, so the float32 distances agree except in the rare voxel whose value lies within a few
+// float64 ulps of a float32 rounding boundary (then by one float32 ulp).
+#include "common.cuh"
+#include "scan.cuh"
+#include <cmath>
+#include <limits>
+#include <vector>
+
+extern "C" int fb_edt_pair_device(const uint8_t* d_mask, int nx, int ny, int nz, double pitch, float* d_signed,
+                                  int32_t* d_squared, void* d_scratch, int64_t scratch_len, void* stream) noexcept;
+extern "C" int64_t fb_edt_scratch_bytes(int nx, int ny, int nz, int paired);
+
+namespace {
+
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dd(double a, double b) { return __ddiv_rn(a, b); }
+
+struct Grid {
+    double ox, oy, oz, pitch, jx, jy;
+    int64_t nx, ny, nz;
+};
+
+// Column range and orientation of triangle t (field.cpp:44-67); false when it casts no hit.
+struct Tri {
+    double ax, ay, az, bx, by, bz, cx, cy, cz, a2, sg;
+    int64_t i0, i1, j0, j1;
+    int8_t tk;
+    bool local;
+};
+
+__device__ bool setup_tri(const double* __restrict__ V, const int64_t* __restrict__ T, int64_t t, const Grid& g,
+                          Tri& r) {
+    const double* A = V + 3 * T[3 * t];
+    const double* B = V + 3 * T[3 * t + 1];
+    const double* C = V + 3 * T[3 * t + 2];
+    const double e1x = ds(B[0], A[0]), e1y = ds(B[1], A[1]), e2x = ds(C[0], A[0]), e2y = ds(C[1], A[1]);
+    r.a2 = ds(dm(e1x, e2y), dm(e1y, e2x));
+    const double skala = fmax(fmax(fabs(e1x), fabs(e1y)), fmax(fabs(e2x), fabs(e2y)));
+    if (!(fabs(r.a2) > dm(dm(1e-12, skala), skala))) return false;
+    const double xmin = fmin(fmin(A[0], B[0]), C[0]), xmax = fmax(fmax(A[0], B[0]), C[0]);
+    const double ymin = fmin(fmin(A[1], B[1]), C[1]), ymax = fmax(fmax(A[1], B[1]), C[1]);
+    int64_t i0 = (int64_t)ceil(ds(dd(ds(ds(xmin, g.jx), g.ox), g.pitch), 0.0));
+    int64_t i1 = (int64_t)floor(ds(dd(ds(ds(xmax, g.jx), g.ox), g.pitch), 0.0));
+    int64_t j0 = (int64_t)ceil(ds(dd(ds(ds(ymin, g.jy), g.oy), g.pitch), 0.0));
+    int64_t j1 = (int64_t)floor(ds(dd(ds(ds(ymax, g.jy), g.oy), g.pitch), 0.0));
+    i0 = min(max(i0, (int64_t)0), g.nx);
+    i1 = min(max(i1, (int64_t)-1), g.nx - 1);
+    j0 = min(max(j0, (int64_t)0), g.ny);
+    j1 = min(max(j1, (int64_t)-1), g.ny - 1);
+    if (i1 < i0 || j1 < j0) return false;
+    r.i0 = i0; r.i1 = i1; r.j0 = j0; r.j1 = j1;
+    r.sg = r.a2 > 0 ? 1.0 : (r.a2 < 0 ? -1.0 : 0.0);
+    r.tk = (int8_t)(r.a2 > 0 ? 1 : (r.a2 < 0 ? -1 : 0));
+    r.ax = A[0]; r.ay = A[1]; r.az = A[2];
+    r.bx = B[0]; r.by = B[1]; r.bz = B[2];
+    r.cx = C[0]; r.cy = C[1]; r.cz = C[2];
+    const double e3 = fmax(fmax(fabs(ds(r.bx, r.ax)), fabs(ds(r.by, r.ay))), fabs(ds(r.bz, r.az)));
+    const double e4 = fmax(fmax(fabs(ds(r.cx, r.ax)), fabs(ds(r.cy, r.ay))), fabs(ds(r.cz, r.az)));
+    r.local = fabs(r.az) > dm(1024.0, fmax(e3, e4));
+    return true;
+}
+
+// The hit of column (ii, jj), or false (field.cpp:68-80).
+__device__ __forceinline__ bool column_hit(const Tri& r, const Grid& g, int64_t ii, int64_t jj, double& z) {
+    const double px = da(da(g.ox, dm(da((double)ii, 0.0), g.pitch)), g.jx);
+    const double py = da(da(g.oy, dm(da((double)jj, 0.0), g.pitch)), g.jy);
+    const double l0 = ds(dm(ds(r.bx, px), ds(r.cy, py)), dm(ds(r.by, py), ds(r.cx, px)));
+    if (!(dm(l0, r.sg) >= 0)) return false;
+    const double l1 = ds(dm(ds(r.cx, px), ds(r.ay, py)), dm(ds(r.cy, py), ds(r.ax, px)));
+    if (!(dm(l1, r.sg) >= 0)) return false;
+    const double l2 = ds(dm(ds(r.ax, px), ds(r.by, py)), dm(ds(r.ay, py), ds(r.bx, px)));
+    if (!(dm(l2, r.sg) >= 0)) return false;
+    if (r.local) z = da(r.az, dd(da(dm(l1, ds(r.bz, r.az)), dm(l2, ds(r.cz, r.az))), r.a2));
+    else z = dd(da(da(dm(l0, r.az), dm(l1, r.bz)), dm(l2, r.cz)), r.a2);
+    return true;
+}
+
+// count[t] = hits of triangle t; misc[0] += its column pairs, misc[5] += its hits (64-bit totals).
+__global__ void k_mesh_tri_count(const double* __restrict__ V, const int64_t* __restrict__ T, int64_t nt, Grid g,
+                                 int32_t* __restrict__ count, unsigned long long* __restrict__ misc) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    Tri r;
+    int32_t c = 0;
+    if (setup_tri(V, T, t, g, r)) {
+        atomicAdd(&misc[0], (unsigned long long)((r.i1 - r.i0 + 1) * (r.j1 - r.j0 + 1)));
+        for (int64_t ii = r.i0; ii <= r.i1; ++ii)
+            for (int64_t jj = r.j0; jj <= r.j1; ++jj) {
+                double z;
+                c += column_hit(r, g, ii, jj, z);
+            }
+        if (c) atomicAdd(&misc[5], (unsigned long long)c);
+    }
+    count[t] = c;
+}
+
+// Order-preserving map of a float64 onto uint64 (for atomic min / max).
+__device__ __forceinline__ unsigned long long order_key(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_key(unsigned long long k) {
+    return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
+}
+
+__global__ void k_mesh_tri_fill(const double* __restrict__ V, const int64_t* __restrict__ T, int64_t nt, Grid g,
+                                const int32_t* __restrict__ offset, int64_t* __restrict__ hcol,
+                                double* __restrict__ hz, int8_t* __restrict__ hs, unsigned long long* __restrict__ zkey) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    Tri r;
+    if (!setup_tri(V, T, t, g, r)) return;
+    int64_t at = offset[t];
+    double lo = INFINITY, hi = -INFINITY;
+    for (int64_t ii = r.i0; ii <= r.i1; ++ii)
+        for (int64_t jj = r.j0; jj <= r.j1; ++jj) {
+            double z;
+            if (!column_hit(r, g, ii, jj, z)) continue;
+            hcol[at] = ii * g.ny + jj;
+            hz[at] = z;
+            hs[at] = r.tk;
+            ++at;
+            lo = fmin(lo, z);
+            hi = fmax(hi, z);
+        }
+    if (lo <= hi) {
+        atomicMin(&zkey[0], order_key(lo));
+        atomicMax(&zkey[1], order_key(hi));
+    }
+}
+
+__global__ void k_mesh_col_count(const int64_t* __restrict__ hcol, int64_t nh, int32_t* __restrict__ cnt) {
+    const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (h < nh) atomicAdd(&cnt[hcol[h]], 1);
+}
+
+__global__ void k_mesh_col_scatter(const int64_t* __restrict__ hcol, const double* __restrict__ hz,
+                                   const int8_t* __restrict__ hs, int64_t nh, int32_t* __restrict__ cursor,
+                                   double* __restrict__ cz, int8_t* __restrict__ cs) {
+    const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    const int32_t k = atomicAdd(&cursor[hcol[h]], 1);
+    cz[k] = hz[h];
+    cs[k] = hs[h];
+}
+
+// One voxel per thread (field.cpp:100-123): w = sum of the orientations of the hits whose key lies
+// above the voxel's key; solid = (w != 0); differs from ray parity when (count & 1) != solid.
+__global__ void k_mesh_winding(const int32_t* __restrict__ start, const double* __restrict__ cz,
+                               const int8_t* __restrict__ cs, Grid g, const unsigned long long* __restrict__ zkey,
+                               uint8_t* __restrict__ solid, unsigned long long* __restrict__ counters) {
+    const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t N = g.nx * g.ny * g.nz;
+    unsigned diff = 0, nsolid = 0;
+    if (v < N) {
+        const int64_t c = v / g.nz, k = v - c * g.nz;
+        const int32_t h0 = start[c], h1 = start[c + 1];
+        uint8_t s = 0;
+        if (h1 > h0) {
+            const double zmin = from_key(zkey[0]), zmax = from_key(zkey[1]);
+            const double span = fmax(ds(zmax, zmin), 1e-12);
+            const double fc = (double)c;
+            const double zc = da(g.oz, dm(da((double)k, 0.0), g.pitch));
+            const double vv = da(0.25, dd(dm(0.5, ds(zc, zmin)), span));
+            const double kc = da(fc, fmin(fmax(vv, 0.0), 0.999));
+            const double base = da(fc, 0.25);
+            int w = 0, np = 0;
+            for (int32_t h = h0; h < h1; ++h) {
+                const double key = da(base, dd(dm(0.5, ds(cz[h], zmin)), span));
+                if (key > kc) {
+                    w += cs[h];
+                    ++np;
+                }
+            }
+            s = (uint8_t)(w != 0);
+            diff = (unsigned)((np & 1) != s);
+        }
+        solid[v] = s;
+        nsolid = s;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        diff += __shfl_xor_sync(0xffffffffu, diff, o);
+        nsolid += __shfl_xor_sync(0xffffffffu, nsolid, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (diff) atomicAdd(&counters[0], (unsigned long long)diff);
+        if (nsolid) atomicAdd(&counters[1], (unsigned long long)nsolid);
+    }
+}
+
+// sd and the surface layer (field.cpp:197-214).  sq: the pair [to solid | to non-solid], or nullptr
+// when one class is empty: that class's distance is then -1 (the reference's value for lines with
+// no feature) and the other's 0 (every voxel is its own feature).
+__global__ void k_mesh_finish(const uint8_t* __restrict__ solid, const int32_t* __restrict__ sq, Grid g,
+                              int empty_class, int ytkorr, float* __restrict__ sd, uint8_t* __restrict__ yta) {
+    const int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t N = g.nx * g.ny * g.nz;
+    if (lin >= N) return;
+    float d[2];
+    for (int cls = 0; cls < 2; ++cls) {
+        if (!sq) d[cls] = cls == empty_class ? -1.0f : 0.0f;
+        else d[cls] = __double2float_rn(__dmul_rn(__dsqrt_rn((double)sq[cls * N + lin]), g.pitch));
+    }
+    float v = __fsub_rn(d[0], d[1]);
+    if (ytkorr) {
+        const float half = __double2float_rn(0.5 * g.pitch);
+        const float sgn = v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f);
+        v = __fsub_rn(v, __fmul_rn(sgn, half));
+    }
+    sd[lin] = v;
+    const uint8_t s = solid[lin];
+    uint8_t y = 0;
+    if (s) {
+        const int64_t k = lin % g.nz, j = (lin / g.nz) % g.ny, i = lin / (g.nz * g.ny);
+        const int64_t pl = g.ny * g.nz;
+        if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1 || k == 0 || k == g.nz - 1) y = 1;
+        else if (!solid[lin - pl] || !solid[lin + pl] || !solid[lin - g.nz] || !solid[lin + g.nz] || !solid[lin - 1] ||
+                 !solid[lin + 1])
+            y = 1;
+    }
+    yta[lin] = y;
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(int64_t n) {
+        return cudaMalloc(&p, std::max<int64_t>(n, 1) * sizeof(T)) == cudaSuccess ? FB_OK : FB_RUNTIME;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Replaces meshsdf_field_cpu, src/field_engine/mesh_sdf_native_v1/field.cpp:19-226, with the same
+// arguments, outputs and status codes (1 contract, 2 face index outside [0, nv), 3 more than
+// 2^31 - 2 hits), computed on the current GPU; nthreads is accepted and ignored, tstage[0..4] are
+// the stage times in seconds (hits, grouping, winding, EDT, finish).  Host pointers.
+int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt, double ox, double oy, double oz,
+                      double pitch, double jx, double jy, int64_t nx, int64_t ny, int64_t nz, int ytkorr,
+                      int nthreads, uint8_t* solid, float* sd, uint8_t* yta, int64_t* stats, double* tstage) noexcept {
+    (void)nthreads;
+    const int64_t CELLS_MAX = (int64_t)std::numeric_limits<int32_t>::max() - 1;
+    if (!V || !T || !solid || !sd || !yta || !stats || !tstage) return 1;
+    if (nv < 1 || nt < 1 || nt > CELLS_MAX || nv > std::numeric_limits<int64_t>::max() / 3) return 1;
+    if (nx < 1 || ny < 1 || nz < 1 || nx > CELLS_MAX / ny || nx * ny > CELLS_MAX / nz) return 1;
+    if (!(std::isfinite(pitch) && pitch > 0) || !std::isfinite(ox) || !std::isfinite(oy) || !std::isfinite(oz) ||
+        !std::isfinite(jx) || !std::isfinite(jy))
+        return 1;
+    for (int64_t t = 0; t < 3 * nt; ++t)
+        if (T[t] < 0 || T[t] >= nv) return 2;
+    // the EDT's axis contract
+    if (nx > 512 || ny > 512 || nz > 512) return 1;
+    const Grid g{ox, oy, oz, pitch, jx, jy, nx, ny, nz};
+    const int64_t ncol = nx * ny, N = ncol * nz;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return FB_RUNTIME;
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{st};
+    cudaEvent_t ev[6];
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return FB_RUNTIME;
+    struct EventGuard {
+        cudaEvent_t* e;
+        ~EventGuard() {
+            for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
+        }
+    } eguard{ev};
+    DevBuf<double> dV;
+    DevBuf<int64_t> dT;
+    DevBuf<int32_t> tri_count;
+    DevBuf<unsigned long long> misc;  // npairs, zmin key, zmax key, ndiff, nsolid, nh
+    if (dV.alloc(3 * nv) || dT.alloc(3 * nt) || tri_count.alloc(nt + 1) || misc.alloc(8)) return FB_RUNTIME;
+    FB_CUDA(cudaMemcpyAsync(dV.p, V, 3 * nv * sizeof(double), cudaMemcpyHostToDevice, st));
+    FB_CUDA(cudaMemcpyAsync(dT.p, T, 3 * nt * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    const unsigned long long init[8] = {0, ~0ull, 0, 0, 0, 0, 0, 0};
+    FB_CUDA(cudaMemcpyAsync(misc.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    FB_CUDA(cudaEventRecord(ev[0], st));
+    // 1. hits per triangle, scanned to offsets
+    const unsigned tb = (unsigned)((nt + 255) / 256);
+    k_mesh_tri_count<<<tb, 256, 0, st>>>(dV.p, dT.p, nt, g, tri_count.p, misc.p);
+    FB_LAUNCH();
+    DevBuf<int32_t> scan_scratch;
+    const int64_t words_t = scan_scratch_words(nt);
+    if (scan_scratch.alloc(std::max<int64_t>(words_t, scan_scratch_words(ncol + 1)))) return FB_RUNTIME;
+    int32_t* d_total = tri_count.p + nt;
+    if (int rc = scan_exclusive(tri_count.p, nt, d_total, scan_scratch.p, words_t, st)) return rc;
+    unsigned long long nh64 = 0;
+    FB_CUDA(cudaMemcpyAsync(&nh64, misc.p + 5, sizeof(nh64), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    // hit offsets are int32 (the scan above): beyond that the reference refuses too, before any output
+    if (nh64 > (unsigned long long)CELLS_MAX) return 3;
+    const int64_t nh = (int64_t)nh64;
+    (void)d_total;
+    DevBuf<int64_t> hcol;
+    DevBuf<double> hz, cz;
+    DevBuf<int8_t> hs, cs;
+    if (hcol.alloc(nh) || hz.alloc(nh) || hs.alloc(nh) || cz.alloc(nh) || cs.alloc(nh)) return FB_RUNTIME;
+    k_mesh_tri_fill<<<tb, 256, 0, st>>>(dV.p, dT.p, nt, g, tri_count.p, hcol.p, hz.p, hs.p, misc.p + 1);
+    FB_LAUNCH();
+    FB_CUDA(cudaEventRecord(ev[1], st));
+    // 2. hits grouped by column
+    DevBuf<int32_t> start, cursor;
+    if (start.alloc(ncol + 1) || cursor.alloc(ncol + 1)) return FB_RUNTIME;
+    FB_CUDA(cudaMemsetAsync(start.p, 0, (ncol + 1) * sizeof(int32_t), st));
+    const unsigned hb = (unsigned)((nh + 255) / 256);
+    if (nh > 0) {
+        k_mesh_col_count<<<hb, 256, 0, st>>>(hcol.p, nh, start.p);
+        FB_LAUNCH();
+    }
+    // exclusive scan over ncol + 1 entries: start[ncol] becomes nh
+    if (int rc = scan_exclusive(start.p, ncol + 1, cursor.p + ncol, scan_scratch.p, scan_scratch_words(ncol + 1), st))
+        return rc;
+    FB_CUDA(cudaMemcpyAsync(cursor.p, start.p, (ncol + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    if (nh > 0) {
+        k_mesh_col_scatter<<<hb, 256, 0, st>>>(hcol.p, hz.p, hs.p, nh, cursor.p, cz.p, cs.p);
+        FB_LAUNCH();
+    }
+    FB_CUDA(cudaEventRecord(ev[2], st));
+    // 3. winding
+    DevBuf<uint8_t> dsolid, dyta;
+    DevBuf<float> dsd;
+    if (dsolid.alloc(N) || dyta.alloc(N) || dsd.alloc(N)) return FB_RUNTIME;
+    k_mesh_winding<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(start.p, cz.p, cs.p, g, misc.p + 1, dsolid.p,
+                                                                   misc.p + 3);
+    FB_LAUNCH();
+    unsigned long long host_misc[8];
+    FB_CUDA(cudaMemcpyAsync(host_misc, misc.p, sizeof(host_misc), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    FB_CUDA(cudaEventRecord(ev[3], st));
+    const int64_t nsolid = (int64_t)host_misc[4];
+    // 4. paired EDT when both classes are present
+    DevBuf<int32_t> sq;
+    DevBuf<uint8_t> edt_scratch;
+    int empty = -1;
+    if (nsolid == 0) empty = 0;       // no solid voxel: no feature for the distance to the solid
+    else if (nsolid == N) empty = 1;  // no empty voxel
+    if (empty < 0) {
+        const int64_t sb = fb_edt_scratch_bytes((int)nx, (int)ny, (int)nz, 1);
+        if (sb < 0 || sq.alloc(2 * N) || edt_scratch.alloc(sb)) return FB_RUNTIME;
+        if (int rc = fb_edt_pair_device(dsolid.p, (int)nx, (int)ny, (int)nz, pitch, dsd.p, sq.p, edt_scratch.p, sb, st))
+            return rc == FB_INVALID ? 1 : FB_RUNTIME;
+    }
+    FB_CUDA(cudaEventRecord(ev[4], st));
+    // 5. sd and the surface layer
+    k_mesh_finish<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dsolid.p, empty < 0 ? sq.p : nullptr, g, empty,
+                                                                  ytkorr ? 1 : 0, dsd.p, dyta.p);
+    FB_LAUNCH();
+    FB_CUDA(cudaEventRecord(ev[5], st));
+    FB_CUDA(cudaMemcpyAsync(solid, dsolid.p, N, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(sd, dsd.p, N * sizeof(float), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(yta, dyta.p, N, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    stats[0] = (int64_t)host_misc[0];
+    stats[1] = nh;
+    stats[2] = (int64_t)host_misc[3];
+    stats[3] = nsolid;
+    for (int i = 0; i < 5; ++i) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        tstage[i] = ms * 1e-3;
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -149,3 +149,77 @@ def tangent_pairs(seed=4, n_pairs=1000, pitch=1.0 / 512, walls=64):
         h[rng.integers(0, 3)] = 0.25 * pitch
         nodes.append(X.box(h, c))
     return X.union_all(nodes)
+
+
+# ------------------------------------------------------------------------------------ meshes
+# Closed, outward-oriented triangle meshes (float64 vertices, int64 faces) for the mesh -> field stage.
+
+def mesh_sphere(center, radius, n_theta=24, n_phi=48):
+    """UV sphere."""
+    th = np.linspace(0, np.pi, n_theta + 1)[1:-1]
+    ph = np.linspace(0, 2 * np.pi, n_phi, endpoint=False)
+    ring = np.stack([np.outer(np.sin(th), np.cos(ph)), np.outer(np.sin(th), np.sin(ph)),
+                     np.outer(np.cos(th), np.ones_like(ph))], axis=-1).reshape(-1, 3)
+    V = np.vstack([[0, 0, 1], ring, [0, 0, -1]]) * radius + np.asarray(center)
+    top, bot = 0, len(V) - 1
+    idx = lambda i, j: 1 + i * n_phi + (j % n_phi)
+    T = []
+    for j in range(n_phi):
+        T.append((top, idx(0, j), idx(0, j + 1)))
+        T.append((bot, idx(n_theta - 2, j + 1), idx(n_theta - 2, j)))
+    for i in range(n_theta - 2):
+        for j in range(n_phi):
+            a, b, c, d = idx(i, j), idx(i, j + 1), idx(i + 1, j), idx(i + 1, j + 1)
+            T.append((a, c, b))
+            T.append((b, c, d))
+    return V.astype(np.float64), np.asarray(T, np.int64)
+
+
+def mesh_box(lo, hi):
+    """Axis-aligned box, 12 triangles."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    V = np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])])
+    T = np.array([(0, 1, 3), (0, 3, 2), (4, 6, 7), (4, 7, 5), (0, 4, 5), (0, 5, 1),
+                  (2, 3, 7), (2, 7, 6), (0, 2, 6), (0, 6, 4), (1, 5, 7), (1, 7, 3)], np.int64)
+    return V, T
+
+
+def mesh_torus(center, R, r, n_u=48, n_v=24):
+    """Torus around the z axis through `center`."""
+    u = np.linspace(0, 2 * np.pi, n_u, endpoint=False)
+    v = np.linspace(0, 2 * np.pi, n_v, endpoint=False)
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    V = np.stack([(R + r * np.cos(vv)) * np.cos(uu), (R + r * np.cos(vv)) * np.sin(uu), r * np.sin(vv)], -1)
+    V = V.reshape(-1, 3) + np.asarray(center)
+    idx = lambda i, j: (i % n_u) * n_v + (j % n_v)
+    T = []
+    for i in range(n_u):
+        for j in range(n_v):
+            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i, j + 1), idx(i + 1, j + 1)
+            T.append((a, b, d))
+            T.append((a, d, c))
+    return V.astype(np.float64), np.asarray(T, np.int64)
+
+
+def mesh_merge(*meshes):
+    """One mesh of several (face indices offset)."""
+    Vs, Ts, off = [], [], 0
+    for V, T in meshes:
+        Vs.append(V)
+        Ts.append(T + off)
+        off += len(V)
+    return np.vstack(Vs), np.vstack(Ts)
+
+
+def mesh_scene(seed=0, offset=0.0, fine=1):
+    """A sphere, a rotated box and a torus in a ~20 mm region (mm units), moved by `offset`."""
+    rng = np.random.default_rng(seed)
+    s = mesh_sphere(rng.uniform(4, 6, 3), rng.uniform(2.5, 3.5), 24 * fine, 48 * fine)
+    b = mesh_box(rng.uniform(9, 10, 3), rng.uniform(13, 15, 3))
+    th = rng.uniform(0.2, 0.8)
+    Rz = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+    c = b[0].mean(0)
+    b = ((b[0] - c) @ Rz.T + c, b[1])
+    t = mesh_torus(rng.uniform(5, 7, 3) + np.array([0, 8, 0]), rng.uniform(3, 4), rng.uniform(0.8, 1.4), 48 * fine, 24 * fine)
+    V, T = mesh_merge(s, b, t)
+    return V + offset, T

@@ -52,10 +52,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--check-bricks", type=int, default=24, help="precision: bricks checked per level")
-    ap.add_argument("--workload", choices=("plain", "batched", "serve", "precision", "tree"), default="plain",
+    ap.add_argument("--workload", choices=("plain", "batched", "serve", "precision", "tree", "mesh"), default="plain",
                     help="plain: the plain method at scale (default line); batched: 256 recipes, plain vs "
                          "graph-batched; serve: the request loop; precision: float32 vs float64 at mixed pitch; "
-                         "tree: packed adaptive block tree of a dense 512^3 field, built and sampled")
+                         "tree: packed adaptive block tree of a dense 512^3 field, built and sampled; "
+                         "mesh: mesh -> signed distance field stage")
     ap.add_argument("--recipes", type=int, default=256)
     ap.add_argument("--streams", type=int, default=16, help="batched: streams the graph's branches spread over")
     ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
@@ -728,6 +729,60 @@ def run_tree(args, n=512, samples=50_000_000):
     }
 
 
+def run_mesh(args, pitch=0.08):
+    """Mesh -> signed distance field (ray-winding solid, paired exact EDT, surface layer) of a seeded
+    scene of a sphere, a rotated box and a torus (about 55 k triangles) on a grid of pitch 0.08 mm
+    around it, through the C entry point with host buffers (mesh in, solid / sd / surface out, all
+    inside the timed region), against the reference's own meshsdf_field_cpu compiled from its source
+    (OpenMP, every host thread) on the same input."""
+    import torch
+    import field_b200.mesh as M
+    import field_b200.recipes as R
+    torch.cuda.set_device(0)
+    V, T = R.mesh_scene(7, 0.0, fine=4)
+    lo = V.min(0) - 2 * pitch
+    gmin, shape = M.window(V, pitch, lo)
+    origin = lo + gmin * pitch
+    jit = (pitch * M.JITTER_FRAC * M.GOLDEN[0], pitch * M.JITTER_FRAC * M.GOLDEN[1])
+    run = lambda: M.field_grid(V, T, origin, pitch, shape, jitter=jit)
+    for _ in range(max(args.warmup, 3)):
+        run()
+    clocks = ClockSampler(0)
+    clocks.start()
+    walls, stages = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = run()
+        walls.append(time.perf_counter() - t0)
+        stages.append(out[4])
+    clk = clocks.stop()
+    voxels = int(np.prod(shape))
+    wall = statistics.median(walls)
+    dev = np.median(np.array(stages), axis=0)
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        t0 = time.perf_counter()
+        rc, *_ = oracle.ref_mesh_field(V, T, origin, pitch, jit, shape, True, nthreads=0)
+        dt = time.perf_counter() - t0
+        cpu = {"value": voxels / dt / 1e9, "unit": "Gvox/s", "cores": len(os.sched_getaffinity(0)),
+               "kind": "reference", "seconds": dt,
+               "sample": "the reference's meshsdf_field_cpu (oracle/_ref, OpenMP) on the same mesh and grid"}
+    h2d = V.nbytes + T.nbytes
+    d2h = voxels * (1 + 4 + 1)
+    return {
+        "metric": "mesh -> signed distance field: grid voxels/s", "workload": "mesh_field", "value": voxels / wall / 1e9,
+        "unit": "Gvox/s", "higher_is_better": True, "steps": args.steps, "ms_per_call": wall * 1e3,
+        "device_stage_ms": {k: float(v) * 1e3 for k, v in zip(("hits", "grouping", "winding", "edt", "finish"), dev)},
+        "triangles": int(len(T)), "grid": list(shape), "voxels": voxels, "hits": int(out[3][1]),
+        "solid_voxels": int(out[3][3]),
+        "e2e": {"value": voxels / wall / 1e9, "unit": "Gvox/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "api": "meshsdf_field_cpu (host buffers)"},
+        "cpu_baseline": cpu, "clocks": clk, "dtype": "f64 rays, int32 EDT, f32 sd", "data": "synthetic",
+        "config": {"workload": f"mesh_scene_{len(T)}tris_pitch{pitch}", "grid": list(shape)},
+    }
+
+
 def run_precision(args):
     """Precision stress: 1000 near-tangent sphere pairs (gap U[0, 0.5] fine pitches) and 64 walls half
     a fine voxel thick, as a per-block-pitch field mixing pitch 1/128 (level 0) and 1/512 (level 2)
@@ -812,6 +867,9 @@ def main():
         return
     if args.workload == "tree":
         print(json.dumps(run_tree(args)), flush=True)
+        return
+    if args.workload == "mesh":
+        print(json.dumps(run_mesh(args)), flush=True)
         return
     if args.workload == "serve":
         print(json.dumps(run_serve(args, rate=args.rate, seconds=args.seconds)), flush=True)

@@ -247,6 +247,14 @@ int fb_multires_query_device(const double* lo, double h, int32_t B, const int32_
                              const float* d_pool, const double* d_points, int64_t n, double* d_value, double* d_grad,
                              void* stream);
 
+/* Replaces meshsdf_field_cpu, src/field_engine/mesh_sdf_native_v1/field.cpp:19-226 (same arguments and
+ * statuses: 1 contract, 2 face index outside [0, nv), 3 more than 2^31 - 2 ray hits); computed on the
+ * current GPU, host pointers; window axes up to 512 (the EDT's contract); nthreads ignored; tstage[5]
+ * = seconds of the hits, grouping, winding, EDT and finishing stages. */
+int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt, double ox, double oy, double oz,
+                      double pitch, double jx, double jy, int64_t nx, int64_t ny, int64_t nz, int ytkorr,
+                      int nthreads, uint8_t* solid, float* sd, uint8_t* yta, int64_t* stats, double* tstage);
+
 #ifdef __cplusplus
 }
 #endif

@@ -496,3 +496,29 @@ def tree_sample(tree, indices, pitch):
         size[br] = half
         todo = br
     return out
+
+
+# ----------------------------------------------------------------------------------------- mesh -> field
+def ref_mesh_field(V, T, origin, pitch, jitter, shape, surface_correction=True, nthreads=0):
+    """The reference's meshsdf_field_cpu (src/field_engine/mesh_sdf_native_v1/field.cpp:19-226, OpenMP),
+    compiled from its source into oracle/_ref: (status, solid bool, sd float32, surface bool,
+    stats int64[4])."""
+    L = ref_library("mesh_sdf")
+    if L is None:
+        raise RuntimeError("oracle/_ref/libref_mesh_sdf.so is not built")
+    P, I64, D, I = ct.c_void_p, ct.c_int64, ct.c_double, ct.c_int
+    L.meshsdf_field_cpu.argtypes = [P, I64, P, I64, D, D, D, D, D, D, I64, I64, I64, I, I, P, P, P, P, P]
+    L.meshsdf_field_cpu.restype = I
+    Vf = np.ascontiguousarray(V, dtype=np.float64)
+    Ti = np.ascontiguousarray(T, dtype=np.int64)
+    nx, ny, nz = (int(v) for v in shape)
+    solid = np.zeros((nx, ny, nz), np.uint8)
+    sd = np.zeros((nx, ny, nz), np.float32)
+    yta = np.zeros((nx, ny, nz), np.uint8)
+    stats = np.zeros(4, np.int64)
+    ts = np.zeros(5, np.float64)
+    rc = L.meshsdf_field_cpu(Vf.ctypes.data, len(Vf), Ti.ctypes.data, len(Ti), float(origin[0]), float(origin[1]),
+                             float(origin[2]), float(pitch), float(jitter[0]), float(jitter[1]), nx, ny, nz,
+                             int(bool(surface_correction)), int(nthreads), solid.ctypes.data, sd.ctypes.data,
+                             yta.ctypes.data, stats.ctypes.data, ts.ctypes.data)
+    return rc, solid.view(bool), sd, yta.view(bool), stats
