@@ -243,14 +243,24 @@ __global__ void k_mesh_finish(const uint8_t* __restrict__ solid, const int32_t* 
     yta[lin] = y;
 }
 
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFree(p);
+// One device allocation carved into 256-byte aligned parts (a call makes two: one sized before the
+// ray hits are counted, one for the hits), so a call meets cudaMalloc / cudaFree twice, not per array.
+struct Slab {
+    char* base = nullptr;
+    size_t size = 0;
+    ~Slab() {
+        if (base) cudaFree(base);
     }
-    int alloc(int64_t n) {
-        return cudaMalloc(&p, std::max<int64_t>(n, 1) * sizeof(T)) == cudaSuccess ? FB_OK : FB_RUNTIME;
+    template <typename T>
+    size_t reserve(int64_t n) {
+        const size_t at = size;
+        size += (std::max<int64_t>(n, 1) * sizeof(T) + 255) / 256 * 256;
+        return at;
+    }
+    int allocate() { return cudaMalloc(&base, std::max<size_t>(size, 256)) == cudaSuccess ? FB_OK : FB_RUNTIME; }
+    template <typename T>
+    T* at(size_t offset) const {
+        return reinterpret_cast<T*>(base + offset);
     }
 };
 
@@ -297,90 +307,100 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
             for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
         }
     } eguard{ev};
-    DevBuf<double> dV;
-    DevBuf<int64_t> dT;
-    DevBuf<int32_t> tri_count;
-    DevBuf<unsigned long long> misc;  // npairs, zmin key, zmax key, ndiff, nsolid, nh
-    if (dV.alloc(3 * nv) || dT.alloc(3 * nt) || tri_count.alloc(nt + 1) || misc.alloc(8)) return FB_RUNTIME;
-    FB_CUDA(cudaMemcpyAsync(dV.p, V, 3 * nv * sizeof(double), cudaMemcpyHostToDevice, st));
-    FB_CUDA(cudaMemcpyAsync(dT.p, T, 3 * nt * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    const int64_t sb = fb_edt_scratch_bytes((int)nx, (int)ny, (int)nz, 1);
+    if (sb < 0) return 1;
+    const int64_t words_t = scan_scratch_words(nt), words_c = scan_scratch_words(ncol + 1);
+    Slab A;
+    const size_t oV = A.reserve<double>(3 * nv), oT = A.reserve<int64_t>(3 * nt), oCount = A.reserve<int32_t>(nt + 1),
+                 oMisc = A.reserve<unsigned long long>(8), oScan = A.reserve<int32_t>(std::max(words_t, words_c)),
+                 oStart = A.reserve<int32_t>(ncol + 1), oCursor = A.reserve<int32_t>(ncol + 1),
+                 oSolid = A.reserve<uint8_t>(N), oYta = A.reserve<uint8_t>(N), oSd = A.reserve<float>(N),
+                 oSq = A.reserve<int32_t>(2 * N), oEdt = A.reserve<uint8_t>(sb);
+    if (A.allocate()) return FB_RUNTIME;
+    double* const dV = A.at<double>(oV);
+    int64_t* const dT = A.at<int64_t>(oT);
+    int32_t* const tri_count = A.at<int32_t>(oCount);
+    int32_t* const scan_scratch = A.at<int32_t>(oScan);
+    int32_t* const start = A.at<int32_t>(oStart);
+    int32_t* const cursor = A.at<int32_t>(oCursor);
+    int32_t* const sq = A.at<int32_t>(oSq);
+    unsigned long long* const misc = A.at<unsigned long long>(oMisc);  // npairs, zmin key, zmax key, ndiff, nsolid, nh
+    uint8_t* const dsolid = A.at<uint8_t>(oSolid);
+    uint8_t* const dyta = A.at<uint8_t>(oYta);
+    uint8_t* const edt_scratch = A.at<uint8_t>(oEdt);
+    float* const dsd = A.at<float>(oSd);
+    FB_CUDA(cudaMemcpyAsync(dV, V, 3 * nv * sizeof(double), cudaMemcpyHostToDevice, st));
+    FB_CUDA(cudaMemcpyAsync(dT, T, 3 * nt * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     const unsigned long long init[8] = {0, ~0ull, 0, 0, 0, 0, 0, 0};
-    FB_CUDA(cudaMemcpyAsync(misc.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    FB_CUDA(cudaMemcpyAsync(misc, init, sizeof(init), cudaMemcpyHostToDevice, st));
     FB_CUDA(cudaEventRecord(ev[0], st));
     // 1. hits per triangle, scanned to offsets
     const unsigned tb = (unsigned)((nt + 255) / 256);
-    k_mesh_tri_count<<<tb, 256, 0, st>>>(dV.p, dT.p, nt, g, tri_count.p, misc.p);
+    k_mesh_tri_count<<<tb, 256, 0, st>>>(dV, dT, nt, g, tri_count, misc);
     FB_LAUNCH();
-    DevBuf<int32_t> scan_scratch;
-    const int64_t words_t = scan_scratch_words(nt);
-    if (scan_scratch.alloc(std::max<int64_t>(words_t, scan_scratch_words(ncol + 1)))) return FB_RUNTIME;
-    int32_t* d_total = tri_count.p + nt;
-    if (int rc = scan_exclusive(tri_count.p, nt, d_total, scan_scratch.p, words_t, st)) return rc;
+    int32_t* d_total = tri_count + nt;
+    if (int rc = scan_exclusive(tri_count, nt, d_total, scan_scratch, words_t, st)) return rc;
     unsigned long long nh64 = 0;
-    FB_CUDA(cudaMemcpyAsync(&nh64, misc.p + 5, sizeof(nh64), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(&nh64, misc + 5, sizeof(nh64), cudaMemcpyDeviceToHost, st));
     FB_CUDA(cudaStreamSynchronize(st));
     // hit offsets are int32 (the scan above): beyond that the reference refuses too, before any output
     if (nh64 > (unsigned long long)CELLS_MAX) return 3;
     const int64_t nh = (int64_t)nh64;
     (void)d_total;
-    DevBuf<int64_t> hcol;
-    DevBuf<double> hz, cz;
-    DevBuf<int8_t> hs, cs;
-    if (hcol.alloc(nh) || hz.alloc(nh) || hs.alloc(nh) || cz.alloc(nh) || cs.alloc(nh)) return FB_RUNTIME;
-    k_mesh_tri_fill<<<tb, 256, 0, st>>>(dV.p, dT.p, nt, g, tri_count.p, hcol.p, hz.p, hs.p, misc.p + 1);
+    Slab B;
+    const size_t oHcol = B.reserve<int64_t>(nh), oHz = B.reserve<double>(nh), oCz = B.reserve<double>(nh),
+                 oHs = B.reserve<int8_t>(nh), oCs = B.reserve<int8_t>(nh);
+    if (B.allocate()) return FB_RUNTIME;
+    int64_t* const hcol = B.at<int64_t>(oHcol);
+    double* const hz = B.at<double>(oHz);
+    double* const cz = B.at<double>(oCz);
+    int8_t* const hs = B.at<int8_t>(oHs);
+    int8_t* const cs = B.at<int8_t>(oCs);
+    k_mesh_tri_fill<<<tb, 256, 0, st>>>(dV, dT, nt, g, tri_count, hcol, hz, hs, misc + 1);
     FB_LAUNCH();
     FB_CUDA(cudaEventRecord(ev[1], st));
     // 2. hits grouped by column
-    DevBuf<int32_t> start, cursor;
-    if (start.alloc(ncol + 1) || cursor.alloc(ncol + 1)) return FB_RUNTIME;
-    FB_CUDA(cudaMemsetAsync(start.p, 0, (ncol + 1) * sizeof(int32_t), st));
+    FB_CUDA(cudaMemsetAsync(start, 0, (ncol + 1) * sizeof(int32_t), st));
     const unsigned hb = (unsigned)((nh + 255) / 256);
     if (nh > 0) {
-        k_mesh_col_count<<<hb, 256, 0, st>>>(hcol.p, nh, start.p);
+        k_mesh_col_count<<<hb, 256, 0, st>>>(hcol, nh, start);
         FB_LAUNCH();
     }
     // exclusive scan over ncol + 1 entries: start[ncol] becomes nh
-    if (int rc = scan_exclusive(start.p, ncol + 1, cursor.p + ncol, scan_scratch.p, scan_scratch_words(ncol + 1), st))
+    if (int rc = scan_exclusive(start, ncol + 1, cursor + ncol, scan_scratch, words_c, st))
         return rc;
-    FB_CUDA(cudaMemcpyAsync(cursor.p, start.p, (ncol + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    FB_CUDA(cudaMemcpyAsync(cursor, start, (ncol + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
     if (nh > 0) {
-        k_mesh_col_scatter<<<hb, 256, 0, st>>>(hcol.p, hz.p, hs.p, nh, cursor.p, cz.p, cs.p);
+        k_mesh_col_scatter<<<hb, 256, 0, st>>>(hcol, hz, hs, nh, cursor, cz, cs);
         FB_LAUNCH();
     }
     FB_CUDA(cudaEventRecord(ev[2], st));
     // 3. winding
-    DevBuf<uint8_t> dsolid, dyta;
-    DevBuf<float> dsd;
-    if (dsolid.alloc(N) || dyta.alloc(N) || dsd.alloc(N)) return FB_RUNTIME;
-    k_mesh_winding<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(start.p, cz.p, cs.p, g, misc.p + 1, dsolid.p,
-                                                                   misc.p + 3);
+    k_mesh_winding<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(start, cz, cs, g, misc + 1, dsolid,
+                                                                   misc + 3);
     FB_LAUNCH();
     unsigned long long host_misc[8];
-    FB_CUDA(cudaMemcpyAsync(host_misc, misc.p, sizeof(host_misc), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(host_misc, misc, sizeof(host_misc), cudaMemcpyDeviceToHost, st));
     FB_CUDA(cudaStreamSynchronize(st));
     FB_CUDA(cudaEventRecord(ev[3], st));
     const int64_t nsolid = (int64_t)host_misc[4];
     // 4. paired EDT when both classes are present
-    DevBuf<int32_t> sq;
-    DevBuf<uint8_t> edt_scratch;
     int empty = -1;
     if (nsolid == 0) empty = 0;       // no solid voxel: no feature for the distance to the solid
     else if (nsolid == N) empty = 1;  // no empty voxel
     if (empty < 0) {
-        const int64_t sb = fb_edt_scratch_bytes((int)nx, (int)ny, (int)nz, 1);
-        if (sb < 0 || sq.alloc(2 * N) || edt_scratch.alloc(sb)) return FB_RUNTIME;
-        if (int rc = fb_edt_pair_device(dsolid.p, (int)nx, (int)ny, (int)nz, pitch, dsd.p, sq.p, edt_scratch.p, sb, st))
+        if (int rc = fb_edt_pair_device(dsolid, (int)nx, (int)ny, (int)nz, pitch, dsd, sq, edt_scratch, sb, st))
             return rc == FB_INVALID ? 1 : FB_RUNTIME;
     }
     FB_CUDA(cudaEventRecord(ev[4], st));
     // 5. sd and the surface layer
-    k_mesh_finish<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dsolid.p, empty < 0 ? sq.p : nullptr, g, empty,
-                                                                  ytkorr ? 1 : 0, dsd.p, dyta.p);
+    k_mesh_finish<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dsolid, empty < 0 ? sq : nullptr, g, empty,
+                                                                  ytkorr ? 1 : 0, dsd, dyta);
     FB_LAUNCH();
     FB_CUDA(cudaEventRecord(ev[5], st));
-    FB_CUDA(cudaMemcpyAsync(solid, dsolid.p, N, cudaMemcpyDeviceToHost, st));
-    FB_CUDA(cudaMemcpyAsync(sd, dsd.p, N * sizeof(float), cudaMemcpyDeviceToHost, st));
-    FB_CUDA(cudaMemcpyAsync(yta, dyta.p, N, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(solid, dsolid, N, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(sd, dsd, N * sizeof(float), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaMemcpyAsync(yta, dyta, N, cudaMemcpyDeviceToHost, st));
     FB_CUDA(cudaStreamSynchronize(st));
     stats[0] = (int64_t)host_misc[0];
     stats[1] = nh;
