@@ -2,9 +2,9 @@
 // paired exact EDT (src/field_engine/mesh_sdf_native_v1/field.cpp:19-226, the native form of
 // faltkarna_v1_mesh_to_sdf's raypar_vindning path).
 //
-//   1. k_mesh_tri_count / k_mesh_tri_fill : for every triangle, the vertical rays of the (x, y)
-//      columns inside its bounding box that it crosses, each hit's z and the triangle's xy
-//      orientation; count, scan, fill.  Float64 with the reference's operation order and no
+//   1. k_mesh_tri_count / k_mesh_tri_fill : for every triangle (a warp each, lanes over the
+//      columns), the vertical rays of the (x, y) columns inside its bounding box that it crosses,
+//      each hit's z and the triangle's xy orientation; count, scan, fill.  Float64 with the reference's operation order and no
 //      contraction (every product and sum an explicit _rn operation), so each hit is the same bits.
 //   2. k_mesh_col_count / scan / k_mesh_col_scatter : hits grouped by column (the winding sum does
 //      not depend on their order within a column); the global z range by order-preserving atomics.
@@ -97,23 +97,31 @@ __device__ __forceinline__ bool column_hit(const Tri& r, const Grid& g, int64_t 
     return true;
 }
 
-// count[t] = hits of triangle t; misc[0] += its column pairs, misc[5] += its hits (64-bit totals).
+// A warp per triangle: lanes take its bounding-box columns 32 at a time (large triangles would
+// otherwise run thousands of column tests in one thread).  count[t] = hits of triangle t;
+// misc[0] += its column pairs, misc[5] += its hits (64-bit totals).
 __global__ void k_mesh_tri_count(const double* __restrict__ V, const int64_t* __restrict__ T, int64_t nt, Grid g,
                                  int32_t* __restrict__ count, unsigned long long* __restrict__ misc) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= nt) return;
+    const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= nt) return;  // uniform across the warp
     Tri r;
-    int32_t c = 0;
-    if (setup_tri(V, T, t, g, r)) {
-        atomicAdd(&misc[0], (unsigned long long)((r.i1 - r.i0 + 1) * (r.j1 - r.j0 + 1)));
-        for (int64_t ii = r.i0; ii <= r.i1; ++ii)
-            for (int64_t jj = r.j0; jj <= r.j1; ++jj) {
-                double z;
-                c += column_hit(r, g, ii, jj, z);
-            }
+    if (!setup_tri(V, T, t, g, r)) {  // uniform: every lane computes the same setup
+        if (lane == 0) count[t] = 0;
+        return;
+    }
+    const int64_t w = r.j1 - r.j0 + 1, ncols = (r.i1 - r.i0 + 1) * w;
+    int c = 0;
+    for (int64_t q = lane; q < ncols; q += 32) {
+        double z;
+        c += column_hit(r, g, r.i0 + q / w, r.j0 + q % w, z);
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) {
+        count[t] = c;
+        atomicAdd(&misc[0], (unsigned long long)ncols);
         if (c) atomicAdd(&misc[5], (unsigned long long)c);
     }
-    count[t] = c;
 }
 
 // Order-preserving map of a float64 onto uint64 (for atomic min / max).
@@ -125,27 +133,40 @@ __device__ __forceinline__ double from_key(unsigned long long k) {
     return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
 }
 
+// A warp per triangle, as k_mesh_tri_count; the hits of one 32-column step are placed by a ballot
+// prefix (their order within the triangle's range does not matter: they are regrouped by column).
 __global__ void k_mesh_tri_fill(const double* __restrict__ V, const int64_t* __restrict__ T, int64_t nt, Grid g,
                                 const int32_t* __restrict__ offset, int64_t* __restrict__ hcol,
                                 double* __restrict__ hz, int8_t* __restrict__ hs, unsigned long long* __restrict__ zkey) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= nt) return;
+    const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= nt) return;  // uniform across the warp
     Tri r;
-    if (!setup_tri(V, T, t, g, r)) return;
+    if (!setup_tri(V, T, t, g, r)) return;  // uniform
+    const int64_t w = r.j1 - r.j0 + 1, ncols = (r.i1 - r.i0 + 1) * w;
     int64_t at = offset[t];
     double lo = INFINITY, hi = -INFINITY;
-    for (int64_t ii = r.i0; ii <= r.i1; ++ii)
-        for (int64_t jj = r.j0; jj <= r.j1; ++jj) {
-            double z;
-            if (!column_hit(r, g, ii, jj, z)) continue;
-            hcol[at] = ii * g.ny + jj;
-            hz[at] = z;
-            hs[at] = r.tk;
-            ++at;
+    for (int64_t q0 = 0; q0 < ncols; q0 += 32) {
+        const int64_t q = q0 + lane;
+        double z = 0.0;
+        const int64_t ii = r.i0 + q / w, jj = r.j0 + q % w;
+        const bool hit = q < ncols && column_hit(r, g, ii, jj, z);
+        const unsigned mask = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const int64_t k = at + __popc(mask & ((1u << lane) - 1u));
+            hcol[k] = ii * g.ny + jj;
+            hz[k] = z;
+            hs[k] = r.tk;
             lo = fmin(lo, z);
             hi = fmax(hi, z);
         }
-    if (lo <= hi) {
+        at += __popc(mask);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0 && lo <= hi) {
         atomicMin(&zkey[0], order_key(lo));
         atomicMax(&zkey[1], order_key(hi));
     }
@@ -335,7 +356,7 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
     FB_CUDA(cudaMemcpyAsync(misc, init, sizeof(init), cudaMemcpyHostToDevice, st));
     FB_CUDA(cudaEventRecord(ev[0], st));
     // 1. hits per triangle, scanned to offsets
-    const unsigned tb = (unsigned)((nt + 255) / 256);
+    const unsigned tb = (unsigned)((nt + 7) / 8);  // a warp per triangle, 8 per block
     k_mesh_tri_count<<<tb, 256, 0, st>>>(dV, dT, nt, g, tri_count, misc);
     FB_LAUNCH();
     int32_t* d_total = tri_count + nt;
