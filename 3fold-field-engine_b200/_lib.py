@@ -55,7 +55,9 @@ SIGNATURES = {
     "fb_tree_values_device": (I, [P, I64, I64, I64, P, P, P, I64, P, P]),
     "fb_tree_pack_scratch_bytes": (I64, [I64]),
     "fb_tree_pack_device": (I, [P, I64, P, P, P, P, I64, P]),
-    "fb_tree_sample_device": (I, [P, I64, P, P, P, I64, I64, I64, I64, I64, I64, I64, I64, D, P, I64, P, P, P]),
+    "fb_tree_rank_words_scratch_bytes": (I64, [I64]),
+    "fb_tree_rank_words_device": (I, [P, I64, P, P, P, I64, P]),
+    "fb_tree_sample_device": (I, [P, I64, P, P, P, P, P, I64, I64, I64, I64, I64, I64, I64, I64, D, P, I64, P, P, P]),
     "fb_field_occupancy_device": (I, [P, P, P, P, I64, I64, I64, I64, I, P, P, P]),
     "fb_field_leaf_work_device": (I, [P, P, I, P, I, I, P, P, P, P, I64, P, I64, P, P]),
     "fb_fp32_peak_launch": (I64, [P, I, I, P]),

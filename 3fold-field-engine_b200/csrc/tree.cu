@@ -130,11 +130,32 @@ __device__ __forceinline__ int64_t rank_before(const uint32_t* __restrict__ word
     return r;
 }
 
+// counts[j] of code 2 / code 3 in word j (16 nodes), for the per-word rank table of the sampler.
+__global__ void k_tree_word_counts(const uint32_t* __restrict__ words, int64_t nwords, int32_t* __restrict__ branch,
+                                   int32_t* __restrict__ value) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nwords) return;
+    const uint32_t w = words[j];
+    branch[j] = __popc(code_hits(w, 2));
+    value[j] = __popc(code_hits(w, 3));
+}
+
+// Nodes of `code` before `node` from the per-word table (its exclusive prefix over words).
+__device__ __forceinline__ int64_t rank_word(const uint32_t* __restrict__ words, const int32_t* __restrict__ table,
+                                             int64_t node, int code) {
+    const int64_t w = node >> 4;
+    const int rem = (int)(node & 15);
+    int64_t r = table[w];
+    if (rem) r += __popc(code_hits(words[w], code) & ((1u << (2 * rem)) - 1u));
+    return r;
+}
+
 // Status bits of a sample launch.
 enum { kBadIndex = 1, kBadDepth = 2, kBadNode = 4 };
 
 __global__ void k_tree_sample(const uint32_t* __restrict__ words, int64_t node_count, const int32_t* __restrict__ bprefix,
-                              const int32_t* __restrict__ vprefix, const float* __restrict__ values, int64_t n_values,
+                              const int32_t* __restrict__ vprefix, const int32_t* __restrict__ bword,
+                              const int32_t* __restrict__ vword, const float* __restrict__ values, int64_t n_values,
                               int64_t root_count, int64_t r1, int64_t r2, int64_t nx, int64_t ny, int64_t nz,
                               double pitch, const int64_t* __restrict__ ijk, int64_t n, float* __restrict__ out,
                               int* __restrict__ status) {
@@ -159,7 +180,7 @@ __global__ void k_tree_sample(const uint32_t* __restrict__ words, int64_t node_c
             return;
         }
         if (code == 3) {
-            const int64_t r = rank_before(words, vprefix, node, 3);
+            const int64_t r = vword ? rank_word(words, vword, node, 3) : rank_before(words, vprefix, node, 3);
             if (r < 0 || r >= n_values) break;
             out[q] = values[r];
             return;
@@ -171,7 +192,7 @@ __global__ void k_tree_sample(const uint32_t* __restrict__ words, int64_t node_c
             return;
         }
         const int child = (int)(4 * ((i / half) & 1) + 2 * ((j / half) & 1) + ((k / half) & 1));
-        node = root_count + 8 * rank_before(words, bprefix, node, 2) + child;
+        node = root_count + 8 * (bword ? rank_word(words, bword, node, 2) : rank_before(words, bprefix, node, 2)) + child;
         size = half;
     }
     out[q] = __int_as_float(0x7fc00000);
@@ -278,12 +299,43 @@ int fb_tree_pack_device(const uint8_t* d_codes, int64_t node_count, uint8_t* d_p
     return FB_OK;
 }
 
+// Scratch bytes of fb_tree_rank_words_device for node_count nodes.
+int64_t fb_tree_rank_words_scratch_bytes(int64_t node_count) noexcept {
+    if (node_count < 0) return -1;
+    return (scan_scratch_words((node_count + 15) / 16 + 1) + 1) * 4;  // the scans' scratch, then their totals word
+}
+
+// The sampler's per-word rank tables (not part of the stored format): d_branch_words /
+// d_value_words[w] = nodes of code 2 / 3 before word w (16 nodes per word), ceil(node_count / 16)
+// + 1 entries each.
+int fb_tree_rank_words_device(const uint8_t* d_packed, int64_t node_count, int32_t* d_branch_words,
+                              int32_t* d_value_words, void* d_scratch, int64_t scratch_len, void* stream) noexcept {
+    if (!d_packed || !d_branch_words || !d_value_words || !d_scratch || node_count < 1 ||
+        node_count >= (int64_t(1) << 31) || (reinterpret_cast<uintptr_t>(d_packed) & 3))
+        return FB_INVALID;
+    if (scratch_len < fb_tree_rank_words_scratch_bytes(node_count)) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t nwords = (node_count + 15) / 16;
+    k_tree_word_counts<<<(unsigned)((nwords + 255) / 256), 256, 0, st>>>(reinterpret_cast<const uint32_t*>(d_packed),
+                                                                        nwords, d_branch_words, d_value_words);
+    FB_LAUNCH();
+    FB_CUDA(cudaMemsetAsync(d_branch_words + nwords, 0, sizeof(int32_t), st));
+    FB_CUDA(cudaMemsetAsync(d_value_words + nwords, 0, sizeof(int32_t), st));
+    int32_t* scratch = static_cast<int32_t*>(d_scratch);
+    const int64_t words = scratch_len / 4;
+    if (int rc = scan_exclusive(d_branch_words, nwords + 1, scratch + words - 1, scratch, words - 1, st)) return rc;
+    if (int rc = scan_exclusive(d_value_words, nwords + 1, scratch + words - 1, scratch, words - 1, st)) return rc;
+    return FB_OK;
+}
+
 // Values at grid indices ijk[n][3] (int64) of a packed tree; out[n] float32.  d_packed must be
 // 4-byte aligned with its bytes up to a multiple of 4 readable (fb_tree_pack_device writes them).
-// *d_status (device, OR-ed): 1 an index outside the grid, 2 a branch below side 1, 4 a node or
-// value rank outside the arrays; those outputs are NaN.
+// d_branch_words / d_value_words: the per-word rank tables of fb_tree_rank_words_device, or NULL
+// to rank from the 64-byte checkpoints alone.  *d_status (device, OR-ed): 1 an index outside the
+// grid, 2 a branch below side 1, 4 a node or value rank outside the arrays; those outputs are NaN.
 int fb_tree_sample_device(const uint8_t* d_packed, int64_t node_count, const int32_t* d_branch_prefix,
-                          const int32_t* d_value_prefix, const float* d_values, int64_t n_values, int64_t root_count,
+                          const int32_t* d_value_prefix, const int32_t* d_branch_words, const int32_t* d_value_words,
+                          const float* d_values, int64_t n_values, int64_t root_count,
                           int64_t r0, int64_t r1, int64_t r2, int64_t nx, int64_t ny, int64_t nz, double pitch,
                           const int64_t* d_ijk, int64_t n, float* d_out, int32_t* d_status, void* stream) noexcept {
     if (!d_packed || !d_branch_prefix || !d_value_prefix || !d_ijk || !d_out || !d_status || n < 0 || node_count < 1 ||
@@ -293,8 +345,10 @@ int fb_tree_sample_device(const uint8_t* d_packed, int64_t node_count, const int
     if (n_values > 0 && !d_values) return FB_INVALID;
     if (n == 0) return FB_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if ((d_branch_words == nullptr) != (d_value_words == nullptr)) return FB_INVALID;
     k_tree_sample<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(reinterpret_cast<const uint32_t*>(d_packed), node_count,
-                                                               d_branch_prefix, d_value_prefix, d_values, n_values,
+                                                               d_branch_prefix, d_value_prefix, d_branch_words,
+                                                               d_value_words, d_values, n_values,
                                                                root_count, r1, r2, nx, ny, nz, pitch, d_ijk, n, d_out,
                                                                d_status);
     FB_LAUNCH();

@@ -79,7 +79,23 @@ class AdaptiveBlocks:
         tree._dev = dict(packed=t["packed"], branch=t["branch"], value=t["value"], n_values=n_values,
                          values=t["values"] if n_values else torch.zeros(1, dtype=torch.float32, device=dev),
                          status=torch.zeros(1, dtype=torch.int32, device=dev))
+        tree._rank_words()
         return tree
+
+    def _rank_words(self):
+        """The sampler's per-word rank tables (nodes of code 2 / 3 before each 16-node word): a rank
+        is then one table read and one popcount instead of a walk from the 64-byte checkpoint."""
+        import torch
+        d = self._dev
+        nwords = (self.node_count + 15) // 16
+        dev = d["packed"].device
+        d["bword"] = torch.empty(nwords + 1, dtype=torch.int32, device=dev)
+        d["vword"] = torch.empty(nwords + 1, dtype=torch.int32, device=dev)
+        lib = _lib.lib()
+        scratch = torch.empty(int(lib.fb_tree_rank_words_scratch_bytes(self.node_count)), dtype=torch.uint8, device=dev)
+        _check(lib.fb_tree_rank_words_device(d["packed"].data_ptr(), self.node_count, d["bword"].data_ptr(),
+                                             d["vword"].data_ptr(), scratch.data_ptr(), scratch.numel(),
+                                             _lib.stream_handle()), "tree rank words")
 
     def _device(self):
         import torch
@@ -95,6 +111,7 @@ class AdaptiveBlocks:
                              values=torch.from_numpy(np.ascontiguousarray(self.values, np.float32)).to(dev)
                              if n_values else torch.zeros(1, dtype=torch.float32, device=dev),
                              status=torch.zeros(1, dtype=torch.int32, device=dev))
+            self._rank_words()
         return self._dev
 
     def sample_device(self, ijk, *, stream=None):
@@ -106,6 +123,7 @@ class AdaptiveBlocks:
         out = torch.empty(ijk.shape[0], dtype=torch.float32, device=ijk.device)
         _check(_lib.lib().fb_tree_sample_device(
             d["packed"].data_ptr(), self.node_count, d["branch"].data_ptr(), d["value"].data_ptr(),
+            d["bword"].data_ptr(), d["vword"].data_ptr(),
             d["values"].data_ptr() if d["n_values"] else None, d["n_values"], self.root_count,
             *self.root_shape, *self.shape, float(self.pitch), ijk.data_ptr(), ijk.shape[0], out.data_ptr(),
             d["status"].data_ptr(), _lib.stream_handle(stream)), "tree sample")

@@ -169,8 +169,11 @@ int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* 
  * 8 * rank + child.  fb_tree_values_device: dense samples of the side-1 value leaves by rank.
  * fb_tree_pack_device: 2-bit codes four per byte (d_packed 4-byte aligned, sized to a multiple of
  * 4 bytes) and the checkpoints every 64 bytes (floor(bytes / 64) + 1 entries each).
- * fb_tree_sample_device: values at int64 grid indices [n][3]; *d_status OR-ed with 1 (index outside
- * the grid), 2 (branch below side 1), 4 (rank outside the arrays), those outputs NaN. */
+ * fb_tree_rank_words_device: the sampler's per-word rank tables (nodes of code 2 / 3 before each
+ * 16-node word; not part of the stored format).  fb_tree_sample_device: values at int64 grid
+ * indices [n][3], ranking from those tables when given (else from the checkpoints); *d_status OR-ed
+ * with 1 (index outside the grid), 2 (branch below side 1), 4 (rank outside the arrays), those
+ * outputs NaN. */
 int64_t fb_tree_scan_bytes(int64_t n);
 int fb_tree_codes_device(const float* d_dense, int64_t nx, int64_t ny, int64_t nz, int32_t side, float margin,
                          const int32_t* d_coords, int64_t rx, int64_t ry, int64_t rz, int64_t n, uint8_t* d_codes,
@@ -182,8 +185,12 @@ int fb_tree_values_device(const float* d_dense, int64_t nx, int64_t ny, int64_t 
 int64_t fb_tree_pack_scratch_bytes(int64_t node_count);
 int fb_tree_pack_device(const uint8_t* d_codes, int64_t node_count, uint8_t* d_packed, int32_t* d_branch_prefix,
                         int32_t* d_value_prefix, void* d_scratch, int64_t scratch_len, void* stream);
+int64_t fb_tree_rank_words_scratch_bytes(int64_t node_count);
+int fb_tree_rank_words_device(const uint8_t* d_packed, int64_t node_count, int32_t* d_branch_words,
+                              int32_t* d_value_words, void* d_scratch, int64_t scratch_len, void* stream);
 int fb_tree_sample_device(const uint8_t* d_packed, int64_t node_count, const int32_t* d_branch_prefix,
-                          const int32_t* d_value_prefix, const float* d_values, int64_t n_values, int64_t root_count,
+                          const int32_t* d_value_prefix, const int32_t* d_branch_words, const int32_t* d_value_words,
+                          const float* d_values, int64_t n_values, int64_t root_count,
                           int64_t r0, int64_t r1, int64_t r2, int64_t nx, int64_t ny, int64_t nz, double pitch,
                           const int64_t* d_ijk, int64_t n, float* d_out, int32_t* d_status, void* stream);
 

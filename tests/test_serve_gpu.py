@@ -147,3 +147,17 @@ def test_a_full_arena_evicts_idle_fields_instead_of_leaving_it():
                 assert base <= t.data_ptr() and t.data_ptr() + t.numel() * t.element_size() <= end
         v, g = srv.submit("query", field=ids[-1], points=np.full((8, 3), 0.5, np.float32)).result(timeout=60)
         assert v.shape == (8,) and np.isfinite(v).all()
+
+
+@pytest.mark.parametrize("n", [0, 1, 4097, 1_000_003])
+def test_int32_sum_kernel_equals_numpy(n):
+    """fb_sum_i32_device, the served EDT request's summary: the exact int64 sum of int32 values
+    (negative ones included), its output word zeroed by the call itself."""
+    import torch
+    import field_b200._lib as L
+    rng = np.random.default_rng(n)
+    a = rng.integers(-(2 ** 31), 2 ** 31 - 1, size=n, dtype=np.int64).astype(np.int32)
+    d = torch.from_numpy(a).cuda() if n else torch.empty(0, dtype=torch.int32, device="cuda")
+    out = torch.full((1,), 12345, dtype=torch.int64, device="cuda")  # stale content: the call clears it
+    L.check(L.lib().fb_sum_i32_device(d.data_ptr() if n else None, n, out.data_ptr(), L.stream_handle()), "sum")
+    assert int(out.item()) == int(a.astype(np.int64).sum())
