@@ -24,7 +24,6 @@
 #include "scan.cuh"
 #include <cmath>
 #include <limits>
-#include <vector>
 
 extern "C" int fb_edt_pair_device(const uint8_t* d_mask, int nx, int ny, int nz, double pitch, float* d_signed,
                                   int32_t* d_squared, void* d_scratch, int64_t scratch_len, void* stream) noexcept;
@@ -359,15 +358,15 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
     const unsigned tb = (unsigned)((nt + 7) / 8);  // a warp per triangle, 8 per block
     k_mesh_tri_count<<<tb, 256, 0, st>>>(dV, dT, nt, g, tri_count, misc);
     FB_LAUNCH();
-    int32_t* d_total = tri_count + nt;
-    if (int rc = scan_exclusive(tri_count, nt, d_total, scan_scratch, words_t, st)) return rc;
+    // offsets of each triangle's hits; the int32 total lands in the spare last word (the 64-bit
+    // total in misc[5] is the one checked)
+    if (int rc = scan_exclusive(tri_count, nt, tri_count + nt, scan_scratch, words_t, st)) return rc;
     unsigned long long nh64 = 0;
     FB_CUDA(cudaMemcpyAsync(&nh64, misc + 5, sizeof(nh64), cudaMemcpyDeviceToHost, st));
     FB_CUDA(cudaStreamSynchronize(st));
     // hit offsets are int32 (the scan above): beyond that the reference refuses too, before any output
     if (nh64 > (unsigned long long)CELLS_MAX) return 3;
     const int64_t nh = (int64_t)nh64;
-    (void)d_total;
     Slab B;
     const size_t oHcol = B.reserve<int64_t>(nh), oHz = B.reserve<double>(nh), oCz = B.reserve<double>(nh),
                  oHs = B.reserve<int8_t>(nh), oCs = B.reserve<int8_t>(nh);
