@@ -98,3 +98,19 @@ def test_pinned_pool_recycles_a_block_when_its_array_is_dropped():
     assert len(pool.free[S.PinnedPool.MIN * 64]) == 2
     _, tiny = pool.take(10)  # 64 classes up is beyond the span: the 2*MIN block, not a reserved one
     assert tiny[0] == 2 * S.PinnedPool.MIN and len(pool.free[S.PinnedPool.MIN * 64]) == 2
+
+
+def test_mesh_window_rule():
+    """field_b200.mesh.window: floor/ceil of the vertex range in pitches from `lo`, widened by the
+    margin (and one more voxel above), clamped to a global grid when one is given, never negative
+    in extent (faltkarna_v1_mesh_to_sdf.py:153-166)."""
+    import field_b200.mesh as M
+    V = np.array([[0.25, 1.0, -0.5], [2.0, 1.75, 0.5]])
+    gmin, shape = M.window(V, 0.5, np.zeros(3), margin_vox_pad=2)
+    # x: floor(0.5) - 2 = -2 .. ceil(4) + 3 = 7; y: 2 - 2 = 0 .. 4 + 3 = 7; z: -1 - 2 = -3 .. 1 + 3 = 4
+    assert list(gmin) == [-2, 0, -3] and shape == (9, 7, 7)
+    gmin, shape = M.window(V, 0.5, np.zeros(3), global_shape=(5, 100, 2), margin_vox_pad=2)
+    assert list(gmin) == [0, 0, 0] and shape == (5, 7, 2)
+    far = V + 100.0  # entirely above a small global grid: empty extent, not negative
+    gmin, shape = M.window(far, 0.5, np.zeros(3), global_shape=(4, 4, 4))
+    assert shape == (0, 0, 0)
