@@ -41,6 +41,16 @@ SIGNATURES = {
     "fb_field_leaf_device": (I, [P, P, I, P, I, I, P, P, P, P, I64, P, I64, P]),
     "fb_field_build_device": (I, [P, P, I, P, I, I, P, P, P, P, P, I64, P, I64, P]),
     "fb_field_compact_error": (I, [P, I, I, P, P]),
+    "fb_compact_timeout_probe": (I, [P, I64, P, P, P, I64, I64, P]),
+    # batched builds
+    "fb_batch_create": (P, [P, I, P]),
+    "fb_batch_build_device": (I, [P, P, I64, I, P]),
+    "fb_batch_build_timed_device": (I, [P, P, I64, I, P, P, P]),
+    "fb_batch_outputs": (I, [P, P, P]),
+    "fb_batch_occupancy_device": (I, [P, P, P]),
+    "fb_batch_launches": (I, [P]),
+    "fb_batch_status": (I, [P, P]),
+    "fb_batch_destroy": (None, [P]),
     "fb_dense_scratch_bytes": (I64, [I64, I64, I64, I]),
     "fb_dense_classify_device": (I, [P, I64, I64, I64, I, F, P, P, P, P, P, I64, P, I64, P]),
     "fb_field_reconstruct_device": (I, [P, P, I64, P, I64, I64, I64, I, F, P, P, P]),

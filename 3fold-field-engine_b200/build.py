@@ -55,12 +55,23 @@ class DeviceField:
         self.n_active = n_active
 
     def to_host(self) -> SparseField:
+        """The field as host arrays.  They land in page-locked memory from torch's caching host
+        allocator (copies at full link speed; blocks return to the cache when the arrays are
+        dropped, so repeated calls allocate no new pinned memory), one synchronisation for all."""
+        import torch
         n = int(self.n_active)
         b = self.meta.block
-        kind = self.kind.cpu().numpy()
-        return SparseField(meta=self.meta, kind=kind, active_ids=self.active[:n].cpu().numpy().astype(np.int32),
-                           tiles=self.tiles[:n].reshape(n, b, b, b).cpu().numpy(),
-                           corner_min_abs=self.corner_min_abs.cpu().numpy(), stats=stats_of(self.meta, kind, n))
+
+        def pinned(t):
+            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h.copy_(t, non_blocking=True)
+            return h
+        parts = [pinned(self.kind), pinned(self.active[:n]), pinned(self.tiles[:n].reshape(n, b, b, b)),
+                 pinned(self.corner_min_abs)]
+        torch.cuda.current_stream(self.kind.device).synchronize()
+        kind, active, tiles, cma = (p.numpy() for p in parts)
+        return SparseField(meta=self.meta, kind=kind, active_ids=active, tiles=tiles, corner_min_abs=cma,
+                           stats=stats_of(self.meta, kind, n))
 
 
 def device_tables(comp: Compiled, device, stream, *, alloc=None, pinned=None):
@@ -130,10 +141,12 @@ class FieldBuilder:
     leaf launches); ``enqueue(capacity_tiles)`` runs the whole build stream-ordered into a fixed
     tile buffer (CUDA-graph capturable).  ``alloc`` (optional) supplies the one device allocation
     the builder makes (outputs + scratch), e.g. from a server's memory pool, and -- with
-    ``pinned`` -- the recipe's tables when they are first uploaded (see device_tables)."""
+    ``pinned`` -- the recipe's tables when they are first uploaded (see device_tables).  ``tables``
+    (a pair of uint8 device tensors: primitive records, chain or program records) uses tables the
+    caller placed on the device instead, e.g. a batch's table arena."""
 
     def __init__(self, recipe, meta: GridMeta, *, device="cuda", guard=None, library=None, alloc=None,
-                 pinned=None):
+                 pinned=None, tables=None):
         import torch
         self.lib = _lib.lib(library)
         self.meta = meta
@@ -147,8 +160,15 @@ class FieldBuilder:
         if self.n_prims < 1:
             raise ValueError("recipe has no primitive")
         self.geom = geom_of(meta, guard)
-        self.prims, self.chain = device_tables(c, self.device, torch.cuda.current_stream(self.device),
-                                               alloc=alloc, pinned=pinned)
+        if tables is not None:
+            # the caller placed the tables on the device (e.g. a batch's table arena); still checked
+            _validate_program(c.prims, insns, self.mode)
+            self.prims, self.chain = tables
+            if self.prims.numel() != c.prims.nbytes or self.chain.numel() != insns.nbytes:
+                raise ValueError("device tables do not match the compiled recipe")
+        else:
+            self.prims, self.chain = device_tables(c, self.device, torch.cuda.current_stream(self.device),
+                                                   alloc=alloc, pinned=pinned)
         nbytes = self.lib.fb_field_scratch_bytes(ct.addressof(self.geom), self.n_prims, self.n_chain)
         if nbytes < 0:
             raise ValueError("grid outside the build contract")

@@ -12,6 +12,7 @@ enum {
     FB_RUNTIME = 2,
     FB_TIMEOUT = 6,   // a bounded device-side wait gave up; the context stays usable
     FB_NOALLOC_LIMIT = 7,  // the grid exceeds the fixed scratch of an allocation-free entry point
+    FB_CAPACITY = 8,  // an output arena was too small for the result (what fitted is written)
 };
 
 #define FB_CUDA(call)                                    \

@@ -517,12 +517,21 @@ int64_t scratch_bytes(int nx, int ny, int nz, int npol) {
     return 256 + bits + (int64_t)npol * size * 4;
 }
 
-int configure_once() {
-    static int done = 0;
-    if (done) return FB_OK;
+// The column passes use more than 48 KB of dynamic shared memory at 512 rows, an opt-in that is a
+// per-device function attribute: set once for every device that runs a transform (under a lock,
+// since serving threads enqueue transforms concurrently).
+constexpr int kMaxDevices = 64;
+std::mutex g_configure_lock;
+bool g_configured[kMaxDevices] = {};
+
+int configure_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FB_RUNTIME;
+    std::lock_guard<std::mutex> guard(g_configure_lock);
+    if (g_configured[dev]) return FB_OK;
     FB_CUDA(cudaFuncSetAttribute(k_edt_zy, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes(kMaxAxis)));
     FB_CUDA(cudaFuncSetAttribute(k_edt_x, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem_bytes(kMaxAxis)));
-    done = 1;
+    g_configured[dev] = true;
     return FB_OK;
 }
 
@@ -532,7 +541,7 @@ int configure_once() {
 int enqueue(const uint8_t* d_mask, int nx, int ny, int nz, int paired, int sites_nonzero, double pitch,
             int32_t* out_sq, float* out_signed, void* scratch, int64_t scratch_len, cudaStream_t stream,
             bool count) {
-    if (int rc = configure_once()) return rc;
+    if (int rc = configure_device()) return rc;
     const int npol = paired ? 2 : 1;
     if (scratch_len < scratch_bytes(nx, ny, nz, npol)) return FB_INVALID;
     const int W = words_of(nz);
@@ -616,21 +625,46 @@ namespace {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_lock;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+struct NoAllocEntry {
+    void* context;  // the driver context the address belongs to
+    void* ptr;
+};
+NoAllocEntry g_noalloc[kNoAllocMaxDevices] = {};
 
-// Device address of the array on the current device, looked up once per device.  The name
-// g_edt_noalloc_scratch in host code is a host-side stand-in, not a device address, so kernels
-// get this pointer instead.
+// The current driver context (CUcontext), through the runtime's driver entry point so the library
+// does not link libcuda itself; nullptr when it cannot be had.
+void* current_context() {
+    using GetCurrent = int (*)(void**);
+    static GetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<GetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
+// Device address of the array on the current device, looked up once per device and context.  The
+// name g_edt_noalloc_scratch in host code is a host-side stand-in, not a device address, so kernels
+// get this pointer instead.  A context torn down and created again (cudaDeviceReset) maps the array
+// at a new address: the lookup is keyed on the context and repeated for a new one.
 int noalloc_scratch(void** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return FB_RUNTIME;
+    void* ctx = current_context();  // nullptr before the runtime has made a context current
     std::lock_guard<std::mutex> guard(g_noalloc_lock);
-    if (!g_noalloc_ptr[dev]) {
+    NoAllocEntry& e = g_noalloc[dev];
+    if (!e.ptr || !ctx || e.context != ctx) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_edt_noalloc_scratch) != cudaSuccess || !p) return FB_RUNTIME;
-        g_noalloc_ptr[dev] = p;
+        e.ptr = p;
+        e.context = ctx ? ctx : current_context();
     }
-    *out = g_noalloc_ptr[dev];
+    *out = e.ptr;
     return FB_OK;
 }
 
@@ -640,8 +674,9 @@ extern "C" {
 
 // Squared EDT exactly as fb_edt_squared_device, with no allocation and no caller scratch: the
 // scratch is the library's fixed device array.  Inputs and outputs are the caller's device
-// buffers.  Status 0 ok, 1 invalid arguments, 2 CUDA failure, 7 grid larger than the fixed
-// scratch (more than 2^20 voxels) -- rejected before anything is enqueued.
+// buffers.  Status 0 ok, 1 invalid arguments (a null pointer, an axis below 1), 2 CUDA failure,
+// 7 grid beyond the fixed scratch (an axis above 512 or more than 2^20 voxels) -- both rejected
+// before anything is enqueued.
 // The first call on each device looks the array up (cudaGetSymbolAddress) with that device
 // current; make that first call before any stream capture.  The array is shared by every call
 // and keeps the last call's contents (nothing in it needs to start at zero: every word a call
@@ -649,8 +684,8 @@ extern "C" {
 // from different threads -- race on it and must be serialised by the caller.
 int fb_edt_squared_device_noalloc(const uint8_t* d_mask, int nx, int ny, int nz, int sites_nonzero,
                                   int32_t* d_out, void* stream) noexcept {
-    if (!d_mask || !d_out || !shape_ok(nx, ny, nz)) return FB_INVALID;
-    if ((int64_t)nx * ny * nz > kNoAllocVoxels) return FB_NOALLOC_LIMIT;
+    if (!d_mask || !d_out || nx < 1 || ny < 1 || nz < 1) return FB_INVALID;
+    if (!shape_ok(nx, ny, nz) || (int64_t)nx * ny * nz > kNoAllocVoxels) return FB_NOALLOC_LIMIT;
     const int64_t need = scratch_bytes(nx, ny, nz, 1);
     if (need > kNoAllocScratchBytes) return FB_NOALLOC_LIMIT;
     void* scratch = nullptr;

@@ -24,6 +24,9 @@
 #include "prims.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
 
 // Grid geometry of one build, fb_geom in include/field_b200.h.
 struct FbGeom {
@@ -34,13 +37,30 @@ struct FbGeom {
 };
 static_assert(sizeof(FbGeom) == 64, "fb_geom layout");
 
+// One recipe of a batch, as fb_batch_item in include/field_b200.h.
+struct FbBatchItem {
+    const FbGeom* geom;
+    const FbPrim* d_prims;
+    const FbInsn* d_chain;
+    int32_t n_prims, n_chain;
+    int32_t* d_kind;
+    float* d_cma;
+    int32_t* d_active;
+    int32_t* d_count;
+    void* d_scratch;
+    int64_t scratch_len;
+    int32_t* d_slot;  // nullable: with d_mask, the recipe takes part in fb_batch_occupancy_device
+    uint8_t* d_mask;
+};
+static_assert(sizeof(FbBatchItem) == 96, "fb_batch_item layout");
+
 namespace {
 
 constexpr float kBig = 1.0e6f;  // background of interior (-) and exterior (+) blocks, faltkarna_v1.py:46
 constexpr int kCapCoarse = 1024;           // least list capacity of a coarse region
 constexpr int kCapSuper = 256;             // least list capacity of a superblock
 constexpr int64_t kCapBudget = 8 << 20;    // list entries per level beyond which capacities stop growing
-constexpr int kCapBlock = 48;              // per-block list of the thread-per-block cull; leaf staging chunk
+constexpr int kCapBlock = 48;              // leaf staging chunk and the leaf pass's own culled-list capacity
 constexpr int kCapBlockWarp = 96;          // least per-block list of the warp-per-block cull
 constexpr int kCapBlockWarpMax = 1024;     // ... grown while the lists stay within kCapBlockBudget
 constexpr int64_t kCapBlockBudget = 4 << 20;
@@ -149,9 +169,7 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
 int64_t compact_scratch(int64_t nblocks) { return align256((nblocks + kTile - 1) / kTile * 8) + 256; }
 
 // ------------------------------------------------------------------------------------ prepare
-__global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ void prepare_prim(const FbPrim* __restrict__ prims, int i, PrimF* __restrict__ out) {
     const FbPrim P = prims[i];
     PrimF F;
     F.type = P.type;
@@ -196,6 +214,8 @@ __global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* 
         const double bb = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
         for (int j = 0; j < 4; ++j) F.p[j] = (float)p[j];
         F.p[4] = bb > 0 ? (float)(1.0 / bb) : 0.f;
+        F.p[5] = 0.f;  // segment parameter range [0, 1] in the canonical frame
+        F.p[6] = 1.f;
         break;
     }
     default:
@@ -242,6 +262,11 @@ __global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* 
         F.p[11] = (float)(rw * (1.0 + 1e-6) + 1e-6 * mag);  // covers rounding the centre to float32
     }
     out[i] = F;
+}
+
+__global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) prepare_prim(prims, i, out);
 }
 
 __global__ void k_full_list(uint32_t* __restrict__ list, int n) {
@@ -526,78 +551,14 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
     return n;
 }
 
-// The same walk by one thread (block-level culling in k_classify).
-__device__ int seq_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn* __restrict__ chain,
-                        const PrimF* __restrict__ primf, float cx, float cy, float cz, float R, float eps,
-                        uint32_t* __restrict__ out, int cap) {
-    float alo = 0.f, ahi = 0.f;
-    int n = 0;
-    int i = 0;
-    while (i < n_in) {
-        const Elem head = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, false);
-        if (!runnable(head.op, head.k)) {
-            const Elem E = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, true);
-            float plo = E.lo, phi = E.hi;  // back to the primitive's own bounds
-            if (E.op == CH_SUBTRACT || E.op == CH_SETNEG) { plo = -E.hi; phi = -E.lo; }
-            const int act = interval_step(E.op, E.k, plo, phi, alo, ahi);
-            if (act) {
-                uint32_t rec = E.ent;
-                if (act == 2) { n = 0; rec = (E.ent & ~3u) | 1u; }
-                if (act == 3) { n = 0; rec = (E.ent & ~3u) | 2u; }
-                if (n < cap) out[n] = rec;
-                ++n;
-            }
-            ++i;
-            continue;
-        }
-        const int op = head.op;
-        // pass 1: the run's end and its aggregate bound in one traversal
-        float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
-        int j = i;
-        while (j < n_in) {
-            const Elem E = load_elem(in, j, chain, primf, cx, cy, cz, R, eps, true);
-            if (j > i && !(E.op == op && runnable(E.op, E.k))) break;
-            agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
-            ++j;
-        }
-        const RunState rs = run_decide(op, agg, alo, ahi);
-        if (rs.reset) n = 0;
-        bool first = rs.reset;
-        float klo = 3.0e38f, khi = -3.0e38f;
-        for (int e = i; e < j; ++e) {
-            const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
-            if (!run_keep(op, E, rs.bound)) continue;
-            klo = fminf(klo, E.lo);
-            khi = fmaxf(khi, E.hi);
-            uint32_t rec = E.ent;
-            if (first) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
-            first = false;
-            if (n < cap) out[n] = rec;
-            ++n;
-        }
-        if (op == CH_UNION) {
-            alo = rs.reset ? klo : fminf(alo, klo);
-            ahi = rs.bound;
-        } else {
-            alo = rs.bound;
-            ahi = rs.reset ? khi : fmaxf(ahi, khi);
-        }
-        i = j;
-    }
-    return n;
-}
-
 // Level cull.  Regions of `edge` voxels on a (rnx, rny, rnz) grid; parent region = coords / div
 // on a (pnx, pny, pnz) grid (parent_off == nullptr: the single full list [0, n_full)).
 template <bool kBall>
-__global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
-                       uint32_t* __restrict__ pool, const int64_t* __restrict__ parent_off,
-                       const int32_t* __restrict__ parent_len, int n_full, int div, int pny, int pnz,
-                       int64_t* __restrict__ off, int32_t* __restrict__ len, int64_t pool_base, int cap, int edge,
-                       int rnx, int rny, int rnz) {
-    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nreg = (int64_t)rnx * rny * rnz;
-    if (r >= nreg) return;
+__device__ void cull_region(const Geo& G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
+                            uint32_t* __restrict__ pool, const int64_t* __restrict__ parent_off,
+                            const int32_t* __restrict__ parent_len, int n_full, int div, int pny, int pnz,
+                            int64_t* __restrict__ off, int32_t* __restrict__ len, int64_t pool_base, int cap, int edge,
+                            int rny, int rnz, int64_t r) {
     const int rz = (int)(r % rnz), ry = (int)((r / rnz) % rny), rx = (int)(r / ((int64_t)rnz * rny));
     int64_t poff = 0;
     int plen = n_full;
@@ -625,18 +586,26 @@ __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __r
     }
 }
 
+template <bool kBall>
+__global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
+                       uint32_t* __restrict__ pool, const int64_t* __restrict__ parent_off,
+                       const int32_t* __restrict__ parent_len, int n_full, int div, int pny, int pnz,
+                       int64_t* __restrict__ off, int32_t* __restrict__ len, int64_t pool_base, int cap, int edge,
+                       int rnx, int rny, int rnz) {
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (r >= (int64_t)rnx * rny * rnz) return;
+    cull_region<kBall>(G, chain, primf, pool, parent_off, parent_len, n_full, div, pny, pnz, off, len, pool_base, cap,
+                       edge, rny, rnz, r);
+}
+
 // Block-level cull with one warp per block, for grids of few blocks (where one thread per block
 // would leave most of the GPU idle): the superblock list culled to the block's own list, stored at
 // blk_pool + b * cap.  blk_len[b] = -1 when it does not fit; that block then uses the superblock list
 // (exact, only slower).
-__global__ void __launch_bounds__(128) k_cull_blocks(Geo G, const FbInsn* __restrict__ chain,
-                                                     const PrimF* __restrict__ primf, const uint32_t* __restrict__ pool,
-                                                     const int64_t* __restrict__ sb_off,
-                                                     const int32_t* __restrict__ sb_len, int32_t* __restrict__ blk_off,
-                                                     int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool,
-                                                     int cap) {
-    const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (b >= G.nblocks) return;
+__device__ void cull_block(const Geo& G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
+                           const uint32_t* __restrict__ pool, const int64_t* __restrict__ sb_off,
+                           const int32_t* __restrict__ sb_len, int32_t* __restrict__ blk_off,
+                           int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int cap, int64_t b) {
     const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
     const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
     const float half = 0.5f * G.B;
@@ -649,6 +618,76 @@ __global__ void __launch_bounds__(128) k_cull_blocks(Geo G, const FbInsn* __rest
         blk_off[b] = (int32_t)(b * cap);
         blk_len[b] = n <= cap ? n : -1;
     }
+}
+
+__global__ void __launch_bounds__(128) k_cull_blocks(Geo G, const FbInsn* __restrict__ chain,
+                                                     const PrimF* __restrict__ primf, const uint32_t* __restrict__ pool,
+                                                     const int64_t* __restrict__ sb_off,
+                                                     const int32_t* __restrict__ sb_len, int32_t* __restrict__ blk_off,
+                                                     int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool,
+                                                     int cap) {
+    const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (b >= G.nblocks) return;
+    cull_block(G, chain, primf, pool, sb_off, sb_len, blk_off, blk_len, blk_pool, cap, b);
+}
+
+// Per-block lists of the active blocks of a lattice-classified grid: a warp per active block culls
+// its superblock's list to the block (the same walk as k_cull_blocks) into shared memory, then
+// reserves room in blk_pool with one atomic and copies it there.  A list longer than kCapActive, or
+// one that finds the pool full, is not stored (blk_len stays -1: the leaf pass culls that block
+// itself, and queries use the superblock list -- exact, only slower).
+constexpr int kCapActive = 256;
+constexpr int kCullActiveWarps = 4;
+
+// One active block's list (every lane of the warp calls it with the same block b).
+__device__ void cull_active_block(const Geo& G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
+                                  const uint32_t* __restrict__ pool, const int64_t* __restrict__ sb_off,
+                                  const int32_t* __restrict__ sb_len, int64_t b, int32_t* __restrict__ blk_off,
+                                  int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                                  int* __restrict__ cursor, uint32_t* sl) {
+    const int lane = threadIdx.x & 31;
+    if (b < 0 || b >= G.nblocks) return;
+    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
+    const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
+    const float half = 0.5f * G.B;
+    const float cx = G.fx0 + (bi * G.B + half) * G.fpitch;
+    const float cy = G.fy0 + (bj * G.B + half) * G.fpitch;
+    const float cz = G.fz0 + (bk * G.B + half) * G.fpitch;
+    const float R = 1.7320509f * half * G.fpitch;
+    __syncwarp();
+    const int nk = warp_walk(pool + sb_off[s], sb_len[s], chain, primf, cx, cy, cz, R, G.eps, sl, kCapActive);
+    __syncwarp();
+    if (nk > kCapActive) return;
+    int slot = 0;
+    if (lane == 0) slot = atomicAdd(cursor, nk);
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if ((int64_t)slot + nk > blk_cap) return;
+    for (int i = lane; i < nk; i += 32) blk_pool[slot + i] = sl[i];
+    if (lane == 0) {
+        blk_off[b] = slot;
+        blk_len[b] = nk;
+    }
+}
+
+__global__ void __launch_bounds__(32 * kCullActiveWarps) k_cull_active(Geo G, const FbInsn* __restrict__ chain,
+                                                                      const PrimF* __restrict__ primf,
+                                                                      const uint32_t* __restrict__ pool,
+                                                                      const int64_t* __restrict__ sb_off,
+                                                                      const int32_t* __restrict__ sb_len,
+                                                                      const int32_t* __restrict__ active,
+                                                                      const int32_t* __restrict__ count,
+                                                                      int32_t* __restrict__ blk_off,
+                                                                      int32_t* __restrict__ blk_len,
+                                                                      uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                                                                      int* __restrict__ cursor) {
+    __shared__ uint32_t s_list[kCullActiveWarps][kCapActive];
+    const int warp = threadIdx.x >> 5;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t n = min((int64_t)count[0], G.nblocks);
+    for (int64_t a = gwarp; a < n; a += nwarps)
+        cull_active_block(G, chain, primf, pool, sb_off, sb_len, active[a], blk_off, blk_len, blk_pool, blk_cap, cursor,
+                          s_list[warp]);
 }
 
 // ------------------------------------------------------------------------------------ localisation
@@ -671,21 +710,55 @@ __device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, in
 // mode), so the walk over the superblock's list runs in lockstep with broadcast loads.
 __host__ __device__ __forceinline__ int threads_per_super(int S) { return ((S * S * S + 31) / 32) * 32; }
 
-// kListed: the per-block lists are already in blk_pool (k_cull_blocks); read them instead of culling.
-// 10 CTAs per SM (48 registers): the walk and the corner folds wait on loads and on the instruction
-// cache, and more resident warps hide that better than the few spills cost.
-template <bool kChain, bool kListed>
-__global__ void __launch_bounds__(128, 10) k_classify(Geo G, const FbPrim* __restrict__ prims,
-                                                  const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
-                                                  int n_chain, const uint32_t* __restrict__ pool,
-                                                  const int64_t* __restrict__ sb_off,
-                                                  const int32_t* __restrict__ sb_len, int32_t* __restrict__ kind,
-                                                  float* __restrict__ cma, int32_t* __restrict__ blk_off,
-                                                  int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool,
-                                                  int64_t blk_cap, int* __restrict__ blk_cursor) {
+// Kind and corner_min_abs of one block from its 8 corner values: float32 decisions unless a corner
+// lies within the guard band of 0 or of the margin (or is NaN); then all 8 corners are re-evaluated
+// in float64 by `corner_d(c)` and the decision is taken in float64, exactly as the oracle's.
+template <typename CornerD>
+__device__ __forceinline__ int decide_block(const Geo& G, const float* v, float& cma_out, CornerD corner_d) {
+    bool use_d = false;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float a = fabsf(v[c]);
+        use_d |= a < G.guard || fabsf(a - G.margin) < G.guard || !(a == a);
+    }
+    bool pos = false, neg = false;
+    if (use_d) {
+        double mn = 1.0e30;
+        for (int c = 0; c < 8; ++c) {
+            const double vd = corner_d(c);
+            mn = fmin(mn, fabs(vd));
+            if (vd >= 0.0) pos = true; else neg = true;
+        }
+        cma_out = (float)mn;
+        return (pos && neg) ? 0 : (mn <= (double)G.margin ? 0 : (neg ? -1 : 1));
+    }
+    float mn = 1.0e30f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        mn = fminf(mn, fabsf(v[c]));
+        if (v[c] >= 0.f) pos = true; else neg = true;
+    }
+    cma_out = mn;
+    return (pos && neg) ? 0 : (mn <= G.margin ? 0 : (neg ? -1 : 1));
+}
+
+// World coordinate of grid vertex index i along one axis, in float64 (the oracle's sample point).
+__device__ __forceinline__ double vertex_d(double origin, int64_t i, double pitch) {
+    return rn_add(origin, rn_mul((double)i, pitch));
+}
+
+// Thread-per-block classification of a chain recipe whose per-block lists k_cull_blocks left in
+// blk_pool (grids of few blocks): thread t of the superblock-major order -- threads of one
+// superblock are consecutive, so a warp never spans two superblocks and walks in lockstep with
+// broadcast loads -- evaluates its block's 8 corners in float32 in block-local coordinates.
+__device__ void classify_listed(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
+                                const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
+                                const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
+                                int32_t* __restrict__ kind, float* __restrict__ cma,
+                                const int32_t* __restrict__ blk_off, const int32_t* __restrict__ blk_len,
+                                const uint32_t* __restrict__ blk_pool, int64_t t) {
     const int S = G.S;
     const int T = threads_per_super(S);
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t s_id = t / T;
     const int local = (int)(t % T);
     if (s_id >= G.nsuper || local >= S * S * S) return;
@@ -694,112 +767,78 @@ __global__ void __launch_bounds__(128, 10) k_classify(Geo G, const FbPrim* __res
     if (bi >= G.nbx || bj >= G.nby || bk >= G.nbz) return;
     const int64_t b = ((int64_t)bi * G.nby + bj) * G.nbz + bk;
     const int B = G.B;
+    const int n = blk_len[b];
+    const uint32_t* list = n >= 0 ? blk_pool + blk_off[b] : pool + sb_off[s_id];
+    const int len = n >= 0 ? n : sb_len[s_id];
+    const double ox = G.x0 + (double)(bi * B) * G.pitch;
+    const double oy = G.y0 + (double)(bj * B) * G.pitch;
+    const double oz = G.z0 + (double)(bk * B) * G.pitch;
+    const float side = (float)B * G.fpitch;
     float v[8];
-    double vd[8];
-    bool use_d = false;
-    uint32_t blist[kCapBlock];
-    int nblist = -1;
-    if (kChain) {
-        const uint32_t* plist = pool + sb_off[s_id];
-        const int plen = sb_len[s_id];
-        const uint32_t* list;
-        int len;
-        if (kListed) {
-            const int n = blk_len[b];
-            list = n >= 0 ? blk_pool + blk_off[b] : plist;
-            len = n >= 0 ? n : plen;
-        } else {
-            // block-level cull of the superblock list
-            const float half = 0.5f * B;
-            const float cx = G.fx0 + (bi * B + half) * G.fpitch;
-            const float cy = G.fy0 + (bj * B + half) * G.fpitch;
-            const float cz = G.fz0 + (bk * B + half) * G.fpitch;
-            const float R = 1.7320509f * half * G.fpitch;
-            const int n = seq_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, blist, kCapBlock);
-            nblist = n;
-            list = n <= kCapBlock ? blist : plist;
-            len = n <= kCapBlock ? n : plen;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = 0.f;
+    for (int i = 0; i < len; ++i) {
+        const uint32_t e = list[i];
+        const FbInsn I = chain[e >> 2];
+        const int op = effective_op(e, I.op);
+        const float k = (float)I.k;
+        if (op == CH_OFFSET) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) v[c] -= k;
+            continue;
         }
-        const double ox = G.x0 + (double)(bi * B) * G.pitch;
-        const double oy = G.y0 + (double)(bj * B) * G.pitch;
-        const double oz = G.z0 + (double)(bk * B) * G.pitch;
-        const float side = (float)B * G.fpitch;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) v[c] = 0.f;
-        for (int i = 0; i < len; ++i) {
-            const uint32_t e = list[i];
-            const FbInsn I = chain[e >> 2];
-            const int op = effective_op(e, I.op);
-            const float k = (float)I.k;
-            if (op == CH_OFFSET) {
-#pragma unroll
-                for (int c = 0; c < 8; ++c) v[c] -= k;
-                continue;
-            }
-            LocalPrim P;
-            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const float pv = local_eval(P, (c & 1) ? side : 0.f, ((c >> 1) & 1) ? side : 0.f,
-                                            ((c >> 2) & 1) ? side : 0.f);
-                v[c] = chain_apply(op, v[c], pv, k);
-            }
-        }
+        LocalPrim P;
+        localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            const float a = fabsf(v[c]);
-            use_d |= a < G.guard || fabsf(a - G.margin) < G.guard || !(a == a);
-        }
-        if (use_d) {
-            for (int c = 0; c < 8; ++c) {
-                const int64_t ix = (int64_t)bi * B + (c & 1) * B, iy = (int64_t)bj * B + ((c >> 1) & 1) * B,
-                              iz = (int64_t)bk * B + ((c >> 2) & 1) * B;
-                vd[c] = list_eval_d(list, len, chain, prims, rn_add(G.x0, rn_mul((double)ix, G.pitch)),
-                                    rn_add(G.y0, rn_mul((double)iy, G.pitch)), rn_add(G.z0, rn_mul((double)iz, G.pitch)));
-            }
-        }
-    } else {
-        use_d = true;
-        for (int c = 0; c < 8; ++c) {
-            const int64_t ix = (int64_t)bi * B + (c & 1) * B, iy = (int64_t)bj * B + ((c >> 1) & 1) * B,
-                          iz = (int64_t)bk * B + ((c >> 2) & 1) * B;
-            vd[c] = program_eval_d(prims, chain, n_chain, rn_add(G.x0, rn_mul((double)ix, G.pitch)),
-                                   rn_add(G.y0, rn_mul((double)iy, G.pitch)), rn_add(G.z0, rn_mul((double)iz, G.pitch)));
+            const float pv = local_eval(P, (c & 1) ? side : 0.f, ((c >> 1) & 1) ? side : 0.f, ((c >> 2) & 1) ? side : 0.f);
+            v[c] = chain_apply(op, v[c], pv, k);
         }
     }
+    float m;
+    kind[b] = decide_block(G, v, m, [&](int c) {
+        return list_eval_d(list, len, chain, prims, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
+                           vertex_d(G.y0, (int64_t)bj * B + ((c >> 1) & 1) * B, G.pitch),
+                           vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
+    });
+    cma[b] = m;
+}
+
+// 10 CTAs per SM (48 registers): the walk and the corner folds wait on loads and on the instruction
+// cache, and more resident warps hide that better than the few spills cost.
+__global__ void __launch_bounds__(128, 10) k_classify_listed(Geo G, const FbPrim* __restrict__ prims,
+                                                             const PrimF* __restrict__ primf,
+                                                             const FbInsn* __restrict__ chain,
+                                                             const uint32_t* __restrict__ pool,
+                                                             const int64_t* __restrict__ sb_off,
+                                                             const int32_t* __restrict__ sb_len,
+                                                             int32_t* __restrict__ kind, float* __restrict__ cma,
+                                                             const int32_t* __restrict__ blk_off,
+                                                             const int32_t* __restrict__ blk_len,
+                                                             const uint32_t* __restrict__ blk_pool) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    classify_listed(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, t);
+}
+
+// General postfix programs: every corner of every block in float64, no culling.
+__global__ void __launch_bounds__(128) k_classify_program(Geo G, const FbPrim* __restrict__ prims,
+                                                          const FbInsn* __restrict__ prog, int n_prog,
+                                                          int32_t* __restrict__ kind, float* __restrict__ cma) {
+    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (b >= G.nblocks) return;
+    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
+    const int B = G.B;
+    double mn = 1.0e30;
     bool pos = false, neg = false;
-    int kd;
-    if (use_d) {
-        double mn = 1.0e30;
-        for (int c = 0; c < 8; ++c) {
-            mn = fmin(mn, fabs(vd[c]));
-            if (vd[c] >= 0.0) pos = true; else neg = true;
-        }
-        kd = (pos && neg) ? 0 : (mn <= (double)G.margin ? 0 : (neg ? -1 : 1));
-        cma[b] = (float)mn;
-    } else {
-        float mn = 1.0e30f;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            mn = fminf(mn, fabsf(v[c]));
-            if (v[c] >= 0.f) pos = true; else neg = true;
-        }
-        kd = (pos && neg) ? 0 : (mn <= G.margin ? 0 : (neg ? -1 : 1));
-        cma[b] = mn;
+    for (int c = 0; c < 8; ++c) {
+        const double vd = program_eval_d(prims, prog, n_prog, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
+                                         vertex_d(G.y0, (int64_t)bj * B + ((c >> 1) & 1) * B, G.pitch),
+                                         vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
+        mn = fmin(mn, fabs(vd));
+        if (vd >= 0.0) pos = true; else neg = true;
     }
-    kind[b] = kd;
-    if (kChain && !kListed && kd == 0) {  // keep the culled list for the leaf pass
-        int len = -1;
-        if (nblist >= 0 && nblist <= kCapBlock) {
-            const int slot = atomicAdd(blk_cursor, nblist);
-            if ((int64_t)slot + nblist <= blk_cap) {
-                for (int i = 0; i < nblist; ++i) blk_pool[slot + i] = blist[i];
-                blk_off[b] = slot;
-                len = nblist;
-            }
-        }
-        blk_len[b] = len;  // -1: the leaf pass culls from the superblock list itself
-    }
+    kind[b] = (pos && neg) ? 0 : (mn <= (double)G.margin ? 0 : (neg ? -1 : 1));
+    cma[b] = (float)mn;
 }
 
 // ------------------------------------------------------------------------------------ compaction
@@ -812,16 +851,16 @@ __device__ __forceinline__ unsigned long long ld_status(const unsigned long long
     return v;
 }
 
-__global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kind, int64_t n,
-                                                 int32_t* __restrict__ active, int32_t* __restrict__ count,
-                                                 unsigned long long* __restrict__ status, int* __restrict__ misc,
-                                                 int64_t ntiles) {
-    __shared__ int s_tile;
+constexpr long long kLookbackSpins = 1ll << 24;  // ~0.5 s of 32 ns sleeps before a wait gives up
+
+// One tile of the scan.  `tile` is this CTA's tile of the kind array, taken in order from a ticket
+// counter by the caller (so every predecessor tile is already running); `err` is raised when a wait
+// gives up.  Every thread of the CTA calls it.
+__device__ void compact_tile(const int32_t* __restrict__ kind, int64_t n, int32_t* __restrict__ active,
+                             int32_t* __restrict__ count, unsigned long long* __restrict__ status, int64_t tile,
+                             int64_t ntiles, int* __restrict__ err, long long spin_limit) {
     __shared__ int s_warp[8];
     __shared__ long long s_prefix;
-    if (threadIdx.x == 0) s_tile = atomicAdd(&misc[0], 1);
-    __syncthreads();
-    const int64_t tile = s_tile;
     const int64_t base = tile * kTile + (int64_t)threadIdx.x * 8;
     unsigned flags = 0;
 #pragma unroll
@@ -858,8 +897,8 @@ __global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kin
                 const unsigned long long s = ld_status(&status[j]);
                 const unsigned long long flag = s & ~kMask;
                 if (flag == 0) {
-                    if (++spins > (1ll << 24)) {
-                        atomicExch(&misc[1], 1);
+                    if (++spins > spin_limit) {
+                        atomicExch(err, 1);
                         break;
                     }
                     __nanosleep(32);
@@ -883,6 +922,16 @@ __global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kin
         if (flags & (1u << j)) active[start + k++] = (int32_t)(base + j);
 }
 
+__global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kind, int64_t n,
+                                                 int32_t* __restrict__ active, int32_t* __restrict__ count,
+                                                 unsigned long long* __restrict__ status, int* __restrict__ misc,
+                                                 int64_t ntiles, long long spin_limit) {
+    __shared__ int s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&misc[0], 1);
+    __syncthreads();
+    compact_tile(kind, n, active, count, status, s_tile, ntiles, &misc[1], spin_limit);
+}
+
 // ------------------------------------------------------------------------------------ leaf eval
 
 // Canonical primitive of a fixed type (the switch is taken once per primitive and group of
@@ -897,7 +946,7 @@ __device__ __forceinline__ float canon_t(const float* __restrict__ p, float x, f
         return sqrtf(fmaf(oz, oz, fmaf(ox, ox, oy * oy))) + fminf(fmaxf(qz, fmaxf(qx, qy)), 0.f);
     }
     if (T == P_CAPSULE) {
-        const float h = fminf(fmaxf(fmaf(z, p[2], fmaf(x, p[0], y * p[1])) * p[4], 0.f), 1.f);
+        const float h = fminf(fmaxf(fmaf(z, p[2], fmaf(x, p[0], y * p[1])) * p[4], p[5]), p[6]);
         const float dx = fmaf(-p[0], h, x), dy = fmaf(-p[1], h, y), dz = fmaf(-p[2], h, z);
         return sqrtf(fmaf(dz, dz, fmaf(dx, dx, dy * dy))) - p[3];
     }
@@ -1042,8 +1091,253 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
     }
 }
 
+// ------------------------------------------------------------------------------------ lattice classify
+// Block kinds of a chain recipe from the corner lattice of each superblock (grids of many blocks).
+// A block's 8 corners are lattice points of spacing B pitches shared with up to 7 neighbours; the
+// superblock evaluates its (S+1)^3 lattice once with its own culled list (exact for every point of
+// its closed region) instead of each block culling that list again and evaluating its corners.  A
+// warp per superblock: the list is localised to the superblock origin kLatChunk primitives at a
+// time into shared memory (a capsule re-anchored on its segment, as in localise), and each lane
+// evaluates whole lattice columns along z (the primitive switch taken once per column), keeping the
+// partial folds in shared memory between chunks.  Decisions then follow the per-block rule: a block
+// with a corner value within the guard band of 0 or of the margin (or NaN) re-evaluates all 8
+// corners in float64 with the superblock list and decides in float64, exactly as the oracle.
+constexpr int kLatWarps = 4;
+constexpr int kLatChunk = 32;
+
+// One superblock of the lattice classification (every lane of the warp calls it with the same s):
+// sp holds kLatChunk localised primitives, val the (S+1)^3 lattice values.  Also marks the
+// superblock's blocks as having no per-block list yet (blk_len = -1).
+template <int B>
+__device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
+                              const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
+                              const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
+                              int32_t* __restrict__ kind, float* __restrict__ cma, int32_t* __restrict__ blk_len,
+                              int64_t s, LocalPrim* sp, float* val) {
+    constexpr int S = 32 / B;          // blocks per superblock edge
+    constexpr int P1 = S + 1;          // lattice points per edge
+    constexpr int NC = P1 * P1;        // lattice columns (along z)
+    const int lane = threadIdx.x & 31;
+    float dz[P1];
+#pragma unroll
+    for (int k = 0; k < P1; ++k) dz[k] = (float)(k * B) * G.fpitch;
+    const int sz = (int)(s % G.nsz), sy = (int)((s / G.nsz) % G.nsy), sx = (int)(s / ((int64_t)G.nsz * G.nsy));
+    const int64_t ix0 = (int64_t)sx * 32, iy0 = (int64_t)sy * 32, iz0 = (int64_t)sz * 32;
+    const double ox = G.x0 + (double)ix0 * G.pitch;
+    const double oy = G.y0 + (double)iy0 * G.pitch;
+    const double oz = G.z0 + (double)iz0 * G.pitch;
+    const uint32_t* list = pool + sb_off[s];
+    const int len = sb_len[s];
+    for (int c0 = 0; c0 == 0 || c0 < len; c0 += kLatChunk) {  // one pass even for an empty list
+        const int clen = max(0, min(kLatChunk, len - c0));
+        const bool first = c0 == 0;
+        __syncwarp();
+        for (int i = lane; i < clen; i += 32) {
+            const uint32_t e = list[c0 + i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            if (op == CH_OFFSET) {
+                sp[i].op = op;
+                sp[i].k = (float)I.k;
+            } else {
+                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
+            }
+        }
+        __syncwarp();
+        for (int col = lane; col < NC; col += 32) {
+            const int pi = col / P1, pj = col - pi * P1;
+            const float dx = (float)(pi * B) * G.fpitch, dy = (float)(pj * B) * G.fpitch;
+            float acc[P1], v[P1];
+            float* out = val + col * P1;
+#pragma unroll
+            for (int k = 0; k < P1; ++k) acc[k] = first ? 0.f : out[k];
+            for (int i = 0; i < clen; ++i) {
+                const LocalPrim& P = sp[i];
+                if (P.op == CH_OFFSET) {
+#pragma unroll
+                    for (int k = 0; k < P1; ++k) acc[k] -= P.k;
+                    continue;
+                }
+                eval_group<P1>(P, dx, dy, dz, v);
+                combine_group<P1>(P.op, P.k, acc, v);
+            }
+#pragma unroll
+            for (int k = 0; k < P1; ++k) out[k] = acc[k];
+        }
+    }
+    __syncwarp();
+    // decisions of the superblock's blocks inside the grid
+    for (int t = lane; t < S * S * S; t += 32) {
+        const int li = t / (S * S), lj = (t / S) % S, lk = t % S;
+        const int bi = sx * S + li, bj = sy * S + lj, bk = sz * S + lk;
+        if (bi >= G.nbx || bj >= G.nby || bk >= G.nbz) continue;
+        const int64_t b = ((int64_t)bi * G.nby + bj) * G.nbz + bk;
+        float vc[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            vc[c] = val[((li + (c & 1)) * P1 + (lj + ((c >> 1) & 1))) * P1 + lk + ((c >> 2) & 1)];
+        float m;
+        kind[b] = decide_block(G, vc, m, [&](int c) {
+            return list_eval_d(list, len, chain, prims, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
+                               vertex_d(G.y0, (int64_t)bj * B + ((c >> 1) & 1) * B, G.pitch),
+                               vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
+        });
+        cma[b] = m;
+        blk_len[b] = -1;
+    }
+    __syncwarp();
+}
+
+template <int B>
+__global__ void __launch_bounds__(32 * kLatWarps) k_classify_lattice(Geo G, const FbPrim* __restrict__ prims,
+                                                                     const PrimF* __restrict__ primf,
+                                                                     const FbInsn* __restrict__ chain,
+                                                                     const uint32_t* __restrict__ pool,
+                                                                     const int64_t* __restrict__ sb_off,
+                                                                     const int32_t* __restrict__ sb_len,
+                                                                     int32_t* __restrict__ kind, float* __restrict__ cma,
+                                                                     int32_t* __restrict__ blk_len) {
+    constexpr int P1 = 32 / B + 1;
+    __shared__ LocalPrim s_prim[kLatWarps][kLatChunk];
+    __shared__ float s_val[kLatWarps][P1 * P1 * P1];
+    const int warp = threadIdx.x >> 5;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = gwarp; s < G.nsuper; s += nwarps)
+        lattice_super<B>(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_len, s, s_prim[warp], s_val[warp]);
+}
+
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
 // voxels along z (VG = 4, or 2 for 4^3 blocks) and stores each group with one vector store.
+// One active block's tile: the block's culled list (as the classification left it, else culled
+// here from the superblock list into `sl`), localised kCapBlock primitives at a time into `sp`, each
+// lane evaluating groups of VG consecutive voxels along z (VG = 4, or 2 for 4^3 blocks) and storing
+// each group with one vector store.  Every lane of the warp calls it with the same block.
+template <int B>
+__device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
+                           const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
+                           const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len, int64_t blk,
+                           float* __restrict__ out, unsigned long long* __restrict__ work,
+                           const int32_t* __restrict__ kind, const int32_t* __restrict__ blk_off,
+                           const int32_t* __restrict__ blk_len, const uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                           LocalPrim* sp, uint32_t* sl) {
+    constexpr int kVox = B * B * B;
+    constexpr int VG = B == 4 ? 2 : 4;
+    constexpr int kGroups = kVox / (32 * VG);
+    const int lane = threadIdx.x & 31;
+    if (blk < 0 || blk >= G.nblocks) {  // an id outside the grid (a corrupted list) reads as exterior
+        for (int v = lane; v < kVox; v += 32) out[v] = kBig;
+        return;
+    }
+    const int bk = (int)(blk % G.nbz), bj = (int)((blk / G.nbz) % G.nby), bi = (int)(blk / ((int64_t)G.nbz * G.nby));
+    const double ox = G.x0 + (double)(bi * B) * G.pitch;
+    const double oy = G.y0 + (double)(bj * B) * G.pitch;
+    const double oz = G.z0 + (double)(bk * B) * G.pitch;
+    // the block's culled list, as the classification left it; cull again if it is not there
+    const uint32_t* list;
+    int len;
+    bool fits = true;
+    int stored = kind[blk] == 0 ? blk_len[blk] : -1;
+    const int64_t soff = stored >= 0 ? (int64_t)blk_off[blk] : 0;
+    if (stored < 0 || soff < 0 || soff + stored > blk_cap) stored = -1;
+    if (stored >= 0) {
+        list = blk_pool + soff;
+        len = stored;
+    } else {
+        const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
+        const uint32_t* plist = pool + sb_off[s];
+        const int plen = sb_len[s];
+        const float half = 0.5f * B;
+        const float cx = G.fx0 + (bi * B + half) * G.fpitch;
+        const float cy = G.fy0 + (bj * B + half) * G.fpitch;
+        const float cz = G.fz0 + (bk * B + half) * G.fpitch;
+        const float R = 1.7320509f * half * G.fpitch;
+        __syncwarp();
+        const int nk = warp_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, sl, kCapBlock);
+        __syncwarp();
+        fits = nk <= kCapBlock;
+        list = fits ? sl : plist;
+        len = fits ? nk : plen;
+    }
+    if (work) {  // executed primitive evaluations and their float32 operation count
+        unsigned long long evals = 0, flops = 0;
+        for (int i = lane; i < len; i += 32) {
+            const FbInsn I = chain[list[i] >> 2];
+            const int op = effective_op(list[i], I.op);
+            if (op == CH_OFFSET) { flops += 1; continue; }
+            evals += 1;
+            flops += prim_flops(primf[I.arg].type, primf[I.arg].ident) + (I.k > 0 ? 8 : 1);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            evals += __shfl_xor_sync(0xffffffffu, evals, o);
+            flops += __shfl_xor_sync(0xffffffffu, flops, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&work[0], evals * kVox);
+            atomicAdd(&work[1], flops * kVox);
+        }
+    }
+    (void)fits;
+    // the list in chunks of kCapBlock localised primitives; between chunks each lane keeps its
+    // partial fold in its own part of the tile (the same float operations in the same order)
+    for (int c0 = 0; c0 == 0 || c0 < len; c0 += kCapBlock) {  // one pass even for an empty list
+        const int clen = max(0, min(kCapBlock, len - c0));
+        const bool first = c0 == 0, last = c0 + clen >= len;
+        __syncwarp();
+        for (int i = lane; i < clen; i += 32) {
+            const uint32_t e = list[c0 + i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            if (op == CH_OFFSET) {
+                sp[i].op = op;
+                sp[i].k = (float)I.k;
+            } else {
+                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
+            }
+        }
+        __syncwarp();
+        for (int g = 0; g < kGroups; ++g) {
+            const int v0 = (g * 32 + lane) * VG;
+            const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
+            const float dx = li * G.fpitch, dy = lj * G.fpitch;
+            float dz[VG], acc[VG], v[VG];
+#pragma unroll
+            for (int k = 0; k < VG; ++k) dz[k] = (lk0 + k) * G.fpitch;
+            if (first) {
+#pragma unroll
+                for (int k = 0; k < VG; ++k) acc[k] = 0.f;
+            } else {
+                load_group<VG>(out, g * 32 + lane, acc);
+            }
+            for (int i = 0; i < clen; ++i) {
+                const LocalPrim& P = sp[i];
+                const int op = P.op;
+                if (op == CH_OFFSET) {
+#pragma unroll
+                    for (int k = 0; k < VG; ++k) acc[k] -= P.k;
+                    continue;
+                }
+                eval_group<VG>(P, dx, dy, dz, v);
+                combine_group<VG>(op, P.k, acc, v);
+            }
+            if (last) {
+                // guard band: float64 recheck so the sign never disagrees with the float64 value
+                bool near = false;
+#pragma unroll
+                for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
+                if (near) {
+                    for (int k = 0; k < VG; ++k)
+                        if (!(fabsf(acc[k]) >= G.guard))
+                            acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
+                                                        (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
+                }
+            }
+            store_group<VG>(out, g * 32 + lane, acc);
+        }
+    }
+}
+
+// Leaf tiles of a chain recipe: a warp per active block (leaf_block).
 template <int B>
 __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_leaf(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
@@ -1059,131 +1353,15 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_leaf(Geo G, const FbPrim
                                                              const int32_t* __restrict__ blk_off,
                                                              const int32_t* __restrict__ blk_len,
                                                              const uint32_t* __restrict__ blk_pool, int64_t blk_cap) {
-    constexpr int kVox = B * B * B;
-    constexpr int VG = B == 4 ? 2 : 4;
-    constexpr int kGroups = kVox / (32 * VG);
     __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
     __shared__ uint32_t s_list[kLeafWarps][kCapBlock];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t n_active = min((int64_t)count[0], capacity);
-    LocalPrim* sp = s_prim[warp];
-    uint32_t* sl = s_list[warp];
-    for (int64_t a = gwarp; a < n_active; a += nwarps) {
-        const int64_t blk = active[a];
-        float* out = tiles + a * kVox;
-        if (blk < 0 || blk >= G.nblocks) {  // an id outside the grid (a corrupted list) reads as exterior
-            for (int v = lane; v < kVox; v += 32) out[v] = kBig;
-            continue;
-        }
-        const int bk = (int)(blk % G.nbz), bj = (int)((blk / G.nbz) % G.nby), bi = (int)(blk / ((int64_t)G.nbz * G.nby));
-        const double ox = G.x0 + (double)(bi * B) * G.pitch;
-        const double oy = G.y0 + (double)(bj * B) * G.pitch;
-        const double oz = G.z0 + (double)(bk * B) * G.pitch;
-        // the block's culled list, as the classification left it; cull again if it is not there
-        const uint32_t* list;
-        int len;
-        bool fits = true;
-        int stored = kind[blk] == 0 ? blk_len[blk] : -1;
-        const int64_t soff = stored >= 0 ? (int64_t)blk_off[blk] : 0;
-        if (stored < 0 || soff < 0 || soff + stored > blk_cap) stored = -1;
-        if (stored >= 0) {
-            list = blk_pool + soff;
-            len = stored;
-        } else {
-            const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
-            const uint32_t* plist = pool + sb_off[s];
-            const int plen = sb_len[s];
-            const float half = 0.5f * B;
-            const float cx = G.fx0 + (bi * B + half) * G.fpitch;
-            const float cy = G.fy0 + (bj * B + half) * G.fpitch;
-            const float cz = G.fz0 + (bk * B + half) * G.fpitch;
-            const float R = 1.7320509f * half * G.fpitch;
-            __syncwarp();
-            const int nk = warp_walk(plist, plen, chain, primf, cx, cy, cz, R, G.eps, sl, kCapBlock);
-            __syncwarp();
-            fits = nk <= kCapBlock;
-            list = fits ? sl : plist;
-            len = fits ? nk : plen;
-        }
-        if (work) {  // executed primitive evaluations and their float32 operation count
-            unsigned long long evals = 0, flops = 0;
-            for (int i = lane; i < len; i += 32) {
-                const FbInsn I = chain[list[i] >> 2];
-                const int op = effective_op(list[i], I.op);
-                if (op == CH_OFFSET) { flops += 1; continue; }
-                evals += 1;
-                flops += prim_flops(primf[I.arg].type, primf[I.arg].ident) + (I.k > 0 ? 8 : 1);
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                evals += __shfl_xor_sync(0xffffffffu, evals, o);
-                flops += __shfl_xor_sync(0xffffffffu, flops, o);
-            }
-            if (lane == 0) {
-                atomicAdd(&work[0], evals * kVox);
-                atomicAdd(&work[1], flops * kVox);
-            }
-        }
-        (void)fits;
-        // the list in chunks of kCapBlock localised primitives; between chunks each lane keeps its
-        // partial fold in its own part of the tile (the same float operations in the same order)
-        for (int c0 = 0; c0 == 0 || c0 < len; c0 += kCapBlock) {  // one pass even for an empty list
-            const int clen = max(0, min(kCapBlock, len - c0));
-            const bool first = c0 == 0, last = c0 + clen >= len;
-            __syncwarp();
-            for (int i = lane; i < clen; i += 32) {
-                const uint32_t e = list[c0 + i];
-                const FbInsn I = chain[e >> 2];
-                const int op = effective_op(e, I.op);
-                if (op == CH_OFFSET) {
-                    sp[i].op = op;
-                    sp[i].k = (float)I.k;
-                } else {
-                    localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
-                }
-            }
-            __syncwarp();
-            for (int g = 0; g < kGroups; ++g) {
-                const int v0 = (g * 32 + lane) * VG;
-                const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
-                const float dx = li * G.fpitch, dy = lj * G.fpitch;
-                float dz[VG], acc[VG], v[VG];
-#pragma unroll
-                for (int k = 0; k < VG; ++k) dz[k] = (lk0 + k) * G.fpitch;
-                if (first) {
-#pragma unroll
-                    for (int k = 0; k < VG; ++k) acc[k] = 0.f;
-                } else {
-                    load_group<VG>(out, g * 32 + lane, acc);
-                }
-                for (int i = 0; i < clen; ++i) {
-                    const LocalPrim& P = sp[i];
-                    const int op = P.op;
-                    if (op == CH_OFFSET) {
-#pragma unroll
-                        for (int k = 0; k < VG; ++k) acc[k] -= P.k;
-                        continue;
-                    }
-                    eval_group<VG>(P, dx, dy, dz, v);
-                    combine_group<VG>(op, P.k, acc, v);
-                }
-                if (last) {
-                    // guard band: float64 recheck so the sign never disagrees with the float64 value
-                    bool near = false;
-#pragma unroll
-                    for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
-                    if (near) {
-                        for (int k = 0; k < VG; ++k)
-                            if (!(fabsf(acc[k]) >= G.guard))
-                                acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
-                                                            (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
-                    }
-                }
-                store_group<VG>(out, g * 32 + lane, acc);
-            }
-        }
-    }
+    for (int64_t a = gwarp; a < n_active; a += nwarps)
+        leaf_block<B>(G, prims, primf, chain, pool, sb_off, sb_len, active[a], tiles + a * (B * B * B), work, kind,
+                      blk_off, blk_len, blk_pool, blk_cap, s_prim[warp], s_list[warp]);
 }
 
 // Leaf tiles of a general postfix program: float64 per voxel, no culling.
@@ -1283,56 +1461,63 @@ __global__ void k_slot_map_dev(const int32_t* __restrict__ active, const int32_t
 // block kind elsewhere.  One thread per 16 consecutive z voxels of an (x, y) row: the row's block
 // runs are read as float4 from the tiles (a tile row of B floats is contiguous along z) and the 16
 // bytes leave in one 128-bit store when rows are 16-byte aligned (nz % 16 == 0).
+// Item t of the occupancy pass (one row of 16 z voxels).
+template <int B>
+__device__ __forceinline__ void occupancy_item(const int32_t* __restrict__ kind, const int32_t* __restrict__ slot,
+                                               const float* __restrict__ tiles, int nx, int ny, int nz, int nby,
+                                               int nbz, uint8_t* __restrict__ mask, int64_t t) {
+    constexpr int kB3 = B * B * B;
+    const int chunks = (nz + 15) >> 4;
+    const bool vec = (nz & 15) == 0;
+    const int64_t row = t / chunks;
+    const int c = (int)(t - row * chunks);
+    const int x = (int)(row / ny), y = (int)(row - (int64_t)x * ny);
+    const int z0 = c << 4;
+    const int64_t blk_row = ((int64_t)(x / B) * nby + y / B) * nbz;
+    const int lxy = ((x % B) * B + (y % B)) * B;
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int seg = 0; seg < 16; seg += (B < 16 ? B : 16)) {
+        const int z = z0 + seg;
+        if (z >= nz) continue;  // (not break: the loop stays fully unrolled, w[] in registers)
+        const int64_t blk = blk_row + z / B;
+        const int32_t s = slot[blk];
+        constexpr int kRun = B < 16 ? B : 16;
+        if (s >= 0) {
+            const float4* src = reinterpret_cast<const float4*>(tiles + (int64_t)s * kB3 + lxy + (z % B));
+#pragma unroll
+            for (int q = 0; q < kRun / 4; ++q) {
+                const float4 v = src[q];
+                const int k = seg + 4 * q;  // byte index within the 16
+                const uint32_t bits = (uint32_t)(v.x < 0.f) | ((uint32_t)(v.y < 0.f) << 8) |
+                                      ((uint32_t)(v.z < 0.f) << 16) | ((uint32_t)(v.w < 0.f) << 24);
+                w[k >> 2] = bits;
+            }
+        } else {
+            const uint32_t fill = kind[blk] < 0 ? 0x01010101u : 0u;
+#pragma unroll
+            for (int q = 0; q < kRun / 4; ++q) w[(seg >> 2) + q] = fill;
+        }
+    }
+    uint8_t* dst = mask + row * nz + z0;
+    if (vec) {
+        *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+        const int n = min(16, nz - z0);
+        for (int k = 0; k < n; ++k) {
+            const uint32_t wk = k < 8 ? (k < 4 ? w[0] : w[1]) : (k < 12 ? w[2] : w[3]);
+            dst[k] = (uint8_t)(wk >> (8 * (k & 3)));
+        }
+    }
+}
+
 template <int B>
 __global__ void __launch_bounds__(256) k_occupancy(const int32_t* __restrict__ kind, const int32_t* __restrict__ slot,
                                                    const float* __restrict__ tiles, int nx, int ny, int nz, int nby,
                                                    int nbz, uint8_t* __restrict__ mask) {
-    constexpr int kB3 = B * B * B;
-    const int chunks = (nz + 15) >> 4;
-    const int64_t total = (int64_t)nx * ny * chunks;
-    const bool vec = (nz & 15) == 0;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = t / chunks;
-        const int c = (int)(t - row * chunks);
-        const int x = (int)(row / ny), y = (int)(row - (int64_t)x * ny);
-        const int z0 = c << 4;
-        const int64_t blk_row = ((int64_t)(x / B) * nby + y / B) * nbz;
-        const int lxy = ((x % B) * B + (y % B)) * B;
-        uint32_t w[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-        for (int seg = 0; seg < 16; seg += (B < 16 ? B : 16)) {
-            const int z = z0 + seg;
-            if (z >= nz) continue;  // (not break: the loop stays fully unrolled, w[] in registers)
-            const int64_t blk = blk_row + z / B;
-            const int32_t s = slot[blk];
-            constexpr int kRun = B < 16 ? B : 16;
-            if (s >= 0) {
-                const float4* src = reinterpret_cast<const float4*>(tiles + (int64_t)s * kB3 + lxy + (z % B));
-#pragma unroll
-                for (int q = 0; q < kRun / 4; ++q) {
-                    const float4 v = src[q];
-                    const int k = seg + 4 * q;  // byte index within the 16
-                    const uint32_t bits = (uint32_t)(v.x < 0.f) | ((uint32_t)(v.y < 0.f) << 8) |
-                                          ((uint32_t)(v.z < 0.f) << 16) | ((uint32_t)(v.w < 0.f) << 24);
-                    w[k >> 2] = bits;
-                }
-            } else {
-                const uint32_t fill = kind[blk] < 0 ? 0x01010101u : 0u;
-#pragma unroll
-                for (int q = 0; q < kRun / 4; ++q) w[(seg >> 2) + q] = fill;
-            }
-        }
-        uint8_t* dst = mask + row * nz + z0;
-        if (vec) {
-            *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
-        } else {
-            const int n = min(16, nz - z0);
-            for (int k = 0; k < n; ++k) {
-                const uint32_t wk = k < 8 ? (k < 4 ? w[0] : w[1]) : (k < 12 ? w[2] : w[3]);
-                dst[k] = (uint8_t)(wk >> (8 * (k & 3)));
-            }
-        }
-    }
+    const int64_t total = (int64_t)nx * ny * ((nz + 15) >> 4);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x)
+        occupancy_item<B>(kind, slot, tiles, nx, ny, nz, nby, nbz, mask, t);
 }
 
 // Sum of trunc(v * scale) over negative values, in int64 (determinism-safe checksum,
@@ -1391,7 +1576,7 @@ int launch_compact(const int32_t* kind, int64_t nblocks, int32_t* active, int32_
     const int64_t ntiles = (nblocks + kTile - 1) / kTile;
     FB_CUDA(cudaMemsetAsync(status, 0, ntiles * 8, st));
     FB_CUDA(cudaMemsetAsync(misc, 0, 256, st));
-    k_compact<<<(unsigned)ntiles, 256, 0, st>>>(kind, nblocks, active, count, status, misc, ntiles);
+    k_compact<<<(unsigned)ntiles, 256, 0, st>>>(kind, nblocks, active, count, status, misc, ntiles, kLookbackSpins);
     FB_LAUNCH();
     return FB_OK;
 }
@@ -1429,21 +1614,42 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
                                                                          S.len + G.ncoarse, S.blk_off, S.blk_len,
                                                                          S.blk_pool, P.cap_block);
             FB_LAUNCH();
-            k_classify<true, true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
-                G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
-                S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
+            k_classify_listed<<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+                G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
+                S.blk_pool);
         } else {
-            k_classify<true, false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
-                G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
-                S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
+            // per-block lists come after the compaction, for the active blocks only (k_cull_active)
+            const int grid = (int)std::min<int64_t>(fb_div_up(G.nsuper, kLatWarps), (int64_t)fb_sm_count() * 64);
+            const int64_t* sb_off = S.off + G.ncoarse;
+            const int32_t* sb_len = S.len + G.ncoarse;
+            switch (G.B) {
+            case 4:
+                k_classify_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
+                                                                       kind, cma, S.blk_len);
+                break;
+            case 8:
+                k_classify_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
+                                                                       kind, cma, S.blk_len);
+                break;
+            default:
+                k_classify_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
+                                                                       kind, cma, S.blk_len);
+            }
         }
     } else {
-        k_classify<false, false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
-            G, prims, S.primf, chain, n_chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off,
-            S.blk_len, S.blk_pool, P.blk_cap, S.misc + 2);
+        k_classify_program<<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, chain, n_chain, kind, cma);
     }
     FB_LAUNCH();
-    return launch_compact(kind, G.nblocks, active, count, S.status, S.misc, st);
+    if (int rc = launch_compact(kind, G.nblocks, active, count, S.status, S.misc, st)) return rc;
+    if (mode == 1 && !P.warp_blocks) {
+        // the compaction left misc[2] (the block-list pool cursor) at zero
+        const int grid = fb_sm_count() * 16;
+        k_cull_active<<<grid, 32 * kCullActiveWarps, 0, st>>>(G, chain, S.primf, S.pool, S.off + G.ncoarse,
+                                                              S.len + G.ncoarse, active, count, S.blk_off, S.blk_len,
+                                                              S.blk_pool, P.blk_cap, S.misc + 2);
+        FB_LAUNCH();
+    }
+    return FB_OK;
 }
 
 int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* chain, int n_chain, int mode,
@@ -1486,6 +1692,617 @@ int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* c
     FB_LAUNCH();
     return FB_OK;
 }
+
+// ------------------------------------------------------------------------------------ batched builds
+// Many chain recipes built together: every phase is one launch over a work-list spanning all the
+// recipes (their coarse regions, superblocks, blocks, compaction tiles, active blocks), so small
+// recipes fill the GPU beside large ones and a batch costs about fifteen launches instead of ~9
+// per recipe.  Work-list g of a phase maps to (recipe, item) through the phase's group: the recipes
+// taking part (rec[j]) and the exclusive prefix of their item counts (pre[j]); a warp or thread
+// finds j by binary search.  Static groups (everything fixed by the geometry) are built on the
+// host once per batch; the active-block groups are built on the device after the compaction
+// (k_batch_offsets), which also places every recipe's tiles in the caller's arena in recipe order.
+// Each recipe keeps its own culling scratch and outputs (the FieldBuilder layout); the batch adds
+// one device table of descriptors, the groups, and the compaction state of all recipes.
+struct RecDesc {
+    Geo G;
+    const FbPrim* prims;
+    PrimF* primf;
+    const FbInsn* chain;
+    int32_t n_prims, n_chain;
+    uint32_t* pool;
+    int64_t* off;  // coarse regions then superblocks
+    int32_t* len;
+    int64_t pool_coarse, pool_super;
+    int32_t cap_coarse, cap_super, cap_block, warp_blocks;
+    int32_t* kind;
+    float* cma;
+    int32_t* active;
+    int32_t* count;
+    int32_t* blk_off;
+    int32_t* blk_len;
+    uint32_t* blk_pool;
+    int64_t blk_cap;
+    unsigned long long* status;  // this recipe's compaction status words (batch state)
+    int64_t ntiles;
+    int32_t* slot;  // occupancy: block -> tile slot (n_blocks), nullable
+    uint8_t* mask;  // occupancy mask (nx, ny, nz), nullable
+};
+
+struct Group {  // device arrays of one phase's work-list
+    const int32_t* rec;
+    const int64_t* pre;  // m + 1 entries
+    int32_t m;
+};
+
+// j with pre[j] <= g < pre[j + 1] (g < pre[m]).
+__device__ __forceinline__ int group_find(const Group& W, int64_t g) {
+    int lo = 0, hi = W.m - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (W.pre[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_b_prepare(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    const RecDesc& R = D[W.rec[j]];
+    prepare_prim(R.prims, (int)(g - W.pre[j]), R.primf);
+}
+
+__global__ void k_b_full_list(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    const int64_t i = g - W.pre[j];
+    D[W.rec[j]].pool[i] = (uint32_t)i << 2;
+}
+
+// kLevel 0: coarse regions from the full chain (bounding-ball bounds); 1: superblocks from their
+// coarse region.
+template <int kLevel>
+__global__ void __launch_bounds__(128) k_b_cull(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    const RecDesc& R = D[W.rec[j]];
+    const Geo& G = R.G;
+    const int64_t r = g - W.pre[j];
+    if (kLevel == 0)
+        cull_region<true>(G, R.chain, R.primf, R.pool, nullptr, nullptr, R.n_chain, 1, 1, 1, R.off, R.len,
+                          R.pool_coarse, R.cap_coarse, G.S * G.B * kCoarseDiv, G.ncy, G.ncz, r);
+    else
+        cull_region<false>(G, R.chain, R.primf, R.pool, R.off, R.len, 0, kCoarseDiv, G.ncy, G.ncz, R.off + G.ncoarse,
+                           R.len + G.ncoarse, R.pool_super, R.cap_super, G.S * G.B, G.nsy, G.nsz, r);
+}
+
+__global__ void __launch_bounds__(128) k_b_cull_blocks(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    const RecDesc& R = D[W.rec[j]];
+    cull_block(R.G, R.chain, R.primf, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.blk_off, R.blk_len,
+               R.blk_pool, R.cap_block, g - W.pre[j]);
+}
+
+// Each recipe's thread range is a multiple of 32 (nsuper x threads_per_super), so a warp never
+// spans two recipes.
+__global__ void __launch_bounds__(128, 10) k_b_classify_listed(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    const RecDesc& R = D[W.rec[j]];
+    classify_listed(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind, R.cma,
+                    R.blk_off, R.blk_len, R.blk_pool, g - W.pre[j]);
+}
+
+template <int B>
+__global__ void __launch_bounds__(32 * kLatWarps) k_b_lattice(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    constexpr int P1 = 32 / B + 1;
+    __shared__ LocalPrim s_prim[kLatWarps][kLatChunk];
+    __shared__ float s_val[kLatWarps][P1 * P1 * P1];
+    const int warp = threadIdx.x >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < total; g += nwarps) {
+        const int j = group_find(W, g);
+        const RecDesc& R = D[W.rec[j]];
+        lattice_super<B>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind,
+                         R.cma, R.blk_len, g - W.pre[j], s_prim[warp], s_val[warp]);
+    }
+}
+
+// Compaction of every recipe: tiles are taken from one ticket counter in the group's order, so a
+// recipe's predecessor tiles always hold smaller tickets (already running when a tile waits).
+__global__ void __launch_bounds__(256) k_b_compact(const RecDesc* __restrict__ D, Group W, int* __restrict__ misc,
+                                                   long long spin_limit) {
+    __shared__ int s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&misc[0], 1);
+    __syncthreads();
+    const int j = group_find(W, s_tile);
+    const RecDesc& R = D[W.rec[j]];
+    compact_tile(R.kind, R.G.nblocks, R.active, R.count, R.status, s_tile - W.pre[j], R.ntiles, &misc[1], spin_limit);
+}
+
+// After the compaction: each recipe's tile offset in the arena (recipe order, floats), the tiles it
+// gets (count, clipped to the room left; the overflow flag misc[2] raised when clipped), and the
+// prefixes of the active-block groups: act (lattice recipes, list culling) and leaf[0..2] (B = 4, 8,
+// 16).  One thread: a batch holds a few hundred to a few thousand recipes.
+__global__ void k_batch_offsets(const RecDesc* __restrict__ D, int n, int64_t capacity,
+                                int64_t* __restrict__ tile_off, int32_t* __restrict__ leaf_count,
+                                Group act, int64_t* __restrict__ act_pre, Group l4, int64_t* __restrict__ l4_pre,
+                                Group l8, int64_t* __restrict__ l8_pre, Group l16, int64_t* __restrict__ l16_pre,
+                                Group occ, int64_t* __restrict__ occ_pre, int* __restrict__ misc) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int64_t at = 0;
+    for (int r = 0; r < n; ++r) {
+        const int64_t b3 = (int64_t)D[r].G.B * D[r].G.B * D[r].G.B;
+        const int64_t c = min((int64_t)D[r].count[0], D[r].G.nblocks);
+        const int64_t room = max((int64_t)0, (capacity - at) / b3);
+        const int64_t take = min(c, room);
+        if (take < c) misc[2] = 1;
+        tile_off[r] = at;
+        leaf_count[r] = (int32_t)take;
+        at += take * b3;
+    }
+    int64_t t = 0;
+    for (int j = 0; j < act.m; ++j) {
+        act_pre[j] = t;
+        const RecDesc& R = D[act.rec[j]];
+        t += min((int64_t)R.count[0], R.G.nblocks);
+    }
+    act_pre[act.m] = t;
+    const Group* L[3] = {&l4, &l8, &l16};
+    int64_t* P[3] = {l4_pre, l8_pre, l16_pre};
+    for (int q = 0; q < 3; ++q) {
+        t = 0;
+        for (int j = 0; j < L[q]->m; ++j) {
+            P[q][j] = t;
+            t += leaf_count[L[q]->rec[j]];
+        }
+        P[q][L[q]->m] = t;
+    }
+    t = 0;
+    for (int j = 0; j < occ.m; ++j) {
+        occ_pre[j] = t;
+        t += leaf_count[occ.rec[j]];
+    }
+    occ_pre[occ.m] = t;
+}
+
+// Occupancy of every recipe that carries a mask: slot map (-1, then the slot of each tiled block),
+// then one thread per 16 z voxels (occupancy_item).
+__global__ void k_b_fill_slot(const RecDesc* __restrict__ D, Group W, int64_t total) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    D[W.rec[j]].slot[g - W.pre[j]] = -1;
+}
+
+__global__ void k_b_slot_map(const RecDesc* __restrict__ D, Group W) {
+    const int64_t total = W.pre[W.m];
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+        const int j = group_find(W, g);
+        const RecDesc& R = D[W.rec[j]];
+        const int64_t a = g - W.pre[j];
+        R.slot[R.active[a]] = (int32_t)a;
+    }
+}
+
+template <int B>
+__global__ void __launch_bounds__(256) k_b_occupancy(const RecDesc* __restrict__ D, Group W, int64_t total,
+                                                     const float* __restrict__ tiles,
+                                                     const int64_t* __restrict__ tile_off) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int j = group_find(W, g);
+    const int r = W.rec[j];
+    const RecDesc& R = D[r];
+    const Geo& G = R.G;
+    occupancy_item<B>(R.kind, R.slot, tiles + tile_off[r], G.nx, G.ny, G.nz, G.nby, G.nbz, R.mask, g - W.pre[j]);
+}
+
+__global__ void __launch_bounds__(32 * kCullActiveWarps) k_b_cull_active(const RecDesc* __restrict__ D, Group W,
+                                                                         int* __restrict__ cursors) {
+    __shared__ uint32_t s_list[kCullActiveWarps][kCapActive];
+    const int warp = threadIdx.x >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t total = W.pre[W.m];
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < total; g += nwarps) {
+        const int j = group_find(W, g);
+        const int r = W.rec[j];
+        const RecDesc& R = D[r];
+        cull_active_block(R.G, R.chain, R.primf, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse,
+                          R.active[g - W.pre[j]], R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[r],
+                          s_list[warp]);
+    }
+}
+
+template <int B>
+__global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __restrict__ D, Group W,
+                                                               float* __restrict__ tiles,
+                                                               const int64_t* __restrict__ tile_off,
+                                                               unsigned long long* __restrict__ work) {
+    __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
+    __shared__ uint32_t s_list[kLeafWarps][kCapBlock];
+    const int warp = threadIdx.x >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t total = W.pre[W.m];
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < total; g += nwarps) {
+        const int j = group_find(W, g);
+        const int r = W.rec[j];
+        const RecDesc& R = D[r];
+        const int64_t a = g - W.pre[j];
+        leaf_block<B>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.active[a],
+                      tiles + tile_off[r] + a * (B * B * B), work, R.kind, R.blk_off, R.blk_len, R.blk_pool,
+                      R.blk_cap, s_prim[warp], s_list[warp]);
+    }
+}
+
+// Host plan of a batch: the descriptors, the groups and the batch state in one device allocation
+// made at creation; building enqueues the phases on a stream and allocates nothing.
+struct BatchHost {
+    int n = 0;
+    std::vector<RecDesc> desc;
+    char* dev = nullptr;  // device allocation
+    int64_t dev_bytes = 0;
+    RecDesc* d_desc = nullptr;
+    // static groups and their totals
+    Group prims{}, chain{}, coarse{}, super_{}, wblocks{}, wclass{}, lat[3]{}, tiles{};
+    int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_wblocks = 0, n_wclass = 0, n_lat[3] = {0, 0, 0},
+            n_tiles = 0;
+    // dynamic groups (prefixes written by k_batch_offsets)
+    Group act{}, leaf[3]{}, occ{};
+    int64_t* act_pre = nullptr;
+    int64_t* leaf_pre[3] = {nullptr, nullptr, nullptr};
+    int64_t* occ_pre = nullptr;
+    // occupancy groups (recipes carrying a mask): their blocks, and their rows of 16 z voxels per B
+    Group occ_blocks{}, occ_rows[3]{};
+    int64_t n_occ_blocks = 0, n_occ_rows[3] = {0, 0, 0};
+    unsigned long long* status = nullptr;
+    int* misc = nullptr;     // [0] ticket, [1] wait error, [2] tile overflow
+    int* cursors = nullptr;  // per recipe
+    int64_t* tile_off = nullptr;
+    int32_t* leaf_count = nullptr;
+    int64_t state_bytes = 0;  // status + misc + cursors, cleared per build
+};
+
+int b_index(int B) { return B == 4 ? 0 : (B == 8 ? 1 : 2); }
+
+}  // namespace
+
+extern "C" {
+
+// A batch of chain recipes built together (see the batched-builds section above).  Validates every
+// item as fb_field_build_device would (chain form only), builds the descriptors and work-lists, and
+// makes the batch's one device allocation; synchronises `stream`.  NULL on invalid input or
+// failure.  The items' device buffers must outlive the batch.
+void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcept {
+    if (!items || n < 1) return nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BatchHost* H = new (std::nothrow) BatchHost;
+    if (!H) return nullptr;
+    try {
+        H->n = n;
+        H->desc.resize(n);
+        std::vector<int64_t> tile_pre(n + 1, 0);
+        for (int r = 0; r < n; ++r) {
+            const FbBatchItem& it = items[r];
+            if (!it.geom || !geom_ok(*it.geom) || !it.d_prims || !it.d_chain || it.n_prims < 1 || it.n_chain < 1 ||
+                !it.d_kind || !it.d_cma || !it.d_active || !it.d_count || !it.d_scratch) {
+                delete H;
+                return nullptr;
+            }
+            const Geo G = make_geo(*it.geom);
+            const Plan P = make_plan(G, it.n_prims, it.n_chain);
+            if (it.scratch_len < P.total) {
+                delete H;
+                return nullptr;
+            }
+            const Scratch S = carve(it.d_scratch, P, G);
+            RecDesc& d = H->desc[r];
+            std::memset(&d, 0, sizeof(d));
+            d.G = G;
+            d.prims = it.d_prims;
+            d.primf = S.primf;
+            d.chain = it.d_chain;
+            d.n_prims = it.n_prims;
+            d.n_chain = it.n_chain;
+            d.pool = S.pool;
+            d.off = S.off;
+            d.len = S.len;
+            d.pool_coarse = P.pool_coarse;
+            d.pool_super = P.pool_super;
+            d.cap_coarse = P.cap_coarse;
+            d.cap_super = P.cap_super;
+            d.cap_block = P.cap_block;
+            d.warp_blocks = P.warp_blocks ? 1 : 0;
+            d.kind = it.d_kind;
+            d.cma = it.d_cma;
+            d.active = it.d_active;
+            d.count = it.d_count;
+            d.blk_off = S.blk_off;
+            d.blk_len = S.blk_len;
+            d.blk_pool = S.blk_pool;
+            d.blk_cap = P.blk_cap;
+            d.ntiles = (G.nblocks + kTile - 1) / kTile;
+            d.slot = it.d_slot;
+            d.mask = it.d_mask;
+            if ((d.slot == nullptr) != (d.mask == nullptr) || (d.mask && (reinterpret_cast<uintptr_t>(d.mask) & 15))) {
+                delete H;
+                return nullptr;
+            }
+            tile_pre[r + 1] = tile_pre[r] + d.ntiles;
+        }
+        // host images of the groups: recipe ids and item prefixes
+        struct HostGroup {
+            std::vector<int32_t> rec;
+            std::vector<int64_t> pre{0};
+            void add(int r, int64_t items) {
+                rec.push_back(r);
+                pre.push_back(pre.back() + items);
+            }
+        };
+        HostGroup g_prims, g_chain, g_coarse, g_super, g_wblocks, g_wclass, g_lat[3], g_tiles, g_act, g_leaf[3], g_occ,
+            g_occ_blocks, g_occ_rows[3];
+        for (int r = 0; r < n; ++r) {
+            const RecDesc& d = H->desc[r];
+            const Geo& G = d.G;
+            g_prims.add(r, d.n_prims);
+            g_chain.add(r, d.n_chain);
+            g_coarse.add(r, G.ncoarse);
+            g_super.add(r, G.nsuper);
+            if (d.warp_blocks) {
+                g_wblocks.add(r, G.nblocks);
+                g_wclass.add(r, G.nsuper * threads_per_super(G.S));
+            } else {
+                g_lat[b_index(G.B)].add(r, G.nsuper);
+                g_act.add(r, 0);
+            }
+            g_tiles.add(r, d.ntiles);
+            g_leaf[b_index(G.B)].add(r, 0);
+            if (d.mask) {
+                g_occ.add(r, 0);
+                g_occ_blocks.add(r, G.nblocks);
+                g_occ_rows[b_index(G.B)].add(r, (int64_t)G.nx * G.ny * ((G.nz + 15) / 16));
+            }
+        }
+        // one device allocation: descriptors, groups, dynamic prefixes, cleared state, outputs
+        int64_t at = 0;
+        auto place = [&](int64_t bytes) {
+            const int64_t o = at;
+            at += align256(std::max<int64_t>(bytes, 1));
+            return o;
+        };
+        const int64_t o_desc = place((int64_t)n * sizeof(RecDesc));
+        struct Placed {
+            int64_t rec, pre;
+        };
+        auto place_group = [&](const HostGroup& hg) {
+            Placed q;
+            q.rec = place((int64_t)hg.rec.size() * 4);
+            q.pre = place((int64_t)hg.pre.size() * 8);
+            return q;
+        };
+        HostGroup* statics[] = {&g_prims, &g_chain, &g_coarse, &g_super, &g_wblocks, &g_wclass,
+                                &g_lat[0], &g_lat[1], &g_lat[2], &g_tiles, &g_act, &g_leaf[0], &g_leaf[1], &g_leaf[2],
+                                &g_occ, &g_occ_blocks, &g_occ_rows[0], &g_occ_rows[1], &g_occ_rows[2]};
+        constexpr int kGroups = 19;
+        Placed placed[kGroups];
+        for (int q = 0; q < kGroups; ++q) placed[q] = place_group(*statics[q]);
+        const int64_t o_state = at;
+        const int64_t o_status = place(tile_pre[n] * 8);
+        const int64_t o_misc = place(256);
+        const int64_t o_cursors = place((int64_t)n * 4);
+        H->state_bytes = at - o_state;
+        const int64_t o_tile_off = place((int64_t)n * 8);
+        const int64_t o_leaf_count = place((int64_t)n * 4);
+        H->dev_bytes = at;
+        if (cudaMalloc(&H->dev, H->dev_bytes) != cudaSuccess) {
+            H->dev = nullptr;
+            delete H;
+            return nullptr;
+        }
+        char* D = H->dev;
+        H->d_desc = reinterpret_cast<RecDesc*>(D + o_desc);
+        H->status = reinterpret_cast<unsigned long long*>(D + o_status);
+        H->misc = reinterpret_cast<int*>(D + o_misc);
+        H->cursors = reinterpret_cast<int*>(D + o_cursors);
+        H->tile_off = reinterpret_cast<int64_t*>(D + o_tile_off);
+        H->leaf_count = reinterpret_cast<int32_t*>(D + o_leaf_count);
+        for (int r = 0; r < n; ++r) H->desc[r].status = H->status + tile_pre[r];
+        // host image of the static part, copied in one transfer
+        std::vector<char> image(o_state, 0);
+        std::memcpy(image.data() + o_desc, H->desc.data(), (size_t)n * sizeof(RecDesc));
+        Group* dst[] = {&H->prims, &H->chain, &H->coarse, &H->super_, &H->wblocks, &H->wclass,
+                        &H->lat[0], &H->lat[1], &H->lat[2], &H->tiles, &H->act, &H->leaf[0], &H->leaf[1], &H->leaf[2],
+                        &H->occ, &H->occ_blocks, &H->occ_rows[0], &H->occ_rows[1], &H->occ_rows[2]};
+        for (int q = 0; q < kGroups; ++q) {
+            const HostGroup& hg = *statics[q];
+            std::memcpy(image.data() + placed[q].rec, hg.rec.data(), hg.rec.size() * 4);
+            std::memcpy(image.data() + placed[q].pre, hg.pre.data(), hg.pre.size() * 8);
+            dst[q]->rec = reinterpret_cast<const int32_t*>(D + placed[q].rec);
+            dst[q]->pre = reinterpret_cast<const int64_t*>(D + placed[q].pre);
+            dst[q]->m = (int32_t)hg.rec.size();
+        }
+        H->act_pre = reinterpret_cast<int64_t*>(D + placed[10].pre);
+        for (int q = 0; q < 3; ++q) H->leaf_pre[q] = reinterpret_cast<int64_t*>(D + placed[11 + q].pre);
+        H->occ_pre = reinterpret_cast<int64_t*>(D + placed[14].pre);
+        H->n_occ_blocks = g_occ_blocks.pre.back();
+        for (int q = 0; q < 3; ++q) H->n_occ_rows[q] = g_occ_rows[q].pre.back();
+        H->n_prims = g_prims.pre.back();
+        H->n_chain = g_chain.pre.back();
+        H->n_coarse = g_coarse.pre.back();
+        H->n_super = g_super.pre.back();
+        H->n_wblocks = g_wblocks.pre.back();
+        H->n_wclass = g_wclass.pre.back();
+        for (int q = 0; q < 3; ++q) H->n_lat[q] = g_lat[q].pre.back();
+        H->n_tiles = g_tiles.pre.back();
+        if (cudaMemcpyAsync(D, image.data(), o_state, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            cudaFree(H->dev);
+            delete H;
+            return nullptr;
+        }
+        return H;
+    } catch (...) {
+        if (H->dev) cudaFree(H->dev);
+        delete H;
+        return nullptr;
+    }
+}
+
+// Build every recipe of the batch, stream-ordered, with no host synchronisation and no allocation:
+// culling, classification, compaction, per-block lists, then the leaf tiles of every recipe into
+// d_tiles (capacity floats), recipe r's tiles at tile offset fb_batch_outputs' tile_off[r] (floats),
+// its first leaf_count[r] active blocks (all of them unless the arena ran out; fb_batch_status then
+// reports 8).  Each recipe's kind / cma / active / count land in its own buffers.  ctas_per_sm
+// (1..64; 0 for the default 16) sizes the grids of the active-block passes, whose work is known
+// only on the device.
+int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm,
+                                void* const* events, uint64_t* d_work, void* stream) noexcept;
+
+int fb_batch_build_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm, void* stream) noexcept {
+    return fb_batch_build_timed_device(batch, d_tiles, capacity, ctas_per_sm, nullptr, nullptr, stream);
+}
+
+// The same build with instrumentation: events (nullable; six cudaEvent_t) are recorded on the stream
+// at the start and after the culling levels, the classification, the compaction (with the tile
+// placement), the per-block lists and the leaf tiles; d_work (nullable; two uint64) accumulates the
+// leaf pass's executed primitive evaluations and float32 operations.
+int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm,
+                                void* const* events, uint64_t* d_work, void* stream) noexcept {
+    BatchHost* H = static_cast<BatchHost*>(batch);
+    if (!H || !d_tiles || capacity < 0 || ctas_per_sm > 64) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto mark = [&](int k) -> int {
+        if (events && events[k]) FB_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(events[k]), st));
+        return FB_OK;
+    };
+    unsigned long long* work = reinterpret_cast<unsigned long long*>(d_work);
+    const RecDesc* D = H->d_desc;
+    const int sms = fb_sm_count();
+    const int dyn = sms * (ctas_per_sm > 0 ? ctas_per_sm : 16);  // CTAs of the active-block passes
+    if (int rc = mark(0)) return rc;
+    FB_CUDA(cudaMemsetAsync(H->status, 0, H->state_bytes, st));
+    k_b_prepare<<<fb_div_up(H->n_prims, 128), 128, 0, st>>>(D, H->prims, H->n_prims);
+    FB_LAUNCH();
+    k_b_full_list<<<fb_div_up(H->n_chain, 256), 256, 0, st>>>(D, H->chain, H->n_chain);
+    FB_LAUNCH();
+    k_b_cull<0><<<fb_div_up(H->n_coarse * 32, 128), 128, 0, st>>>(D, H->coarse, H->n_coarse);
+    FB_LAUNCH();
+    k_b_cull<1><<<fb_div_up(H->n_super * 32, 128), 128, 0, st>>>(D, H->super_, H->n_super);
+    FB_LAUNCH();
+    if (int rc = mark(1)) return rc;
+    if (H->n_wblocks) {
+        k_b_cull_blocks<<<fb_div_up(H->n_wblocks * 32, 128), 128, 0, st>>>(D, H->wblocks, H->n_wblocks);
+        FB_LAUNCH();
+        k_b_classify_listed<<<fb_div_up(H->n_wclass, 128), 128, 0, st>>>(D, H->wclass, H->n_wclass);
+        FB_LAUNCH();
+    }
+    for (int q = 0; q < 3; ++q) {
+        if (!H->n_lat[q]) continue;
+        const int grid = (int)std::min<int64_t>(fb_div_up(H->n_lat[q], kLatWarps), (int64_t)sms * 64);
+        if (q == 0) k_b_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[0], H->n_lat[0]);
+        else if (q == 1) k_b_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[1], H->n_lat[1]);
+        else k_b_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[2], H->n_lat[2]);
+        FB_LAUNCH();
+    }
+    if (int rc = mark(2)) return rc;
+    k_b_compact<<<(unsigned)H->n_tiles, 256, 0, st>>>(D, H->tiles, H->misc, kLookbackSpins);
+    FB_LAUNCH();
+    k_batch_offsets<<<1, 32, 0, st>>>(D, H->n, capacity, H->tile_off, H->leaf_count, H->act, H->act_pre, H->leaf[0],
+                                      H->leaf_pre[0], H->leaf[1], H->leaf_pre[1], H->leaf[2], H->leaf_pre[2], H->occ,
+                                      H->occ_pre, H->misc);
+    FB_LAUNCH();
+    if (int rc = mark(3)) return rc;
+    if (H->act.m) {
+        k_b_cull_active<<<dyn, 32 * kCullActiveWarps, 0, st>>>(D, H->act, H->cursors);
+        FB_LAUNCH();
+    }
+    if (int rc = mark(4)) return rc;
+    for (int q = 0; q < 3; ++q) {
+        if (!H->leaf[q].m) continue;
+        if (q == 0) k_b_leaf<4><<<dyn, 32 * kLeafWarps, 0, st>>>(D, H->leaf[0], d_tiles, H->tile_off, work);
+        else if (q == 1) k_b_leaf<8><<<dyn, 32 * kLeafWarps, 0, st>>>(D, H->leaf[1], d_tiles, H->tile_off, work);
+        else k_b_leaf<16><<<dyn, 32 * kLeafWarps, 0, st>>>(D, H->leaf[2], d_tiles, H->tile_off, work);
+        FB_LAUNCH();
+    }
+    return mark(5);
+}
+
+// Device arrays of a batch's outputs: tile_off[n] (int64, floats into the arena) and
+// leaf_count[n] (int32, tiles written per recipe); valid after a build on the build's stream.
+int fb_batch_outputs(void* batch, const int64_t** tile_off, const int32_t** leaf_count) noexcept {
+    BatchHost* H = static_cast<BatchHost*>(batch);
+    if (!H) return FB_INVALID;
+    if (tile_off) *tile_off = H->tile_off;
+    if (leaf_count) *leaf_count = H->leaf_count;
+    return FB_OK;
+}
+
+// Occupancy masks (uint8, 1 where the field is negative) of the recipes whose items carry d_slot /
+// d_mask, from the last build's tiles in d_tiles; stream-ordered after that build, no host
+// synchronisation (5 launches at most).
+int fb_batch_occupancy_device(void* batch, const float* d_tiles, void* stream) noexcept {
+    BatchHost* H = static_cast<BatchHost*>(batch);
+    if (!H || !d_tiles || (reinterpret_cast<uintptr_t>(d_tiles) & 15)) return FB_INVALID;
+    if (!H->occ.m) return FB_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const RecDesc* D = H->d_desc;
+    k_b_fill_slot<<<fb_div_up(H->n_occ_blocks, 256), 256, 0, st>>>(D, H->occ_blocks, H->n_occ_blocks);
+    FB_LAUNCH();
+    k_b_slot_map<<<fb_sm_count() * 8, 256, 0, st>>>(D, H->occ);
+    FB_LAUNCH();
+    for (int q = 0; q < 3; ++q) {
+        const int64_t n = H->n_occ_rows[q];
+        if (!n) continue;
+        const int grid = fb_div_up(n, 256);
+        if (q == 0) k_b_occupancy<4><<<grid, 256, 0, st>>>(D, H->occ_rows[0], n, d_tiles, H->tile_off);
+        else if (q == 1) k_b_occupancy<8><<<grid, 256, 0, st>>>(D, H->occ_rows[1], n, d_tiles, H->tile_off);
+        else k_b_occupancy<16><<<grid, 256, 0, st>>>(D, H->occ_rows[2], n, d_tiles, H->tile_off);
+        FB_LAUNCH();
+    }
+    return FB_OK;
+}
+
+// Launches one build enqueues (the batch's own kernels and its one memset).
+int32_t fb_batch_launches(void* batch) noexcept {
+    BatchHost* H = static_cast<BatchHost*>(batch);
+    if (!H) return -1;
+    int n = 1 + 4 + 2;  // memset; prepare, full list, two cull levels; compaction, offsets
+    if (H->n_wblocks) n += 2;
+    for (int q = 0; q < 3; ++q) n += (H->n_lat[q] ? 1 : 0) + (H->leaf[q].m ? 1 : 0);
+    if (H->act.m) n += 1;
+    return n;
+}
+
+// Status of the last build (synchronises): 0, 6 when a compaction wait gave up, 8 when the tile
+// arena was too small (recipes beyond it got fewer tiles than active blocks).
+int fb_batch_status(void* batch, void* stream) noexcept {
+    BatchHost* H = static_cast<BatchHost*>(batch);
+    if (!H) return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int flags[3] = {0, 0, 0};
+    FB_CUDA(cudaMemcpyAsync(flags, H->misc, 12, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    if (flags[1]) return FB_TIMEOUT;
+    if (flags[2]) return FB_CAPACITY;
+    return FB_OK;
+}
+
+void fb_batch_destroy(void* batch) noexcept {
+    BatchHost* H = static_cast<BatchHost*>(batch);
+    if (!H) return;
+    if (H->dev) cudaFree(H->dev);  // waits for the device's outstanding work first
+    delete H;
+}
+
+}  // extern "C"
+
+namespace {
 
 }  // namespace
 
@@ -1680,6 +2497,34 @@ int fb_sum_i32_device(const int32_t* d_values, int64_t n, int64_t* d_out, void* 
         d_values, n, reinterpret_cast<unsigned long long*>(d_out));
     FB_LAUNCH();
     return FB_OK;
+}
+
+// Test of the compaction's bounded wait: the tile ticket starts at 1, so no CTA takes tile 0 and its
+// status word is never published; tile 1's look-back waits on it, gives up after `spin_limit`
+// sleeps, raises the error flag and publishes its own status, so every later wait ends.  Returns
+// FB_TIMEOUT (6) when the flag was raised, as the product path reports it.  d_scratch: the
+// compaction state of fb_dense_scratch_bytes(n, 1, 1, 1).  Needs n > 2048 (two tiles or more); the
+// active ids written are not meaningful.
+int fb_compact_timeout_probe(const int32_t* d_kind, int64_t n, int32_t* d_active, int32_t* d_count, void* d_scratch,
+                             int64_t scratch_len, int64_t spin_limit, void* stream) noexcept {
+    const int64_t ntiles = (n + kTile - 1) / kTile;
+    if (!d_kind || !d_active || !d_count || !d_scratch || ntiles < 2 || spin_limit < 1 ||
+        scratch_len < fb_dense_scratch_bytes(n, 1, 1, 1))
+        return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* b = static_cast<char*>(d_scratch);
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(b);
+    int* misc = reinterpret_cast<int*>(b + align256(ntiles * 8));
+    const int one = 1;
+    FB_CUDA(cudaMemsetAsync(status, 0, ntiles * 8, st));
+    FB_CUDA(cudaMemsetAsync(misc, 0, 256, st));
+    FB_CUDA(cudaMemcpyAsync(misc, &one, sizeof(int), cudaMemcpyHostToDevice, st));  // ticket starts at tile 1
+    k_compact<<<(unsigned)(ntiles - 1), 256, 0, st>>>(d_kind, n, d_active, d_count, status, misc, ntiles, spin_limit);
+    FB_LAUNCH();
+    int flags[2] = {0, 0};
+    FB_CUDA(cudaMemcpyAsync(flags, misc, 8, cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    return flags[1] ? FB_TIMEOUT : FB_OK;
 }
 
 // Error flag of the last compaction (1 when a bounded wait gave up), read from the scratch.

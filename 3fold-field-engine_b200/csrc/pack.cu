@@ -302,9 +302,11 @@ bool pack_args_ok(const int32_t* shape, int threshold) {
 }
 
 // ------------------------------------------------------------------------------------------ unpack
-// Node sanity exactly as the reference's gather (gather.cpp:20-30): code 3 on a malformed leaf.
-int check_nodes(const PackNode* nodes, int64_t count, int64_t samples, const int32_t* shape) {
-    if (!nodes || count < 1 || count > 33554432 || samples < 1 || samples > 16777216) return 1;
+// Operand sanity exactly as the reference's gather (gather.cpp:11-30): its argument bounds and every
+// leaf's box and payload range.  Any failure of the gather is status 3 of csg_execute
+// (execute.cpp:28), and these checks fail on the first tile, before any output is written.
+int check_nodes(const PackNode* nodes, const void* payload, int64_t count, int64_t samples, const int32_t* shape) {
+    if (!nodes || !payload || count < 1 || count > 33554432 || samples < 1 || samples > 16777216) return 3;
     for (int64_t n = 0; n < count; ++n) {
         const PackNode& node = nodes[n];
         if (node.children[0] >= 0) continue;
@@ -347,50 +349,73 @@ __global__ void __launch_bounds__(256) k_unpack(const PackNode* __restrict__ nod
     }
 }
 
-__global__ void k_cover_check(const unsigned* __restrict__ cover, int64_t n, int* bad) {
+// The reference's csg_execute walks the grid in tiles of 16 x 32 x 16 voxels (x outermost) and stops
+// at the first tile where a gather or a result fails, after writing every earlier tile.  A failure
+// is recorded as the key 2 * tile + (0 gather, 1 non-finite result); the smallest key over all
+// voxels is the reference's stopping point and status (a gather failure precedes the instructions
+// of its own tile).
+__device__ __forceinline__ unsigned long long csg_tile_of(int64_t v, int sy, int sz) {
+    const int64_t x = v / ((int64_t)sy * sz), y = (v / sz) % sy, z = v % sz;
+    const int64_t nty = (sy + 31) / 32, ntz = (sz + 15) / 16;
+    return (unsigned long long)(((x / 16) * nty + y / 32) * ntz + z / 16);
+}
+
+// Voxels covered by no leaf or by several (the gather's gap / overlap) fail their tile's gather.
+__global__ void k_cover_check(const unsigned* __restrict__ cover, int64_t n, int sy, int sz,
+                              unsigned long long* __restrict__ fail) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        if (cover[i] != 1u) { *bad = 1; return; }
+        if (cover[i] != 1u) atomicMin(fail, 2ull * csg_tile_of(i, sy, sz));
 }
 
 // ------------------------------------------------------------------------------------------ CSG
-// Slot-allocated program: inputs are loaded into slots, each instruction reads two slots (or one
-// and an offset) and writes one; slots are reused after a value's last use (host allocation).
-struct SlotInsn {
-    int32_t op, a, b, dst;  // op 0 union, 1 difference, 2 offset, 3 load input `a` into dst
+// Per-voxel program.  Operands are input fields (read from their dense arrays, operand -1 - f) or
+// intermediate slots (operand >= 0); a slot is reused after its value's last use (host allocation),
+// so a left-deep chain needs two slots whatever its length.  Programs with up to kLocalSlots live
+// intermediates keep them in a per-thread array; larger ones in a global array [slot][voxel]
+// (coalesced across the warp), so every program the reference accepts (256 inputs, 1024
+// instructions) runs.
+struct CsgStep {
+    int32_t op, a, b, dst;  // op 0 union, 1 difference, 2 offset
     double offset;
 };
-constexpr int kMaxSlots = 48;
+constexpr int kLocalSlots = 32;
 
+template <bool kGlobal>
+__device__ __forceinline__ float csg_read(const float* const* __restrict__ inputs, const float* slot,
+                                          const float* __restrict__ gslots, int64_t n, int64_t v, int operand) {
+    if (operand < 0) return inputs[-1 - operand][v];
+    return kGlobal ? gslots[operand * n + v] : slot[operand];
+}
+
+template <bool kGlobal>
 __global__ void __launch_bounds__(256) k_csg_program(const float* const* __restrict__ inputs,
-                                                     const SlotInsn* __restrict__ prog, int n_prog, int result_slot,
-                                                     int64_t n, float* __restrict__ out, int* __restrict__ bad) {
-    extern __shared__ SlotInsn s_prog[];
+                                                     const CsgStep* __restrict__ prog, int n_prog, int result,
+                                                     int64_t n, int sy, int sz, float* __restrict__ out,
+                                                     float* __restrict__ gslots, unsigned long long* __restrict__ fail) {
+    extern __shared__ CsgStep s_prog[];
     for (int i = threadIdx.x; i < n_prog; i += blockDim.x) s_prog[i] = prog[i];
     __syncthreads();
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-        float slot[kMaxSlots];
+        float slot[kGlobal ? 1 : kLocalSlots];
         bool finite = true;
+        float r = 0.f;
         for (int i = 0; i < n_prog; ++i) {
-            const SlotInsn I = s_prog[i];
-            float r;
-            if (I.op == 3) {
-                r = inputs[I.a][v];
-                slot[I.dst] = r;
-                continue;
-            }
-            const float a = slot[I.a];
+            const CsgStep I = s_prog[i];
+            const float a = csg_read<kGlobal>(inputs, slot, gslots, n, v, I.a);
             if (I.op == 2) {
                 r = __double2float_rn(__dsub_rn((double)a, I.offset));
             } else {
-                const float b = I.op == 0 ? slot[I.b] : -slot[I.b];
+                const float b0 = csg_read<kGlobal>(inputs, slot, gslots, n, v, I.b);
+                const float b = I.op == 0 ? b0 : -b0;
                 // NumPy's minimum / maximum keep the second operand on equality, signed zeros included
                 r = I.op == 0 ? (a < b ? a : b) : (a > b ? a : b);
             }
             finite &= isfinite(r);
-            slot[I.dst] = r;
+            if (kGlobal) gslots[I.dst * n + v] = r;
+            else slot[I.dst] = r;
         }
-        if (!finite) *bad = 1;
-        out[v] = slot[result_slot];
+        if (!finite) atomicMin(fail, 2ull * csg_tile_of(v, sy, sz) + 1ull);
+        out[v] = kGlobal ? gslots[result * n + v] : slot[result];
     }
 }
 
@@ -456,8 +481,10 @@ __global__ void k_query(const PackNode* __restrict__ nodes, const float* __restr
 }
 
 // ------------------------------------------------------------------------------------------ host
+// One operand's leaves unpacked into its dense array; voxels its leaves cover other than once fail
+// their tile (a field without leaves leaves every voxel uncovered).
 int upload_unpack(const PackNode* nodes, int64_t count, const void* payload, int64_t samples, const int32_t* shape,
-                  uint32_t* d_dense, unsigned* d_cover, int* d_bad, cudaStream_t st) {
+                  uint32_t* d_dense, unsigned* d_cover, unsigned long long* d_fail, cudaStream_t st) {
     std::vector<int64_t> ids, starts;
     int64_t total = 0;
     for (int64_t k = 0; k < count; ++k) {
@@ -466,28 +493,32 @@ int upload_unpack(const PackNode* nodes, int64_t count, const void* payload, int
         starts.push_back(total);
         total += (int64_t)nodes[k].shape[0] * nodes[k].shape[1] * nodes[k].shape[2];
     }
-    if (ids.empty()) return 4;
     const int64_t vox = (int64_t)shape[0] * shape[1] * shape[2];
     PackNode* d_nodes = nullptr;
     int64_t *d_ids = nullptr, *d_starts = nullptr;
     uint32_t* d_payload = nullptr;
     int status = FB_OK;
-    if (cudaMallocAsync(&d_nodes, count * sizeof(PackNode), st) != cudaSuccess ||
-        cudaMallocAsync(&d_ids, ids.size() * 8, st) != cudaSuccess ||
-        cudaMallocAsync(&d_starts, ids.size() * 8, st) != cudaSuccess ||
-        cudaMallocAsync(&d_payload, samples * 4, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_nodes, nodes, count * sizeof(PackNode), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_starts, starts.data(), ids.size() * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_payload, payload, samples * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemsetAsync(d_cover, 0, vox * 4, st) != cudaSuccess)
-        status = FB_RUNTIME;
+    if (cudaMemsetAsync(d_cover, 0, vox * 4, st) != cudaSuccess) return FB_RUNTIME;
+    if (!ids.empty()) {
+        if (cudaMallocAsync(&d_nodes, count * sizeof(PackNode), st) != cudaSuccess ||
+            cudaMallocAsync(&d_ids, ids.size() * 8, st) != cudaSuccess ||
+            cudaMallocAsync(&d_starts, ids.size() * 8, st) != cudaSuccess ||
+            cudaMallocAsync(&d_payload, samples * 4, st) != cudaSuccess ||
+            cudaMemcpyAsync(d_nodes, nodes, count * sizeof(PackNode), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(d_starts, starts.data(), ids.size() * 8, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(d_payload, payload, samples * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            status = FB_RUNTIME;
+        if (!status) {
+            const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)fb_sm_count() * 16);
+            k_unpack<<<std::max(grid, 1), 256, 0, st>>>(d_nodes, d_ids, d_starts, (int)ids.size(), total, d_payload,
+                                                       shape[0], shape[1], shape[2], d_dense, d_cover);
+            if (cudaGetLastError() != cudaSuccess) status = FB_RUNTIME;
+        }
+    }
     if (!status) {
-        const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)fb_sm_count() * 16);
-        k_unpack<<<std::max(grid, 1), 256, 0, st>>>(d_nodes, d_ids, d_starts, (int)ids.size(), total, d_payload,
-                                                   shape[0], shape[1], shape[2], d_dense, d_cover);
         k_cover_check<<<(int)std::min<int64_t>((vox + 255) / 256, (int64_t)fb_sm_count() * 16), 256, 0, st>>>(
-            d_cover, vox, d_bad);
+            d_cover, vox, shape[1], shape[2], d_fail);
         if (cudaGetLastError() != cudaSuccess) status = FB_RUNTIME;
     }
     if (d_nodes) cudaFreeAsync(d_nodes, st);
@@ -495,6 +526,24 @@ int upload_unpack(const PackNode* nodes, int64_t count, const void* payload, int
     if (d_starts) cudaFreeAsync(d_starts, st);
     if (d_payload) cudaFreeAsync(d_payload, st);
     return status;
+}
+
+// Copy the tiles before `stop` (in the reference's tile order) of a dense result into `output`, row
+// by row as the reference writes them (execute.cpp:44-49).
+void copy_tiles_before(const float* dense, const int32_t* shape, uint64_t stop, float* output) {
+    const int sx = shape[0], sy = shape[1], sz = shape[2];
+    uint64_t tile = 0;
+    for (int x = 0; x < sx; x += 16)
+        for (int y = 0; y < sy; y += 32)
+            for (int z = 0; z < sz; z += 16, ++tile) {
+                if (tile >= stop) return;
+                const int hx = std::min(x + 16, sx), hy = std::min(y + 32, sy), len = std::min(z + 16, sz) - z;
+                for (int a = x; a < hx; ++a)
+                    for (int b = y; b < hy; ++b) {
+                        const int64_t index = ((int64_t)a * sy + b) * sz + z;
+                        std::memcpy(output + index, dense + index, len * sizeof(float));
+                    }
+            }
 }
 
 }  // namespace
@@ -591,8 +640,10 @@ const float* fb_pack_payload_device(const void* pointer) noexcept {
 
 // ------------------------------------------------------------------------------------------ CSG ABI
 // Replaces csg_execute, src/field_engine/csg_batch_native_v1/execute.cpp:10-53: same arguments (host
-// pointers to each operand's 52-byte nodes and float32 payload), same statuses 1-5.  The dense
-// output is written only when the whole program succeeded.
+// pointers to each operand's 52-byte nodes and float32 payload), same statuses 1-5: 1 arguments, 2
+// program, 3 any operand gather failure (bounds, malformed leaf, gap, overlap), 4 a non-finite
+// result, 5 a runtime failure.  On 3 / 4 the output holds the tiles the reference would have
+// written before stopping (its 16 x 32 x 16 tile order), and nothing beyond them.
 int csg_execute(const void* const* nodes, const int64_t* counts, const void* const* payload, const int64_t* lengths,
                 int32_t fields, const int32_t* shape, const CsgInsn* program, int32_t instructions,
                 float* output) noexcept {
@@ -619,15 +670,23 @@ int csg_execute(const void* const* nodes, const int64_t* counts, const void* con
             }
         }
         last.back() = instructions;
+        // only the operands the program reads are gathered, as in the reference
         for (int f = 0; f < fields; ++f)
             if (last[f] >= 0) {
-                if (!nodes[f] || !payload[f]) return 1;
-                const int rc = check_nodes(static_cast<const PackNode*>(nodes[f]), counts[f], lengths[f], shape);
+                const int rc = check_nodes(static_cast<const PackNode*>(nodes[f]), payload[f], counts[f], lengths[f],
+                                           shape);
                 if (rc) return rc;
             }
-        // slot allocation: a value's slot is freed after its last use
-        std::vector<SlotInsn> prog;
-        std::vector<int> slot_of(fields + instructions, -1);
+        // operands: inputs by index (-1 - f), intermediates in slots freed after their last use
+        std::vector<CsgStep> prog;
+        std::vector<int> operand(fields + instructions, 0);
+        std::vector<int> used_inputs, input_of(fields, -1);
+        for (int f = 0; f < fields; ++f)
+            if (last[f] >= 0) {
+                input_of[f] = (int)used_inputs.size();
+                used_inputs.push_back(f);
+                operand[f] = -1 - input_of[f];
+            }
         std::vector<int> free_slots;
         int next_slot = 0;
         auto alloc = [&]() -> int {
@@ -638,104 +697,98 @@ int csg_execute(const void* const* nodes, const int64_t* counts, const void* con
             }
             return next_slot++;
         };
-        std::vector<int> used_inputs;
-        for (int f = 0; f < fields; ++f)
-            if (last[f] >= 0) {
-                slot_of[f] = alloc();
-                used_inputs.push_back(f);
-            }
+        auto release = [&](int id) {
+            if (id >= fields) free_slots.push_back(operand[id]);
+        };
         for (int n = 0; n < instructions; ++n) {
             const CsgInsn& p = program[n];
-            SlotInsn s;
+            CsgStep s;
             s.op = p.op;
-            s.a = slot_of[p.left];
-            s.b = p.op == 2 ? 0 : slot_of[p.right];
+            s.a = operand[p.left];
+            s.b = p.op == 2 ? 0 : operand[p.right];
             s.offset = p.op == 2 ? p.offset : 0.0;
-            // free operands whose last use is this instruction (before allocating the result)
-            if (last[p.left] == n) free_slots.push_back(slot_of[p.left]);
-            if (p.op != 2 && p.right != p.left && last[p.right] == n) free_slots.push_back(slot_of[p.right]);
+            // operands whose last use is this instruction give their slot back before the result takes one
+            if (last[p.left] == n) release(p.left);
+            if (p.op != 2 && p.right != p.left && last[p.right] == n) release(p.right);
             s.dst = alloc();
-            slot_of[fields + n] = s.dst;
+            operand[fields + n] = s.dst;
             prog.push_back(s);
+            if (last[fields + n] < 0) free_slots.push_back(s.dst);  // computed (and checked), never read
         }
-        if (next_slot > kMaxSlots) return 5;
-        const int result_slot = slot_of[fields + instructions - 1];
+        const int result_slot = operand[fields + instructions - 1];
+        const bool global_slots = next_slot > kLocalSlots;
         cudaStream_t st = nullptr;
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return 5;
         const int nin = (int)used_inputs.size();
         std::vector<float*> d_fields(nin, nullptr);
         unsigned* d_cover = nullptr;
-        int* d_bad = nullptr;
+        unsigned long long* d_fail = nullptr;
         float** d_ptrs = nullptr;
-        SlotInsn* d_prog = nullptr;
+        CsgStep* d_prog = nullptr;
         float* d_out = nullptr;
+        float* d_slots = nullptr;
         int status = 0;
-        if (cudaMallocAsync(&d_cover, total * 4, st) != cudaSuccess || cudaMallocAsync(&d_bad, 8, st) != cudaSuccess ||
-            cudaMemsetAsync(d_bad, 0, 8, st) != cudaSuccess)
+        if (cudaMallocAsync(&d_cover, total * 4, st) != cudaSuccess || cudaMallocAsync(&d_fail, 8, st) != cudaSuccess ||
+            cudaMemsetAsync(d_fail, 0xff, 8, st) != cudaSuccess)
             status = 5;
-        // loads first, in input order, then the instructions
-        std::vector<SlotInsn> full;
         for (int i = 0; i < nin && !status; ++i) {
             const int f = used_inputs[i];
             if (cudaMallocAsync(&d_fields[i], total * 4, st) != cudaSuccess) { status = 5; break; }
-            const int rc = upload_unpack(static_cast<const PackNode*>(nodes[f]), counts[f], payload[f], lengths[f], shape,
-                                         reinterpret_cast<uint32_t*>(d_fields[i]), d_cover, d_bad, st);
-            if (rc) { status = rc == FB_RUNTIME ? 5 : rc; break; }
-            SlotInsn ld;
-            ld.op = 3;
-            ld.a = i;
-            ld.b = 0;
-            ld.dst = slot_of[f];
-            ld.offset = 0.0;
-            full.push_back(ld);
+            if (upload_unpack(static_cast<const PackNode*>(nodes[f]), counts[f], payload[f], lengths[f], shape,
+                              reinterpret_cast<uint32_t*>(d_fields[i]), d_cover, d_fail, st))
+                status = 5;
         }
-        int bad[2] = {0, 0};
+        if (!status &&
+            (cudaMallocAsync(&d_ptrs, nin * sizeof(float*), st) != cudaSuccess ||
+             cudaMallocAsync(&d_prog, prog.size() * sizeof(CsgStep), st) != cudaSuccess ||
+             cudaMallocAsync(&d_out, total * 4, st) != cudaSuccess ||
+             (global_slots && cudaMallocAsync(&d_slots, (int64_t)next_slot * total * 4, st) != cudaSuccess) ||
+             cudaMemcpyAsync(d_ptrs, d_fields.data(), nin * sizeof(float*), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+             cudaMemcpyAsync(d_prog, prog.data(), prog.size() * sizeof(CsgStep), cudaMemcpyHostToDevice, st) !=
+                 cudaSuccess))
+            status = 5;
+        unsigned long long fail = ~0ull;
         if (!status) {
-            // coverage result of the unpacking (code 4 like the reference's gather)
-            if (cudaMemcpyAsync(bad, d_bad, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            const size_t smem = prog.size() * sizeof(CsgStep);  // <= 1024 x 24 B
+            const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)fb_sm_count() * 8);
+            if (global_slots)
+                k_csg_program<true><<<grid, 256, smem, st>>>(d_ptrs, d_prog, (int)prog.size(), result_slot, total,
+                                                             shape[1], shape[2], d_out, d_slots, d_fail);
+            else
+                k_csg_program<false><<<grid, 256, smem, st>>>(d_ptrs, d_prog, (int)prog.size(), result_slot, total,
+                                                              shape[1], shape[2], d_out, nullptr, d_fail);
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(&fail, d_fail, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
                 cudaStreamSynchronize(st) != cudaSuccess)
                 status = 5;
-            else if (bad[0])
-                status = 4;
         }
         if (!status) {
-            full.insert(full.end(), prog.begin(), prog.end());
-            if (cudaMallocAsync(&d_ptrs, nin * sizeof(float*), st) != cudaSuccess ||
-                cudaMallocAsync(&d_prog, full.size() * sizeof(SlotInsn), st) != cudaSuccess ||
-                cudaMallocAsync(&d_out, total * 4, st) != cudaSuccess ||
-                cudaMemcpyAsync(d_ptrs, d_fields.data(), nin * sizeof(float*), cudaMemcpyHostToDevice, st) !=
-                    cudaSuccess ||
-                cudaMemcpyAsync(d_prog, full.data(), full.size() * sizeof(SlotInsn), cudaMemcpyHostToDevice, st) !=
-                    cudaSuccess)
-                status = 5;
-        }
-        if (!status) {
-            const size_t smem = full.size() * sizeof(SlotInsn);
-            if (smem > 48 * 1024 &&
-                cudaFuncSetAttribute(k_csg_program, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                    cudaSuccess)
-                status = 5;
-            if (!status) {
-                k_csg_program<<<(int)std::min<int64_t>((total + 255) / 256, (int64_t)fb_sm_count() * 8), 256, smem,
-                                st>>>(d_ptrs, d_prog, (int)full.size(), result_slot, total, d_out, d_bad + 1);
-                if (cudaGetLastError() != cudaSuccess ||
-                    cudaMemcpyAsync(bad, d_bad, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            if (fail == ~0ull) {
+                if (cudaMemcpyAsync(output, d_out, total * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
                     cudaStreamSynchronize(st) != cudaSuccess)
                     status = 5;
-                else if (bad[1])
-                    status = 4;
-                else if (cudaMemcpyAsync(output, d_out, total * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-                         cudaStreamSynchronize(st) != cudaSuccess)
-                    status = 5;
+            } else {
+                // the reference's stopping point: the tiles before it are written, then 3 or 4
+                const uint64_t stop = fail >> 1;
+                if (stop > 0) {
+                    std::vector<float> dense(total);
+                    if (cudaMemcpyAsync(dense.data(), d_out, total * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                        cudaStreamSynchronize(st) != cudaSuccess)
+                        status = 5;
+                    else
+                        copy_tiles_before(dense.data(), shape, stop, output);
+                }
+                if (!status) status = (fail & 1ull) ? 4 : 3;
             }
         }
         for (float* d : d_fields)
             if (d) cudaFreeAsync(d, st);
         if (d_cover) cudaFreeAsync(d_cover, st);
-        if (d_bad) cudaFreeAsync(d_bad, st);
+        if (d_fail) cudaFreeAsync(d_fail, st);
         if (d_ptrs) cudaFreeAsync(d_ptrs, st);
         if (d_prog) cudaFreeAsync(d_prog, st);
         if (d_out) cudaFreeAsync(d_out, st);
+        if (d_slots) cudaFreeAsync(d_slots, st);
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
         return status;

@@ -82,8 +82,10 @@ __device__ __forceinline__ float canon_f(int type, const float* __restrict__ p, 
         d = fmaxf(d, (fmaf(p[6], z, -y) - p[2]) * p[10]);
         return d;
     }
-    case P_CAPSULE: {  // p = {bx, by, bz, r, 1/|b|^2 (0 if degenerate)}
-        const float h = fminf(fmaxf(fmaf(x, p[0], fmaf(y, p[1], z * p[2])) * p[4], 0.f), 1.f);
+    case P_CAPSULE: {  // p = {bx, by, bz, r, 1/|b|^2 (0 if degenerate), h_lo, h_hi}
+        // segment h*b for h in [h_lo, h_hi]: [0, 1] in the canonical frame, shifted when the frame
+        // is re-anchored on the segment (block-local records)
+        const float h = fminf(fmaxf(fmaf(x, p[0], fmaf(y, p[1], z * p[2])) * p[4], p[5]), p[6]);
         const float dx = fmaf(-p[0], h, x), dy = fmaf(-p[1], h, y), dz = fmaf(-p[2], h, z);
         return sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - p[3];
     }
@@ -152,6 +154,11 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
 }
 
 // Block-local float32 record of one primitive: L = A * origin + t in float64, rounded once.
+// A capsule's frame is re-anchored at the projection h0 * b of the block origin onto its segment
+// (float64, before rounding): its local coordinates then stay near the block's own size instead of
+// growing with the distance along the segment (a milling sweep is up to ~1.7 length units long, where
+// one float32 ulp is ~1e-7), and the segment becomes [-h0, 1 - h0] * b.  The clamp bound that can be
+// active inside the block is the one near zero, which float32 holds to a relative 6e-8.
 __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double ox, double oy, double oz, int op,
                                          float k, LocalPrim& out) {
     out.type = F.type;
@@ -161,15 +168,28 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     out.s = F.s;
     out.off = F.off;
     const double* A = D.A;
-    out.L[0] = (float)fma(A[0], ox, fma(A[1], oy, fma(A[2], oz, A[3])));
-    out.L[1] = (float)fma(A[4], ox, fma(A[5], oy, fma(A[6], oz, A[7])));
-    out.L[2] = (float)fma(A[8], ox, fma(A[9], oy, fma(A[10], oz, A[11])));
+    double lx = fma(A[0], ox, fma(A[1], oy, fma(A[2], oz, A[3])));
+    double ly = fma(A[4], ox, fma(A[5], oy, fma(A[6], oz, A[7])));
+    double lz = fma(A[8], ox, fma(A[9], oy, fma(A[10], oz, A[11])));
+#pragma unroll
+    for (int j = 0; j < 12; ++j) out.p[j] = F.p[j];
+    if (F.type == P_CAPSULE) {
+        const double bx = D.p[0], by = D.p[1], bz = D.p[2];
+        const double bb = fma(bx, bx, fma(by, by, bz * bz));
+        const double h0 = bb > 0.0 ? fmin(fmax(fma(lx, bx, fma(ly, by, lz * bz)) / bb, 0.0), 1.0) : 0.0;
+        lx = fma(-bx, h0, lx);
+        ly = fma(-by, h0, ly);
+        lz = fma(-bz, h0, lz);
+        out.p[5] = (float)(-h0);
+        out.p[6] = (float)(1.0 - h0);
+    }
+    out.L[0] = (float)lx;
+    out.L[1] = (float)ly;
+    out.L[2] = (float)lz;
     out.L[3] = 0.f;
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
     out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
-#pragma unroll
-    for (int j = 0; j < 12; ++j) out.p[j] = F.p[j];
 }
 
 // ------------------------------------------------------------------------------------ float64

@@ -66,12 +66,12 @@ int fb_sm_count_c() { return fb_sm_count(); }
 
 extern "C" {
 
-// Stream-ordered device-to-device copy between raw device addresses (e.g. out of a build's
-// scratch); synchronises the stream.
+// Stream-ordered copy between raw addresses, device or host (unified addressing picks the
+// direction), e.g. out of a build's scratch; synchronises the stream.
 int fb_copy_device(void* dst, const void* src, int64_t bytes, void* stream) {
     if (!dst || !src || bytes < 0) return 1;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return 2;
+    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st) != cudaSuccess) return 2;
     return cudaStreamSynchronize(st) == cudaSuccess ? 0 : 2;
 }
 

@@ -27,13 +27,14 @@ MAX_AXIS = 512
 MAX_VOXELS = 512 ** 3
 
 
-def validate(mask):
-    """src/field_engine/native_edt_large_v1.py:6-12 with the voxel cap lifted to 512^3."""
+def validate(mask, classes=True):
+    """src/field_engine/native_edt_large_v1.py:6-12 with the voxel cap lifted to 512^3; classes=False
+    leaves the two-class check to the device."""
     if not isinstance(mask, np.ndarray) or mask.dtype != np.bool_:
         raise ValueError('Expected a boolean array')
     if mask.ndim != 3 or min(mask.shape) < 1 or max(mask.shape) > MAX_AXIS or mask.size > MAX_VOXELS:
         raise ValueError('Expected bounded larger 3D shape')
-    if not mask.any() or mask.all():
+    if classes and (not mask.any() or mask.all()):
         raise ValueError('Both classes must be present')
 
 
@@ -153,13 +154,19 @@ class NativeEDTLarge:
             raise RuntimeError('NativeEDTLarge runtime previously failed; no retry')
 
     def squared_distance(self, binary):
+        """The reference's checks and errors; the two-class check runs on the device (the native call
+        counts the classes while packing the mask, status 1 when one is missing) instead of two host
+        scans, and the result lands in page-locked memory from torch's caching host allocator."""
+        import torch
         self._check()
-        validate(binary)
-        source = np.ascontiguousarray(binary, dtype=np.uint8)
-        output = np.empty(source.shape, dtype=np.int32)
+        validate(binary, classes=False)
+        source = binary.view(np.uint8) if binary.flags.c_contiguous else np.ascontiguousarray(binary, dtype=np.uint8)
+        output = torch.empty(source.shape, dtype=torch.int32, pin_memory=True).numpy()
         status = self._library.edt_squared_large(source.ctypes.data, *source.shape, output.ctypes.data)
+        if status == 1:  # the shape passed the host check: one class only
+            raise ValueError('Both classes must be present')
         if status:
-            self._failed = status != 1
+            self._failed = True
             raise RuntimeError(f'Native EDT status {status}')
         return output
 

@@ -272,21 +272,25 @@ def compose(left, right=None, *, operation="union", distance=0.):
         if right is not None or isinstance(distance, (bool, np.bool_)) or not isinstance(distance, Real) \
                 or not np.isfinite(distance):
             raise ValueError("Finite real offset and no second operand required")
-        try:
-            return evaluate([left], [("offset", 0, float(distance))])
-        except ValueError as e:
-            if "Native CSG" in str(e):
-                raise ValueError("Operation exceeds finite float32 range") from None
-            raise
+        return _compose_native(left, None, [("offset", 0, float(distance))])
     if not isinstance(distance, Real) or isinstance(distance, (bool, np.bool_)) or distance != 0:
         raise ValueError("Offset is only valid for the offset operation")
     if not isinstance(right, AdaptiveSampleBlocks):
         raise ValueError("Second adaptive block operand required")
     if left.shape != right.shape or left.pitch != right.pitch or not np.array_equal(left.origin, right.origin):
         raise ValueError("CSG operands must share the exact sampling grid")
+    return _compose_native(left, right, [(operation, 0, 1)])
+
+
+def _compose_native(left, right, program):
+    """One instruction through csg_execute.  The operands are well-formed packed fields, so the only
+    input-dependent failure is a non-finite result (status 4), which the reference reports as the
+    float32 range error (field_csg_blocks_v1.py:40-41); any other status is a native failure."""
     try:
-        return evaluate([left, right], [(operation, 0, 1)])
+        return evaluate([left] if right is None else [left, right], program)
     except ValueError as e:
-        if "Native CSG" in str(e):
+        if str(e) == "Native CSG validation failed: 4":
             raise ValueError("Operation exceeds finite float32 range") from None
+        if str(e).startswith("Native CSG validation failed"):
+            raise RuntimeError(f"compose: native failure ({e})") from None
         raise

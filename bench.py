@@ -1,20 +1,28 @@
 #!/usr/bin/env python3
 """Benchmark of the block-sparse SDF field hot path: one JSON line on rank 0.
 
-Workload (the plain method at scale, synthetic and seeded): a 1024^3 grid (pitch 1/1024, 8^3 leaf
-blocks) built from 3584 primitives (spheres, boxes, capsules, tori in equal numbers) unioned and
-then 512 milling-tool capsules subtracted, plus the exact int32 squared EDT of a 512^3 uint8
-obstacle grid of 2000 random boxes (~8 % fill), distances to the obstacles.  One step = one field
-build (cull + classify + compact + fused leaf evaluation with CSG) + one EDT, inputs resident in HBM.
+Default workload (the metric "leaf Gvox/s batched vs plain at <=1e-5 pitch err; EDT GB/s; serve
+p50/p99 ms", synthetic and seeded): 256 independent recipes -- primitive counts log-uniform in
+[8, 2048], cubic domains drawn from {64, 128, 256, 512}^3, leaf size 4^3 / 8^3 / 16^3 per recipe
+from the autotuner -- built as one batch (culling, classification, compaction, per-block lists and
+fused leaf evaluation with CSG, every phase one launch over all recipes, sizing on the device).
+One step = one build of the whole batch, recipe tables resident in HBM.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
 
-value: leaf voxels produced per second over the whole step (Gvox/s), all ranks.  Each rank builds
-its own replica (the path shards by recipe with no exchange: weak scaling).  Timing: CUDA events
-per step on the launching stream, L2 flushed between steps outside the events, max over ranks.
-`--impl reference` times the reference algorithm on the host cores instead (the CPU oracle port of
-the reference's float64 evaluator and integer EDT, OpenMP, on a bounded sample of the same
-workload, extrapolated to the full workload).
+value: leaf voxels built per second over the whole step (Gvox/s), all ranks.  The same line
+carries the recipe-by-recipe figure of the same batch (the single-build path with its host read of
+the active count) and their ratio, the float64-oracle accuracy of >= 1000 leaf blocks, the batch
+with each recipe followed by occupancy + squared EDT, the exact EDT of a 512^3 obstacle grid (GB/s
+on 13 B/voxel), and a short serving run (Poisson 1000 req/s: p50 / p99).  Each rank builds its own
+replica (independent recipes, no exchange: weak scaling).  Timing: CUDA events on the launching
+stream, a 256 MiB buffer written between steps outside the events, max over ranks.
+`--impl reference` times the reference algorithm on the host cores instead: the CPU oracle port of
+the reference's float64 classification and tile evaluation over a proportional random sample of
+every recipe's blocks (each step), on the same metric.
+`--workload plain` is the plain method at scale (one 1024^3 part of 3584 primitives minus 512
+milling tools, plus the 512^3 EDT); serve / precision / tree / mesh are the other lines.
+`--gpus N` without torchrun starts N ranks itself.
 """
 from __future__ import annotations
 
@@ -36,8 +44,9 @@ sys.path.insert(0, str(REPO))
 METRIC = "leaf Gvox/s batched vs plain at ≤1e-5·pitch err; EDT GB/s; serve p50/p99 ms"
 UNIT = "Gvox/s"
 EDT_BYTES_PER_VOXEL = 13  # 1 B mask + 4 B output + 8 B int32 intermediate round trip
-LAUNCHES_PER_STEP = 10    # prepare, full list, 2 x cull, classify, compact, leaf, 3 x EDT
+LAUNCHES_PER_STEP = 11    # prepare, full list, 2 x cull, classify, compact, list cull, leaf, 3 x EDT
 WORKLOAD = "plain_at_scale_1024^3_3584prims_512tools_B8+edt_512^3_2000boxes"
+BATCH_WORKLOAD = "batched_256_recipes_8-2048prims_64-512^3_autotuned_leaf"
 
 
 def parse():
@@ -52,13 +61,16 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--check-bricks", type=int, default=24, help="precision: bricks checked per level")
-    ap.add_argument("--workload", choices=("plain", "batched", "serve", "precision", "tree", "mesh"), default="plain",
-                    help="plain: the plain method at scale (default line); batched: 256 recipes, plain vs "
-                         "graph-batched; serve: the request loop; precision: float32 vs float64 at mixed pitch; "
-                         "tree: packed adaptive block tree of a dense 512^3 field, built and sampled; "
+    ap.add_argument("--workload", choices=("batched", "plain", "serve", "precision", "tree", "mesh"), default="batched",
+                    help="batched: 256 recipes built as one batch against recipe by recipe (default line); plain: "
+                         "the plain method at scale; serve: the request loop; precision: float32 vs float64 at "
+                         "mixed pitch; tree: packed adaptive block tree of a dense 512^3 field, built and sampled; "
                          "mesh: mesh -> signed distance field stage")
+    ap.add_argument("--no-serve", action="store_true", help="batched: leave out the short serving run")
+    ap.add_argument("--cpu-fraction", type=float, default=0.0005,
+                    help="share of every recipe's blocks in one CPU-baseline / reference-arm sample")
     ap.add_argument("--recipes", type=int, default=256)
-    ap.add_argument("--streams", type=int, default=16, help="batched: streams the graph's branches spread over")
+    ap.add_argument("--streams", type=int, default=16, help="batched: side streams of the per-recipe EDTs")
     ap.add_argument("--rate", type=float, default=1000.0, help="serve: Poisson arrival rate, req/s")
     ap.add_argument("--seconds", type=float, default=5.0, help="serve: arrival window")
     ap.add_argument("--arena-gb", type=float, default=150.0, help="serve: device arena for resident fields and request temporaries (0: none)")
@@ -182,39 +194,10 @@ def traffic_of(kernel):
     return None
 
 
-# ------------------------------------------------------------------------------------------ CPU leg
-def cpu_sample(comp, meta, mask, n_active=None, n_classify=8000, n_tiles=200, seed=0):
-    """Reference-algorithm CPU time of one full step, extrapolated from a bounded sample: float64
-    8-corner classification of n_classify random blocks, leaf evaluation of up to n_tiles of the
-    active blocks among them (every primitive at every point, as the reference kernels do), plus
-    the full integer EDT of the obstacle grid (OpenMP).  When n_active is None it is estimated from
-    the sampled active fraction.  Returns (seconds per step, description, threads, n_active)."""
-    import oracle
-    rng = np.random.default_rng(seed)
-    blocks = np.sort(rng.choice(meta.n_blocks, size=min(n_classify, meta.n_blocks), replace=False)).astype(np.int64)
-    t0 = time.perf_counter()
-    kinds, _ = oracle.classify_blocks(comp.prims, comp.program, meta, blocks)
-    t_cls = (time.perf_counter() - t0) / len(blocks)
-    sampled_active = blocks[kinds == 0]
-    if n_active is None:
-        n_active = int(round(len(sampled_active) / len(blocks) * meta.n_blocks))
-    pick = sampled_active[:n_tiles].astype(np.int32)
-    t_tile = 0.0
-    if len(pick):
-        t0 = time.perf_counter()
-        oracle.tiles_program(comp.prims, comp.program, meta, pick)
-        t_tile = (time.perf_counter() - t0) / len(pick)
-    t0 = time.perf_counter()
-    oracle.edt_squared(1 - mask)  # distance to the obstacles: sites are the nonzero voxels
-    t_edt = time.perf_counter() - t0
-    total = t_cls * meta.n_blocks + t_tile * n_active + t_edt
-    desc = (f"float64 classify of {len(blocks)} random blocks + leaf eval of {len(pick)} sampled active blocks "
-            f"(extrapolated to {meta.n_blocks} blocks / {n_active} active) + full {mask.shape[0]}^3 integer EDT")
-    return total, desc, oracle.threads(), n_active
-
-
 # ------------------------------------------------------------------------------------------ ours
-def run_ours(args, rank, world, local_rank):
+def run_plain(args, rank, world, local_rank):
+    """The plain method at scale: one 1024^3 part (3584 primitives minus 512 milling tools, 8^3
+    leaves) and the 512^3 EDT per step."""
     import torch
     import torch.distributed as dist
     import field_b200.build as B
@@ -344,11 +327,14 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_e2e:
         result["e2e"] = e2e_leg(comp, meta, mask_np, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
-        secs, desc, cores, _ = cpu_sample(comp, meta, mask_np, n_active=n_active)
-        result["cpu_baseline"] = {"value": leaf_voxels / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
-                                  "sample": desc, "seconds_per_step": secs}
+        secs, leaf, ncls, ntile, cores = cpu_batch_sample([(comp, meta)], args.cpu_fraction * 4)
+        result["cpu_baseline"] = {"value": leaf / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+                                  "seconds": secs,
+                                  "sample": f"{args.cpu_fraction * 4:g} of the part's blocks ({ncls}) classified in "
+                                            f"float64, the {ntile} active ones among them evaluated with every "
+                                            f"primitive; leaf voxels per second of that sample (field build only)"}
         # the float64 oracle, as the checker, on a sample of the timed run's leaf tiles
-        result["accuracy"] = leaf_accuracy(comp, meta, builder, tiles, n_active)
+        result["accuracy"] = leaf_accuracy(comp, meta, builder, tiles, n_active, n_blocks=1000)
     return result
 
 
@@ -397,126 +383,381 @@ def e2e_leg(comp, meta, mask_np, dev, steps=2):
 
 # ------------------------------------------------------------------------------------------ reference arm
 def run_reference(args, rank, world):
-    """The reference algorithm on the host cores only (no GPU code on this path)."""
+    """The reference algorithm on the host cores only (no GPU code on this path), on the same
+    workload, metric and unit as our arm: every step is a proportional random sample of the
+    workload's blocks (--cpu-fraction of each recipe's blocks classified in float64, the active ones
+    among them evaluated at every voxel, OpenMP on every host thread), its rate the leaf voxels that
+    step produced over that step's measured time.  Under torchrun rank 0 alone runs."""
     if rank != 0:
         return None
-    comp, meta, mask_np = workload(args.n, args.edt_n)
-    secs, estimates = [], []
-    desc = cores = None
-    for i in range(max(args.warmup, 3) + args.steps):
-        s, desc, cores, n_active = cpu_sample(comp, meta, mask_np, n_classify=4000, n_tiles=100, seed=i)
-        if i >= max(args.warmup, 3):
-            secs.append(s)
-            estimates.append(n_active)
-    sec = float(statistics.median(secs))
-    n_active = int(statistics.median(estimates))
-    leaf_voxels = n_active * meta.block ** 3
-    value = leaf_voxels / sec / 1e9
+    import field_b200.batch as BT
+    W = max(args.warmup, 3)
+    if args.workload == "batched":
+        comps = batch_workload(args.recipes)
+        blocks = reference_leaf_sizes(comps)
+        recipes = [(c, BT.cube_meta(n, b)) for (c, n), b in zip(comps, blocks)]
+        config = {"workload": BATCH_WORKLOAD, "recipes": len(recipes),
+                  "leaf_sizes": {str(b): blocks.count(b) for b in (4, 8, 16)},
+                  "n_blocks": int(sum(m.n_blocks for _, m in recipes))}
+    else:
+        comp, meta, _ = workload(args.n, args.edt_n)
+        recipes = [(comp, meta)]
+        config = {"workload": WORKLOAD + " (field build)", "grid": [meta.nx, meta.ny, meta.nz], "block": meta.block,
+                  "n_blocks": int(meta.n_blocks)}
+    rates, secs = [], []
+    leaf = ncls = ntile = cores = 0
+    for i in range(W + args.steps):
+        sec, leaf, ncls, ntile, cores = cpu_batch_sample(recipes, args.cpu_fraction, seed=i)
+        if i >= W:
+            rates.append(leaf / sec / 1e9)
+            secs.append(sec)
+    value = float(statistics.median(rates))
+    desc = (f"each step {args.cpu_fraction:g} of every recipe's blocks ({ncls} blocks) classified in float64 and "
+            f"the active ones among them ({ntile}) evaluated at every voxel with every primitive (the reference's "
+            f"per-block work), rate = leaf voxels produced / measured step time")
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 evaluator, int32 EDT", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [meta.nx, meta.ny, meta.nz], "block": meta.block,
-                   "n_active_estimate": n_active, "leaf_voxels": leaf_voxels, "edt_grid": list(mask_np.shape)},
+        "warmup": W, "ms_per_step": float(statistics.median(secs)) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 evaluator", "data": "synthetic", "config": config,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
-def run_batched(args):
-    """256 independent recipes (primitive counts log-uniform in [8, 2048], grids from
-    {64, 128, 256, 512}^3, leaf size by the autotuner): the recipe-by-recipe build path against one
-    CUDA-graph replay of the whole batch.  The headline is the field build (culling,
-    classification, compaction, leaf evaluation); the same pair is also timed with each build
-    followed by occupancy rasterisation and the squared EDT of that occupancy."""
-    import torch
+TUNING = REPO / "3fold-field-engine_b200" / "tuning" / "leaf_sizes_b200.json"
+
+
+def reference_leaf_sizes(comps):
+    """Leaf size per recipe from the autotuner's table measured on B200 (the same choice our arm
+    makes), without measuring: buckets missing from the table take 8."""
     import field_b200.batch as BT
+    table = json.loads(TUNING.read_text()) if TUNING.exists() else {}
+    return [int(table.get(BT.Autotuner.bucket(n, len(c.prims)), {}).get("block", 8)) for c, n in comps]
+
+
+# ------------------------------------------------------------------------------------------ batched (default)
+def batch_workload(count):
+    """The batched workload's compiled recipes and grid edges (seeded)."""
     import field_b200.expr as X
     import field_b200.recipes as R
-    torch.cuda.set_device(0)
+    return [(X.compile_recipe(r), n) for r, n, _ in R.batch_recipes(count=count, seed=3)]
+
+
+def cpu_batch_sample(recipes, fraction, seed=0):
+    """The reference algorithm on the host cores over a proportional random sample of the batch:
+    for every recipe, float64 8-corner classification of `fraction` of its blocks (at least one)
+    and float64 leaf evaluation of the active ones among them (every primitive at every point, as
+    the reference's kernels do), OpenMP.  Returns (seconds, leaf voxels produced, blocks classified,
+    blocks evaluated, threads)."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    secs = 0.0
+    leaf = classified = tiled = 0
+    for comp, meta in recipes:
+        k = max(1, int(round(fraction * meta.n_blocks)))
+        blocks = np.sort(rng.choice(meta.n_blocks, size=min(k, meta.n_blocks), replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        kinds, _ = oracle.classify_blocks(comp.prims, comp.program, meta, blocks)
+        act = blocks[kinds == 0].astype(np.int32)
+        if len(act):
+            oracle.tiles_program(comp.prims, comp.program, meta, act)
+        secs += time.perf_counter() - t0
+        leaf += len(act) * meta.block ** 3
+        classified += len(blocks)
+        tiled += len(act)
+    return secs, leaf, classified, tiled, oracle.threads()
+
+
+def batch_accuracy(bb, recipes, n_recipes=40, per=25, seed=8):
+    """Max |d_f32 - d_f64| / pitch and sign disagreements over `per` seeded active blocks of each of
+    `n_recipes` seeded recipes of a built batch (all their voxels, and within 3 pitches of the
+    surface), against the float64 oracle."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    off, cnt = bb.tile_offsets(), bb.leaf_counts()
+    cand = [i for i in range(len(bb)) if cnt[i] > 0]
+    worst = worst_band = 0.0
+    sign = nblk = nvox = 0
+    by_grid = {}
+    for i in sorted(rng.choice(cand, size=min(n_recipes, len(cand)), replace=False)):
+        comp, meta = recipes[int(i)]
+        f = bb.field(int(i), off, cnt)
+        pick = np.sort(rng.choice(f.n_active, size=min(per, f.n_active), replace=False))
+        ids = f.active[:f.n_active].cpu().numpy()[pick].astype(np.int32)
+        got = f.tiles[torch_index(pick, f.tiles.device)].cpu().numpy().astype(np.float64).reshape(len(pick), -1)
+        want = oracle.tiles_program(comp.prims, comp.program, meta, ids).reshape(len(pick), -1)
+        err = np.abs(got - want) / meta.pitch
+        band = np.abs(want) <= 3 * meta.pitch
+        worst = max(worst, float(err.max()))
+        e_band = float(err[band].max()) if band.any() else 0.0
+        worst_band = max(worst_band, e_band)
+        sign += int(np.count_nonzero((got >= 0) != (want >= 0)))
+        nblk += len(pick)
+        nvox += got.size
+        key = f"{meta.nx}/B{meta.block}"
+        by_grid[key] = max(by_grid.get(key, 0.0), float(err.max()))
+    return {"recipes": min(n_recipes, len(cand)), "blocks": nblk, "voxels": nvox,
+            "max_err_pitch": worst, "max_err_pitch_band": worst_band, "max_err_pitch_by_grid": by_grid,
+            "sign_disagreements": sign, "checker": "float64 oracle"}
+
+
+def torch_index(idx, device):
+    import torch
+    return torch.from_numpy(np.asarray(idx, np.int64)).to(device)
+
+
+def edt_extra(steps, flush, dev, check=True):
+    """The exact int32 squared EDT of the 512^3 obstacle grid (2000 boxes, ~8 % fill), distances to
+    the obstacles: CUDA-event time per transform, GB/s on the 13 B/voxel basis, and the result
+    compared with the oracle's bit for bit."""
+    import torch
+    import field_b200._lib as L
+    import field_b200.edt as E
+    import field_b200.recipes as R
+    mask_np = R.obstacle_grid(seed=2, n=512, n_boxes=2000, fill=0.08)
+    mask = torch.from_numpy(mask_np).to(dev)
+    out = torch.empty(mask.shape, dtype=torch.int32, device=dev)
+    scratch = torch.empty(int(L.lib().fb_edt_scratch_bytes(*mask.shape, 0)), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    ts = []
+    for k in range(3 + steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        E.squared_distance_device(mask, sites_nonzero=True, out=out, scratch=scratch, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k >= 3:
+            ts.append(e0.elapsed_time(e1))
+    ms = float(statistics.median(ts))
+    voxels = int(mask.numel())
+    gbs = voxels * EDT_BYTES_PER_VOXEL / (ms * 1e-3) / 1e9
+    peak, src = measured_peaks()
+    res = {"grid": list(mask.shape), "fill": float(mask_np.mean()), "ms": ms, "gbs": gbs, "frac_hbm": gbs / peak,
+           "peak_source": src, "basis": f"{EDT_BYTES_PER_VOXEL} B/voxel (1 B mask, 4 B out, 8 B intermediate)"}
+    if check:
+        import oracle
+        res["bit_exact_vs_oracle"] = bool((out.cpu().numpy() == oracle.edt_squared(1 - mask_np)).all())
+    return res
+
+
+def run_headline(args, rank, world, local_rank):
+    """The batched workload: build timing (value), the recipe-by-recipe figure, the EDT form, the
+    accuracy, the 512^3 EDT, a short serving run, roofline, CPU baseline and end to end."""
+    import torch
+    import torch.distributed as dist
+    import field_b200.batch as BT
+    import field_b200._lib as L
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
     t0 = time.perf_counter()
-    raw = R.batch_recipes(count=args.recipes, seed=3)
-    comps = [(X.compile_recipe(r), n) for r, n, _ in raw]
+    comps = batch_workload(args.recipes)
     t_compile = time.perf_counter() - t0
     t0 = time.perf_counter()
-    tuner = BT.Autotuner()
+    tuner = BT.Autotuner(TUNING if TUNING.exists() else None, device=dev)
+    known = len(tuner.table)
     blocks = tuner.tune(comps)
     t_tune = time.perf_counter() - t0
     recipes = [(c, BT.cube_meta(n, b)) for (c, n), b in zip(comps, blocks)]
+    # a fresh batch: set-up (tables, scratch, work-lists), its first build into the default arena
+    # (grown once if the device reports it too small), graph capture
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    bb = BT.BatchBuilder(recipes, streams=args.streams)
-    t_setup = time.perf_counter() - t0
-    voxels = bb.leaf_voxels
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-
-    def timed(fn, reps):
-        out = []
-        for _ in range(reps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            fn()
-            e1.record()
-            torch.cuda.synchronize()
-            out.append(e0.elapsed_time(e1))
-        return out
-
-    plain = lambda: BT.plain_build(bb.items)
-    timed(plain, max(args.warmup, 3))
-    t_plain = timed(plain, args.steps)
-    bb.capture(edt=False)
-    replay = lambda: bb.replay(edt=False)
-    timed(replay, max(args.warmup, 3))
-    clocks = ClockSampler(0)
+    bb = BT.BatchBuilder(recipes, device=dev, edt=True, streams=args.streams)
+    bb.enqueue(edt=False)
+    grew = bb.ensure_capacity(edt=False)
+    torch.cuda.synchronize()
+    t_first = time.perf_counter() - t0
+    schedule = bb.tune_schedule()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    W = max(args.warmup, 3)
+    warm = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    for _ in range(W):
+        flush.zero_()
+        bb.enqueue_timed(warm)
+    torch.cuda.synchronize()
+    if bb.status() != 0:
+        raise RuntimeError("batched build failed")
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
     clocks.start()
-    t_batch = timed(replay, args.steps)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        bb.enqueue_timed(events[k])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     clk = clocks.stop()
-    assert bb.check_counts()
-    mp, mb = statistics.median(t_plain), statistics.median(t_batch)
-    # the same builds, each followed by occupancy + squared EDT
-    plain_edt = lambda: BT.plain_build(bb.items, bb.edt_scratch[0])
-    timed(plain_edt, max(args.warmup, 3))
-    mpe = statistics.median(timed(plain_edt, args.steps))
-    bb.capture(edt=True)
-    replay_edt = lambda: bb.replay(edt=True)
-    timed(replay_edt, max(args.warmup, 3))
-    mbe = statistics.median(timed(replay_edt, args.steps))
-    hist = {}
-    for b in blocks:
-        hist[str(b)] = hist.get(str(b), 0) + 1
-    accuracy = None
-    if not args.no_cpu:  # the float64 oracle, as the checker, on sampled blocks of sampled recipes
-        rng = np.random.default_rng(8)
-        worst, worst_band, sign, nblk = 0.0, 0.0, 0, 0
-        by_grid = {}
-        for i in sorted(rng.choice(len(bb.items), size=min(24, len(bb.items)), replace=False)):
-            it, (comp, _) = bb.items[int(i)], comps[int(i)]
-            a = leaf_accuracy(comp, it.meta, it.fb, it.tiles, it.capacity, n_blocks=8, seed=int(i))
-            worst, worst_band = max(worst, a["max_err_pitch"]), max(worst_band, a["max_err_pitch_band"])
-            sign += a["sign_disagreements"]
-            nblk += a["blocks"]
-            g = by_grid.setdefault(str(it.meta.nx), 0.0)
-            by_grid[str(it.meta.nx)] = max(g, a["max_err_pitch_band"])
-        accuracy = {"recipes": 24, "blocks": nblk, "max_err_pitch": worst, "max_err_pitch_band": worst_band,
-                    "max_err_pitch_band_by_grid": by_grid, "sign_disagreements": sign, "checker": "float64 oracle"}
-    return {
-        "accuracy": accuracy,
-        "metric": METRIC, "workload": "batched_256_recipes", "value": voxels / (mb * 1e-3) / 1e9, "unit": UNIT,
-        "plain_gvox_s": voxels / (mp * 1e-3) / 1e9, "batched_gvox_s": voxels / (mb * 1e-3) / 1e9,
-        "speedup_batched_vs_plain": mp / mb, "ms_plain": mp, "ms_batched": mb, "steps": args.steps,
-        "recipes": len(recipes), "streams": args.streams, "leaf_voxels": voxels, "recipes_per_s": len(recipes) / (mb * 1e-3),
-        "leaf_sizes": hist, "autotune_s": t_tune, "compile_s": t_compile, "setup_s": t_setup,
-        "with_edt": {"ms_plain": mpe, "ms_batched": mbe, "plain_gvox_s": voxels / (mpe * 1e-3) / 1e9,
-                     "batched_gvox_s": voxels / (mbe * 1e-3) / 1e9, "speedup_batched_vs_plain": mpe / mbe,
-                     "edt_voxels": int(sum(it.meta.nx * it.meta.ny * it.meta.nz for it in bb.items)),
-                     "note": "each build followed by occupancy rasterisation + squared EDT of the occupancy"},
-        "grid_sizes": {str(n): sum(1 for _, m in recipes if m.nx == n) for n in (64, 128, 256, 512)},
-        "clocks": clk, "dtype": "f32 (f64 guard band); int32 EDT", "data": "synthetic",
+    if bb.status() != 0:
+        raise RuntimeError("batched build failed")
+    step_ms = [e[0].elapsed_time(e[5]) for e in events]
+    names = ("cull", "classify", "compact", "lists", "leaf")
+    phases = {nm: float(statistics.median(e[i].elapsed_time(e[i + 1]) for e in events)) for i, nm in enumerate(names)}
+    total_ms = max_over_ranks(float(sum(step_ms)), world, dev)
+    counts = bb.active_counts()
+    leaf_voxels = bb.leaf_voxels
+    value = job_rate(leaf_voxels, world, args.steps, total_ms)
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": W,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 guard band)", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "recipes": len(recipes),
+                   "grid_sizes": {str(n): sum(1 for _, m in recipes if m.nx == n) for n in (64, 128, 256, 512)},
+                   "leaf_sizes": {str(b): blocks.count(b) for b in (4, 8, 16)},
+                   "primitives": int(sum(len(c.prims) for c, _ in comps)), "n_blocks": int(sum(m.n_blocks for _, m in recipes)),
+                   "n_active": int(counts.sum()), "leaf_voxels": leaf_voxels, "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between steps, outside the per-step events"},
+        "phases_ms_median": phases,
+        "batch": {"launches_per_step": bb.launches - (5 + 3 * len(bb)), "schedule_ctas_per_sm": bb.ctas_per_sm,
+                  "schedule_ms": schedule, "arena_grown": bool(grew), "compile_s": t_compile, "autotune_s": t_tune,
+                  "autotune_buckets": {"from_table": known, "measured_now": len(tuner.table) - known,
+                                       "table": tuner.table},
+                  "fresh_batch_first_build_s": t_first},
+        "clocks": clk,
+        "gpu_launches": (bb.launches - (5 + 3 * len(bb))) * args.steps,
     }
+    # the same build from one CUDA graph (captured once)
+    t0 = time.perf_counter()
+    bb.capture(edt=False)
+    result["batch"]["capture_s"] = time.perf_counter() - t0
+    result["batch"]["graph_replay_ms"] = float(statistics.median(timed_device(lambda: bb.replay(edt=False), args.steps, flush)))
+    # recipe by recipe through the single-build path (host read of the count between launches)
+    buf = BT.PlainBuffers(bb.builders, counts)
+    plain = lambda: BT.plain_build(buf)
+    timed_device(plain, W, flush)
+    plain_ms = max_over_ranks(float(statistics.median(timed_device(plain, args.steps, flush))), world, dev)
+    batched_ms = total_ms / args.steps
+    result["plain"] = {"gvox_s": leaf_voxels / (plain_ms * 1e-3) / 1e9, "ms_per_step": plain_ms,
+                       "path": "FieldBuilder.classify + host count read + FieldBuilder.leaf, recipe by recipe"}
+    result["speedup_batched_vs_plain"] = plain_ms / batched_ms
+    # executed work of the leaf pass and the float32 peak (untimed)
+    work = torch.zeros(2, dtype=torch.int64, device=dev)
+    bb.enqueue_timed(warm, work=work)
+    torch.cuda.synchronize()
+    evals, flops = (int(x) for x in work.cpu().numpy())
+    fp32_peak = fp32_probe(dev)
+    hbm_peak, hbm_src = measured_peaks()
+    leaf_tflops = flops / (phases["leaf"] * 1e-3) / 1e12
+    dominant = max(phases, key=phases.get)
+    result["roofline"] = {"kernel": "k_b_leaf<B> (leaf phase)", "bound": "fp32", "achieved": leaf_tflops,
+                          "peak": fp32_peak, "unit": "TFLOP/s", "frac": leaf_tflops / fp32_peak,
+                          "traffic": traffic_of("k_b_leaf"), "dominant_phase": dominant,
+                          "basis": "executed float32 ops of the culled primitive evaluations (FMA = 2) per leaf phase; "
+                                   "peak = FFMA probe measured in this run",
+                          "leaf_evals_per_voxel": evals / max(leaf_voxels, 1),
+                          "leaf_gbs_tile_store": leaf_voxels * 4 / (phases["leaf"] * 1e-3) / 1e9, "hbm_peak": hbm_peak,
+                          "hbm_peak_source": hbm_src}
+    # each recipe followed by occupancy rasterisation + squared EDT of it, both forms
+    buf.slot, buf.mask, buf.edt = bb.slots, bb.masks, bb.edts
+    plain_edt = lambda: BT.plain_build(buf, bb.edt_scratch[0])
+    timed_device(plain_edt, 2, flush)
+    pe = float(statistics.median(timed_device(plain_edt, max(3, args.steps // 2), flush)))
+    bb.capture(edt=True)
+    timed_device(lambda: bb.replay(edt=True), 2, flush)
+    be = float(statistics.median(timed_device(lambda: bb.replay(edt=True), max(3, args.steps // 2), flush)))
+    edt_vox = int(sum(m.nx * m.ny * m.nz for _, m in recipes))
+    result["with_edt"] = {"ms_plain": pe, "ms_batched": be, "plain_gvox_s": leaf_voxels / (pe * 1e-3) / 1e9,
+                          "batched_gvox_s": leaf_voxels / (be * 1e-3) / 1e9, "speedup_batched_vs_plain": pe / be,
+                          "edt_voxels": edt_vox, "edt_gbs_batched": edt_vox * EDT_BYTES_PER_VOXEL / (be * 1e-3) / 1e9,
+                          "note": "each build followed by occupancy rasterisation + squared EDT of the occupancy"}
+    if rank == 0 and not args.no_cpu:
+        result["accuracy"] = batch_accuracy(bb, recipes)
+    if rank == 0 and not args.no_e2e:
+        result["e2e"] = e2e_batched(bb, args.steps)
+    bb.graphs = {}
+    del buf, plain, plain_edt
+    result["edt"] = edt_extra(args.steps, flush, dev, check=(rank == 0 and not args.no_cpu))
+    if rank == 0 and world == 1 and not args.no_cpu:
+        secs, leaf, ncls, ntile, cores = cpu_batch_sample(recipes, args.cpu_fraction)
+        result["cpu_baseline"] = {"value": leaf / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+                                  "seconds": secs,
+                                  "sample": f"{args.cpu_fraction:g} of every recipe's blocks ({ncls} blocks) classified "
+                                            f"in float64, the {ntile} active ones among them evaluated (every "
+                                            f"primitive at every voxel); leaf voxels per second of that sample"}
+    bb.close()
+    del bb
+    gc.collect()
+    torch.cuda.empty_cache()
+    if rank == 0 and not args.no_serve:
+        sv = run_serve(args, rate=1000.0, seconds=2.0, arena_gb=min(getattr(args, "arena_gb", 150.0), 100.0))
+        result["serve"] = {k: sv[k] for k in ("rate_req_s", "seconds", "requests", "throughput_req_s", "p50_ms",
+                                               "p99_ms", "errors", "worst_ms_per_half_second", "by_kind", "slots")}
+    return result
 
 
-def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
+def timed_device(fn, reps, flush):
+    """CUDA-event times (ms) of `reps` calls of fn on the current stream, the L2 flushed before each."""
+    import torch
+    out = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def fp32_probe(dev):
+    """float32 FMA throughput of this GPU (TFLOP/s), best of five probe launches."""
+    import torch
+    import field_b200._lib as L
+    stream = torch.cuda.current_stream()
+    probe = torch.empty(L.lib().fb_sm_count_c() * 8, dtype=torch.float32, device=dev)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nflop = L.lib().fb_fp32_peak_launch(probe.data_ptr(), probe.numel(), 4096, L.stream_handle(stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = max(best, nflop / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def e2e_batched(bb, steps):
+    """The batched build through the public API with host buffers: every step uploads all recipe
+    tables from pinned host memory (one copy), builds, reads each recipe's tile count and offset,
+    and copies the tiles, the block kinds and the active ids into pinned host memory."""
+    import torch
+    off, cnt = bb.tile_offsets(), bb.leaf_counts()
+    used = int((cnt.astype(np.int64) * bb.b3).sum())
+    host_tiles = torch.empty(used, dtype=torch.float32).pin_memory()
+    host_kind = [torch.empty(fb.kind.numel(), dtype=torch.int32).pin_memory() for fb in bb.builders]
+    host_act = [torch.empty(fb.active.numel(), dtype=torch.int32).pin_memory() for fb in bb.builders]
+    times = []
+    d2h = 0
+    for _ in range(max(2, min(steps, 4)) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bb.upload_tables()
+        bb.enqueue(edt=False)
+        off, cnt = bb.tile_offsets(), bb.leaf_counts()   # host reads (synchronise)
+        n = int((cnt.astype(np.int64) * bb.b3).sum())
+        host_tiles[:n].copy_(bb.tiles[:n], non_blocking=True)
+        d2h = n * 4 + 8 * len(bb) + 4 * len(bb)
+        for i, fb in enumerate(bb.builders):
+            host_kind[i].copy_(fb.kind, non_blocking=True)
+            host_act[i][:int(cnt[i])].copy_(fb.active[:int(cnt[i])], non_blocking=True)
+            d2h += fb.kind.numel() * 4 + int(cnt[i]) * 4
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    times = times[1:]
+    sec = float(statistics.median(times))
+    return {"value": n and sum(int(c) * int(b) for c, b in zip(cnt, bb.b3)) / sec / 1e9, "unit": UNIT,
+            "h2d_bytes_per_step": bb.table_bytes, "d2h_bytes_per_step": int(d2h), "seconds_per_step": sec,
+            "api": "field_b200.batch.BatchBuilder (upload_tables, enqueue, tile_offsets / leaf_counts) with pinned "
+                   "host buffers for the tiles, kinds and active ids"}
+
+
+def run_serve(args, rate=1000.0, seconds=10.0, seed=7, arena_gb=None):
     """Poisson arrivals at `rate` req/s for `seconds`: 40 % builds (recipes as the batched
     workload), 30 % edits (1-64 tool capsules subtracted from a resident field), 20 % point queries
     (1e5-1e6 points, value + gradient), 10 % EDT recomputations; latency = completion - arrival.
@@ -541,7 +782,8 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
     # resident field buffers and request temporaries from one arena the size of the budget: no
     # cudaMalloc (or cudaFree, which synchronises the device) on the request path once it is taken
     slots = int(getattr(args, "slots", 16))
-    srv = S.FieldServer(slots=slots, budget_bytes=150e9, arena_bytes=getattr(args, "arena_gb", 150.0) * 1e9)
+    arena_gb = getattr(args, "arena_gb", 150.0) if arena_gb is None else arena_gb
+    srv = S.FieldServer(slots=slots, budget_bytes=150e9, arena_bytes=arena_gb * 1e9)
     try:
         # warm start: a resident field of every grid size, every kernel configured, one EDT per
         # grid size and one query per point-set size (pinned staging of each size allocated once)
@@ -644,7 +886,7 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7):
         "allocator": {k: int(alloc1.get(k, 0) - alloc0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
                                                                            "num_alloc_retries")},
         "resident_gb": round(srv.resident_bytes() / 1e9, 2),
-        "slots": slots, "budget_gb": 150, "arena_gb": getattr(args, "arena_gb", 150.0), "data": "synthetic",
+        "slots": slots, "budget_gb": 150, "arena_gb": arena_gb, "data": "synthetic",
     }
 
 
@@ -857,22 +1099,27 @@ def run_precision(args):
     }
 
 
+def spawn_ranks(n):
+    """`--gpus N` without torchrun: run this command under torch.distributed.run with N ranks (one
+    per GPU, rendezvous on 127.0.0.1) and return its exit status."""
+    import socket
+    import subprocess
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse()
-    if args.workload == "batched":
-        print(json.dumps(run_batched(args)), flush=True)
-        return
-    if args.workload == "precision":
-        print(json.dumps(run_precision(args)), flush=True)
-        return
-    if args.workload == "tree":
-        print(json.dumps(run_tree(args)), flush=True)
-        return
-    if args.workload == "mesh":
-        print(json.dumps(run_mesh(args)), flush=True)
-        return
-    if args.workload == "serve":
-        print(json.dumps(run_serve(args, rate=args.rate, seconds=args.seconds)), flush=True)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
+    if args.impl == "ours" and args.workload in ("serve", "precision", "tree", "mesh"):
+        fn = {"precision": run_precision, "tree": run_tree, "mesh": run_mesh,
+              "serve": lambda a: run_serve(a, rate=a.rate, seconds=a.seconds)}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -889,8 +1136,10 @@ def main():
     try:
         if args.impl == "reference":
             res = run_reference(args, rank, world)
+        elif args.workload == "plain":
+            res = run_plain(args, rank, world, local_rank)
         else:
-            res = run_ours(args, rank, world, local_rank)
+            res = run_headline(args, rank, world, local_rank)
         if rank == 0 and res is not None:
             print(json.dumps(res), flush=True)
     finally:

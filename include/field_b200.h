@@ -6,7 +6,7 @@
  *   - every entry point is extern "C" and noexcept; integer status: 0 ok, 1 invalid input,
  *     2 runtime / CUDA failure, 3-5 the CSG codes of execute.cpp/gather.cpp, 6 a bounded device
  *     wait gave up (the context stays usable), 7 a grid beyond an allocation-free entry point's
- *     fixed scratch;
+ *     fixed scratch, 8 an output arena too small for the result (what fitted is written);
  *   - arguments are validated before any output is written;
  *   - handles are created and destroyed explicitly; a handle that failed stays failed;
  *   - *_device entry points take device pointers and a cudaStream_t (as void*), enqueue their
@@ -63,7 +63,7 @@ int fb_device_arch(void);     /* no reference counterpart: compute capability x1
 int fb_sm_count_c(void);      /* no reference counterpart: SM count of the current device */
 /* No reference counterpart: float32 FMA throughput probe (roofline denominator); returns its flops. */
 int64_t fb_fp32_peak_launch(float* d_out, int blocks, int iters, void* stream);
-/* No reference counterpart: stream-ordered device-to-device copy between raw addresses (synchronises). */
+/* No reference counterpart: stream-ordered copy between raw device or host addresses (synchronises). */
 int fb_copy_device(void* dst, const void* src, int64_t bytes, void* stream);
 
 /* ------------------------------------------------------------------------------------------ EDT */
@@ -99,8 +99,10 @@ int fb_edt_validate_device(const uint8_t* d_mask, int nx, int ny, int nz, void* 
  * every device byte through their own allocator, loops that must never meet cudaMalloc's implicit
  * synchronisation): fb_edt_squared_device without caller scratch -- the scratch is a fixed
  * ~5.1 MiB device array inside this library, so grids are limited to 2^20 voxels and 512 per axis
- * (status 7 beyond that).  The first call on a device resolves the array's address and should come
- * before any stream capture; calls that overlap on the GPU share the array and race.
+ * (status 7 for an axis above 512 or more than 2^20 voxels; status 1 for a null pointer or an axis
+ * below 1).  The first call on a device (and again after a device reset, which maps the array at a
+ * new address) resolves the array's address and should come before any stream capture; calls that
+ * overlap on the GPU share the array and race.
  * fb_edt_noalloc_capacity returns the array's size and writes the voxel limit. */
 int fb_edt_squared_device_noalloc(const uint8_t* d_mask, int nx, int ny, int nz, int sites_nonzero,
                                   int32_t* d_out, void* stream);
@@ -132,6 +134,54 @@ int fb_field_build_device(const fb_geom* g, const fb_prim* d_prims, int32_t n_pr
                           int64_t scratch_len, void* stream);
 /* Status 6 when the last compaction's bounded look-back wait gave up (synchronises). */
 int fb_field_compact_error(const fb_geom* g, int32_t n_prims, int32_t n_chain, const void* d_scratch, void* stream);
+/* Batched builds of many chain recipes, replacing the reference's recipe-by-recipe orchestration
+ * (src/field_engine/faltkarna_v1_g7_fix.py:56-112: classify, host read of the kinds, compaction, tile
+ * evaluation, per part).  Every phase is one launch over a device work-list spanning all recipes;
+ * the active counts, each recipe's place in the tile arena and the active-block work-lists are
+ * formed on the device, so a build has no host synchronisation and allocates nothing (CUDA-graph
+ * capturable).  Each item carries the buffers of one fb_field_build_device call (chain form, mode 1);
+ * they must outlive the batch.  fb_batch_create synchronises its stream and returns NULL on invalid
+ * input.  fb_batch_build_device writes recipe r's tiles at d_tiles + tile_off[r] (floats, recipe
+ * order), leaf_count[r] of its active blocks (all of them unless the arena of `capacity` floats ran
+ * out: fb_batch_status then returns 8; 6 when a compaction wait gave up); ctas_per_sm (0 = 16) sizes
+ * the active-block passes.  fb_batch_outputs gives the device arrays tile_off[n] (int64) and
+ * leaf_count[n] (int32); fb_batch_launches the launches one build enqueues. */
+typedef struct fb_batch_item {
+    const fb_geom* geom;
+    const fb_prim* d_prims;
+    const fb_insn* d_chain;
+    int32_t n_prims, n_chain;
+    int32_t* d_kind;
+    float* d_cma;
+    int32_t* d_active;
+    int32_t* d_count;
+    void* d_scratch;
+    int64_t scratch_len;
+    int32_t* d_slot;  /* nullable; with d_mask (16-byte aligned, nx*ny*nz bytes) the recipe takes part */
+    uint8_t* d_mask;  /* in fb_batch_occupancy_device; d_slot holds n_blocks int32 */
+} fb_batch_item; /* 96 bytes */
+void* fb_batch_create(const fb_batch_item* items, int32_t n, void* stream);
+int fb_batch_build_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm, void* stream);
+/* No reference counterpart: the same build, recording events[0..5] (nullable cudaEvent_t) at its
+ * start and after culling, classification, compaction, per-block lists and leaves, and adding the
+ * leaf pass's executed primitive evaluations and float32 operations to d_work[0..1] (nullable). */
+int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm,
+                                void* const* events, uint64_t* d_work, void* stream);
+int fb_batch_outputs(void* batch, const int64_t** tile_off, const int32_t** leaf_count);
+/* Occupancy masks (1 where the field is negative) of the items that carry d_slot / d_mask, from the
+ * last build's tiles; stream-ordered after it (the reference rasterises occupancy on the host). */
+int fb_batch_occupancy_device(void* batch, const float* d_tiles, void* stream);
+int32_t fb_batch_launches(void* batch);
+int fb_batch_status(void* batch, void* stream);
+void fb_batch_destroy(void* batch);
+
+/* No counterpart in the reference (the reference compacts on the host).  Test of the bounded wait in
+ * the compaction's look-back: runs the compaction kernel over n kinds with tile 0's status never
+ * published and a wait limit of spin_limit sleeps; returns 6 when the wait gave up and raised the
+ * error flag, as the product path reports it.  d_scratch: fb_dense_scratch_bytes(n, 1, 1, 1) bytes;
+ * n > 2048.  The active ids it writes are not meaningful. */
+int fb_compact_timeout_probe(const int32_t* d_kind, int64_t n, int32_t* d_active, int32_t* d_count,
+                             void* d_scratch, int64_t scratch_len, int64_t spin_limit, void* stream);
 
 /* Replace meshsdf_classify_cpu / meshsdf_tiles_cpu, src/field_engine/mesh_sdf_native_v1/field.cpp:229,254,
  * and k_classify_dense / k_eval_tile_dense, src/field_engine/faltkarna_v1_mesh_to_sdf.py:602-657. */

@@ -2,7 +2,7 @@
 
 Run once where the reference is mounted (it is read, never written):
 
-    python tests/golden/make_golden.py [/root/reference]
+    FIELD_REFERENCE=<reference checkout> python tests/golden/make_golden.py   (or the checkout as argv[1])
 
 Sources, all the reference's own:
 * EDT -- the captured arrays of its probes (artifacts/field_edt_integer_v1_arrays.npz,
@@ -26,6 +26,7 @@ from __future__ import annotations
 import hashlib
 import json
 import subprocess
+import os
 import sys
 from pathlib import Path
 
@@ -33,7 +34,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+_ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FIELD_REFERENCE")
+if not _ref_root:
+    sys.exit("set FIELD_REFERENCE (or pass the reference checkout as the first argument)")
+REF = Path(_ref_root)
 FULL_LIMIT = 70000  # voxels up to which expected arrays are stored whole
 
 

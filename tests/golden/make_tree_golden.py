@@ -3,7 +3,7 @@
 
 Run where the reference is mounted (it is read, never written) after `make -C oracle`:
 
-    python tests/golden/make_tree_golden.py [/root/reference]
+    FIELD_REFERENCE=<reference checkout> python tests/golden/make_tree_golden.py   (or the checkout as argv[1])
 
 The reference module itself builds and samples every tree: its `build(wp, dense, pitch)` and
 `AdaptiveBlocks.sample`.  Its one Warp call, the dense block classification
@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 import types
 from pathlib import Path
@@ -26,7 +27,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+_ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FIELD_REFERENCE")
+if not _ref_root:
+    sys.exit("set FIELD_REFERENCE (or pass the reference checkout as the first argument)")
+REF = Path(_ref_root)
 sys.path.insert(0, str(REPO))
 sys.path.insert(0, str(HERE))
 

@@ -39,6 +39,8 @@ def test_record_layouts_match_python():
     assert X.PRIM.itemsize == 216
     assert X.INSN.itemsize == 16
     assert ctypes.sizeof(B.FbGeom) == 64
+    import field_b200.batch as BT
+    assert ctypes.sizeof(BT._Item) == 96  # fb_batch_item
 
 
 def test_product_fails_loudly_without_gpu(monkeypatch):

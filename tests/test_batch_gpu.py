@@ -1,5 +1,5 @@
-"""Batched builds (one CUDA graph over many recipes and streams) equal the recipe-by-recipe path
-bit for bit, and the autotuner picks a timed leaf size per bucket (GPU)."""
+"""Batched builds (one launch per phase over work-lists spanning every recipe) equal the
+recipe-by-recipe path bit for bit, and the autotuner picks a timed leaf size per bucket (GPU)."""
 import numpy as np
 import pytest
 
@@ -18,69 +18,110 @@ def _recipes(count, sizes=(64, 128), seed=13):
     return out
 
 
-def test_graph_batch_equals_plain_builds():
+def _plain_fields(recipes):
+    """Recipe by recipe through the single-build path: (kind, active ids, tiles) on the host."""
+    import field_b200.build as FB
+    out = []
+    for comp, meta in recipes:
+        f = FB.FieldBuilder(comp, meta).build()
+        n = f.n_active
+        out.append((f.kind.cpu().numpy(), f.active[:n].cpu().numpy(), f.tiles[:n].cpu().numpy()))
+    return out
+
+
+def _batch_fields(bb):
+    off, cnt = bb.tile_offsets(), bb.leaf_counts()
+    out = []
+    for i in range(len(bb)):
+        f = bb.field(i, off, cnt)
+        n = f.n_active
+        out.append((f.kind.cpu().numpy(), f.active[:n].cpu().numpy(), f.tiles.cpu().numpy()))
+    return out
+
+
+def test_batch_equals_plain_builds():
+    """One batched build (work-lists over every recipe, device-side sizing) gives every recipe the
+    kinds, ascending active ids and tiles of its own single build, bit for bit -- small grids
+    (warp-culled blocks) and large ones (corner lattice, 256^3 at 4^3 leaves and 512^3 at 8^3)."""
     import torch
     import field_b200.batch as BT
-    recipes = _recipes(12)
-    bb = BT.BatchBuilder(recipes, streams=4)
-    bb.capture()
-    bb.replay()
+    import field_b200.expr as X
+    import field_b200.recipes as R
+    recipes = _recipes(9)
+    for n, b, seed in ((256, 4, 31), (512, 8, 32)):
+        recipe, n_, _ = R.batch_recipes(count=1, seed=seed, sizes=(n,))[0]
+        recipes.append((X.compile_recipe(recipe), BT.cube_meta(n, b)))
+    bb = BT.BatchBuilder(recipes)
+    bb.enqueue()
     torch.cuda.synchronize()
-    assert bb.check_counts()
-    got = [(it.fb.kind.clone(), it.tiles.clone(), it.mask.clone(), it.edt.clone()) for it in bb.items]
-    # recipe by recipe through the single-build path, into the same buffers
-    for it in bb.items:
-        it.tiles.zero_()
-        it.edt.zero_()
-    BT.plain_build(bb.items, bb.edt_scratch[0])
-    for (kind, tiles, mask, edt), it in zip(got, bb.items):
-        assert torch.equal(kind, it.fb.kind)
-        assert torch.equal(tiles, it.tiles)
-        assert torch.equal(mask, it.mask)
-        assert torch.equal(edt, it.edt)
-    # one recipe end to end against the oracle: block kinds and the EDT of the occupancy
+    assert bb.status() == 0
+    got = _batch_fields(bb)
+    want = _plain_fields(recipes)
+    assert any(fb.meta.n_blocks > (1 << 17) for fb in bb.builders)  # the lattice path is covered
+    for i, ((k1, a1, t1), (k2, a2, t2)) in enumerate(zip(got, want)):
+        assert np.array_equal(k1, k2), i
+        assert np.array_equal(a1, a2), i
+        assert t1.tobytes() == t2.tobytes(), i
+    # one small recipe against the oracle
     comp, meta = recipes[0]
-    it = bb.items[0]
     kind, _ = oracle.classify_program(comp.prims, comp.program, meta)
-    assert (it.fb.kind.cpu().numpy() == kind).all()
-    m = it.mask.cpu().numpy()
-    if 0 < m.sum() < m.size:
-        assert (it.edt.cpu().numpy() == oracle.edt_squared(1 - m)).all()
+    assert (got[0][0] == kind).all()
+    bb.close()
 
 
-def test_build_only_graph_equals_plain_builds():
-    """The build-only graph (no occupancy / EDT) gives the same kinds and tiles as the plain
-    build-only path, and a builder made without EDT buffers refuses the EDT form."""
+def test_batch_arena_overflow_is_reported_and_recovered():
     import torch
     import field_b200.batch as BT
-    recipes = _recipes(9, seed=17)
-    bb = BT.BatchBuilder(recipes, streams=3, edt=False)
-    assert all(it.edt is None for it in bb.items)
-    bb.replay(edt=False)
-    torch.cuda.synchronize()
-    assert bb.check_counts()
-    got = [(it.fb.kind.clone(), it.tiles.clone()) for it in bb.items]
-    for it in bb.items:
-        it.tiles.zero_()
-    BT.plain_build(bb.items)
-    for (kind, tiles), it in zip(got, bb.items):
-        assert torch.equal(kind, it.fb.kind)
-        assert torch.equal(tiles, it.tiles)
-    with pytest.raises(ValueError):
-        bb.capture(edt=True)
+    recipes = _recipes(6, seed=19)
+    bb = BT.BatchBuilder(recipes, capacity=1000)
+    bb.enqueue()
+    assert bb.status() == 8
+    counts = bb.active_counts()
+    assert (bb.leaf_counts() <= counts).all() and bb.leaf_counts().sum() < counts.sum()
+    assert bb.ensure_capacity()
+    assert bb.status() == 0
+    assert (bb.leaf_counts() == counts).all()
+    got = _batch_fields(bb)
+    for (k1, a1, t1), (k2, a2, t2) in zip(got, _plain_fields(recipes)):
+        assert np.array_equal(k1, k2) and np.array_equal(a1, a2) and t1.tobytes() == t2.tobytes()
 
 
-def test_replays_are_deterministic():
+def test_graph_replays_equal_eager_builds_and_are_deterministic():
     import torch
     import field_b200.batch as BT
-    bb = BT.BatchBuilder(_recipes(6, seed=21), streams=3)
-    bb.replay()
+    bb = BT.BatchBuilder(_recipes(8, seed=21))
+    bb.enqueue()
     torch.cuda.synchronize()
-    first = [it.tiles.clone() for it in bb.items]
+    eager = [f[2].copy() for f in _batch_fields(bb)]
+    bb.tiles.zero_()
     for _ in range(3):
         bb.replay()
     torch.cuda.synchronize()
-    assert all(torch.equal(a, it.tiles) for a, it in zip(first, bb.items))
+    assert bb.status() == 0
+    assert all(a.tobytes() == f[2].tobytes() for a, f in zip(eager, _batch_fields(bb)))
+    assert bb.launches <= 20
+
+
+def test_batch_with_edt_equals_plain_path():
+    """Each recipe followed by its occupancy and the squared EDT of that occupancy: batched
+    occupancy and side-stream EDTs equal the recipe-by-recipe path, and one EDT the oracle."""
+    import torch
+    import field_b200.batch as BT
+    recipes = _recipes(7, seed=23)
+    bb = BT.BatchBuilder(recipes, edt=True, streams=3)
+    bb.replay(edt=True)
+    torch.cuda.synchronize()
+    assert bb.status() == 0
+    masks = [m.clone() for m in bb.masks]
+    edts = [e.clone() for e in bb.edts]
+    buf = BT.PlainBuffers(bb.builders, bb.active_counts(), edt=True)
+    BT.plain_build(buf, bb.edt_scratch[0])
+    for i in range(len(bb)):
+        assert torch.equal(masks[i], buf.mask[i]), i
+        assert torch.equal(edts[i], buf.edt[i]), i
+    m = masks[0].cpu().numpy()
+    if 0 < m.sum() < m.size:
+        assert (edts[0].cpu().numpy() == oracle.edt_squared(1 - m)).all()
 
 
 def test_autotuner_times_each_bucket(tmp_path):

@@ -128,3 +128,27 @@ def test_checksum_is_deterministic(fb):
     b = fb.checksum_i64(v)
     expect = int(np.sum(np.trunc(v[v < 0].astype(np.float64) * 1e6).astype(np.int64)))
     assert a == b == expect
+
+
+def test_compaction_wait_runs_out_and_reports():
+    """The look-back wait of the compaction is bounded: with tile 0's status never published, tile
+    1's wait gives up after a short limit, raises the error flag (status 6) and the kernel ends;
+    the context stays usable and the product path's compaction is exact right after."""
+    import torch
+    import field_b200._lib as L
+    lib = L.lib()
+    n = 5 * 2048 + 17
+    kind = torch.zeros(n, dtype=torch.int32, device="cuda")
+    active = torch.empty(n, dtype=torch.int32, device="cuda")
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    scratch = torch.empty(int(lib.fb_dense_scratch_bytes(n, 1, 1, 1)), dtype=torch.uint8, device="cuda")
+    rc = lib.fb_compact_timeout_probe(kind.data_ptr(), n, active.data_ptr(), count.data_ptr(), scratch.data_ptr(),
+                                      scratch.numel(), 2000, L.stream_handle())
+    assert rc == 6
+    assert lib.fb_compact_timeout_probe(kind.data_ptr(), 2048, active.data_ptr(), count.data_ptr(),
+                                        scratch.data_ptr(), scratch.numel(), 2000, L.stream_handle()) == 1
+    # the same device compacts correctly afterwards (the dense path's classification + compaction)
+    import field_b200.build as B
+    dense = np.random.default_rng(3).normal(size=(40, 36, 44)).astype(np.float32)
+    r = B.klassificera_och_evaluera_fran_tatt_falt(None, dense, 0.5, 4)
+    assert (r["active_ids"] == np.where(r["kind"] == 0)[0]).all()

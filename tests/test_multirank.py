@@ -52,11 +52,25 @@ def test_reference_arm_under_torchrun_prints_once_from_rank_zero():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(REPO, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--grid", "128", "--edt-n", "64"]
-    out = subprocess.run(cmd, cwd=REPO, capture_output=True, text=True, timeout=600)
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--recipes", "6"]
+    _check_one_reference_line(subprocess.run(cmd, cwd=REPO, capture_output=True, text=True, timeout=600))
+
+
+def _check_one_reference_line(out):
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     res = json.loads(lines[0])
     assert res["impl"] == "reference" and res["n_gpus"] == 2 and res["value"] > 0
     assert res["cpu_baseline"]["kind"] == "port" and res["e2e"]["h2d_bytes_per_step"] == 0
+    # the step time is the measured time of that step's sample, not a projection
+    assert 0 < res["ms_per_step"] < 600_000
+
+
+def test_gpus_flag_without_torchrun_starts_the_ranks_itself():
+    """`bench.py --gpus 2` run directly re-executes itself under torch.distributed.run with two
+    ranks; rank 0 alone prints the reference arm's line."""
+    cmd = [sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "0", "--recipes", "6"]
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    _check_one_reference_line(subprocess.run(cmd, cwd=REPO, capture_output=True, text=True, timeout=600, env=env))
