@@ -80,6 +80,8 @@ SIGNATURES = {
     "fb_query_scratch_bytes": (I64, [P, I64, I]),
     "fb_multires_tiles_device": (I, [P, P, I, I, P, P, D, I, P, P, P, P, I64, P, P, P, F, P, P]),
     "fb_multires_query_device": (I, [P, D, I, P, D, P, P, P, P, P, I64, P, P, P]),
+    "fb_grid_pairs_device": (I, [P, I, P, P, I64, P, P, I, P, P]),
+    "fb_multires_band_device": (I, [P, D, I, P, P, P, P, P, I64, P, P, P, P, P]),
 }
 
 

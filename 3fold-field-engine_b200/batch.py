@@ -3,8 +3,8 @@
 ``BatchBuilder(recipes)`` keeps every recipe's compiled tables, culling scratch and outputs resident
 (one FieldBuilder slab each) and builds them all with ``fb_batch_build_device``: each phase -- the
 float32 mirror of the tables, two culling levels, classification (warp-culled blocks on grids of
-few blocks, the corner lattice on the others), compaction, per-block lists of the active blocks,
-the leaf tiles -- is one launch over a work-list spanning every recipe, so the small recipes fill
+few blocks, the corner lattice with the active blocks' own lists on the others), compaction, the
+leaf tiles -- is one launch over a work-list spanning every recipe, so the small recipes fill
 the GPU beside the large ones.  The active counts, each recipe's place in the tile arena and the
 active-block work-lists are formed on the device: a build has no host synchronisation and
 allocates nothing, and the ~15 launches can be captured into one CUDA graph.  With ``edt=True``
@@ -32,7 +32,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _lib
-from .build import DeviceField, FieldBuilder
+from .build import DeviceField, FieldBuilder, device_table_addresses
 from .expr import Compiled, compile_recipe
 from .grid import GridMeta
 
@@ -122,7 +122,11 @@ class BatchBuilder:
         # a pinned host image: upload_tables() refreshes all of them with one copy
         parts, sizes = [], []
         for comp in comps:
-            for arr in (comp.prims, comp.chain):
+            prims = comp.prims
+            if comp.tables:  # leaf tables live in their own per-device buffers (see device_table_addresses)
+                prims = comp.with_table_addresses(device_table_addresses(comp, self.device,
+                                                                         torch.cuda.current_stream(self.device)))
+            for arr in (prims, comp.chain):
                 b = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
                 parts.append(b)
                 sizes.append((b.nbytes + 255) // 256 * 256)
@@ -229,7 +233,8 @@ class BatchBuilder:
 
     def enqueue_timed(self, events, work=None, stream=None, edt=False):
         """enqueue() recording six torch CUDA events at the phase boundaries (start, culling,
-        classification, compaction, per-block lists, leaves); `work` (int64[2] device tensor) adds
+        classification with the active blocks' lists, compaction, an empty phase, leaves); `work`
+        (int64[2] device tensor) adds
         the leaf pass's executed evaluations and float32 operations."""
         import torch
         st = stream if stream is not None else torch.cuda.current_stream(self.device)

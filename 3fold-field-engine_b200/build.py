@@ -91,8 +91,9 @@ def device_tables(comp: Compiled, device, stream, *, alloc=None, pinned=None):
         insns = comp.chain if mode == 1 else comp.program
         if len(comp.prims) < 1:
             raise ValueError("recipe has no primitive")
-        _validate_program(comp.prims, insns, mode)
-        host = [np.ascontiguousarray(comp.prims).view(np.uint8).reshape(-1),
+        _validate_program(comp.prims, insns, mode, len(comp.tables))
+        prims = comp.with_table_addresses(device_table_addresses(comp, device, stream)) if comp.tables else comp.prims
+        host = [np.ascontiguousarray(prims).view(np.uint8).reshape(-1),
                 np.ascontiguousarray(insns).view(np.uint8).reshape(-1)]
         handles = []
         with torch.cuda.stream(stream):
@@ -119,6 +120,25 @@ def device_tables(comp: Compiled, device, stream, *, alloc=None, pinned=None):
     dprims, dchain, done = cache[key][:3]
     stream.wait_event(done)
     return dprims, dchain
+
+
+def device_table_addresses(comp: Compiled, device, stream):
+    """Device addresses of comp's leaf tables (float32, 256-byte aligned in one buffer), uploaded once
+    per device and kept on the Compiled object; `stream` is made to wait for the upload."""
+    import torch
+    cache = comp.__dict__.setdefault("_device_table_data", {})
+    key = str(device)
+    if key not in cache:
+        sizes = [(t.nbytes + 255) // 256 * 256 for t in comp.tables]
+        buf = torch.empty(max(sum(sizes), 256), dtype=torch.uint8, device=device)
+        addrs, at = [], 0
+        with torch.cuda.stream(stream):
+            for t, size in zip(comp.tables, sizes):
+                buf[at:at + t.nbytes].copy_(torch.from_numpy(t.view(np.uint8).reshape(-1)))
+                addrs.append(buf.data_ptr() + at)
+                at += size
+        cache[key] = (buf, addrs)
+    return cache[key][1]
 
 
 def _give_back_all(pinned, handles):
@@ -159,10 +179,12 @@ class FieldBuilder:
         self.n_chain = len(insns)
         if self.n_prims < 1:
             raise ValueError("recipe has no primitive")
+        if guard is None and c.tables:  # float32 table samples carry more error than the default band
+            guard = max(meta.guard(), c.sampling_guard())
         self.geom = geom_of(meta, guard)
         if tables is not None:
             # the caller placed the tables on the device (e.g. a batch's table arena); still checked
-            _validate_program(c.prims, insns, self.mode)
+            _validate_program(c.prims, insns, self.mode, len(c.tables))
             self.prims, self.chain = tables
             if self.prims.numel() != c.prims.nbytes or self.chain.numel() != insns.nbytes:
                 raise ValueError("device tables do not match the compiled recipe")
@@ -238,10 +260,18 @@ class FieldBuilder:
         return DeviceField(self.meta, self.kind, self.cma, self.active, self.count, tiles, n)
 
 
-def _validate_program(prims, insns, mode):
+def _validate_program(prims, insns, mode, n_tables=0):
     """Every instruction names a valid operation and, where it reads one, an existing primitive;
-    the device kernels index the primitive table with these arguments unchecked."""
+    the device kernels index the primitive table with these arguments unchecked.  Primitive kinds
+    are known ones and every table-backed record names an existing table."""
     n = len(prims)
+    if len(prims) and ((prims["type"] < X.P_SPHERE) | (prims["type"] > X.P_XBORE)).any():
+        raise ValueError("unknown primitive kind")
+    tab = np.isin(prims["type"], X.TABLE_KINDS)
+    if tab.any():
+        idx = prims["p"][tab, 9]
+        if ((idx < 0) | (idx >= n_tables) | (idx != np.floor(idx))).any():
+            raise ValueError("table-backed primitive names no table")
     ops = insns["op"]
     args = insns["arg"]
     if mode == 1:

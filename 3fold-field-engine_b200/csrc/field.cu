@@ -218,6 +218,18 @@ __device__ void prepare_prim(const FbPrim* __restrict__ prims, int i, PrimF* __r
         F.p[6] = 1.f;
         break;
     }
+    case P_GRID:
+    case P_REVOLVE:
+    case P_POCKET: {
+        // no Lipschitz bound (a table's jump to 1e6 outside its grid, the arch's vertical tangents):
+        // an unbounded interval, so these elements are never culled and never cull another
+        canon = 1.0e30;
+        for (int j = 0; j < 10; ++j) F.p[j] = (float)p[j];
+        const unsigned long long t = (unsigned long long)__double_as_longlong(p[10]);  // table address
+        F.p[10] = __uint_as_float((unsigned)(t & 0xffffffffull));
+        F.p[11] = __uint_as_float((unsigned)(t >> 32));
+        break;
+    }
     default:
         for (int j = 0; j < 12; ++j) F.p[j] = (float)p[j];
     }
@@ -551,6 +563,68 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
     return n;
 }
 
+// The same walk by one thread (per-block lists in the lattice classification): the lanes of a warp
+// walk the same superblock list together, so its loads are broadcasts.
+__device__ int seq_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn* __restrict__ chain,
+                        const PrimF* __restrict__ primf, float cx, float cy, float cz, float R, float eps,
+                        uint32_t* __restrict__ out, int cap) {
+    float alo = 0.f, ahi = 0.f;
+    int n = 0;
+    int i = 0;
+    while (i < n_in) {
+        const Elem head = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, false);
+        if (!runnable(head.op, head.k)) {
+            const Elem E = load_elem(in, i, chain, primf, cx, cy, cz, R, eps, true);
+            float plo = E.lo, phi = E.hi;  // back to the primitive's own bounds
+            if (E.op == CH_SUBTRACT || E.op == CH_SETNEG) { plo = -E.hi; phi = -E.lo; }
+            const int act = interval_step(E.op, E.k, plo, phi, alo, ahi);
+            if (act) {
+                uint32_t rec = E.ent;
+                if (act == 2) { n = 0; rec = (E.ent & ~3u) | 1u; }
+                if (act == 3) { n = 0; rec = (E.ent & ~3u) | 2u; }
+                if (n < cap) out[n] = rec;
+                ++n;
+            }
+            ++i;
+            continue;
+        }
+        const int op = head.op;
+        // pass 1: the run's end and its aggregate bound in one traversal
+        float agg = op == CH_UNION ? 3.0e38f : -3.0e38f;
+        int j = i;
+        while (j < n_in) {
+            const Elem E = load_elem(in, j, chain, primf, cx, cy, cz, R, eps, true);
+            if (j > i && !(E.op == op && runnable(E.op, E.k))) break;
+            agg = op == CH_UNION ? fminf(agg, E.hi) : fmaxf(agg, E.lo);
+            ++j;
+        }
+        const RunState rs = run_decide(op, agg, alo, ahi);
+        if (rs.reset) n = 0;
+        bool first = rs.reset;
+        float klo = 3.0e38f, khi = -3.0e38f;
+        for (int e = i; e < j; ++e) {
+            const Elem E = load_elem(in, e, chain, primf, cx, cy, cz, R, eps, true);
+            if (!run_keep(op, E, rs.bound)) continue;
+            klo = fminf(klo, E.lo);
+            khi = fmaxf(khi, E.hi);
+            uint32_t rec = E.ent;
+            if (first) rec = (E.ent & ~3u) | (op == CH_SUBTRACT ? 2u : 1u);
+            first = false;
+            if (n < cap) out[n] = rec;
+            ++n;
+        }
+        if (op == CH_UNION) {
+            alo = rs.reset ? klo : fminf(alo, klo);
+            ahi = rs.bound;
+        } else {
+            alo = rs.bound;
+            ahi = rs.reset ? khi : fmaxf(ahi, khi);
+        }
+        i = j;
+    }
+    return n;
+}
+
 // Level cull.  Regions of `edge` voxels on a (rnx, rny, rnz) grid; parent region = coords / div
 // on a (pnx, pny, pnz) grid (parent_off == nullptr: the single full list [0, n_full)).
 template <bool kBall>
@@ -629,65 +703,6 @@ __global__ void __launch_bounds__(128) k_cull_blocks(Geo G, const FbInsn* __rest
     const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (b >= G.nblocks) return;
     cull_block(G, chain, primf, pool, sb_off, sb_len, blk_off, blk_len, blk_pool, cap, b);
-}
-
-// Per-block lists of the active blocks of a lattice-classified grid: a warp per active block culls
-// its superblock's list to the block (the same walk as k_cull_blocks) into shared memory, then
-// reserves room in blk_pool with one atomic and copies it there.  A list longer than kCapActive, or
-// one that finds the pool full, is not stored (blk_len stays -1: the leaf pass culls that block
-// itself, and queries use the superblock list -- exact, only slower).
-constexpr int kCapActive = 256;
-constexpr int kCullActiveWarps = 4;
-
-// One active block's list (every lane of the warp calls it with the same block b).
-__device__ void cull_active_block(const Geo& G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
-                                  const uint32_t* __restrict__ pool, const int64_t* __restrict__ sb_off,
-                                  const int32_t* __restrict__ sb_len, int64_t b, int32_t* __restrict__ blk_off,
-                                  int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int64_t blk_cap,
-                                  int* __restrict__ cursor, uint32_t* sl) {
-    const int lane = threadIdx.x & 31;
-    if (b < 0 || b >= G.nblocks) return;
-    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
-    const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
-    const float half = 0.5f * G.B;
-    const float cx = G.fx0 + (bi * G.B + half) * G.fpitch;
-    const float cy = G.fy0 + (bj * G.B + half) * G.fpitch;
-    const float cz = G.fz0 + (bk * G.B + half) * G.fpitch;
-    const float R = 1.7320509f * half * G.fpitch;
-    __syncwarp();
-    const int nk = warp_walk(pool + sb_off[s], sb_len[s], chain, primf, cx, cy, cz, R, G.eps, sl, kCapActive);
-    __syncwarp();
-    if (nk > kCapActive) return;
-    int slot = 0;
-    if (lane == 0) slot = atomicAdd(cursor, nk);
-    slot = __shfl_sync(0xffffffffu, slot, 0);
-    if ((int64_t)slot + nk > blk_cap) return;
-    for (int i = lane; i < nk; i += 32) blk_pool[slot + i] = sl[i];
-    if (lane == 0) {
-        blk_off[b] = slot;
-        blk_len[b] = nk;
-    }
-}
-
-__global__ void __launch_bounds__(32 * kCullActiveWarps) k_cull_active(Geo G, const FbInsn* __restrict__ chain,
-                                                                      const PrimF* __restrict__ primf,
-                                                                      const uint32_t* __restrict__ pool,
-                                                                      const int64_t* __restrict__ sb_off,
-                                                                      const int32_t* __restrict__ sb_len,
-                                                                      const int32_t* __restrict__ active,
-                                                                      const int32_t* __restrict__ count,
-                                                                      int32_t* __restrict__ blk_off,
-                                                                      int32_t* __restrict__ blk_len,
-                                                                      uint32_t* __restrict__ blk_pool, int64_t blk_cap,
-                                                                      int* __restrict__ cursor) {
-    __shared__ uint32_t s_list[kCullActiveWarps][kCapActive];
-    const int warp = threadIdx.x >> 5;
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t n = min((int64_t)count[0], G.nblocks);
-    for (int64_t a = gwarp; a < n; a += nwarps)
-        cull_active_block(G, chain, primf, pool, sb_off, sb_len, active[a], blk_off, blk_len, blk_pool, blk_cap, cursor,
-                          s_list[warp]);
 }
 
 // ------------------------------------------------------------------------------------ localisation
@@ -957,9 +972,40 @@ __device__ __forceinline__ float canon_t(const float* __restrict__ p, float x, f
     return canon_f(T, p, x, y, z);
 }
 
+// Sphere in difference form: with q = L + e (e the voxel's offset in the sphere's frame),
+// |q| - r = (|L|^2 - r^2 + e.(2L + e)) / (|q| + r).  The constant |L|^2 - r^2 is formed in float64 per
+// block (LocalPrim.L[3]); the numerator then carries only small per-voxel terms, so the error stays
+// near one rounding of the value instead of growing with the sphere's size (coordinates of up to
+// ~50 pitches put the direct form near 1e-5 pitch).
+template <int VG>
+__device__ __forceinline__ void eval_group_sphere(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+    const float L0 = P.L[0], L1 = P.L[1], L2 = P.L[2], K = P.L[3], r = P.p[0];
+    float ebx, eby, ebz, cx, cy, cz;  // e = eb + c * dz
+    if (P.ident) {
+        ebx = dx; eby = dy; ebz = 0.f; cx = 0.f; cy = 0.f; cz = 1.f;
+    } else {
+        ebx = fmaf(P.A[0], dx, P.A[1] * dy);
+        eby = fmaf(P.A[3], dx, P.A[4] * dy);
+        ebz = fmaf(P.A[6], dx, P.A[7] * dy);
+        cx = P.A[2]; cy = P.A[5]; cz = P.A[8];
+    }
+#pragma unroll
+    for (int k = 0; k < VG; ++k) {
+        const float ex = fmaf(cx, dz[k], ebx), ey = fmaf(cy, dz[k], eby), ez = fmaf(cz, dz[k], ebz);
+        const float x = L0 + ex, y = L1 + ey, z = L2 + ez;
+        const float num = fmaf(ez, fmaf(2.f, L2, ez), fmaf(ey, fmaf(2.f, L1, ey), fmaf(ex, fmaf(2.f, L0, ex), K)));
+        const float den = sqrtf(fmaf(z, z, fmaf(x, x, y * y))) + r;
+        v[k] = fmaf(P.s, __fdiv_rn(num, den), -P.off);
+    }
+}
+
 // VG voxels along z of one lane: values of primitive P at block offsets (dx, dy, dz0 + k*pz).
 template <int VG, int T>
 __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+    if (T == P_SPHERE) {
+        eval_group_sphere<VG>(P, dx, dy, dz, v);
+        return;
+    }
     const float* p = P.p;
     if (P.ident) {
         const float x = P.L[0] + dx, y = P.L[1] + dy;
@@ -1056,6 +1102,11 @@ __device__ __forceinline__ unsigned prim_flops(int type, int ident) {
     case P_FRUSTUM: f = 30; break;
     case P_CAPSULE: f = 22; break;
     case P_TORUS: f = 12; break;
+    case P_GRID: f = 40; break;
+    case P_REVOLVE: f = 32; break;
+    case P_BAR: f = 9; break;
+    case P_POCKET: f = 24; break;
+    case P_XBORE: f = 9; break;
     default: f = 5;
     }
     return affine + f + 2;
@@ -1112,8 +1163,9 @@ template <int B>
 __device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
                               const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
                               const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
-                              int32_t* __restrict__ kind, float* __restrict__ cma, int32_t* __restrict__ blk_len,
-                              int64_t s, LocalPrim* sp, float* val) {
+                              int32_t* __restrict__ kind, float* __restrict__ cma, int32_t* __restrict__ blk_off,
+                              int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                              int* __restrict__ cursor, int64_t s, LocalPrim* sp, float* val) {
     constexpr int S = 32 / B;          // blocks per superblock edge
     constexpr int P1 = S + 1;          // lattice points per edge
     constexpr int NC = P1 * P1;        // lattice columns (along z)
@@ -1183,7 +1235,24 @@ __device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, co
                                vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
         });
         cma[b] = m;
-        blk_len[b] = -1;
+        int len_b = -1;
+        if (kind[b] == 0) {
+            // the block's own list, culled from the superblock's for the leaf pass and point queries
+            uint32_t blist[kCapBlock];
+            const float half = 0.5f * B;
+            const int n = seq_walk(list, len, chain, primf, G.fx0 + (bi * B + half) * G.fpitch,
+                                   G.fy0 + (bj * B + half) * G.fpitch, G.fz0 + (bk * B + half) * G.fpitch,
+                                   1.7320509f * half * G.fpitch, G.eps, blist, kCapBlock);
+            if (n <= kCapBlock) {
+                const int slot = atomicAdd(cursor, n);
+                if ((int64_t)slot + n <= blk_cap) {
+                    for (int i = 0; i < n; ++i) blk_pool[slot + i] = blist[i];
+                    blk_off[b] = slot;
+                    len_b = n;
+                }
+            }
+        }
+        blk_len[b] = len_b;  // -1: the leaf pass culls the block itself
     }
     __syncwarp();
 }
@@ -1196,7 +1265,10 @@ __global__ void __launch_bounds__(32 * kLatWarps) k_classify_lattice(Geo G, cons
                                                                      const int64_t* __restrict__ sb_off,
                                                                      const int32_t* __restrict__ sb_len,
                                                                      int32_t* __restrict__ kind, float* __restrict__ cma,
-                                                                     int32_t* __restrict__ blk_len) {
+                                                                     int32_t* __restrict__ blk_off,
+                                                                     int32_t* __restrict__ blk_len,
+                                                                     uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                                                                     int* __restrict__ cursor) {
     constexpr int P1 = 32 / B + 1;
     __shared__ LocalPrim s_prim[kLatWarps][kLatChunk];
     __shared__ float s_val[kLatWarps][P1 * P1 * P1];
@@ -1204,7 +1276,8 @@ __global__ void __launch_bounds__(32 * kLatWarps) k_classify_lattice(Geo G, cons
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s = gwarp; s < G.nsuper; s += nwarps)
-        lattice_super<B>(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_len, s, s_prim[warp], s_val[warp]);
+        lattice_super<B>(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, blk_cap,
+                         cursor, s, s_prim[warp], s_val[warp]);
 }
 
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
@@ -1625,15 +1698,18 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
             switch (G.B) {
             case 4:
                 k_classify_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
-                                                                       kind, cma, S.blk_len);
+                                                                       kind, cma, S.blk_off, S.blk_len, S.blk_pool, P.blk_cap,
+                                                                       S.misc + 2);
                 break;
             case 8:
                 k_classify_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
-                                                                       kind, cma, S.blk_len);
+                                                                       kind, cma, S.blk_off, S.blk_len, S.blk_pool, P.blk_cap,
+                                                                       S.misc + 2);
                 break;
             default:
                 k_classify_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
-                                                                       kind, cma, S.blk_len);
+                                                                       kind, cma, S.blk_off, S.blk_len, S.blk_pool, P.blk_cap,
+                                                                       S.misc + 2);
             }
         }
     } else {
@@ -1641,14 +1717,6 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
     }
     FB_LAUNCH();
     if (int rc = launch_compact(kind, G.nblocks, active, count, S.status, S.misc, st)) return rc;
-    if (mode == 1 && !P.warp_blocks) {
-        // the compaction left misc[2] (the block-list pool cursor) at zero
-        const int grid = fb_sm_count() * 16;
-        k_cull_active<<<grid, 32 * kCullActiveWarps, 0, st>>>(G, chain, S.primf, S.pool, S.off + G.ncoarse,
-                                                              S.len + G.ncoarse, active, count, S.blk_off, S.blk_len,
-                                                              S.blk_pool, P.blk_cap, S.misc + 2);
-        FB_LAUNCH();
-    }
     return FB_OK;
 }
 
@@ -1800,7 +1868,8 @@ __global__ void __launch_bounds__(128, 10) k_b_classify_listed(const RecDesc* __
 }
 
 template <int B>
-__global__ void __launch_bounds__(32 * kLatWarps) k_b_lattice(const RecDesc* __restrict__ D, Group W, int64_t total) {
+__global__ void __launch_bounds__(32 * kLatWarps) k_b_lattice(const RecDesc* __restrict__ D, Group W, int64_t total,
+                                                              int* __restrict__ cursors) {
     constexpr int P1 = 32 / B + 1;
     __shared__ LocalPrim s_prim[kLatWarps][kLatChunk];
     __shared__ float s_val[kLatWarps][P1 * P1 * P1];
@@ -1810,7 +1879,8 @@ __global__ void __launch_bounds__(32 * kLatWarps) k_b_lattice(const RecDesc* __r
         const int j = group_find(W, g);
         const RecDesc& R = D[W.rec[j]];
         lattice_super<B>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind,
-                         R.cma, R.blk_len, g - W.pre[j], s_prim[warp], s_val[warp]);
+                         R.cma, R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[W.rec[j]], g - W.pre[j],
+                         s_prim[warp], s_val[warp]);
     }
 }
 
@@ -1828,11 +1898,11 @@ __global__ void __launch_bounds__(256) k_b_compact(const RecDesc* __restrict__ D
 
 // After the compaction: each recipe's tile offset in the arena (recipe order, floats), the tiles it
 // gets (count, clipped to the room left; the overflow flag misc[2] raised when clipped), and the
-// prefixes of the active-block groups: act (lattice recipes, list culling) and leaf[0..2] (B = 4, 8,
-// 16).  One thread: a batch holds a few hundred to a few thousand recipes.
+// prefixes of the active-block groups leaf[0..2] (B = 4, 8, 16) and occ (recipes with a mask).  One
+// thread: a batch holds a few hundred to a few thousand recipes.
 __global__ void k_batch_offsets(const RecDesc* __restrict__ D, int n, int64_t capacity,
                                 int64_t* __restrict__ tile_off, int32_t* __restrict__ leaf_count,
-                                Group act, int64_t* __restrict__ act_pre, Group l4, int64_t* __restrict__ l4_pre,
+                                Group l4, int64_t* __restrict__ l4_pre,
                                 Group l8, int64_t* __restrict__ l8_pre, Group l16, int64_t* __restrict__ l16_pre,
                                 Group occ, int64_t* __restrict__ occ_pre, int* __restrict__ misc) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -1848,12 +1918,6 @@ __global__ void k_batch_offsets(const RecDesc* __restrict__ D, int n, int64_t ca
         at += take * b3;
     }
     int64_t t = 0;
-    for (int j = 0; j < act.m; ++j) {
-        act_pre[j] = t;
-        const RecDesc& R = D[act.rec[j]];
-        t += min((int64_t)R.count[0], R.G.nblocks);
-    }
-    act_pre[act.m] = t;
     const Group* L[3] = {&l4, &l8, &l16};
     int64_t* P[3] = {l4_pre, l8_pre, l16_pre};
     for (int q = 0; q < 3; ++q) {
@@ -1904,22 +1968,6 @@ __global__ void __launch_bounds__(256) k_b_occupancy(const RecDesc* __restrict__
     occupancy_item<B>(R.kind, R.slot, tiles + tile_off[r], G.nx, G.ny, G.nz, G.nby, G.nbz, R.mask, g - W.pre[j]);
 }
 
-__global__ void __launch_bounds__(32 * kCullActiveWarps) k_b_cull_active(const RecDesc* __restrict__ D, Group W,
-                                                                         int* __restrict__ cursors) {
-    __shared__ uint32_t s_list[kCullActiveWarps][kCapActive];
-    const int warp = threadIdx.x >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t total = W.pre[W.m];
-    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < total; g += nwarps) {
-        const int j = group_find(W, g);
-        const int r = W.rec[j];
-        const RecDesc& R = D[r];
-        cull_active_block(R.G, R.chain, R.primf, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse,
-                          R.active[g - W.pre[j]], R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[r],
-                          s_list[warp]);
-    }
-}
-
 template <int B>
 __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __restrict__ D, Group W,
                                                                float* __restrict__ tiles,
@@ -1954,8 +2002,7 @@ struct BatchHost {
     int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_wblocks = 0, n_wclass = 0, n_lat[3] = {0, 0, 0},
             n_tiles = 0;
     // dynamic groups (prefixes written by k_batch_offsets)
-    Group act{}, leaf[3]{}, occ{};
-    int64_t* act_pre = nullptr;
+    Group leaf[3]{}, occ{};
     int64_t* leaf_pre[3] = {nullptr, nullptr, nullptr};
     int64_t* occ_pre = nullptr;
     // occupancy groups (recipes carrying a mask): their blocks, and their rows of 16 z voxels per B
@@ -2045,7 +2092,7 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
                 pre.push_back(pre.back() + items);
             }
         };
-        HostGroup g_prims, g_chain, g_coarse, g_super, g_wblocks, g_wclass, g_lat[3], g_tiles, g_act, g_leaf[3], g_occ,
+        HostGroup g_prims, g_chain, g_coarse, g_super, g_wblocks, g_wclass, g_lat[3], g_tiles, g_leaf[3], g_occ,
             g_occ_blocks, g_occ_rows[3];
         for (int r = 0; r < n; ++r) {
             const RecDesc& d = H->desc[r];
@@ -2059,7 +2106,6 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
                 g_wclass.add(r, G.nsuper * threads_per_super(G.S));
             } else {
                 g_lat[b_index(G.B)].add(r, G.nsuper);
-                g_act.add(r, 0);
             }
             g_tiles.add(r, d.ntiles);
             g_leaf[b_index(G.B)].add(r, 0);
@@ -2087,9 +2133,9 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             return q;
         };
         HostGroup* statics[] = {&g_prims, &g_chain, &g_coarse, &g_super, &g_wblocks, &g_wclass,
-                                &g_lat[0], &g_lat[1], &g_lat[2], &g_tiles, &g_act, &g_leaf[0], &g_leaf[1], &g_leaf[2],
+                                &g_lat[0], &g_lat[1], &g_lat[2], &g_tiles, &g_leaf[0], &g_leaf[1], &g_leaf[2],
                                 &g_occ, &g_occ_blocks, &g_occ_rows[0], &g_occ_rows[1], &g_occ_rows[2]};
-        constexpr int kGroups = 19;
+        constexpr int kGroups = 18;
         Placed placed[kGroups];
         for (int q = 0; q < kGroups; ++q) placed[q] = place_group(*statics[q]);
         const int64_t o_state = at;
@@ -2117,7 +2163,7 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
         std::vector<char> image(o_state, 0);
         std::memcpy(image.data() + o_desc, H->desc.data(), (size_t)n * sizeof(RecDesc));
         Group* dst[] = {&H->prims, &H->chain, &H->coarse, &H->super_, &H->wblocks, &H->wclass,
-                        &H->lat[0], &H->lat[1], &H->lat[2], &H->tiles, &H->act, &H->leaf[0], &H->leaf[1], &H->leaf[2],
+                        &H->lat[0], &H->lat[1], &H->lat[2], &H->tiles, &H->leaf[0], &H->leaf[1], &H->leaf[2],
                         &H->occ, &H->occ_blocks, &H->occ_rows[0], &H->occ_rows[1], &H->occ_rows[2]};
         for (int q = 0; q < kGroups; ++q) {
             const HostGroup& hg = *statics[q];
@@ -2127,9 +2173,8 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             dst[q]->pre = reinterpret_cast<const int64_t*>(D + placed[q].pre);
             dst[q]->m = (int32_t)hg.rec.size();
         }
-        H->act_pre = reinterpret_cast<int64_t*>(D + placed[10].pre);
-        for (int q = 0; q < 3; ++q) H->leaf_pre[q] = reinterpret_cast<int64_t*>(D + placed[11 + q].pre);
-        H->occ_pre = reinterpret_cast<int64_t*>(D + placed[14].pre);
+        for (int q = 0; q < 3; ++q) H->leaf_pre[q] = reinterpret_cast<int64_t*>(D + placed[10 + q].pre);
+        H->occ_pre = reinterpret_cast<int64_t*>(D + placed[13].pre);
         H->n_occ_blocks = g_occ_blocks.pre.back();
         for (int q = 0; q < 3; ++q) H->n_occ_rows[q] = g_occ_rows[q].pre.back();
         H->n_prims = g_prims.pre.back();
@@ -2169,8 +2214,9 @@ int fb_batch_build_device(void* batch, float* d_tiles, int64_t capacity, int32_t
 }
 
 // The same build with instrumentation: events (nullable; six cudaEvent_t) are recorded on the stream
-// at the start and after the culling levels, the classification, the compaction (with the tile
-// placement), the per-block lists and the leaf tiles; d_work (nullable; two uint64) accumulates the
+// at the start and after the culling levels, the classification (with the active blocks' own
+// lists), the compaction (with the tile placement), an empty phase kept for the six-event layout,
+// and the leaf tiles; d_work (nullable; two uint64) accumulates the
 // leaf pass's executed primitive evaluations and float32 operations.
 int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm,
                                 void* const* events, uint64_t* d_work, void* stream) noexcept {
@@ -2205,23 +2251,19 @@ int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, i
     for (int q = 0; q < 3; ++q) {
         if (!H->n_lat[q]) continue;
         const int grid = (int)std::min<int64_t>(fb_div_up(H->n_lat[q], kLatWarps), (int64_t)sms * 64);
-        if (q == 0) k_b_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[0], H->n_lat[0]);
-        else if (q == 1) k_b_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[1], H->n_lat[1]);
-        else k_b_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[2], H->n_lat[2]);
+        if (q == 0) k_b_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[0], H->n_lat[0], H->cursors);
+        else if (q == 1) k_b_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[1], H->n_lat[1], H->cursors);
+        else k_b_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[2], H->n_lat[2], H->cursors);
         FB_LAUNCH();
     }
     if (int rc = mark(2)) return rc;
     k_b_compact<<<(unsigned)H->n_tiles, 256, 0, st>>>(D, H->tiles, H->misc, kLookbackSpins);
     FB_LAUNCH();
-    k_batch_offsets<<<1, 32, 0, st>>>(D, H->n, capacity, H->tile_off, H->leaf_count, H->act, H->act_pre, H->leaf[0],
+    k_batch_offsets<<<1, 32, 0, st>>>(D, H->n, capacity, H->tile_off, H->leaf_count, H->leaf[0],
                                       H->leaf_pre[0], H->leaf[1], H->leaf_pre[1], H->leaf[2], H->leaf_pre[2], H->occ,
                                       H->occ_pre, H->misc);
     FB_LAUNCH();
     if (int rc = mark(3)) return rc;
-    if (H->act.m) {
-        k_b_cull_active<<<dyn, 32 * kCullActiveWarps, 0, st>>>(D, H->act, H->cursors);
-        FB_LAUNCH();
-    }
     if (int rc = mark(4)) return rc;
     for (int q = 0; q < 3; ++q) {
         if (!H->leaf[q].m) continue;
@@ -2275,7 +2317,6 @@ int32_t fb_batch_launches(void* batch) noexcept {
     int n = 1 + 4 + 2;  // memset; prepare, full list, two cull levels; compaction, offsets
     if (H->n_wblocks) n += 2;
     for (int q = 0; q < 3; ++q) n += (H->n_lat[q] ? 1 : 0) + (H->leaf[q].m ? 1 : 0);
-    if (H->act.m) n += 1;
     return n;
 }
 

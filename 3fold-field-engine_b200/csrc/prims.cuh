@@ -6,10 +6,19 @@
 // into A, t, s, off).  Canonical formulas: sphere, box, cylinder, cone, halfspace and rect_frustum
 // follow src/field_engine/ikarus_v1/expr.py:268-340 (box also faltkarna_v1.py:91-99), the
 // unbounded z cylinder faltkarna_v1.py:102-104; capsule and torus are the textbook closed forms.
+// Table-backed kinds read a float32 table whose address the host writes into the record (p[10] of
+// the float64 record as raw bits; p[10] / p[11] of the float32 mirror as its two 32-bit halves):
+// the gridfield leaf's trilinear sample (src/field_engine/ikarus_v1/eval_warp.py:94-147) and the
+// revolved (r, z) table of the machining scene (tillverkningsfalt_v1_kernel.py:265-277); that scene's
+// round bar, arched rounded-box pocket and x-clipped cross bore follow its :262-300.
 #pragma once
 #include <cstdint>
 
-enum : int32_t { P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF };
+enum : int32_t {
+    P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF,
+    // table-backed and machining-scene kinds (never culled where no Lipschitz bound holds)
+    P_GRID, P_REVOLVE, P_BAR, P_POCKET, P_XBORE
+};
 enum : int32_t { OP_PUSH = 0, OP_UNION, OP_INTERSECT, OP_SUBTRACT, OP_OFFSET };
 enum : int32_t { CH_SET = 0, CH_SETNEG, CH_UNION, CH_INTERSECT, CH_SUBTRACT, CH_OFFSET };
 
@@ -38,7 +47,8 @@ struct __align__(16) PrimF {
     float p[12];
 };
 
-// Block-localised float32 record: q = L + A_lin * d, d the offset from the block origin.
+// Block-localised float32 record: q = L + A_lin * d, d the offset from the block origin; L[3] holds
+// a kind's per-block float64 constant rounded once (the sphere's |L|^2 - r^2).
 struct __align__(16) LocalPrim {
     int32_t type, op, ident, pad;
     float k, s, off, pad1;
@@ -50,6 +60,56 @@ struct __align__(16) LocalPrim {
 // ------------------------------------------------------------------------------------ float32
 __device__ __forceinline__ float sel_min(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float sel_max(float a, float b) { return a > b ? a : b; }
+
+// float32 lerp with the product form a*(1-t) + b*t, each operation rounded once.
+__device__ __forceinline__ float lerp_f(float a, float b, float t) {
+    return __fadd_rn(__fmul_rn(a, __fsub_rn(1.f, t)), __fmul_rn(b, t));
+}
+
+__device__ __forceinline__ const float* table_of(const float* __restrict__ p) {
+    return reinterpret_cast<const float*>((uint64_t)__float_as_uint(p[10]) | ((uint64_t)__float_as_uint(p[11]) << 32));
+}
+
+// Gridfield leaf, p = {ox, oy, oz, pitch, iso, is_sdf, nx, ny, nz, -, table}: 1e6 outside the grid
+// (NaN coordinates included), else the trilinear sample; occupancy tables read (iso - v) * pitch.
+static __device__ __noinline__ float grid_sample_f(const float* __restrict__ p, float x, float y, float z) {
+    const int nx = (int)p[6], ny = (int)p[7], nz = (int)p[8];
+    const float pitch = p[3];
+    const float fx = __fdiv_rn(__fsub_rn(x, p[0]), pitch);
+    const float fy = __fdiv_rn(__fsub_rn(y, p[1]), pitch);
+    const float fz = __fdiv_rn(__fsub_rn(z, p[2]), pitch);
+    if (!(fx >= 0.f && fy >= 0.f && fz >= 0.f && fx <= (float)(nx - 1) && fy <= (float)(ny - 1) &&
+          fz <= (float)(nz - 1)))
+        return 1.0e6f;
+    const int ix = (int)floorf(fx), iy = (int)floorf(fy), iz = (int)floorf(fz);
+    const int ix1 = min(ix + 1, nx - 1), iy1 = min(iy + 1, ny - 1), iz1 = min(iz + 1, nz - 1);
+    const float tx = __fsub_rn(fx, (float)ix), ty = __fsub_rn(fy, (float)iy), tz = __fsub_rn(fz, (float)iz);
+    const float* g = table_of(p);
+    auto at = [&](int i, int j, int k) { return g[((int64_t)i * ny + j) * nz + k]; };
+    const float c00 = lerp_f(at(ix, iy, iz), at(ix1, iy, iz), tx), c10 = lerp_f(at(ix, iy1, iz), at(ix1, iy1, iz), tx);
+    const float c01 = lerp_f(at(ix, iy, iz1), at(ix1, iy, iz1), tx), c11 = lerp_f(at(ix, iy1, iz1), at(ix1, iy1, iz1), tx);
+    const float val = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
+    return p[5] != 0.f ? val : __fmul_rn(__fsub_rn(p[4], val), pitch);
+}
+
+// Revolved (r, z) table, p = {r0, z0, pitch, nr, nz, -, ..., table}: bilinear at (r, z), r the
+// distance from the z axis, cell indices truncated and clamped to the table, weights clamped to [0, 1].
+static __device__ __noinline__ float revolve_sample_f(const float* __restrict__ p, float x, float y, float z) {
+    const int nr = (int)p[3], nz = (int)p[4];
+    const float r = sqrtf(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
+    const float fr = __fdiv_rn(__fsub_rn(r, p[0]), p[2]), fz = __fdiv_rn(__fsub_rn(z, p[1]), p[2]);
+    const float cr = fminf(fmaxf(fr, -1.0e9f), 1.0e9f), cz = fminf(fmaxf(fz, -1.0e9f), 1.0e9f);  // int range
+    const int ir = min(max((int)cr, 0), nr - 2), iz = min(max((int)cz, 0), nz - 2);
+    const float tr = fminf(fmaxf(__fsub_rn(fr, (float)ir), 0.f), 1.f), tz = fminf(fmaxf(__fsub_rn(fz, (float)iz), 0.f), 1.f);
+    const float* g = table_of(p);
+    const float v00 = g[(int64_t)ir * nz + iz], v01 = g[(int64_t)ir * nz + iz + 1];
+    const float v10 = g[(int64_t)(ir + 1) * nz + iz], v11 = g[(int64_t)(ir + 1) * nz + iz + 1];
+    const float ur = __fsub_rn(1.f, tr), uz = __fsub_rn(1.f, tz);
+    float v = __fmul_rn(__fmul_rn(v00, ur), uz);
+    v = __fadd_rn(v, __fmul_rn(__fmul_rn(v01, ur), tz));
+    v = __fadd_rn(v, __fmul_rn(__fmul_rn(v10, tr), uz));
+    return __fadd_rn(v, __fmul_rn(__fmul_rn(v11, tr), tz));
+}
 
 __device__ __forceinline__ float canon_f(int type, const float* __restrict__ p, float x, float y, float z) {
     switch (type) {
@@ -95,6 +155,25 @@ __device__ __forceinline__ float canon_f(int type, const float* __restrict__ p, 
     }
     case P_CYL_INF:
         return sqrtf(fmaf(x, x, y * y)) - p[0];
+    case P_GRID:
+        return grid_sample_f(p, x, y, z);
+    case P_REVOLVE:
+        return revolve_sample_f(p, x, y, z);
+    case P_BAR: {  // p = {R, z_lo, z_hi}: max(r - R, max(z_lo - z, z - z_hi))
+        const float r = sqrtf(fmaf(x, x, y * y));
+        return fmaxf(r - p[0], fmaxf(p[1] - z, z - p[2]));
+    }
+    case P_POCKET: {  // p = {half_x, half_y, edge_r, arch_r, arch_cz}
+        const float qx = fabsf(x) - (p[0] - p[2]), qy = fabsf(y) - (p[1] - p[2]);
+        const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f);
+        const float dxy = sqrtf(fmaf(ox, ox, oy * oy)) + fminf(fmaxf(qx, qy), 0.f) - p[2];
+        const float roof = p[4] + sqrtf(fmaxf(fmaf(-x, x, p[3] * p[3]), 0.f));
+        return fmaxf(dxy, z - roof);
+    }
+    case P_XBORE: {  // p = {radius, axis_z, half_length}
+        const float dz = z - p[1];
+        return fmaxf(sqrtf(fmaf(y, y, dz * dz)) - p[0], fabsf(x) - p[2]);
+    }
     default:
         return __int_as_float(0x7fc00000);
     }
@@ -186,7 +265,8 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     out.L[0] = (float)lx;
     out.L[1] = (float)ly;
     out.L[2] = (float)lz;
-    out.L[3] = 0.f;
+    // sphere: |L|^2 - r^2 in float64, the constant term of the difference form of |q| - r
+    out.L[3] = F.type == P_SPHERE ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0]) : 0.f;
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
     out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
@@ -201,6 +281,51 @@ __device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(
 __device__ __forceinline__ double rn_div(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double rn_max(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double rn_min(double a, double b) { return a < b ? a : b; }
+
+static __device__ __forceinline__ const float* table_of_d(const double* __restrict__ p) {
+    return reinterpret_cast<const float*>(__double_as_longlong(p[10]));
+}
+
+static __device__ __forceinline__ double lerp_d(double a, double b, double t) {
+    return rn_add(rn_mul(a, rn_sub(1.0, t)), rn_mul(b, t));
+}
+
+// The same samples in float64 (the table's float32 values promoted).
+static __device__ double grid_sample_d(const double* __restrict__ p, double x, double y, double z) {
+    const int nx = (int)p[6], ny = (int)p[7], nz = (int)p[8];
+    const double pitch = p[3];
+    const double fx = rn_div(rn_sub(x, p[0]), pitch), fy = rn_div(rn_sub(y, p[1]), pitch),
+                 fz = rn_div(rn_sub(z, p[2]), pitch);
+    if (!(fx >= 0.0 && fy >= 0.0 && fz >= 0.0 && fx <= (double)(nx - 1) && fy <= (double)(ny - 1) &&
+          fz <= (double)(nz - 1)))
+        return 1.0e6;
+    const int ix = (int)floor(fx), iy = (int)floor(fy), iz = (int)floor(fz);
+    const int ix1 = min(ix + 1, nx - 1), iy1 = min(iy + 1, ny - 1), iz1 = min(iz + 1, nz - 1);
+    const double tx = rn_sub(fx, (double)ix), ty = rn_sub(fy, (double)iy), tz = rn_sub(fz, (double)iz);
+    const float* g = table_of_d(p);
+    auto at = [&](int i, int j, int k) { return (double)g[((int64_t)i * ny + j) * nz + k]; };
+    const double c00 = lerp_d(at(ix, iy, iz), at(ix1, iy, iz), tx), c10 = lerp_d(at(ix, iy1, iz), at(ix1, iy1, iz), tx);
+    const double c01 = lerp_d(at(ix, iy, iz1), at(ix1, iy, iz1), tx), c11 = lerp_d(at(ix, iy1, iz1), at(ix1, iy1, iz1), tx);
+    const double val = lerp_d(lerp_d(c00, c10, ty), lerp_d(c01, c11, ty), tz);
+    return p[5] != 0.0 ? val : rn_mul(rn_sub(p[4], val), pitch);
+}
+
+static __device__ double revolve_sample_d(const double* __restrict__ p, double x, double y, double z) {
+    const int nr = (int)p[3], nz = (int)p[4];
+    const double r = __dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y)));
+    const double fr = rn_div(rn_sub(r, p[0]), p[2]), fz = rn_div(rn_sub(z, p[1]), p[2]);
+    const double cr = fmin(fmax(fr, -1.0e9), 1.0e9), cz = fmin(fmax(fz, -1.0e9), 1.0e9);
+    const int ir = min(max((int)cr, 0), nr - 2), iz = min(max((int)cz, 0), nz - 2);
+    const double tr = fmin(fmax(rn_sub(fr, (double)ir), 0.0), 1.0), tz = fmin(fmax(rn_sub(fz, (double)iz), 0.0), 1.0);
+    const float* g = table_of_d(p);
+    const double v00 = g[(int64_t)ir * nz + iz], v01 = g[(int64_t)ir * nz + iz + 1];
+    const double v10 = g[(int64_t)(ir + 1) * nz + iz], v11 = g[(int64_t)(ir + 1) * nz + iz + 1];
+    const double ur = rn_sub(1.0, tr), uz = rn_sub(1.0, tz);
+    double v = rn_mul(rn_mul(v00, ur), uz);
+    v = rn_add(v, rn_mul(rn_mul(v01, ur), tz));
+    v = rn_add(v, rn_mul(rn_mul(v10, tr), uz));
+    return rn_add(v, rn_mul(rn_mul(v11, tr), tz));
+}
 
 static __device__ __noinline__ double canon_d(int type, const double* __restrict__ p, double x, double y, double z) {
     switch (type) {
@@ -257,6 +382,25 @@ static __device__ __noinline__ double canon_d(int type, const double* __restrict
     }
     case P_CYL_INF:
         return rn_sub(__dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y))), p[0]);
+    case P_GRID:
+        return grid_sample_d(p, x, y, z);
+    case P_REVOLVE:
+        return revolve_sample_d(p, x, y, z);
+    case P_BAR: {
+        const double r = __dsqrt_rn(rn_add(rn_mul(x, x), rn_mul(y, y)));
+        return rn_max(rn_sub(r, p[0]), rn_max(rn_sub(p[1], z), rn_sub(z, p[2])));
+    }
+    case P_POCKET: {
+        const double qx = rn_sub(fabs(x), rn_sub(p[0], p[2])), qy = rn_sub(fabs(y), rn_sub(p[1], p[2]));
+        const double ox = rn_max(qx, 0.0), oy = rn_max(qy, 0.0);
+        const double dxy = rn_sub(rn_add(__dsqrt_rn(rn_add(rn_mul(ox, ox), rn_mul(oy, oy))), rn_min(rn_max(qx, qy), 0.0)), p[2]);
+        const double roof = rn_add(p[4], __dsqrt_rn(rn_max(rn_sub(rn_mul(p[3], p[3]), rn_mul(x, x)), 0.0)));
+        return rn_max(dxy, rn_sub(z, roof));
+    }
+    case P_XBORE: {
+        const double dz = rn_sub(z, p[1]);
+        return rn_max(rn_sub(__dsqrt_rn(rn_add(rn_mul(y, y), rn_mul(dz, dz))), p[0]), rn_sub(fabs(x), p[2]));
+    }
     default:
         return __longlong_as_double(0x7ff8000000000000ll);
     }

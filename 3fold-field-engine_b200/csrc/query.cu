@@ -522,6 +522,65 @@ __global__ void k_multires_gradient(Multi M, const int8_t* __restrict__ kind, co
     }
 }
 
+// Overlap band (faltkarna_v1_multires.py:211-251): every face of a fine brick whose neighbour is an
+// active brick of a coarser level takes the trilinear sample of the neighbour's lattice at the face's
+// own sample points.  One CTA per brick of the launch's level, its six faces in the reference's order
+// (axis 0..2, side -1 then +1; a later face overwrites the edges it shares with an earlier one).  The
+// reference walks the bricks in ascending id and overwrites lattices in place, so a neighbour of level
+// >= 1 is read as overwritten when its id is smaller than this brick's and as built otherwise: the
+// host launches level 1, 2, 3 in turn and passes `orig`, a copy of the pool taken before the band.
+__global__ void __launch_bounds__(256) k_multires_band(Multi M, const int8_t* __restrict__ kind,
+                                                       const int8_t* __restrict__ level,
+                                                       const int64_t* __restrict__ tile_off, float* __restrict__ pool,
+                                                       const float* __restrict__ orig,
+                                                       const int32_t* __restrict__ bricks, int n_bricks, int lvl,
+                                                       int* __restrict__ faces) {
+    const int idx = blockIdx.x;
+    if (idx >= n_bricks) return;
+    const int lin = bricks[idx];
+    const int b[3] = {lin / (M.by * M.bz), (lin / M.bz) % M.by, lin % M.bz};
+    const double L = rn_mul((double)M.B, M.h);
+    const double lo[3] = {M.lx, M.ly, M.lz};
+    const int shp[3] = {M.bx, M.by, M.bz};
+    const int n_l = M.B << lvl, m = n_l + 1;
+    const double h_f = rn_div(M.h, (double)(1 << lvl));
+    double bo[3];
+    for (int a = 0; a < 3; ++a) bo[a] = rn_add(lo[a], rn_mul((double)b[a], L));
+    float* tile = pool + tile_off[lin];
+    for (int ax = 0; ax < 3; ++ax) {
+        for (int sida = -1; sida <= 1; sida += 2) {
+            int nb[3] = {b[0], b[1], b[2]};
+            nb[ax] += sida;
+            if (nb[ax] < 0 || nb[ax] >= shp[ax]) continue;
+            const int64_t nlin = ((int64_t)nb[0] * M.by + nb[1]) * M.bz + nb[2];
+            if (kind[nlin] != 0) continue;
+            const int lvl_n = level[nlin];
+            if (lvl_n < 0 || lvl_n >= lvl) continue;
+            const float* src = (lvl_n >= 1 && nlin < lin ? pool : orig) + tile_off[nlin];
+            const int m_n = (M.B << lvl_n) + 1;
+            const double h_n = rn_div(M.h, (double)(1 << lvl_n));
+            double no[3];
+            for (int a = 0; a < 3; ++a) no[a] = rn_add(lo[a], rn_mul((double)nb[a], L));
+            const int u = ax == 0 ? 1 : 0, w = ax == 2 ? 1 : 2;  // the face's free axes, ascending
+            const int fixed = sida < 0 ? 0 : n_l;
+            for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
+                int g[3];
+                g[ax] = fixed;
+                g[u] = k / m;
+                g[w] = k % m;
+                double c[3];
+                for (int a = 0; a < 3; ++a) {
+                    const double pt = rn_add(rn_mul((double)g[a], h_f), bo[a]);
+                    c[a] = rn_div(rn_sub(pt, no[a]), h_n);
+                }
+                tile[((int64_t)g[0] * m + g[1]) * m + g[2]] = (float)tile_trilinear(src, m_n, c[0], c[1], c[2]);
+            }
+            if (threadIdx.x == 0) atomicAdd(faces, 1);
+            __syncthreads();
+        }
+    }
+}
+
 Multi make_multi(const double* lo, double h, int B, const int32_t* bshape, double margin) {
     Multi M;
     M.lx = lo[0];
@@ -536,9 +595,76 @@ Multi make_multi(const double* lo, double h, int B, const int32_t* bshape, doubl
     return M;
 }
 
+// Many (leaf A, leaf B) gridfield pairs in one launch (src/field_engine/ikarus_v1/eval_warp.py:521-564):
+// thread per point, pair = pair_of_point[i], value max(sample(A), sample(B)) with the gridfield
+// sampler.  params: 12 floats per leaf (the gridfield record layout: origin, pitch, iso, is_sdf, nx,
+// ny, nz, -, table address halves).  An index outside its table reads NaN.
+__global__ void k_grid_pairs(const float* __restrict__ params, int n_leaves, const float* __restrict__ pts,
+                             const int32_t* __restrict__ pair, int64_t n, const int32_t* __restrict__ la,
+                             const int32_t* __restrict__ lb, int n_pairs, float* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int pid = pair[i];
+        float v = __int_as_float(0x7fc00000);
+        if (pid >= 0 && pid < n_pairs) {
+            const int a = la[pid], b = lb[pid];
+            if (a >= 0 && a < n_leaves && b >= 0 && b < n_leaves) {
+                const float x = pts[3 * i], y = pts[3 * i + 1], z = pts[3 * i + 2];
+                v = fmaxf(grid_sample_f(params + 12 * a, x, y, z), grid_sample_f(params + 12 * b, x, y, z));
+            }
+        }
+        out[i] = v;
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+// Overlap band of a per-block-pitch field (k_multires_band): d_orig is caller scratch the size of
+// the pool (its state before the band); d_bricks lists the active bricks of level >= 1 sorted by
+// level (n_of_level[l] of level l = 1..3 after n_of_level[0] = 0); d_faces (one int) counts the faces
+// written.  Stream-ordered.
+int fb_multires_band_device(const double* lo, double h, int32_t B, const int32_t* bshape, const int8_t* d_kind,
+                            const int8_t* d_level, const int64_t* d_tile_off, float* d_pool, int64_t pool_len,
+                            float* d_orig, const int32_t* d_bricks, const int32_t* n_of_level, int32_t* d_faces,
+                            void* stream) noexcept {
+    if (!lo || !bshape || !d_kind || !d_level || !d_tile_off || !d_pool || !d_orig || !n_of_level || !d_faces ||
+        B < 1 || !(h > 0) || pool_len < 0)
+        return FB_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Multi M = make_multi(lo, h, B, bshape, 0.0);
+    FB_CUDA(cudaMemsetAsync(d_faces, 0, sizeof(int32_t), st));
+    FB_CUDA(cudaMemcpyAsync(d_orig, d_pool, pool_len * 4, cudaMemcpyDeviceToDevice, st));
+    int at = 0;
+    for (int l = 1; l <= 3; ++l) {
+        const int n = n_of_level[l];
+        if (n < 0) return FB_INVALID;
+        if (n > 0) {
+            if (!d_bricks) return FB_INVALID;
+            k_multires_band<<<n, 256, 0, st>>>(M, d_kind, d_level, d_tile_off, d_pool, d_orig, d_bricks + at, n, l,
+                                               d_faces);
+            FB_LAUNCH();
+        }
+        at += n;
+    }
+    return FB_OK;
+}
+
+// The multi-pair gridfield sweep (k_grid_pairs); all pointers on the device, stream-ordered.
+int fb_grid_pairs_device(const float* d_params, int32_t n_leaves, const float* d_pts, const int32_t* d_pair,
+                         int64_t n, const int32_t* d_leaf_a, const int32_t* d_leaf_b, int32_t n_pairs, float* d_out,
+                         void* stream) noexcept {
+    if (n < 0 || n_leaves < 1 || n_pairs < 1 || !d_params ||
+        (n > 0 && (!d_pts || !d_pair || !d_leaf_a || !d_leaf_b || !d_out)))
+        return FB_INVALID;
+    if (n == 0) return FB_OK;
+    k_grid_pairs<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)fb_sm_count() * 16), 256, 0,
+                   static_cast<cudaStream_t>(stream)>>>(d_params, n_leaves, d_pts, d_pair, n, d_leaf_a, d_leaf_b,
+                                                        n_pairs, d_out);
+    FB_LAUNCH();
+    return FB_OK;
+}
+
 
 // Values (and gradients) of a compiled recipe at float32 points, device pointers.  d_primf is the
 // float32 primitive mirror a field build prepared (fb_query_prepare fills one).  accel_* (all

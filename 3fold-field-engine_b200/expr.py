@@ -27,14 +27,16 @@ PRIM = np.dtype([("type", "<i4"), ("flags", "<i4"), ("p", "<f8", (12,)), ("A", "
 INSN = np.dtype([("op", "<i4"), ("arg", "<i4"), ("k", "<f8")])
 
 # primitive types (canonical frames)
-P_SPHERE, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF = range(9)
+(P_SPHERE, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF,
+ P_GRID, P_REVOLVE, P_BAR, P_POCKET, P_XBORE) = range(14)
+TABLE_KINDS = (P_GRID, P_REVOLVE)  # records whose p[9] names a table and p[10] holds its address
 # postfix program ops
 OP_PUSH, OP_UNION, OP_INTERSECT, OP_SUBTRACT, OP_OFFSET = range(5)
 # chain ops (device culling form)
 CH_SET, CH_SETNEG, CH_UNION, CH_INTERSECT, CH_SUBTRACT, CH_OFFSET = range(6)
 
 LEAF_OPS = ("halfspace", "sphere", "box", "cylinder", "cone", "rect_frustum", "capsule", "torus",
-            "cylinder_z_infinite")
+            "cylinder_z_infinite", "gridfield", "revolve_table", "round_bar", "arched_pocket", "cross_bore")
 
 
 # --------------------------------------------------------------------------------------------- transforms
@@ -131,6 +133,43 @@ def cylinder_z_infinite(radius, center=(0.0, 0.0)):
     return {"op": "cylinder_z_infinite", "radius": float(radius), "center": list(map(float, center))}
 
 
+def gridfield(npz_path, key="occupancy", mode="occupancy", iso=0.5, pitch_override=None):
+    """Leaf sampling an existing voxel grid trilinearly (src/field_engine/ikarus_v1/expr.py:143-152):
+    the npz holds the (nx, ny, nz) array under `key` and, optionally, ``global_origin_mm`` and
+    ``pitch_mm``.  mode "sdf": values are signed distances; "occupancy": (iso - value) * pitch."""
+    return {"op": "gridfield", "npz_path": npz_path, "key": key, "mode": mode, "iso": float(iso),
+            "pitch_override": pitch_override}
+
+
+def revolve_table(table, r0, z0, pitch):
+    """A 2-D signed-distance table over (r, z) -- r the distance from the z axis, rows r0 + i*pitch,
+    columns z0 + j*pitch -- revolved about z and sampled bilinearly: the turned-profile term of the
+    reference's machining kernel (src/field_engine/tillverkningsfalt_v1_kernel.py:265-277)."""
+    return {"op": "revolve_table", "table": np.ascontiguousarray(table, dtype=np.float32), "r0": float(r0),
+            "z0": float(z0), "pitch": float(pitch)}
+
+
+def round_bar(radius, z_lo, z_hi):
+    """max(r - radius, max(z_lo - z, z - z_hi)): the round bar (blank) of the reference's machining
+    kernel (tillverkningsfalt_v1_kernel.py:262-263)."""
+    return {"op": "round_bar", "radius": float(radius), "z_lo": float(z_lo), "z_hi": float(z_hi)}
+
+
+def arched_pocket(half_x, half_y, edge_radius, arch_radius, arch_center_z):
+    """A rounded rectangle in x/y (side-edge radius edge_radius) under an arched roof
+    z <= arch_center_z + sqrt(arch_radius^2 - x^2), open below: the milled pocket of the reference's
+    machining kernel (tillverkningsfalt_v1_kernel.py:281-291); subtract it from the part."""
+    return {"op": "arched_pocket", "half_x": float(half_x), "half_y": float(half_y),
+            "edge_radius": float(edge_radius), "arch_radius": float(arch_radius),
+            "arch_center_z": float(arch_center_z)}
+
+
+def cross_bore(radius, axis_z, half_length):
+    """A bore along x at height axis_z clipped to |x| <= half_length, in the max form of the
+    reference's machining kernel (tillverkningsfalt_v1_kernel.py:294-297); subtract it."""
+    return {"op": "cross_bore", "radius": float(radius), "axis_z": float(axis_z), "half_length": float(half_length)}
+
+
 def transform(child, mat4):
     return {"op": "transform", "child": child, "mat4": mat4}
 
@@ -221,13 +260,53 @@ def _affine(rows3x4):
 
 
 class Compiled:
-    """A compiled recipe: ``prims`` (PRIM records), ``program`` (postfix INSN), and ``chain``
-    (left-deep CH_* INSN records, or None when the tree does not reduce to a chain)."""
+    """A compiled recipe: ``prims`` (PRIM records), ``program`` (postfix INSN), ``chain``
+    (left-deep CH_* INSN records, or None when the tree does not reduce to a chain) and ``tables``
+    (float32 arrays of the table-backed leaves, named by their records' p[9])."""
 
-    def __init__(self, prims, program, chain):
+    def __init__(self, prims, program, chain, tables=()):
         self.prims = prims
         self.program = program
         self.chain = chain
+        self.tables = [np.ascontiguousarray(t, dtype=np.float32) for t in tables]
+
+    def with_table_addresses(self, addresses):
+        """A copy of the primitive records with each table-backed record's p[10] set to the raw bits
+        of addresses[p[9]] (the address of its table where the evaluator will read it)."""
+        prims = self.prims.copy()
+        for i in np.where(np.isin(prims["type"], TABLE_KINDS))[0]:
+            prims["p"][i, 10] = np.array([int(addresses[int(prims["p"][i, 9])])], np.uint64).view(np.float64)[0]
+        return prims
+
+    def sampling_guard(self):
+        """A bound on the float32 error of the table-backed leaves' samples (0 without them), for the
+        guard band of the float64 recheck: the sample coordinate carries a few float32 ulps of the
+        table's coordinate range, which moves the sample by that many cells times the table's steepest
+        step, and the interpolation rounds about a dozen times at the table's magnitude; doubled."""
+        bound = 0.0
+        for rec in self.prims:
+            if int(rec["type"]) not in TABLE_KINDS:
+                continue
+            t = self.tables[int(rec["p"][9])]
+            p = rec["p"]
+            if int(rec["type"]) == P_GRID:
+                pitch, shape, origin, axes = p[3], t.shape, np.abs(p[:3]), 3
+                scale = 1.0 if p[5] else pitch  # occupancy samples are (iso - v) * pitch
+            else:
+                pitch, shape, origin, axes = p[2], t.shape, np.abs(p[:2]), 2
+                scale = 1.0
+            reach = float(np.max(origin + (np.asarray(shape, np.float64) - 1) * pitch))
+            steep = max(float(np.abs(np.diff(t.astype(np.float64), axis=a)).max()) if t.shape[a] > 1 else 0.0
+                        for a in range(t.ndim))
+            coord = 4.0 * float(np.spacing(np.float32(reach))) / pitch
+            mag = float(np.abs(t).max()) + (abs(p[4]) if int(rec["type"]) == P_GRID else 0.0)
+            err = (axes * coord * steep + 12.0 * float(np.spacing(np.float32(mag)))) * scale
+            bound = max(bound, 2.0 * err * abs(float(rec["s"])))
+        return bound
+
+    def host_prims(self):
+        """The primitive records with the host tables' addresses (for CPU evaluators of them)."""
+        return self.with_table_addresses([t.ctypes.data for t in self.tables])
 
     @property
     def n_prims(self):
@@ -249,9 +328,25 @@ def _canon_lipschitz(p):
     return 1.0
 
 
+def _load_gridfield(node):
+    """(float32 array, origin, pitch) of a gridfield leaf, read as the reference reads it
+    (src/field_engine/ikarus_v1/eval_warp.py:448-452, including its precedence: the override applies
+    only when the npz carries ``pitch_mm``)."""
+    with np.load(node["npz_path"]) as d:
+        arr = np.asarray(d[node["key"]], dtype=np.float32)
+        origin = np.asarray(d["global_origin_mm"], dtype=np.float64) if "global_origin_mm" in d else np.zeros(3)
+        pitch = (node["pitch_override"] or float(d["pitch_mm"])) if "pitch_mm" in d else 1.0
+    if arr.ndim != 3 or min(arr.shape) < 1:
+        raise ValueError("gridfield array must be 3-D and nonempty")
+    if not np.isfinite(arr).all() or not (pitch > 0 and np.isfinite(pitch)):
+        raise ValueError("gridfield values and pitch must be finite (pitch > 0)")
+    return arr, origin, float(pitch)
+
+
 class _Compiler:
     def __init__(self):
         self.prims = []
+        self.tables = []
 
     def leaf(self, node, M, sigma):
         """PRIM record for a leaf under world->frame map M (4x4) and output scale sigma."""
@@ -311,7 +406,31 @@ class _Compiler:
             p[0] = node["radius"]
             typ = P_CYL_INF
         elif op == "gridfield":
-            raise ValueError("gridfield leaves are not supported by the GPU recipe compiler")
+            arr, origin, pitch = _load_gridfield(node)
+            f32 = lambda v: float(np.float32(v))  # the sampler's float32 parameters
+            p[:9] = (f32(origin[0]), f32(origin[1]), f32(origin[2]), f32(pitch), f32(node["iso"]),
+                     1.0 if node["mode"] == "sdf" else 0.0, *arr.shape)
+            p[9] = len(self.tables)
+            self.tables.append(arr)
+            typ = P_GRID
+        elif op == "revolve_table":
+            t = np.ascontiguousarray(node["table"], dtype=np.float32)
+            if t.ndim != 2 or min(t.shape) < 2 or not np.isfinite(t).all() or not node["pitch"] > 0:
+                raise ValueError("revolve_table needs a finite 2-D table of at least 2 x 2 and pitch > 0")
+            f32 = lambda v: float(np.float32(v))
+            p[:5] = (f32(node["r0"]), f32(node["z0"]), f32(node["pitch"]), *t.shape)
+            p[9] = len(self.tables)
+            self.tables.append(t)
+            typ = P_REVOLVE
+        elif op == "round_bar":
+            p[:3] = (node["radius"], node["z_lo"], node["z_hi"])
+            typ = P_BAR
+        elif op == "arched_pocket":
+            p[:5] = (node["half_x"], node["half_y"], node["edge_radius"], node["arch_radius"], node["arch_center_z"])
+            typ = P_POCKET
+        elif op == "cross_bore":
+            p[:3] = (node["radius"], node["axis_z"], node["half_length"])
+            typ = P_XBORE
         else:
             raise ValueError(f"unknown leaf op {op!r}")
         P = np.eye(4)[list(perm) + [3]]
@@ -328,7 +447,7 @@ class _Compiler:
     # ---- general postfix emission (no re-association)
     def emit(self, node, M, sigma, out):
         op = node["op"]
-        if op in LEAF_OPS or op == "gridfield":
+        if op in LEAF_OPS:
             out.append((OP_PUSH, self.leaf(node, M, sigma), 0.0))
         elif op == "transform":
             self.emit(node["child"], np.asarray(mat4_inverse_affine(node["mat4"])) @ M, sigma, out)
@@ -481,7 +600,7 @@ def compile_recipe(node) -> Compiled:
     ch = c.chain(node, np.eye(4), 1.0)
     if ch is not None:
         prims = np.array(c.prims, dtype=PRIM) if c.prims else np.zeros(0, PRIM)
-        return Compiled(prims, _records(_chain_to_program(ch)), _records(ch))
+        return Compiled(prims, _records(_chain_to_program(ch)), _records(ch), c.tables)
     c = _Compiler()
     prog = []
     c.emit(node, np.eye(4), 1.0, prog)
@@ -492,7 +611,7 @@ def compile_recipe(node) -> Compiled:
     if max_depth > 32:
         raise ValueError("expression tree too deep for the GPU stack evaluator (depth > 32)")
     prims = np.array(c.prims, dtype=PRIM) if c.prims else np.zeros(0, PRIM)
-    return Compiled(prims, _records(prog), None)
+    return Compiled(prims, _records(prog), None, c.tables)
 
 
 def compile_tools(tools):
@@ -503,6 +622,8 @@ def compile_tools(tools):
         ch = c.chain(tool, np.eye(4), 1.0)
         if ch is None or len(ch) != 1 or ch[0][0] != CH_SET:
             raise ValueError("an edit tool must be a single primitive")
+        if c.tables:
+            raise ValueError("an edit tool cannot be a table-backed leaf")
         recs.append(c.prims[ch[0][1]])
     return np.array(recs, dtype=PRIM) if recs else np.zeros(0, PRIM)
 
@@ -527,8 +648,9 @@ def extend(comp: Compiled, tool_prims, op="subtract") -> Compiled:
     program = np.concatenate([comp.program, _records(rows)])
     if comp.chain is not None:
         ch = CH_SUBTRACT if op == "subtract" else CH_UNION
-        return Compiled(prims, program, np.concatenate([comp.chain, _records([(ch, i, 0.0) for i in idx])]))
-    return Compiled(prims, program, None)
+        return Compiled(prims, program, np.concatenate([comp.chain, _records([(ch, i, 0.0) for i in idx])]),
+                        comp.tables)
+    return Compiled(prims, program, None, comp.tables)
 
 
 def eval_sdf_py(node, p):
@@ -612,6 +734,14 @@ def _prim_numpy(rec, pts):
         f = np.sqrt(qx * qx + z * z) - p[1]
     elif t == P_CYL_INF:
         f = np.sqrt(x * x + y * y) - p[0]
+    elif t == P_BAR:
+        f = np.maximum(np.sqrt(x * x + y * y) - p[0], np.maximum(p[1] - z, z - p[2]))
+    elif t == P_POCKET:
+        qx, qy = np.abs(x) - (p[0] - p[2]), np.abs(y) - (p[1] - p[2])
+        dxy = np.sqrt(np.maximum(qx, 0) ** 2 + np.maximum(qy, 0) ** 2) + np.minimum(np.maximum(qx, qy), 0) - p[2]
+        f = np.maximum(dxy, z - (p[4] + np.sqrt(np.maximum(p[3] * p[3] - x * x, 0.0))))
+    elif t == P_XBORE:
+        f = np.maximum(np.sqrt(y * y + (z - p[1]) ** 2) - p[0], np.abs(x) - p[2])
     else:
-        raise ValueError(f"unknown primitive type {t}")
+        raise ValueError(f"primitive type {t} has no host evaluator (table-backed kinds run on the device)")
     return rec["s"] * f - rec["off"]

@@ -11,6 +11,7 @@ live on the device; ``tiles`` materialises the reference's {brick id: array} dic
   bricks at their levels); the reference builds from a mesh (bygg_multires, :254-361), which is
   out of scope here.
 * ``avstand(F, punkter)`` and ``gradient(F, punkter)`` -- :405-459 -- answer on the GPU.
+* ``lagg_overlappsband(F)`` (:211-251, on the device) and ``kontinuitetscheck(F)`` (:462-521).
 """
 from __future__ import annotations
 
@@ -82,12 +83,16 @@ def _accel(builder):
     return pool.value, off.value, ln.value, boff.value, blen.value, bpool.value
 
 
-def bygg_multires_fran_recept(recipe, lo, h_grov, brick_shape, block=8, levels=None, device="cuda"):
+def bygg_multires_fran_recept(recipe, lo, h_grov, brick_shape, block=8, levels=None, device="cuda",
+                              overlappsband=True):
     """Build a MultiresField of an analytic recipe.
 
     ``levels``: None (all level 0), an int (one level for every active brick), a callable
     ``levels(list_lengths) -> int8 array`` over the active bricks (e.g. levels_by_list_length) or an
-    (n_bx, n_by, n_bz) int array."""
+    (n_bx, n_by, n_bz) int array.  ``overlappsband`` (the reference's default, bygg_multires
+    :254-361): finish with the overlap band, every fine brick's faces next to an active coarser brick
+    taking that brick's field (_lagg_overlappsband); False keeps every lattice point the recipe's own
+    value."""
     import torch
     lo = np.asarray(lo, dtype=np.float64)
     bx, by, bz = (int(v) for v in brick_shape)
@@ -147,7 +152,92 @@ def bygg_multires_fran_recept(recipe, lo, h_grov, brick_shape, block=8, levels=N
                                  levels={int(l): int(np.sum(lv == l)) for l in NIVAER}))
     F._dev = dict(kind=torch.from_numpy(kind).to(dev), level=torch.from_numpy(niva).to(dev),
                   tile_off=torch.from_numpy(tile_off).to(dev), tile_off_host=tile_off, pool=pool, builder=fb)
+    if overlappsband:
+        F.stats["overlap_faces"] = lagg_overlappsband(F)
     return F
+
+
+def lagg_overlappsband(F: MultiresField) -> int:
+    """Overwrite every fine brick's face layer with the coarser active neighbour's field on that face,
+    in place on the device (faltkarna_v1_multires.py:211-251: the same bricks, faces, order and
+    float64 sampling, so the lattices equal the reference's bit for bit).  Returns the number of faces
+    written."""
+    import torch
+    d = F._dev
+    lv = F.niva.ravel()
+    act = np.flatnonzero(F.kind.ravel() == 0)
+    fine = act[lv[act] >= 1]
+    if not len(fine):
+        return 0
+    order = np.lexsort((fine, lv[fine]))  # by level, then by id
+    bricks = fine[order].astype(np.int32)
+    n_of_level = np.array([0] + [int(np.sum(lv[fine] == l)) for l in (1, 2, 3)], np.int32)
+    pool = d["pool"]
+    dev = pool.device
+    orig = torch.empty_like(pool)
+    faces = torch.zeros(1, dtype=torch.int32, device=dev)
+    d_bricks = torch.from_numpy(bricks).to(dev)
+    bshape = np.array(F.brick_shape, np.int32)
+    st = d["builder"].lib.fb_multires_band_device(F.lo.ctypes.data, F.h_grov, F.block, bshape.ctypes.data,
+                                                  d["kind"].data_ptr(), d["level"].data_ptr(), d["tile_off"].data_ptr(),
+                                                  pool.data_ptr(), pool.numel(), orig.data_ptr(), d_bricks.data_ptr(),
+                                                  n_of_level.ctypes.data, faces.data_ptr(), _lib.stream_handle())
+    _lib.check(st, "multires overlap band")
+    return int(faces.item())
+
+
+def kontinuitetscheck(F: MultiresField, eps_frac=1.0e-3, max_punkter_per_face=None):
+    """Largest jump of the delivered field across every brick face where the pitch changes
+    (faltkarna_v1_multires.py:462-521): each such face sampled at the finer side's face lattice,
+    avstand evaluated a hair (eps_frac of the finer pitch) inside the fine brick and inside the coarse
+    neighbour; the bound is half the coarser pitch.  All faces' points go to the device in two
+    queries.  Returns the reference's dict."""
+    n_bx, n_by, n_bz = F.brick_shape
+    kind, niva = F.kind, F.niva
+    faces, p_in, p_out = [], [], []
+    grans = 0.0
+    for lin in np.flatnonzero(kind.ravel() == 0):
+        bi, bj, bk = int(lin // (n_by * n_bz)), int((lin // n_bz) % n_by), int(lin % n_bz)
+        lvl = int(niva[bi, bj, bk])
+        n_l = F.block * (1 << lvl)
+        h_f = F.pitch_of(lvl)
+        b_origin = F.lo + np.array([bi, bj, bk], dtype=np.float64) * F.L
+        for ax in range(3):
+            for sida in (-1, +1):
+                nb = [bi, bj, bk]
+                nb[ax] += sida
+                if not (0 <= nb[0] < n_bx and 0 <= nb[1] < n_by and 0 <= nb[2] < n_bz):
+                    continue
+                if kind[nb[0], nb[1], nb[2]] != 0:
+                    continue
+                lvl_n = int(niva[nb[0], nb[1], nb[2]])
+                if lvl_n >= lvl:
+                    continue
+                idx = [np.arange(n_l + 1, dtype=np.float64)] * 3
+                idx[ax] = np.array([0.0 if sida < 0 else float(n_l)])
+                gi, gj, gk = np.meshgrid(*idx, indexing="ij")
+                pts = np.stack([gi.ravel(), gj.ravel(), gk.ravel()], axis=1) * h_f + b_origin
+                if max_punkter_per_face is not None and len(pts) > max_punkter_per_face:
+                    pts = pts[::int(np.ceil(len(pts) / max_punkter_per_face))]
+                e = np.zeros(3)
+                e[ax] = eps_frac * h_f
+                p_in.append(pts - sida * e)
+                p_out.append(pts + sida * e)
+                faces.append((len(pts), dict(brick=[bi, bj, bk], axel=ax, sida=sida, niva=lvl, niva_granne=lvl_n)))
+                grans = max(grans, 0.5 * F.pitch_of(lvl_n))
+    if not faces:
+        return dict(n_pitchbyten_faces=0, n_provpunkter=0, max_hopp_mm=0.0, medel_hopp_mm=0.0, grans_mm=0.0,
+                    varsta=None, GRON=True)
+    hopp = np.abs(avstand(F, np.concatenate(p_in)) - avstand(F, np.concatenate(p_out)))
+    bounds = np.cumsum([0] + [n for n, _ in faces])
+    per_face = np.array([hopp[a:b].max() for a, b in zip(bounds[:-1], bounds[1:])])
+    max_hopp, varsta = 0.0, None
+    for (n, info), m in zip(faces, per_face):  # first face with a strictly larger jump, as the reference
+        if float(m) > max_hopp:
+            max_hopp, varsta = float(m), info
+    return dict(n_pitchbyten_faces=len(faces), n_provpunkter=int(len(hopp)), max_hopp_mm=max_hopp,
+                medel_hopp_mm=float(hopp.sum()) / len(hopp), grans_mm=grans, varsta=varsta,
+                GRON=bool(max_hopp <= grans))
 
 
 def _copy_device(dst, src_ptr, nbytes):

@@ -133,3 +133,62 @@ def gradient_batch(node, points_mm, h=0.05, device="cuda"):
     grad = torch.empty((len(pts), 3), dtype=torch.float32, device=q.device)
     q._run(pts_t, None, grad, h=h)
     return grad.cpu().numpy()
+
+
+_GRID_UPLOADS = {}  # (leaf identities, device) -> (params tensor, table buffer)
+
+
+def _pack_gridfields(grid_leaves, device):
+    """Every gridfield leaf's table in one device buffer (256-byte aligned parts) and a float32
+    record of 12 per leaf (origin, pitch, iso, is_sdf, nx, ny, nz, -, table address halves); loaded
+    and uploaded once per (leaves, device), as the reference caches its packing
+    (src/field_engine/ikarus_v1/eval_warp.py:430-475)."""
+    import torch
+    from .expr import _load_gridfield
+    key = (tuple((lf["npz_path"], lf["key"], lf["mode"], float(lf["iso"]), lf.get("pitch_override"))
+                 for lf in grid_leaves), str(device))
+    if key in _GRID_UPLOADS:
+        return _GRID_UPLOADS[key]
+    loaded = [_load_gridfield(lf) for lf in grid_leaves]
+    sizes = [(a.nbytes + 255) // 256 * 256 for a, _, _ in loaded]
+    buf = torch.empty(max(sum(sizes), 256), dtype=torch.uint8, device=device)
+    params = np.zeros((len(loaded), 12), np.float32)
+    at = 0
+    for k, ((arr, origin, pitch), lf, size) in enumerate(zip(loaded, grid_leaves, sizes)):
+        buf[at:at + arr.nbytes].copy_(torch.from_numpy(arr.view(np.uint8).reshape(-1)))
+        addr = buf.data_ptr() + at
+        params[k, :9] = (origin[0], origin[1], origin[2], pitch, lf["iso"], 1.0 if lf["mode"] == "sdf" else 0.0,
+                         *arr.shape)
+        params[k, 10:12] = np.array([addr & 0xFFFFFFFF, addr >> 32], np.uint32).view(np.float32)
+        at += size
+    entry = (torch.from_numpy(params).to(device), buf)
+    _GRID_UPLOADS[key] = entry
+    return entry
+
+
+def eval_batch_multi_pair(points_mm, pair_of_point, leaf_a_of_pair, leaf_b_of_pair, grid_leaves_all,
+                          device="cuda"):
+    """max(sdf_A, sdf_B) at every point, its pair's two gridfield leaves chosen per point, all pairs
+    in one launch (src/field_engine/ikarus_v1/eval_warp.py:545-564): points (N, 3), pair_of_point
+    (N,) pair ids, leaf_a_of_pair / leaf_b_of_pair (n_pairs,) indices into grid_leaves_all (gridfield
+    node dicts).  Returns (N,) float32."""
+    import torch
+    pts = _points(points_mm)
+    pop = np.ascontiguousarray(pair_of_point, dtype=np.int32).reshape(-1)
+    la = np.ascontiguousarray(leaf_a_of_pair, dtype=np.int32).reshape(-1)
+    lb = np.ascontiguousarray(leaf_b_of_pair, dtype=np.int32).reshape(-1)
+    if len(pop) != len(pts) or len(la) != len(lb) or len(la) < 1 or len(grid_leaves_all) < 1:
+        raise ValueError("one pair id per point and two leaves per pair required")
+    if pop.size and (pop.min() < 0 or pop.max() >= len(la)):
+        raise ValueError("pair id outside the pairs")
+    if la.min() < 0 or lb.min() < 0 or max(la.max(), lb.max()) >= len(grid_leaves_all):
+        raise ValueError("leaf index outside grid_leaves_all")
+    dev = torch.device(device)
+    params, _buf = _pack_gridfields(list(grid_leaves_all), dev)
+    d_pts = torch.from_numpy(pts.astype(np.float32)).to(dev)
+    d_pop, d_la, d_lb = (torch.from_numpy(a).to(dev) for a in (pop, la, lb))
+    out = torch.empty(len(pts), dtype=torch.float32, device=dev)
+    _lib.check(_lib.lib().fb_grid_pairs_device(params.data_ptr(), len(grid_leaves_all), d_pts.data_ptr(),
+                                               d_pop.data_ptr(), len(pts), d_la.data_ptr(), d_lb.data_ptr(), len(la),
+                                               out.data_ptr(), _lib.stream_handle()), "eval_batch_multi_pair")
+    return out.cpu().numpy()

@@ -223,3 +223,66 @@ def mesh_scene(seed=0, offset=0.0, fine=1):
     t = mesh_torus(rng.uniform(5, 7, 3) + np.array([0, 8, 0]), rng.uniform(3, 4), rng.uniform(0.8, 1.4), 48 * fine, 24 * fine)
     V, T = mesh_merge(s, b, t)
     return V + offset, T
+
+
+# ------------------------------------------------------------------------------------ machining scene
+# The reference's machining test part (src/field_engine/tillverkningsfalt_v1_kernel.py:56-118, :190-236):
+# a stepped shaft with three ring grooves, turned from a round bar with a 1 mm nose radius, a pocket
+# milled with a 3 mm end mill under an arched roof, and a cross bore.
+MACHINING = dict(rho_turn=1.0, rho_mill=3.0, drill_r=11.15, radial_allowance=1.5, axial_allowance=1.0,
+                 pitch2d=0.04, r_land=47.7, r_groove=45.5, groove_w=3.0, z_lo=-21.0, z_hi=32.0,
+                 groove_centers=(14.0, 19.0, 24.0), half_x=10.4, half_y=23.0, arch_r=10.4, roof_z=17.6,
+                 drill_z=11.15, drill_x_short=30.0)
+
+
+def turned_profile_table(c=MACHINING):
+    """(sdf2d float32 (nr, nz), r0, z0) of the turned profile: the sharp-cornered (r, z) profile
+    rasterised at pitch2d, closed with a disk of the nose radius (what a nose-radius tool reaches:
+    convex corners sharp, concave ones rounded), then signed by exact Euclidean distance transforms
+    (negative inside) -- the construction of tillverkningsfalt_v1_kernel.py:91-131.  The closing is
+    dilation then erosion by thresholding exact distances (outside-the-raster pixels ignored)."""
+    from scipy import ndimage
+    poly = [(c["z_lo"], c["r_land"])]
+    for zc in c["groove_centers"]:
+        h = c["groove_w"] / 2.0
+        poly += [(zc - h, c["r_land"]), (zc - h, c["r_groove"]), (zc + h, c["r_groove"]), (zc + h, c["r_land"])]
+    poly += [(c["z_hi"], c["r_land"])]
+    poly = sorted(poly, key=lambda t: t[0])
+    p2 = c["pitch2d"]
+    z0, z1 = c["z_lo"] - 2.0, c["z_hi"] + 2.0
+    r0, r1 = 0.0, c["r_land"] + 2.0
+    nz = int(round((z1 - z0) / p2)) + 1
+    nr = int(round((r1 - r0) / p2)) + 1
+    zz = np.linspace(z0, z1, nz)
+    rr = np.linspace(r0, r1, nr)
+    r_of_z = np.interp(zz, [q[0] for q in poly], [q[1] for q in poly])
+    mask0 = rr[:, None] <= r_of_z[None, :]
+    rho = max(1, int(round(c["rho_turn"] / p2)))
+    dilated = ndimage.distance_transform_edt(~mask0) <= rho
+    closed = ~(ndimage.distance_transform_edt(dilated) <= rho)
+    d_out = ndimage.distance_transform_edt(~closed) * p2
+    d_in = ndimage.distance_transform_edt(closed) * p2
+    return np.where(closed, -d_in, d_out).astype(np.float32), float(rr[0]), float(zz[0])
+
+
+def machining_scene(pitch3d=0.35, block=8, short_drill=False, c=MACHINING):
+    """(recipe, GridMeta, table, constants) of the machining part: the round bar intersected with the
+    revolved turned profile, minus the arched pocket, minus the cross bore (through the whole bar, or
+    the short negative-control drill) -- the operations and grid of tillverkningsfalt_v1_kernel.py:
+    193-236, 248-300."""
+    from . import expr as X
+    table, r0, z0 = turned_profile_table(c)
+    r_blank = c["r_land"] + c["radial_allowance"]
+    zb_lo, zb_hi = c["z_lo"] - c["axial_allowance"], c["z_hi"] + c["axial_allowance"]
+    arch_cz = c["roof_z"] - c["arch_r"]
+    half = c["drill_x_short"] if short_drill else r_blank + 1
+    recipe = X.intersect(X.round_bar(r_blank, zb_lo, zb_hi), X.revolve_table(table, r0, z0, c["pitch2d"]))
+    recipe = X.subtract(recipe, X.arched_pocket(c["half_x"], c["half_y"], c["rho_mill"], c["arch_r"], arch_cz))
+    recipe = X.subtract(recipe, X.cross_bore(c["drill_r"], c["drill_z"], half))
+    x0 = -r_blank - 1
+    n_xy = int(round((2 * r_blank + 2) / pitch3d)) + 1
+    nz = int(round((zb_hi - zb_lo) / pitch3d)) + 1
+    meta = GridMeta(x0, x0, zb_lo, pitch3d, n_xy, n_xy, nz, block)
+    consts = dict(r_blank=r_blank, z_blank_lo=zb_lo, z_blank_hi=zb_hi, arch_cz=arch_cz, drill_x_half=half,
+                  r0_2d=r0, z0_2d=z0, **c)
+    return recipe, meta, table, consts

@@ -67,6 +67,8 @@ def parse():
                          "mixed pitch; tree: packed adaptive block tree of a dense 512^3 field, built and sampled; "
                          "mesh: mesh -> signed distance field stage")
     ap.add_argument("--no-serve", action="store_true", help="batched: leave out the short serving run")
+    ap.add_argument("--quick", action="store_true",
+                    help="batched: the timed builds only (no plain path, EDT form, accuracy, extras) -- for profiling")
     ap.add_argument("--cpu-fraction", type=float, default=0.0005,
                     help="share of every recipe's blocks in one CPU-baseline / reference-arm sample")
     ap.add_argument("--recipes", type=int, default=256)
@@ -365,7 +367,7 @@ def e2e_leg(comp, meta, mask_np, dev, steps=2):
     times = []
     h2d = d2h = 0
     leaf = 0
-    for _ in range(steps + 1):
+    for _ in range(steps + 2):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sf = B.build_field(comp, meta, device=dev)
@@ -375,7 +377,10 @@ def e2e_leg(comp, meta, mask_np, dev, steps=2):
         leaf = sf.tiles.size
         h2d = comp.prims.nbytes + comp.chain.nbytes + binary.size
         d2h = sf.kind.nbytes + sf.corner_min_abs.nbytes + sf.active_ids.nbytes + sf.tiles.nbytes + sq.nbytes + 4
-    times = times[1:]
+        # the caller is done with this step's arrays: their page-locked blocks go back to the cache
+        del sf, sq
+        gc.collect()
+    times = times[2:]
     return {"value": leaf / statistics.median(times) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "seconds_per_step": statistics.median(times),
             "api": "field_b200.build.build_field + field_b200.edt.NativeEDTLarge.squared_distance"}
@@ -563,7 +568,7 @@ def run_headline(args, rank, world, local_rank):
     # (grown once if the device reports it too small), graph capture
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    bb = BT.BatchBuilder(recipes, device=dev, edt=True, streams=args.streams)
+    bb = BT.BatchBuilder(recipes, device=dev, edt=not args.quick, streams=args.streams)
     bb.enqueue(edt=False)
     grew = bb.ensure_capacity(edt=False)
     torch.cuda.synchronize()
@@ -595,8 +600,9 @@ def run_headline(args, rank, world, local_rank):
     if bb.status() != 0:
         raise RuntimeError("batched build failed")
     step_ms = [e[0].elapsed_time(e[5]) for e in events]
-    names = ("cull", "classify", "compact", "lists", "leaf")
-    phases = {nm: float(statistics.median(e[i].elapsed_time(e[i + 1]) for e in events)) for i, nm in enumerate(names)}
+    # events: start, culling, classification (with the active blocks' lists), compaction, (empty), leaves
+    names = {"cull": 0, "classify": 1, "compact": 2, "leaf": 4}
+    phases = {nm: float(statistics.median(e[i].elapsed_time(e[i + 1]) for e in events)) for nm, i in names.items()}
     total_ms = max_over_ranks(float(sum(step_ms)), world, dev)
     counts = bb.active_counts()
     leaf_voxels = bb.leaf_voxels
@@ -612,14 +618,18 @@ def run_headline(args, rank, world, local_rank):
                    "n_active": int(counts.sum()), "leaf_voxels": leaf_voxels, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between steps, outside the per-step events"},
         "phases_ms_median": phases,
-        "batch": {"launches_per_step": bb.launches - (5 + 3 * len(bb)), "schedule_ctas_per_sm": bb.ctas_per_sm,
+        "batch": {"launches_per_step": bb.launches - (5 + 3 * len(bb) if bb.has_edt else 0),
+                  "schedule_ctas_per_sm": bb.ctas_per_sm,
                   "schedule_ms": schedule, "arena_grown": bool(grew), "compile_s": t_compile, "autotune_s": t_tune,
                   "autotune_buckets": {"from_table": known, "measured_now": len(tuner.table) - known,
                                        "table": tuner.table},
                   "fresh_batch_first_build_s": t_first},
         "clocks": clk,
-        "gpu_launches": (bb.launches - (5 + 3 * len(bb))) * args.steps,
+        "gpu_launches": (bb.launches - (5 + 3 * len(bb) if bb.has_edt else 0)) * args.steps,
     }
+    if args.quick:
+        bb.close()
+        return result
     # the same build from one CUDA graph (captured once)
     t0 = time.perf_counter()
     bb.capture(edt=False)
@@ -1041,7 +1051,8 @@ def run_precision(args):
     comp = X.compile_recipe(recipe)
     # the fine pitch where a brick's culled list is at least the median length (the crowded bricks)
     fine = lambda lens: np.where(np.asarray(lens) >= np.median(lens), 2, 0)
-    build = lambda: M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 128, (16, 16, 16), block=8, levels=fine)
+    build = lambda: M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 128, (16, 16, 16), block=8, levels=fine,
+                                                overlappsband=False)
     build()  # warm-up: kernels configured
     torch.cuda.synchronize()
     t0 = time.perf_counter()

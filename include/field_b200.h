@@ -163,7 +163,8 @@ typedef struct fb_batch_item {
 void* fb_batch_create(const fb_batch_item* items, int32_t n, void* stream);
 int fb_batch_build_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm, void* stream);
 /* No reference counterpart: the same build, recording events[0..5] (nullable cudaEvent_t) at its
- * start and after culling, classification, compaction, per-block lists and leaves, and adding the
+ * start and after culling, classification (with the active blocks' lists), compaction, an empty
+ * phase, and leaves, and adding the
  * leaf pass's executed primitive evaluations and float32 operations to d_work[0..1] (nullable). */
 int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, int32_t ctas_per_sm,
                                 void* const* events, uint64_t* d_work, void* stream);
@@ -271,6 +272,24 @@ int fb_packed_query_device(const void* d_nodes, const float* d_payload, const in
                            double pitch, const double* d_points, int64_t n, float* d_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------ point queries */
+
+/* Replaces _lagg_overlappsband, src/field_engine/faltkarna_v1_multires.py:211-251: every fine brick's
+ * faces that meet an active coarser brick take the trilinear sample (scipy map_coordinates order 1,
+ * mode nearest) of that brick's lattice, in the reference's brick and face order.  d_orig: scratch of
+ * pool_len floats; d_bricks: active bricks of level >= 1 sorted by level and id, n_of_level[1..3]
+ * of each level (n_of_level[0] unused); d_faces: faces written.  Stream-ordered. */
+int fb_multires_band_device(const double* lo, double h, int32_t B, const int32_t* bshape, const int8_t* d_kind,
+                            const int8_t* d_level, const int64_t* d_tile_off, float* d_pool, int64_t pool_len,
+                            float* d_orig, const int32_t* d_bricks, const int32_t* n_of_level, int32_t* d_faces,
+                            void* stream);
+
+/* Replaces eval_batch_multi_pair, src/field_engine/ikarus_v1/eval_warp.py:545-564: max(sample(A),
+ * sample(B)) per point, A / B the gridfield leaves of the point's pair, every pair in one launch.
+ * d_params: 12 float32 per leaf (origin xyz, pitch, iso, is_sdf, nx, ny, nz, unused, the table's
+ * device address as two 32-bit halves); an out-of-range pair or leaf index reads NaN. */
+int fb_grid_pairs_device(const float* d_params, int32_t n_leaves, const float* d_pts, const int32_t* d_pair,
+                         int64_t n, const int32_t* d_leaf_a, const int32_t* d_leaf_b, int32_t n_pairs, float* d_out,
+                         void* stream);
 
 /* Replace eval_batch / gradient_batch, src/field_engine/ikarus_v1/eval_warp.py:478-488,718-733.
  * fb_query_prepare fills the 128-byte float32 primitive mirror; fb_field_accel exposes a

@@ -522,3 +522,75 @@ def ref_mesh_field(V, T, origin, pitch, jitter, shape, surface_correction=True, 
                              int(bool(surface_correction)), int(nthreads), solid.ctypes.data, sd.ctypes.data,
                              yta.ctypes.data, stats.ctypes.data, ts.ctypes.data)
     return rc, solid.view(bool), sd, yta.view(bool), stats
+
+
+# ----------------------------------------------------------------------------------------- machining scene
+def cnc_subtract(table, r0_2d, z0_2d, pitch2d, pts, r_blank, z_blank_lo, z_blank_hi, px, py, arch_r, arch_cz,
+                 rho_mill, drill_r, drill_z, drill_x_half):
+    """float64 material field of the reference's machining kernel at points (N, 3), operation for
+    operation (src/field_engine/tillverkningsfalt_v1_kernel.py:248-300): blank, bilinear turned
+    profile, max, the pocket subtracted, the bore subtracted."""
+    x, y, z = (np.asarray(pts, np.float64)[:, k] for k in range(3))
+    nr2d, nz2d = table.shape
+    r = np.sqrt(x * x + y * y)
+    blank = np.maximum(r - r_blank, np.maximum(z_blank_lo - z, z - z_blank_hi))
+    fr = (r - r0_2d) / pitch2d
+    fz = (z - z0_2d) / pitch2d
+    ir0 = np.clip(np.trunc(fr).astype(np.int64), 0, nr2d - 2)
+    iz0 = np.clip(np.trunc(fz).astype(np.int64), 0, nz2d - 2)
+    tr = np.clip(fr - ir0, 0.0, 1.0)
+    tz = np.clip(fz - iz0, 0.0, 1.0)
+    t = table.astype(np.float64)
+    turned = (t[ir0, iz0] * (1 - tr) * (1 - tz) + t[ir0, iz0 + 1] * (1 - tr) * tz + t[ir0 + 1, iz0] * tr * (1 - tz)
+              + t[ir0 + 1, iz0 + 1] * tr * tz)
+    material = np.maximum(blank, turned)
+    qx = np.abs(x) - (px - rho_mill)
+    qy = np.abs(y) - (py - rho_mill)
+    dxy = np.sqrt(np.maximum(qx, 0) ** 2 + np.maximum(qy, 0) ** 2) + np.minimum(np.maximum(qx, qy), 0) - rho_mill
+    roof = arch_cz + np.sqrt(np.maximum(arch_r * arch_r - x * x, 0.0))
+    material = np.maximum(material, -np.maximum(dxy, z - roof))
+    bore = np.maximum(np.sqrt(y * y + (z - drill_z) ** 2) - drill_r, np.abs(x) - drill_x_half)
+    return np.maximum(material, -bore)
+
+
+def multires_overlap_band(lo, h, block, brick_shape, kind, niva, tiles):
+    """faltkarna_v1_multires.py:211-251 restated: bricks in ascending id, faces axis 0..2, side -1 then
+    +1, each face of a fine brick next to an active coarser brick overwritten in place with
+    scipy.ndimage.map_coordinates(order=1, mode='nearest') of that brick's lattice.  Returns (new
+    tiles dict, faces written)."""
+    from scipy import ndimage
+    tiles = {k: v.copy() for k, v in tiles.items()}
+    n_bx, n_by, n_bz = brick_shape
+    L = block * h
+    faces = 0
+    for lin in sorted(tiles):
+        bi, bj, bk = lin // (n_by * n_bz), (lin // n_bz) % n_by, lin % n_bz
+        lvl = int(niva[bi, bj, bk])
+        if lvl == 0:
+            continue
+        n_l = block * (1 << lvl)
+        b_origin = lo + np.array([bi, bj, bk], dtype=np.float64) * L
+        for ax in range(3):
+            for sida in (-1, +1):
+                nb = [bi, bj, bk]
+                nb[ax] += sida
+                if not (0 <= nb[0] < n_bx and 0 <= nb[1] < n_by and 0 <= nb[2] < n_bz):
+                    continue
+                if kind[nb[0], nb[1], nb[2]] != 0:
+                    continue
+                lvl_n = int(niva[nb[0], nb[1], nb[2]])
+                if lvl_n >= lvl:
+                    continue
+                idx = [np.arange(n_l + 1, dtype=np.float64)] * 3
+                idx[ax] = np.array([0.0 if sida < 0 else float(n_l)])
+                gi, gj, gk = np.meshgrid(*idx, indexing="ij")
+                pts = np.stack([gi.ravel(), gj.ravel(), gk.ravel()], axis=1) * (h / float(1 << lvl)) + b_origin
+                nb_origin = lo + np.array(nb, dtype=np.float64) * L
+                lok = (pts - nb_origin) / (h / float(1 << lvl_n))
+                nlin = (nb[0] * n_by + nb[1]) * n_bz + nb[2]
+                v = ndimage.map_coordinates(tiles[nlin], lok.T, order=1, mode="nearest")
+                sl = [slice(None)] * 3
+                sl[ax] = 0 if sida < 0 else n_l
+                tiles[lin][tuple(sl)] = v.reshape(tiles[lin][tuple(sl)].shape).astype(np.float32)
+                faces += 1
+    return tiles, faces

@@ -514,7 +514,8 @@ typedef struct {
 } or_insn;
 
 enum { OP_PUSH = 0, OP_UNION = 1, OP_INTERSECT = 2, OP_SUBTRACT = 3, OP_OFFSET = 4 };
-enum { P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF };
+enum { P_SPHERE = 0, P_BOX, P_CYLINDER, P_CONE, P_HALFSPACE, P_FRUSTUM, P_CAPSULE, P_TORUS, P_CYL_INF,
+       P_GRID, P_REVOLVE, P_BAR, P_POCKET, P_XBORE };
 
 static double or_max(double a, double b) { return a > b ? a : b; }
 static double or_min(double a, double b) { return a < b ? a : b; }
@@ -524,6 +525,53 @@ static double or_clamp01(double t) { return or_min(or_max(t, 0.0), 1.0); }
  * src/field_engine/ikarus_v1/expr.py:268-340 (and faltkarna_v1.py:91-99 for the box); capsule and
  * torus have no counterpart in the reference and follow the textbook closed forms (segment
  * distance minus radius; distance to the major circle minus the minor radius). */
+/* Table-backed leaves keep the address of their float32 table in p[10] (raw bits). */
+static const float *or_table(const double *p) {
+    uint64_t bits;
+    memcpy(&bits, &p[10], sizeof(bits));
+    return (const float *)(uintptr_t)bits;
+}
+
+static double or_lerp(double a, double b, double t) { return a * (1.0 - t) + b * t; }
+
+/* Gridfield leaf: src/field_engine/ikarus_v1/eval_warp.py:94-147 -- 1e6 outside the grid, else the
+ * trilinear sample (lerps in x, then y, then z); occupancy tables read (iso - v) * pitch.
+ * p = {ox, oy, oz, pitch, iso, is_sdf, nx, ny, nz, -, table}. */
+static double or_grid(const double *p, double x, double y, double z) {
+    const int nx = (int)p[6], ny = (int)p[7], nz = (int)p[8];
+    const double pitch = p[3];
+    const double fx = (x - p[0]) / pitch, fy = (y - p[1]) / pitch, fz = (z - p[2]) / pitch;
+    if (!(fx >= 0.0 && fy >= 0.0 && fz >= 0.0 && fx <= nx - 1 && fy <= ny - 1 && fz <= nz - 1)) return 1.0e6;
+    const int ix = (int)floor(fx), iy = (int)floor(fy), iz = (int)floor(fz);
+    const int ix1 = ix + 1 < nx ? ix + 1 : nx - 1, iy1 = iy + 1 < ny ? iy + 1 : ny - 1, iz1 = iz + 1 < nz ? iz + 1 : nz - 1;
+    const double tx = fx - ix, ty = fy - iy, tz = fz - iz;
+    const float *g = or_table(p);
+#define AT(i, j, k) ((double)g[((int64_t)(i) * ny + (j)) * nz + (k)])
+    const double c00 = or_lerp(AT(ix, iy, iz), AT(ix1, iy, iz), tx), c10 = or_lerp(AT(ix, iy1, iz), AT(ix1, iy1, iz), tx);
+    const double c01 = or_lerp(AT(ix, iy, iz1), AT(ix1, iy, iz1), tx), c11 = or_lerp(AT(ix, iy1, iz1), AT(ix1, iy1, iz1), tx);
+#undef AT
+    const double val = or_lerp(or_lerp(c00, c10, ty), or_lerp(c01, c11, ty), tz);
+    return p[5] != 0.0 ? val : (p[4] - val) * pitch;
+}
+
+/* Revolved (r, z) table: src/field_engine/tillverkningsfalt_v1_kernel.py:265-277 -- r the distance
+ * from the z axis, cell indices truncated then clamped to the table, weights clamped to [0, 1].
+ * p = {r0, z0, pitch, nr, nz, -, ..., table}. */
+static double or_revolve(const double *p, double x, double y, double z) {
+    const int nr = (int)p[3], nz = (int)p[4];
+    const double r = sqrt(x * x + y * y);
+    const double fr = (r - p[0]) / p[2], fz = (z - p[1]) / p[2];
+    const double cr = fr < -1e9 ? -1e9 : (fr > 1e9 ? 1e9 : fr), cz = fz < -1e9 ? -1e9 : (fz > 1e9 ? 1e9 : fz);
+    int ir = (int)cr, iz = (int)cz;
+    ir = ir < 0 ? 0 : (ir > nr - 2 ? nr - 2 : ir);
+    iz = iz < 0 ? 0 : (iz > nz - 2 ? nz - 2 : iz);
+    const double tr = or_clamp01(fr - ir), tz = or_clamp01(fz - iz);
+    const float *g = or_table(p);
+    const double v00 = g[(int64_t)ir * nz + iz], v01 = g[(int64_t)ir * nz + iz + 1];
+    const double v10 = g[(int64_t)(ir + 1) * nz + iz], v11 = g[(int64_t)(ir + 1) * nz + iz + 1];
+    return v00 * (1.0 - tr) * (1.0 - tz) + v01 * (1.0 - tr) * tz + v10 * tr * (1.0 - tz) + v11 * tr * tz;
+}
+
 static double or_prim_local(const or_prim *P, double x, double y, double z) {
     const double *p = P->p;
     switch (P->type) {
@@ -580,6 +628,23 @@ static double or_prim_local(const or_prim *P, double x, double y, double z) {
     }
     case P_CYL_INF: /* unbounded z cylinder, src/field_engine/faltkarna_v1.py:102-104 */
         return sqrt(x * x + y * y) - p[0];
+    case P_GRID:
+        return or_grid(p, x, y, z);
+    case P_REVOLVE:
+        return or_revolve(p, x, y, z);
+    case P_BAR: /* round bar (the blank), src/field_engine/tillverkningsfalt_v1_kernel.py:262-263 */
+        return or_max(sqrt(x * x + y * y) - p[0], or_max(p[1] - z, z - p[2]));
+    case P_POCKET: { /* rounded-box pocket under an arched roof, tillverkningsfalt_v1_kernel.py:281-291 */
+        double qx = fabs(x) - (p[0] - p[2]), qy = fabs(y) - (p[1] - p[2]);
+        double ox = or_max(qx, 0.0), oy = or_max(qy, 0.0);
+        double dxy = sqrt(ox * ox + oy * oy) + or_min(or_max(qx, qy), 0.0) - p[2];
+        double roof = p[4] + sqrt(or_max(p[3] * p[3] - x * x, 0.0));
+        return or_max(dxy, z - roof);
+    }
+    case P_XBORE: { /* cross bore along x clipped to |x| <= half, tillverkningsfalt_v1_kernel.py:294-297 */
+        double dz = z - p[1];
+        return or_max(sqrt(y * y + dz * dz) - p[0], fabs(x) - p[2]);
+    }
     default:
         return NAN;
     }

@@ -91,6 +91,7 @@ def test_graph_replays_equal_eager_builds_and_are_deterministic():
     import field_b200.batch as BT
     bb = BT.BatchBuilder(_recipes(8, seed=21))
     bb.enqueue()
+    bb.ensure_capacity()  # the default arena may be short for the 16^3-leaf recipes
     torch.cuda.synchronize()
     eager = [f[2].copy() for f in _batch_fields(bb)]
     bb.tiles.zero_()
@@ -109,6 +110,8 @@ def test_batch_with_edt_equals_plain_path():
     import field_b200.batch as BT
     recipes = _recipes(7, seed=23)
     bb = BT.BatchBuilder(recipes, edt=True, streams=3)
+    bb.enqueue(edt=True)
+    bb.ensure_capacity(edt=True)
     bb.replay(edt=True)
     torch.cuda.synchronize()
     assert bb.status() == 0

@@ -110,7 +110,7 @@ def test_multires_tiles_and_queries():
     rng = np.random.default_rng(9)
     recipe = X.union_all(R.parts(rng, 12, 12, 6, 6, scale=0.8))
     F = M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 64, (8, 8, 8), block=8,
-                                    levels=lambda lens: M.levels_by_list_length(lens, (2, 3)))
+                                    levels=lambda lens: M.levels_by_list_length(lens, (2, 3)), overlappsband=False)
     assert F.stats["n_active"] > 0
     worst, rel, sign = _multires_check(F, recipe)
     assert sign == 0 and worst <= 1e-5 and rel <= 1e-5, (worst, rel)
@@ -135,9 +135,37 @@ def test_precision_stress_near_tangent_pairs_and_thin_walls():
     import field_b200.multires as M
     import field_b200.recipes as R
     recipe = R.tangent_pairs(seed=4, n_pairs=150, pitch=1.0 / 512, walls=16)
-    F = M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 128, (16, 16, 16), block=8,
+    F = M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 128, (16, 16, 16), block=8, overlappsband=False,
                                     levels=lambda lens: np.where(np.asarray(lens) >= 2, 2, 0))
     assert F.stats["levels"][2] > 0 and F.stats["levels"][0] > 0
     worst, rel, sign = _multires_check(F, recipe, n_check=16, seed=1)
     assert sign == 0
     assert worst <= 1e-5 and rel <= 1e-5, (worst, rel)
+
+
+def test_multires_overlap_band_and_continuity_match_oracle():
+    """The overlap band on the device equals the reference's sequential band (restated with scipy's
+    map_coordinates) lattice for lattice, bit for bit, and kontinuitetscheck's jumps equal the
+    oracle-evaluated ones; with the band the jump across pitch changes stays within the reference's
+    bound (half the coarser pitch)."""
+    import field_b200.multires as M
+    import field_b200.recipes as R
+    import field_b200.expr as X
+    rng = np.random.default_rng(12)
+    recipe = X.union_all(R.parts(rng, 14, 12, 6, 6, scale=0.8))
+    lv = lambda lens: M.levels_by_list_length(lens, (2, 3))
+    F0 = M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 64, (8, 8, 8), block=8, levels=lv, overlappsband=False)
+    F = M.bygg_multires_fran_recept(recipe, [0, 0, 0], 1.0 / 64, (8, 8, 8), block=8, levels=lv)
+    assert len(set(F.niva[F.kind == 0].ravel())) >= 3  # levels 0, 1 and 2 meet
+    want, faces = oracle.multires_overlap_band(F0.lo, F0.h_grov, F0.block, F0.brick_shape, F0.kind, F0.niva, F0.tiles)
+    assert faces > 0 and F.stats["overlap_faces"] == faces
+    got = F.tiles
+    assert sorted(got) == sorted(want)
+    for k in want:
+        assert got[k].tobytes() == want[k].tobytes(), k
+    rep = M.kontinuitetscheck(F)
+    assert rep["n_pitchbyten_faces"] == faces and rep["GRON"]
+    # the same jumps from the oracle's avstand
+    args = (F.lo, F.h_grov, F.block, F.brick_shape, F.kind, F.niva, want, F.margin_mm)
+    pts = np.array([[0.2, 0.3, 0.4]])
+    assert oracle.multires_avstand(*args, pts)[0] == M.avstand(F, pts)[0]
