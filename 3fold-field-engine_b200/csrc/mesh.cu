@@ -11,7 +11,8 @@
 //   3. k_mesh_winding : a voxel is solid when the oriented hits above it (by the reference's
 //      normalised key comparison) do not cancel; the voxels where winding and ray parity disagree
 //      are counted.
-//   4. the paired exact squared EDT of the solid mask (fb_edt_pair_device), then k_mesh_finish:
+//   4. the paired exact squared EDT of the solid mask (fb_edt_pair_device; k_long_z and
+//      k_long_envelope when an axis exceeds the banded EDT's 512), then k_mesh_finish:
 //      sd = float32(sqrt(sq_out) pitch) - float32(sqrt(sq_in) pitch) with the optional half-pitch
 //      correction, and the surface layer (solid voxels on the boundary or next to a non-solid one).
 //
@@ -230,18 +231,122 @@ __global__ void k_mesh_winding(const int32_t* __restrict__ start, const double* 
     }
 }
 
-// sd and the surface layer (field.cpp:197-214).  sq: the pair [to solid | to non-solid], or nullptr
-// when one class is empty: that class's distance is then -1 (the reference's value for lines with
-// no feature) and the other's 0 (every voxel is its own feature).
-__global__ void k_mesh_finish(const uint8_t* __restrict__ solid, const int32_t* __restrict__ sq, Grid g,
-                              int empty_class, int ytkorr, float* __restrict__ sd, uint8_t* __restrict__ yta) {
+// ---- exact EDT for windows with an axis over 512 voxels (field.cpp:127-195) ----
+// The banded pair EDT serves axes up to 512; longer windows (the reference accepts any grid below
+// 2^31 cells) take these three separable passes, one class at a time, entirely in global memory:
+//   z: a warp per (i, j) column, |offset| to the nearest feature along z (ballot scans), -1 if none;
+//   y, x: a thread per line, the lower envelope of the parabolas (x - s)^2 + G(s) over the line's
+//     sites with a finite G (sites without a feature are skipped, as the reference skips BIG), with
+//     integer separation points (Meijster et al. 2000), so every squared distance is exact in int64.
+// Adjacent threads take adjacent lines, whose elements lie next to each other in memory (lines
+// along y differ in k, lines along x in (j, k)), so each step of the envelope reads coalesced.
+
+// A warp per column: gz[v] = distance along z to the nearest voxel with (mask != 0) == feat, or -1.
+__global__ void k_long_z(const uint8_t* __restrict__ mask, int64_t ncol, int64_t nz, int feat,
+                         int32_t* __restrict__ gz) {
+    const int64_t col = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (col >= ncol) return;  // uniform across the warp
+    const uint8_t* m = mask + col * nz;
+    int32_t* o = gz + col * nz;
+    int64_t last = -1;
+    for (int64_t k0 = 0; k0 < nz; k0 += 32) {
+        const int64_t k = k0 + lane;
+        const unsigned b = __ballot_sync(0xffffffffu, k < nz && ((m[k] != 0) == (feat != 0)));
+        const unsigned upto = b & ((2u << lane) - 1u);  // features at or below this lane
+        const int64_t at = upto ? k0 + 31 - __clz(upto) : last;
+        if (k < nz) o[k] = at >= 0 ? (int32_t)(k - at) : -1;
+        if (b) last = k0 + 31 - __clz(b);
+    }
+    int64_t next = -1;
+    for (int64_t k0 = (nz - 1) / 32 * 32; k0 >= 0; k0 -= 32) {
+        const int64_t k = k0 + lane;
+        const unsigned b = __ballot_sync(0xffffffffu, k < nz && ((m[k] != 0) == (feat != 0)));
+        const unsigned from = b & ~((1u << lane) - 1u);  // features at or above this lane
+        const int64_t at = from ? k0 + __ffs(from) - 1 : next;
+        if (k < nz && at >= 0) {
+            const int32_t dn = (int32_t)(at - k), cur = o[k];
+            if (cur < 0 || dn < cur) o[k] = dn;
+        }
+        if (b) next = k0 + __ffs(b) - 1;
+    }
+}
+
+__device__ __forceinline__ int64_t floor_div(int64_t a, int64_t b) {  // b > 0
+    return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
+// A thread per line of n elements, stride `stride` (= the number of lines in one slab of the
+// lines' outer index): line l starts at (l / stride) n stride + l % stride.  Input: int32 offsets
+// (kFromZ, G = d^2) or int64 squared distances; -1 marks a site without a feature.  Output: int64
+// squared distances, or (kToFloat) float32(sqrt(d2) pitch), the finish step's formula; -1 where the
+// line has no site.  site/start: the envelope's stack, entry q of line l at q lines + l.
+template <bool kFromZ, bool kToFloat>
+__global__ void k_long_envelope(const void* __restrict__ in, int64_t lines, int64_t n, int64_t stride, double pitch,
+                                void* __restrict__ out, int32_t* __restrict__ site, int32_t* __restrict__ start) {
+    const int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (l >= lines) return;
+    const int64_t base = l / stride * n * stride + l % stride;
+    auto G = [&](int64_t u) -> int64_t {
+        if (kFromZ) {
+            const int64_t d = static_cast<const int32_t*>(in)[base + u * stride];
+            return d < 0 ? -1 : d * d;
+        }
+        return static_cast<const int64_t*>(in)[base + u * stride];
+    };
+    int64_t q = -1;
+    for (int64_t u = 0; u < n; ++u) {
+        const int64_t gu = G(u);
+        if (gu < 0) continue;
+        while (q >= 0) {  // drop the sites that u beats at the first position they own
+            const int64_t s = site[q * lines + l], t = start[q * lines + l];
+            if ((t - s) * (t - s) + G(s) > (t - u) * (t - u) + gu) --q;
+            else break;
+        }
+        if (q < 0) {
+            q = 0;
+            site[l] = (int32_t)u;
+            start[l] = 0;
+        } else {
+            const int64_t s = site[q * lines + l];
+            const int64_t w = 1 + floor_div(u * u - s * s + gu - G(s), 2 * (u - s));
+            if (w < n) {
+                ++q;
+                site[q * lines + l] = (int32_t)u;
+                start[q * lines + l] = (int32_t)w;
+            }
+        }
+    }
+    for (int64_t u = n - 1; u >= 0; --u) {
+        int64_t d2 = -1;
+        if (q >= 0) {
+            const int64_t s = site[q * lines + l];
+            d2 = (u - s) * (u - s) + G(s);
+            if (u == start[q * lines + l]) --q;
+        }
+        if (kToFloat)
+            static_cast<float*>(out)[base + u * stride] =
+                d2 < 0 ? -1.0f : __double2float_rn(__dmul_rn(__dsqrt_rn((double)d2), pitch));
+        else
+            static_cast<int64_t*>(out)[base + u * stride] = d2;
+    }
+}
+
+// sd and the surface layer (field.cpp:197-214).  sq: the pair [to solid | to non-solid] of squared
+// distances; else dist: the pair of distances; else (both nullptr) one class is empty: that class's
+// distance is then -1 (the reference's value for lines with no feature) and the other's 0 (every
+// voxel is its own feature).
+__global__ void k_mesh_finish(const uint8_t* __restrict__ solid, const int32_t* __restrict__ sq,
+                              const float* __restrict__ dist, Grid g, int empty_class, int ytkorr,
+                              float* __restrict__ sd, uint8_t* __restrict__ yta) {
     const int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t N = g.nx * g.ny * g.nz;
     if (lin >= N) return;
     float d[2];
     for (int cls = 0; cls < 2; ++cls) {
-        if (!sq) d[cls] = cls == empty_class ? -1.0f : 0.0f;
-        else d[cls] = __double2float_rn(__dmul_rn(__dsqrt_rn((double)sq[cls * N + lin]), g.pitch));
+        if (sq) d[cls] = __double2float_rn(__dmul_rn(__dsqrt_rn((double)sq[cls * N + lin]), g.pitch));
+        else if (dist) d[cls] = dist[cls * N + lin];
+        else d[cls] = cls == empty_class ? -1.0f : 0.0f;
     }
     float v = __fsub_rn(d[0], d[1]);
     if (ytkorr) {
@@ -305,8 +410,8 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
         return 1;
     for (int64_t t = 0; t < 3 * nt; ++t)
         if (T[t] < 0 || T[t] >= nv) return 2;
-    // the EDT's axis contract
-    if (nx > 512 || ny > 512 || nz > 512) return 1;
+    // axes over 512 voxels take the long-axis EDT passes instead of the banded pair EDT
+    const bool long_axes = nx > 512 || ny > 512 || nz > 512;
     const Grid g{ox, oy, oz, pitch, jx, jy, nx, ny, nz};
     const int64_t ncol = nx * ny, N = ncol * nz;
     cudaStream_t st = nullptr;
@@ -327,15 +432,18 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
             for (int i = 0; i < 6; ++i) cudaEventDestroy(e[i]);
         }
     } eguard{ev};
-    const int64_t sb = fb_edt_scratch_bytes((int)nx, (int)ny, (int)nz, 1);
+    const int64_t sb = long_axes ? 0 : fb_edt_scratch_bytes((int)nx, (int)ny, (int)nz, 1);
     if (sb < 0) return 1;
+    const int64_t nl = long_axes ? N : 0;  // the long-axis passes' arrays
     const int64_t words_t = scan_scratch_words(nt), words_c = scan_scratch_words(ncol + 1);
     Slab A;
     const size_t oV = A.reserve<double>(3 * nv), oT = A.reserve<int64_t>(3 * nt), oCount = A.reserve<int32_t>(nt + 1),
                  oMisc = A.reserve<unsigned long long>(8), oScan = A.reserve<int32_t>(std::max(words_t, words_c)),
                  oStart = A.reserve<int32_t>(ncol + 1), oCursor = A.reserve<int32_t>(ncol + 1),
                  oSolid = A.reserve<uint8_t>(N), oYta = A.reserve<uint8_t>(N), oSd = A.reserve<float>(N),
-                 oSq = A.reserve<int32_t>(2 * N), oEdt = A.reserve<uint8_t>(sb);
+                 oSq = A.reserve<int32_t>(long_axes ? 0 : 2 * N), oEdt = A.reserve<uint8_t>(sb),
+                 oGz = A.reserve<int32_t>(nl), oF2 = A.reserve<int64_t>(nl), oSite = A.reserve<int32_t>(nl),
+                 oFrom = A.reserve<int32_t>(nl), oDist = A.reserve<float>(2 * nl);
     if (A.allocate()) return FB_RUNTIME;
     double* const dV = A.at<double>(oV);
     int64_t* const dT = A.at<int64_t>(oT);
@@ -408,13 +516,30 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
     int empty = -1;
     if (nsolid == 0) empty = 0;       // no solid voxel: no feature for the distance to the solid
     else if (nsolid == N) empty = 1;  // no empty voxel
-    if (empty < 0) {
+    float* const dist = A.at<float>(oDist);
+    if (empty < 0 && long_axes) {
+        int32_t* const gz = A.at<int32_t>(oGz);
+        int64_t* const f2 = A.at<int64_t>(oF2);
+        int32_t* const site = A.at<int32_t>(oSite);
+        int32_t* const from = A.at<int32_t>(oFrom);
+        for (int cls = 0; cls < 2; ++cls) {  // features: the solid voxels, then the others
+            k_long_z<<<(unsigned)((ncol + 7) / 8), 256, 0, st>>>(dsolid, ncol, nz, cls == 0, gz);
+            FB_LAUNCH();
+            k_long_envelope<true, false><<<(unsigned)((nx * nz + 255) / 256), 256, 0, st>>>(gz, nx * nz, ny, nz, pitch,
+                                                                                         f2, site, from);
+            FB_LAUNCH();
+            k_long_envelope<false, true><<<(unsigned)((ny * nz + 255) / 256), 256, 0, st>>>(
+                f2, ny * nz, nx, ny * nz, pitch, dist + cls * N, site, from);
+            FB_LAUNCH();
+        }
+    } else if (empty < 0) {
         if (int rc = fb_edt_pair_device(dsolid, (int)nx, (int)ny, (int)nz, pitch, dsd, sq, edt_scratch, sb, st))
             return rc == FB_INVALID ? 1 : FB_RUNTIME;
     }
     FB_CUDA(cudaEventRecord(ev[4], st));
     // 5. sd and the surface layer
-    k_mesh_finish<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dsolid, empty < 0 ? sq : nullptr, g, empty,
+    k_mesh_finish<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dsolid, empty < 0 && !long_axes ? sq : nullptr,
+                                                                  empty < 0 && long_axes ? dist : nullptr, g, empty,
                                                                   ytkorr ? 1 : 0, dsd, dyta);
     FB_LAUNCH();
     FB_CUDA(cudaEventRecord(ev[5], st));

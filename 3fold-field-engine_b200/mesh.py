@@ -12,7 +12,8 @@ Drop-in surfaces:
 The solid mask, the surface layer and the statistics are the reference's bit for bit; sd is
 float32(sqrt(d_out^2) pitch) - float32(sqrt(d_in^2) pitch) from the exact squared distances, equal to
 the reference's feature-offset form except where a value lies within float64 rounding of a float32
-rounding boundary (one float32 ulp then).  Window axes are limited to 512 voxels (the EDT's contract).
+rounding boundary (one float32 ulp then).  Windows up to 512 voxels per axis take the banded pair EDT;
+longer ones (any grid below 2^31 cells, as the reference) take separable long-axis passes.
 """
 from __future__ import annotations
 

@@ -74,3 +74,33 @@ def test_window_without_solid_voxel():
     assert rc == 0 and stats[3] == 0
     assert np.array_equal(g_solid, solid) and np.array_equal(g_stats, stats)
     assert g_sd.tobytes() == sd.tobytes()
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_windows_over_512_voxels_equal_the_reference(axis):
+    """A long bar with spheres along it: a window of 700+ voxels on one axis (the banded EDT serves
+    512; these take the long-axis passes).  Solid, surface, statistics and sd bytes equal the
+    reference's, which accepts any grid below 2^31 cells."""
+    import field_b200.mesh as M
+    lo, hi = np.array([0.0, 0.0, 0.0]), np.array([3.0, 2.5, 2.0])
+    hi[axis] = 70.0
+    parts = [R.mesh_box(lo, hi)]
+    for t in (0.2, 0.5, 0.8):
+        c = (lo + hi) / 2
+        c[axis] = t * hi[axis]
+        parts.append(R.mesh_sphere(c, 3.1 + t, 16, 32))
+    V, T = R.mesh_merge(*parts)
+    pitch = 0.097
+    origin, shape, jit = _grid(V, pitch)
+    assert shape[axis] > 512 and max(shape[a] for a in range(3) if a != axis) <= 512
+    rc, solid, sd, yta, stats = oracle.ref_mesh_field(V, T, origin, pitch, jit, shape, True)
+    assert rc == 0
+    g_solid, g_sd, g_yta, g_stats, _ = M.field_grid(V, T, origin, pitch, shape, jitter=jit)
+    assert np.array_equal(g_solid, solid)
+    assert np.array_equal(g_yta, yta)
+    assert np.array_equal(g_stats, stats)
+    assert 0 < stats[3] < solid.size
+    # one float32 ulp where sqrt(n) pitch and the reference's offset form round to either side
+    a, b = g_sd.view(np.int32).astype(np.int64), sd.view(np.int32).astype(np.int64)
+    assert int(np.abs(a - b).max()) <= 1
+    assert np.count_nonzero(a != b) <= 1e-4 * a.size
