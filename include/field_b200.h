@@ -331,6 +331,38 @@ int meshsdf_field_cpu(const double* V, int64_t nv, const int64_t* T, int64_t nt,
                       double pitch, double jx, double jy, int64_t nx, int64_t ny, int64_t nz, int ytkorr,
                       int nthreads, uint8_t* solid, float* sd, uint8_t* yta, int64_t* stats, double* tstage);
 
+/* Export step: the isosurface of a resident sparse field straight from its tiles -- the mesh that
+ * marching cubes gives on the dense reconstruction, replacing rekonstruera_tat(_gpu) followed by
+ * skimage.measure.marching_cubes (src/field_engine/faltkarna_v1.py:302-350) and the enclosed
+ * volume of faltvolym_v1.py:83-104.  Pass 1 (count) then pass 2 (emit) with the same arguments;
+ * block <= 32.  d_bits / d_wpre: n_active x fb_mc_words(block) words; d_vcount / d_tcount:
+ * n_active + 1 int32 (block offsets, totals last); d_totals: 2 int64 (vertex and triangle totals,
+ * valid as int32 offsets below 2^31); d_scan: fb_mc_scan_words(n_active) int32. */
+int64_t fb_mc_words(int32_t block);
+int64_t fb_mc_scan_words(int64_t n_active);
+int fb_mc_count_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
+                       int64_t nx, int64_t ny, int64_t nz, int32_t block, double ox, double oy, double oz,
+                       double pitch, float level, float big, int32_t* d_slot, uint32_t* d_bits, int32_t* d_wpre,
+                       int32_t* d_vcount, int32_t* d_tcount, int64_t* d_totals, int32_t* d_scan,
+                       int64_t scan_words, void* stream);
+/* d_verts: 3 float32 per vertex (world coordinates); d_vkey (optional): per vertex
+ * (linear index of the edge's lower end) * 3 + axis; d_faces: 3 int32 per triangle, outward normals;
+ * d_volume[0]: sum(v0 . (v1 x v2)) / 6 (d_vol_part: n_active float64 scratch); d_err[0]: triangle
+ * corners without a vertex (0 unless the field changed between the passes). */
+int fb_mc_emit_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
+                      int64_t nx, int64_t ny, int64_t nz, int32_t block, double ox, double oy, double oz, double pitch,
+                      float level, float big, const int32_t* d_slot, const uint32_t* d_bits, const int32_t* d_wpre,
+                      const int32_t* d_vcount, const int32_t* d_tcount, float* d_verts, int64_t* d_vkey,
+                      int32_t* d_faces, double* d_vol_part, double* d_volume, int32_t* d_err, void* stream);
+
+/* Connected components of a triangle mesh (the component split of faltvolym_v1.py:95-101):
+ * d_label[v] = smallest vertex id of v's component, d_count[0] = components, d_comp_volume[root] =
+ * the component's signed volume (atomically summed: last bits order-dependent), d_err[0] = unions
+ * that gave up.  d_parent / d_label: n_verts int32, d_comp_volume: n_verts float64. */
+int fb_mesh_components_device(const int32_t* d_faces, int64_t n_faces, const float* d_verts, int64_t n_verts,
+                              int32_t* d_parent, int32_t* d_label, double* d_comp_volume, int32_t* d_count,
+                              int32_t* d_err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -594,3 +594,164 @@ def multires_overlap_band(lo, h, block, brick_shape, kind, niva, tiles):
                 tiles[lin][tuple(sl)] = v.reshape(tiles[lin][tuple(sl)].shape).astype(np.float32)
                 faces += 1
     return tiles, faces
+
+
+def reconstruct(kind, active_ids, tiles, meta, big=1.0e6):
+    """Dense (nx, ny, nz) float32 field of a sparse one: tiles in active blocks, -big / +big by kind
+    elsewhere (src/field_engine/faltkarna_v1.py:302-325)."""
+    b = meta.block
+    nbx, nby, nbz = meta.n_bx, meta.n_by, meta.n_bz
+    bg = np.where(np.asarray(kind).reshape(nbx, nby, nbz) < 0, -big, big).astype(np.float32)
+    padded = np.repeat(np.repeat(np.repeat(bg, b, 0), b, 1), b, 2)
+    view = padded.reshape(nbx, b, nby, b, nbz, b).transpose(0, 2, 4, 1, 3, 5)
+    if len(active_ids):
+        bi, bj, bk = np.unravel_index(np.asarray(active_ids), (nbx, nby, nbz))
+        view[bi, bj, bk] = np.asarray(tiles, np.float32).reshape(len(active_ids), b, b, b)
+    return padded[:meta.nx, :meta.ny, :meta.nz]
+
+
+# Marching cubes of the export step, restated on the dense field (the reference exports through
+# rekonstruera_tat and skimage.measure.marching_cubes, faltkarna_v1.py:302-350; scikit-image is not
+# part of this environment).  The rules written out: a vertex on every grid edge whose ends lie on
+# opposite sides of `level` (inside = value < level), at t = g0 / (g0 - g1), g = float64(value) -
+# float64(level), position float32(origin + pitch (index + t)); per cube, segments on each face that
+# keep the inside on their left seen from outside (four crossings: the asymptotic decider, inside
+# corners joined when the saddle value g00 g11 - g10 g01 over (g00 + g11 - g10 - g01) is negative),
+# joined into loops, each loop fanned with outward (increasing value) normals from its first vertex,
+# in loop order from the lowest cube edge, that lies on no cube face the loop crosses twice (else
+# from the lowest edge): a fan from such a face would lay a flat triangle into it, which the cube
+# on the other side may lay too.  Corner c = x | y << 1 | z << 2; edge e = axis * 4 + w, w the other
+# two bits (lower axis first); face f = axis * 2 + side.
+
+def _edge_corner0(e):
+    a, w = e >> 2, e & 3
+    if a == 0:
+        return ((w & 1) << 1) | ((w >> 1) << 2)
+    if a == 1:
+        return (w & 1) | ((w >> 1) << 2)
+    return (w & 1) | ((w >> 1) << 1)
+
+
+def _edge_of(ca, cb):
+    d = (ca ^ cb).bit_length() - 1
+    c = ca & cb
+    if d == 0:
+        w = ((c >> 1) & 1) | (((c >> 2) & 1) << 1)
+    elif d == 1:
+        w = (c & 1) | (((c >> 2) & 1) << 1)
+    else:
+        w = (c & 1) | (((c >> 1) & 1) << 1)
+    return d * 4 + w
+
+
+def _edge_faces(e):
+    """Bit mask of the two cube faces that contain edge e."""
+    c0, a = _edge_corner0(e), e >> 2
+    return sum(1 << (b * 2 + ((c0 >> b) & 1)) for b in range(3) if b != a)
+
+
+def _fan_start(loop):
+    """The loop rotated to start at its fan centre."""
+    seen, twice = 0, 0
+    for i in range(len(loop)):
+        f = _edge_faces(loop[i]) & _edge_faces(loop[(i + 1) % len(loop)])
+        twice |= seen & f
+        seen |= f
+    for i, e in enumerate(loop):
+        if not _edge_faces(e) & twice:
+            return loop[i:] + loop[:i]
+    return loop
+
+
+def _cube_loops(g):
+    """Loops (lists of cube edges, in traversal order) of one cube; g: 8 float64 values - level."""
+    inside = [g[c] < 0.0 for c in range(8)]
+    if all(inside) or not any(inside):
+        return []
+    cross = [inside[_edge_corner0(e)] != inside[_edge_corner0(e) | (1 << (e >> 2))] for e in range(12)]
+    nxt = {}
+    for f in range(6):
+        a, s = f >> 1, f & 1
+        u, v = (a + 1) % 3, (a + 2) % 3
+        b = s << a
+        q = [b, b | (1 << (u if s else v)), b | (1 << u) | (1 << v), b | (1 << (v if s else u))]
+        E = [_edge_of(q[i], q[(i + 1) % 4]) for i in range(4)]
+        iq = [inside[c] for c in q]
+        k = sum(iq[i] != iq[(i + 1) % 4] for i in range(4))
+        if k == 2:
+            st = [E[i] for i in range(4) if iq[i] and not iq[(i + 1) % 4]][0]
+            en = [E[i] for i in range(4) if not iq[i] and iq[(i + 1) % 4]][0]
+            nxt[st] = en
+        elif k == 4:
+            g00, g10, g11, g01 = g[b], g[b | (1 << u)], g[b | (1 << u) | (1 << v)], g[b | (1 << v)]
+            num = np.float64(g00) * np.float64(g11) - np.float64(g10) * np.float64(g01)
+            joined = (num > 0.0) if g00 < 0.0 else (num < 0.0)
+            for i in range(4):
+                if iq[i]:
+                    nxt[E[i]] = E[(i + 1) % 4] if joined else E[(i + 3) % 4]
+    loops, todo = [], sorted(e for e in range(12) if cross[e])
+    seen = set()
+    for e0 in todo:
+        if e0 in seen:
+            continue
+        loop, e = [], e0
+        while True:
+            seen.add(e)
+            loop.append(e)
+            e = nxt[e]
+            if e == e0:
+                break
+        loops.append(loop)
+    return loops
+
+
+def marching_cubes(dense, level=0.0, origin=(0.0, 0.0, 0.0), pitch=1.0):
+    """(keys, verts, faces): keys int64 ((i ny + j) nz + k) 3 + axis of each crossing edge in
+    ascending order, verts float32 (V, 3), faces (T, 3) as edge keys, cubes in lexicographic order
+    and loops by lowest edge (the rules above)."""
+    f = np.asarray(dense, np.float32)
+    nx, ny, nz = f.shape
+    n = (nx, ny, nz)
+    g = f.astype(np.float64) - np.float64(level)
+    inside = g < 0.0
+    keys, pos = [], []
+    for a in range(3):
+        s0, s1 = [slice(None)] * 3, [slice(None)] * 3
+        s0[a], s1[a] = slice(0, n[a] - 1), slice(1, n[a])
+        cross = inside[tuple(s0)] != inside[tuple(s1)]
+        idx = np.argwhere(cross)
+        g0, g1 = g[tuple(s0)][cross], g[tuple(s1)][cross]
+        p = idx.astype(np.float64)
+        p[:, a] = p[:, a] + g0 / (g0 - g1)
+        pos.append((np.asarray(origin, np.float64) + pitch * p).astype(np.float32))
+        keys.append(((idx[:, 0].astype(np.int64) * ny + idx[:, 1]) * nz + idx[:, 2]) * 3 + a)
+    keys, pos = np.concatenate(keys), np.concatenate(pos)
+    order = np.argsort(keys, kind="stable")
+    keys, pos = keys[order], pos[order]
+    faces = []
+    if nx > 1 and ny > 1 and nz > 1:
+        c = inside[:-1, :-1, :-1].astype(np.int32)
+        cnt = sum(inside[dx:nx - 1 + dx, dy:ny - 1 + dy, dz:nz - 1 + dz].astype(np.int32)
+                  for dx in (0, 1) for dy in (0, 1) for dz in (0, 1))
+        del c
+        for m in np.argwhere((cnt > 0) & (cnt < 8)):
+            i, j, k = (int(x) for x in m)
+            gc = [g[i + (c & 1), j + ((c >> 1) & 1), k + ((c >> 2) & 1)] for c in range(8)]
+            for loop in _cube_loops(gc):
+                loop = _fan_start(loop)
+                ek = []
+                for e in loop:
+                    cc = _edge_corner0(e)
+                    pi, pj, pk = i + (cc & 1), j + ((cc >> 1) & 1), k + ((cc >> 2) & 1)
+                    ek.append(((pi * ny + pj) * nz + pk) * 3 + (e >> 2))
+                for t in range(1, len(ek) - 1):
+                    faces.append((ek[0], ek[t + 1], ek[t]))
+    return keys, pos, np.asarray(faces, np.int64).reshape(-1, 3)
+
+
+def mesh_volume(verts, faces):
+    """Signed volume sum(v0 . (v1 x v2)) / 6 of a triangle mesh, float64 (the divergence theorem,
+    as trimesh's volume in faltvolym_v1.py:83-104)."""
+    v = np.asarray(verts, np.float64)
+    a, b, c = v[faces[:, 0]], v[faces[:, 1]], v[faces[:, 2]]
+    return float(np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6.0)
