@@ -72,8 +72,8 @@ SIGNATURES = {
     # export: marching cubes on the resident leaves
     "fb_mc_words": (I64, [I]),
     "fb_mc_scan_words": (I64, [I64]),
-    "fb_mc_count_device": (I, [P, P, I64, P, I64, I64, I64, I, D, D, D, D, F, F, P, P, P, P, P, P, P, I64, P]),
-    "fb_mc_emit_device": (I, [P, P, I64, P, I64, I64, I64, I, D, D, D, D, F, F, P, P, P, P, P, P, P, P, P, P, P,
+    "fb_mc_count_device": (I, [P, P, I64, P, I64, I64, I64, I, D, D, D, D, D, F, P, P, P, P, P, P, P, I64, P]),
+    "fb_mc_emit_device": (I, [P, P, I64, P, I64, I64, I64, I, D, D, D, D, D, F, P, P, P, P, P, P, P, P, P, P, P,
                               P]),
     "fb_mesh_components_device": (I, [P, I64, P, I64, P, P, P, P, P, P]),
     "fb_field_leaf_work_device": (I, [P, P, I, P, I, I, P, P, P, P, I64, P, I64, P, P]),

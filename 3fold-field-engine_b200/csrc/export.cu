@@ -40,8 +40,8 @@ struct McField {
     const float* tiles;
     int64_t nx, ny, nz;
     int B, nby, nbz;
-    double ox, oy, oz, pitch;
-    float level, big;
+    double ox, oy, oz, pitch, level;
+    float big;
 };
 
 __host__ __device__ inline int64_t mc_slots(int B) { return 3LL * B * B * B + 3LL * B * B; }
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kMcThreads) k_mc(McField F, const int32_t* __r
         }
         __syncthreads();
         auto val = [&](int64_t x, int64_t y, int64_t z) -> double {  // value - level, from the region
-            return __dsub_rn((double)s_val[((x - x0 + 1) * R + (y - y0 + 1)) * R + (z - z0 + 1)], (double)F.level);
+            return __dsub_rn((double)s_val[((x - x0 + 1) * R + (y - y0 + 1)) * R + (z - z0 + 1)], F.level);
         };
         // ---- edges ----
         int run = 0;  // vertices before this chunk (emit) / count (count pass)
@@ -455,9 +455,9 @@ __global__ void k_mc_slot_map(const int32_t* __restrict__ active, int64_t n_acti
 }
 
 int mc_field(McField& F, const int32_t* d_kind, const float* d_tiles, int64_t nx, int64_t ny, int64_t nz, int32_t block,
-             double ox, double oy, double oz, double pitch, float level, float big, const int32_t* d_slot) {
+             double ox, double oy, double oz, double pitch, double level, float big, const int32_t* d_slot) {
     if (!d_kind || !d_slot || nx < 1 || ny < 1 || nz < 1 || block < 1 || block > kMcMaxBlock ||
-        !(pitch > 0) || !(level == level))
+        !(pitch > 0) || !(level == level) || level > 1e300 || level < -1e300)
         return FB_INVALID;
     F = McField{d_kind, d_slot, d_tiles, nx, ny, nz, block, (int)((ny + block - 1) / block),
                 (int)((nz + block - 1) / block), ox, oy, oz, pitch, level, big};
@@ -607,7 +607,7 @@ int64_t fb_mc_scan_words(int64_t n_active) { return n_active < 0 ? -1 : scan_scr
 // Stream-ordered; block <= 32.  Status 1 for invalid arguments.
 int fb_mc_count_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
                        int64_t nx, int64_t ny, int64_t nz, int32_t block, double ox, double oy, double oz,
-                       double pitch, float level, float big, int32_t* d_slot, uint32_t* d_bits, int32_t* d_wpre,
+                       double pitch, double level, float big, int32_t* d_slot, uint32_t* d_bits, int32_t* d_wpre,
                        int32_t* d_vcount, int32_t* d_tcount, int64_t* d_totals, int32_t* d_scan,
                        int64_t scan_words, void* stream) noexcept {
     McField F;
@@ -642,7 +642,7 @@ int fb_mc_count_device(const int32_t* d_kind, const int32_t* d_active, int64_t n
 // vertex (0 unless the field changed in between).
 int fb_mc_emit_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
                       int64_t nx, int64_t ny, int64_t nz, int32_t block, double ox, double oy, double oz, double pitch,
-                      float level, float big, const int32_t* d_slot, const uint32_t* d_bits, const int32_t* d_wpre,
+                      double level, float big, const int32_t* d_slot, const uint32_t* d_bits, const int32_t* d_wpre,
                       const int32_t* d_vcount, const int32_t* d_tcount, float* d_verts, int64_t* d_vkey,
                       int32_t* d_faces, double* d_vol_part, double* d_volume, int32_t* d_err, void* stream) noexcept {
     McField F;

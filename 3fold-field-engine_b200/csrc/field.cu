@@ -1002,7 +1002,7 @@ __device__ __forceinline__ void eval_group_sphere(const LocalPrim& P, float dx, 
 // VG voxels along z of one lane: values of primitive P at block offsets (dx, dy, dz0 + k*pz).
 template <int VG, int T>
 __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
-    if (T == P_SPHERE) {
+    if (T == P_SPHERE && P.diff) {
         eval_group_sphere<VG>(P, dx, dy, dz, v);
         return;
     }
@@ -1192,7 +1192,7 @@ __device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, co
                 sp[i].op = op;
                 sp[i].k = (float)I.k;
             } else {
-                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
+                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], 32 * G.fpitch);
             }
         }
         __syncwarp();
@@ -1365,7 +1365,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                 sp[i].op = op;
                 sp[i].k = (float)I.k;
             } else {
-                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i]);
+                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], B * G.fpitch);
             }
         }
         __syncwarp();
@@ -1399,6 +1399,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
 #pragma unroll
                 for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
                 if (near) {
+#pragma unroll
                     for (int k = 0; k < VG; ++k)
                         if (!(fabsf(acc[k]) >= G.guard))
                             acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,

@@ -48,9 +48,10 @@ struct __align__(16) PrimF {
 };
 
 // Block-localised float32 record: q = L + A_lin * d, d the offset from the block origin; L[3] holds
-// a kind's per-block float64 constant rounded once (the sphere's |L|^2 - r^2).
+// a kind's per-block float64 constant rounded once (the sphere's |L|^2 - r^2); diff selects the
+// sphere's difference form for this block.
 struct __align__(16) LocalPrim {
-    int32_t type, op, ident, pad;
+    int32_t type, op, ident, diff;
     float k, s, off, pad1;
     float L[4];
     float A[12];   // A_lin rows (9 used)
@@ -238,8 +239,14 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
 // growing with the distance along the segment (a milling sweep is up to ~1.7 length units long, where
 // one float32 ulp is ~1e-7), and the segment becomes [-h0, 1 - h0] * b.  The clamp bound that can be
 // active inside the block is the one near zero, which float32 holds to a relative 6e-8.
+//
+// A sphere takes the difference form (|L|^2 - r^2 + e.(2L + e)) / (|q| + r) when its radius exceeds
+// twice the block's extent in its frame, else the direct |q| - r.  Their float32 errors: about
+// u (|d| + 6 |e|) for the difference form (d = |L| - r, independent of r) and u (|L| + 2 |q|) ~ 3 u r for
+// the direct one (u = 2^-24): large spheres against small blocks favour the first, small spheres
+// against large blocks the second.  extent: the largest offset the block's evaluation uses.
 __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double ox, double oy, double oz, int op,
-                                         float k, LocalPrim& out) {
+                                         float k, LocalPrim& out, float extent = 0.f) {
     out.type = F.type;
     out.op = op;
     out.ident = F.ident;
@@ -267,6 +274,13 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     out.L[2] = (float)lz;
     // sphere: |L|^2 - r^2 in float64, the constant term of the difference form of |q| - r
     out.L[3] = F.type == P_SPHERE ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0]) : 0.f;
+    out.diff = 0;
+    if (F.type == P_SPHERE) {
+        // the extent in the sphere's frame: the Frobenius norm bounds the linear part's stretch
+        const double a2 = A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
+                          A[8] * A[8] + A[9] * A[9] + A[10] * A[10];
+        out.diff = D.p[0] > 2.0 * (double)extent * (F.ident ? 1.0 : sqrt(a2)) ? 1 : 0;
+    }
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
     out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];

@@ -80,7 +80,7 @@ def _mesh(kind, active, n, tiles, nx, ny, nz, block, origin, pitch, level, keys,
     words = int(lib.fb_mc_scan_words(n))
     scan = torch.empty(words, **i32)
     ox, oy, oz = (float(v) for v in origin)
-    lv = float(np.float32(level))
+    lv = float(level)
     args = (kind.data_ptr(), active.data_ptr() if n else None, n, tiles.data_ptr() if n else None, nx, ny, nz, block,
             ox, oy, oz, float(pitch), lv, float(BIG))
     _lib.check(lib.fb_mc_count_device(*args, slot.data_ptr(), bits.data_ptr(), wpre.data_ptr(), vcount.data_ptr(),

@@ -342,7 +342,7 @@ int64_t fb_mc_words(int32_t block);
 int64_t fb_mc_scan_words(int64_t n_active);
 int fb_mc_count_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
                        int64_t nx, int64_t ny, int64_t nz, int32_t block, double ox, double oy, double oz,
-                       double pitch, float level, float big, int32_t* d_slot, uint32_t* d_bits, int32_t* d_wpre,
+                       double pitch, double level, float big, int32_t* d_slot, uint32_t* d_bits, int32_t* d_wpre,
                        int32_t* d_vcount, int32_t* d_tcount, int64_t* d_totals, int32_t* d_scan,
                        int64_t scan_words, void* stream);
 /* d_verts: 3 float32 per vertex (world coordinates); d_vkey (optional): per vertex
@@ -351,7 +351,7 @@ int fb_mc_count_device(const int32_t* d_kind, const int32_t* d_active, int64_t n
  * corners without a vertex (0 unless the field changed between the passes). */
 int fb_mc_emit_device(const int32_t* d_kind, const int32_t* d_active, int64_t n_active, const float* d_tiles,
                       int64_t nx, int64_t ny, int64_t nz, int32_t block, double ox, double oy, double oz, double pitch,
-                      float level, float big, const int32_t* d_slot, const uint32_t* d_bits, const int32_t* d_wpre,
+                      double level, float big, const int32_t* d_slot, const uint32_t* d_bits, const int32_t* d_wpre,
                       const int32_t* d_vcount, const int32_t* d_tcount, float* d_verts, int64_t* d_vkey,
                       int32_t* d_faces, double* d_vol_part, double* d_volume, int32_t* d_err, void* stream);
 

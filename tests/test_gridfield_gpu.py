@@ -46,8 +46,12 @@ def test_gridfield_recipe_builds_and_queries_match_oracle(tmp_path):
     meta = GridMeta(-0.34, -0.32, -0.16, 1.0 / 160, 112, 104, 52, 8)  # reaches past the grid's extent
     field = B.FieldBuilder(comp, meta).build()
     hp = comp.host_prims()
-    kind, _ = oracle.classify_program(hp, comp.program, meta)
-    assert (field.kind.cpu().numpy() == kind).all()
+    kind, cma = oracle.classify_program(hp, comp.program, meta)
+    gk, gc = field.kind.cpu().numpy(), field.corner_min_abs.cpu().numpy()
+    bad = np.where(gk != kind)[0]
+    assert not len(bad), (f"{len(bad)} kinds differ; first: ids {bad[:6].tolist()}, gpu {gk[bad[:6]].tolist()}, "
+                          f"oracle {kind[bad[:6]].tolist()}, oracle min|corner| {cma[bad[:6]].tolist()}, "
+                          f"gpu {gc[bad[:6]].tolist()}, margin {meta.margin_mm}")
     n = field.n_active
     ids = field.active[:n].cpu().numpy().astype(np.int32)
     want = oracle.tiles_program(hp, comp.program, meta, ids).reshape(n, -1)
