@@ -762,77 +762,130 @@ __device__ __forceinline__ double vertex_d(double origin, int64_t i, double pitc
     return rn_add(origin, rn_mul((double)i, pitch));
 }
 
-// Thread-per-block classification of a chain recipe whose per-block lists k_cull_blocks left in
-// blk_pool (grids of few blocks): thread t of the superblock-major order -- threads of one
-// superblock are consecutive, so a warp never spans two superblocks and walks in lockstep with
-// broadcast loads -- evaluates its block's 8 corners in float32 in block-local coordinates.
-__device__ void classify_listed(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
-                                const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
-                                const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
-                                int32_t* __restrict__ kind, float* __restrict__ cma,
-                                const int32_t* __restrict__ blk_off, const int32_t* __restrict__ blk_len,
-                                const uint32_t* __restrict__ blk_pool, int64_t t) {
+// Thread-per-block classification of a chain recipe: thread t of the superblock-major order --
+// threads of one superblock are consecutive, so a warp never spans two superblocks and walks in
+// lockstep with broadcast loads -- evaluates its block's 8 corners in float32 in block-local
+// coordinates.  kCull = false: the per-block lists k_cull_blocks left in blk_pool (grids of few
+// blocks).  kCull = true: the block culls the superblock list itself (seq_walk, kCapBlock entries)
+// and an active block keeps that list for the leaf pass and point queries: the warp's lists are
+// placed with one atomicAdd on `cursor` (blk_len -1 where a list overflowed or the pool is full;
+// the leaf pass then culls the block itself).  Every lane of a warp reaches the placement, so
+// threads outside the grid only skip the evaluation.
+template <bool kCull>
+__device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
+                               const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
+                               const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
+                               int32_t* __restrict__ kind, float* __restrict__ cma, int32_t* __restrict__ blk_off,
+                               int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                               int* __restrict__ cursor, int64_t t) {
     const int S = G.S;
     const int T = threads_per_super(S);
     const int64_t s_id = t / T;
     const int local = (int)(t % T);
-    if (s_id >= G.nsuper || local >= S * S * S) return;
     const int sz = (int)(s_id % G.nsz), sy = (int)((s_id / G.nsz) % G.nsy), sx = (int)(s_id / ((int64_t)G.nsz * G.nsy));
     const int bi = sx * S + local / (S * S), bj = sy * S + (local / S) % S, bk = sz * S + local % S;
-    if (bi >= G.nbx || bj >= G.nby || bk >= G.nbz) return;
+    const bool valid = s_id < G.nsuper && local < S * S * S && bi < G.nbx && bj < G.nby && bk < G.nbz;
     const int64_t b = ((int64_t)bi * G.nby + bj) * G.nbz + bk;
     const int B = G.B;
-    const int n = blk_len[b];
-    const uint32_t* list = n >= 0 ? blk_pool + blk_off[b] : pool + sb_off[s_id];
-    const int len = n >= 0 ? n : sb_len[s_id];
-    const double ox = G.x0 + (double)(bi * B) * G.pitch;
-    const double oy = G.y0 + (double)(bj * B) * G.pitch;
-    const double oz = G.z0 + (double)(bk * B) * G.pitch;
-    const float side = (float)B * G.fpitch;
-    float v[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) v[c] = 0.f;
-    for (int i = 0; i < len; ++i) {
-        const uint32_t e = list[i];
-        const FbInsn I = chain[e >> 2];
-        const int op = effective_op(e, I.op);
-        const float k = (float)I.k;
-        if (op == CH_OFFSET) {
-#pragma unroll
-            for (int c = 0; c < 8; ++c) v[c] -= k;
-            continue;
+    uint32_t blist[kCull ? kCapBlock : 1];
+    int nblist = -1;
+    int kd = 1;
+    if (valid) {
+        const uint32_t* list;
+        int len;
+        if (kCull) {
+            const uint32_t* plist = pool + sb_off[s_id];
+            const int plen = sb_len[s_id];
+            const float half = 0.5f * B;
+            const int n = seq_walk(plist, plen, chain, primf, G.fx0 + (bi * B + half) * G.fpitch,
+                                   G.fy0 + (bj * B + half) * G.fpitch, G.fz0 + (bk * B + half) * G.fpitch,
+                                   1.7320509f * half * G.fpitch, G.eps, blist, kCapBlock);
+            nblist = n;
+            list = n <= kCapBlock ? blist : plist;
+            len = n <= kCapBlock ? n : plen;
+        } else {
+            const int n = blk_len[b];
+            list = n >= 0 ? blk_pool + blk_off[b] : pool + sb_off[s_id];
+            len = n >= 0 ? n : sb_len[s_id];
         }
-        LocalPrim P;
-        localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
+        const double ox = G.x0 + (double)(bi * B) * G.pitch;
+        const double oy = G.y0 + (double)(bj * B) * G.pitch;
+        const double oz = G.z0 + (double)(bk * B) * G.pitch;
+        const float side = (float)B * G.fpitch;
+        float v[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const float pv = local_eval(P, (c & 1) ? side : 0.f, ((c >> 1) & 1) ? side : 0.f, ((c >> 2) & 1) ? side : 0.f);
-            v[c] = chain_apply(op, v[c], pv, k);
+        for (int c = 0; c < 8; ++c) v[c] = 0.f;
+        for (int i = 0; i < len; ++i) {
+            const uint32_t e = list[i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            const float k = (float)I.k;
+            if (op == CH_OFFSET) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) v[c] -= k;
+                continue;
+            }
+            LocalPrim P;
+            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const float pv =
+                    local_eval(P, (c & 1) ? side : 0.f, ((c >> 1) & 1) ? side : 0.f, ((c >> 2) & 1) ? side : 0.f);
+                v[c] = chain_apply(op, v[c], pv, k);
+            }
+        }
+        float m;
+        kd = decide_block(G, v, m, [&](int c) {
+            return list_eval_d(list, len, chain, prims, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
+                               vertex_d(G.y0, (int64_t)bj * B + ((c >> 1) & 1) * B, G.pitch),
+                               vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
+        });
+        kind[b] = kd;
+        cma[b] = m;
+    }
+    if (kCull) {
+        // the warp's active blocks' lists: an inclusive scan of their lengths, one atomicAdd
+        const int lane = threadIdx.x & 31;
+        const bool keep = valid && kd == 0 && nblist >= 0 && nblist <= kCapBlock;
+        const int need = keep ? nblist : 0;
+        int incl = need;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int base = 0;
+        if (lane == 31 && total > 0) base = atomicAdd(cursor, total);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        if (valid && kd == 0) {
+            const int64_t slot = (int64_t)base + incl - need;
+            int len_b = -1;
+            if (keep && slot + need <= blk_cap) {
+                for (int i = 0; i < need; ++i) blk_pool[slot + i] = blist[i];
+                blk_off[b] = (int32_t)slot;
+                len_b = need;
+            }
+            blk_len[b] = len_b;  // -1: the leaf pass culls the block itself
         }
     }
-    float m;
-    kind[b] = decide_block(G, v, m, [&](int c) {
-        return list_eval_d(list, len, chain, prims, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
-                           vertex_d(G.y0, (int64_t)bj * B + ((c >> 1) & 1) * B, G.pitch),
-                           vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
-    });
-    cma[b] = m;
 }
 
 // 10 CTAs per SM (48 registers): the walk and the corner folds wait on loads and on the instruction
 // cache, and more resident warps hide that better than the few spills cost.
-__global__ void __launch_bounds__(128, 10) k_classify_listed(Geo G, const FbPrim* __restrict__ prims,
+template <bool kCull>
+__global__ void __launch_bounds__(128, 10) k_classify_blocks(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
                                                              const FbInsn* __restrict__ chain,
                                                              const uint32_t* __restrict__ pool,
                                                              const int64_t* __restrict__ sb_off,
                                                              const int32_t* __restrict__ sb_len,
                                                              int32_t* __restrict__ kind, float* __restrict__ cma,
-                                                             const int32_t* __restrict__ blk_off,
-                                                             const int32_t* __restrict__ blk_len,
-                                                             const uint32_t* __restrict__ blk_pool) {
+                                                             int32_t* __restrict__ blk_off, int32_t* __restrict__ blk_len,
+                                                             uint32_t* __restrict__ blk_pool, int64_t blk_cap,
+                                                             int* __restrict__ cursor) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    classify_listed(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, t);
+    classify_block<kCull>(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, blk_cap,
+                          cursor, t);
 }
 
 // General postfix programs: every corner of every block in float64, no culling.
@@ -1153,6 +1206,7 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
 // partial folds in shared memory between chunks.  Decisions then follow the per-block rule: a block
 // with a corner value within the guard band of 0 or of the margin (or NaN) re-evaluates all 8
 // corners in float64 with the superblock list and decides in float64, exactly as the oracle.
+constexpr bool kClassifyLattice = false;  // large grids: corner lattice per superblock (else a thread per block)
 constexpr int kLatWarps = 4;
 constexpr int kLatChunk = 32;
 
@@ -1297,6 +1351,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
     constexpr int kVox = B * B * B;
     constexpr int VG = B == 4 ? 2 : 4;
     constexpr int kGroups = kVox / (32 * VG);
+    constexpr bool kDeferGuard = kGroups * VG <= 32;  // the lane's voxels fit one bit mask (B <= 8)
     const int lane = threadIdx.x & 31;
     if (blk < 0 || blk >= G.nblocks) {  // an id outside the grid (a corrupted list) reads as exterior
         for (int v = lane; v < kVox; v += 32) out[v] = kBig;
@@ -1353,6 +1408,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
     (void)fits;
     // the list in chunks of kCapBlock localised primitives; between chunks each lane keeps its
     // partial fold in its own part of the tile (the same float operations in the same order)
+    uint32_t near = 0;  // bit g * VG + k: voxel k of this lane's group g lies in the guard band
     for (int c0 = 0; c0 == 0 || c0 < len; c0 += kCapBlock) {  // one pass even for an empty list
         const int clen = max(0, min(kCapBlock, len - c0));
         const bool first = c0 == 0, last = c0 + clen >= len;
@@ -1394,11 +1450,10 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                 combine_group<VG>(op, P.k, acc, v);
             }
             if (last) {
-                // guard band: float64 recheck so the sign never disagrees with the float64 value
-                bool near = false;
+                if (kDeferGuard) {
 #pragma unroll
-                for (int k = 0; k < VG; ++k) near |= !(fabsf(acc[k]) >= G.guard);
-                if (near) {
+                    for (int k = 0; k < VG; ++k) near |= (uint32_t)!(fabsf(acc[k]) >= G.guard) << (g * VG + k);
+                } else {
 #pragma unroll
                     for (int k = 0; k < VG; ++k)
                         if (!(fabsf(acc[k]) >= G.guard))
@@ -1408,6 +1463,16 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
             }
             store_group<VG>(out, g * 32 + lane, acc);
         }
+    }
+    // guard band: a float64 recheck of the few voxels near zero, so the sign never disagrees with
+    // the float64 value -- after the tile is stored, where little else is live across the call
+    while (near) {
+        const int bit = __ffs(near) - 1;
+        near &= near - 1;
+        const int v = ((bit / VG) * 32 + lane) * VG + bit % VG;
+        const int li = v / (B * B), lj = (v / B) % B, lk = v % B;
+        out[v] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li, (int64_t)bj * B + lj,
+                                    (int64_t)bk * B + lk);
     }
 }
 
@@ -1688,11 +1753,16 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
                                                                          S.len + G.ncoarse, S.blk_off, S.blk_len,
                                                                          S.blk_pool, P.cap_block);
             FB_LAUNCH();
-            k_classify_listed<<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+            k_classify_blocks<false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
                 G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
-                S.blk_pool);
+                S.blk_pool, P.blk_cap, S.misc + 2);
+        } else if (!kClassifyLattice) {
+            // a thread per block: its own cull of the superblock list, kept for the active blocks
+            k_classify_blocks<true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+                G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
+                S.blk_pool, P.blk_cap, S.misc + 2);
         } else {
-            // per-block lists come after the compaction, for the active blocks only (k_cull_active)
+            // a warp per superblock: the corner lattice, lists culled for the active blocks
             const int grid = (int)std::min<int64_t>(fb_div_up(G.nsuper, kLatWarps), (int64_t)fb_sm_count() * 64);
             const int64_t* sb_off = S.off + G.ncoarse;
             const int32_t* sb_len = S.len + G.ncoarse;
@@ -1858,14 +1928,16 @@ __global__ void __launch_bounds__(128) k_b_cull_blocks(const RecDesc* __restrict
 }
 
 // Each recipe's thread range is a multiple of 32 (nsuper x threads_per_super), so a warp never
-// spans two recipes.
-__global__ void __launch_bounds__(128, 10) k_b_classify_listed(const RecDesc* __restrict__ D, Group W, int64_t total) {
+// spans two recipes.  kCull: recipes without k_cull_blocks lists cull their blocks here.
+template <bool kCull>
+__global__ void __launch_bounds__(128, 10) k_b_classify_blocks(const RecDesc* __restrict__ D, Group W, int64_t total,
+                                                               int* __restrict__ cursors) {
     const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= total) return;
     const int j = group_find(W, g);
     const RecDesc& R = D[W.rec[j]];
-    classify_listed(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind, R.cma,
-                    R.blk_off, R.blk_len, R.blk_pool, g - W.pre[j]);
+    classify_block<kCull>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind,
+                          R.cma, R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[W.rec[j]], g - W.pre[j]);
 }
 
 template <int B>
@@ -1999,9 +2071,9 @@ struct BatchHost {
     int64_t dev_bytes = 0;
     RecDesc* d_desc = nullptr;
     // static groups and their totals
-    Group prims{}, chain{}, coarse{}, super_{}, wblocks{}, wclass{}, lat[3]{}, tiles{};
-    int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_wblocks = 0, n_wclass = 0, n_lat[3] = {0, 0, 0},
-            n_tiles = 0;
+    Group prims{}, chain{}, coarse{}, super_{}, wblocks{}, wclass{}, cclass{}, lat[3]{}, tiles{};
+    int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_wblocks = 0, n_wclass = 0, n_cclass = 0,
+            n_lat[3] = {0, 0, 0}, n_tiles = 0;
     // dynamic groups (prefixes written by k_batch_offsets)
     Group leaf[3]{}, occ{};
     int64_t* leaf_pre[3] = {nullptr, nullptr, nullptr};
@@ -2093,8 +2165,8 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
                 pre.push_back(pre.back() + items);
             }
         };
-        HostGroup g_prims, g_chain, g_coarse, g_super, g_wblocks, g_wclass, g_lat[3], g_tiles, g_leaf[3], g_occ,
-            g_occ_blocks, g_occ_rows[3];
+        HostGroup g_prims, g_chain, g_coarse, g_super, g_wblocks, g_wclass, g_cclass, g_lat[3], g_tiles, g_leaf[3],
+            g_occ, g_occ_blocks, g_occ_rows[3];
         for (int r = 0; r < n; ++r) {
             const RecDesc& d = H->desc[r];
             const Geo& G = d.G;
@@ -2105,6 +2177,8 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             if (d.warp_blocks) {
                 g_wblocks.add(r, G.nblocks);
                 g_wclass.add(r, G.nsuper * threads_per_super(G.S));
+            } else if (!kClassifyLattice) {
+                g_cclass.add(r, G.nsuper * threads_per_super(G.S));
             } else {
                 g_lat[b_index(G.B)].add(r, G.nsuper);
             }
@@ -2135,8 +2209,8 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
         };
         HostGroup* statics[] = {&g_prims, &g_chain, &g_coarse, &g_super, &g_wblocks, &g_wclass,
                                 &g_lat[0], &g_lat[1], &g_lat[2], &g_tiles, &g_leaf[0], &g_leaf[1], &g_leaf[2],
-                                &g_occ, &g_occ_blocks, &g_occ_rows[0], &g_occ_rows[1], &g_occ_rows[2]};
-        constexpr int kGroups = 18;
+                                &g_occ, &g_occ_blocks, &g_occ_rows[0], &g_occ_rows[1], &g_occ_rows[2], &g_cclass};
+        constexpr int kGroups = 19;
         Placed placed[kGroups];
         for (int q = 0; q < kGroups; ++q) placed[q] = place_group(*statics[q]);
         const int64_t o_state = at;
@@ -2165,7 +2239,7 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
         std::memcpy(image.data() + o_desc, H->desc.data(), (size_t)n * sizeof(RecDesc));
         Group* dst[] = {&H->prims, &H->chain, &H->coarse, &H->super_, &H->wblocks, &H->wclass,
                         &H->lat[0], &H->lat[1], &H->lat[2], &H->tiles, &H->leaf[0], &H->leaf[1], &H->leaf[2],
-                        &H->occ, &H->occ_blocks, &H->occ_rows[0], &H->occ_rows[1], &H->occ_rows[2]};
+                        &H->occ, &H->occ_blocks, &H->occ_rows[0], &H->occ_rows[1], &H->occ_rows[2], &H->cclass};
         for (int q = 0; q < kGroups; ++q) {
             const HostGroup& hg = *statics[q];
             std::memcpy(image.data() + placed[q].rec, hg.rec.data(), hg.rec.size() * 4);
@@ -2184,6 +2258,7 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
         H->n_super = g_super.pre.back();
         H->n_wblocks = g_wblocks.pre.back();
         H->n_wclass = g_wclass.pre.back();
+        H->n_cclass = g_cclass.pre.back();
         for (int q = 0; q < 3; ++q) H->n_lat[q] = g_lat[q].pre.back();
         H->n_tiles = g_tiles.pre.back();
         if (cudaMemcpyAsync(D, image.data(), o_state, cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -2246,7 +2321,11 @@ int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, i
     if (H->n_wblocks) {
         k_b_cull_blocks<<<fb_div_up(H->n_wblocks * 32, 128), 128, 0, st>>>(D, H->wblocks, H->n_wblocks);
         FB_LAUNCH();
-        k_b_classify_listed<<<fb_div_up(H->n_wclass, 128), 128, 0, st>>>(D, H->wclass, H->n_wclass);
+        k_b_classify_blocks<false><<<fb_div_up(H->n_wclass, 128), 128, 0, st>>>(D, H->wclass, H->n_wclass, H->cursors);
+        FB_LAUNCH();
+    }
+    if (H->n_cclass) {
+        k_b_classify_blocks<true><<<fb_div_up(H->n_cclass, 128), 128, 0, st>>>(D, H->cclass, H->n_cclass, H->cursors);
         FB_LAUNCH();
     }
     for (int q = 0; q < 3; ++q) {

@@ -261,8 +261,10 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     for (int j = 0; j < 12; ++j) out.p[j] = F.p[j];
     if (F.type == P_CAPSULE) {
         const double bx = D.p[0], by = D.p[1], bz = D.p[2];
-        const double bb = fma(bx, bx, fma(by, by, bz * bz));
-        const double h0 = bb > 0.0 ? fmin(fmax(fma(lx, bx, fma(ly, by, lz * bz)) / bb, 0.0), 1.0) : 0.0;
+        // any anchor on the segment serves (the bounds below are formed from the same h0), so the
+        // float32 1/|b|^2 of the mirror stands in for a float64 division
+        const double inv = (double)F.p[4];
+        const double h0 = inv > 0.0 ? fmin(fmax(fma(lx, bx, fma(ly, by, lz * bz)) * inv, 0.0), 1.0) : 0.0;
         lx = fma(-bx, h0, lx);
         ly = fma(-by, h0, ly);
         lz = fma(-bz, h0, lz);
