@@ -771,6 +771,11 @@ __device__ __forceinline__ double vertex_d(double origin, int64_t i, double pitc
 // placed with one atomicAdd on `cursor` (blk_len -1 where a list overflowed or the pool is full;
 // the leaf pass then culls the block itself).  Every lane of a warp reaches the placement, so
 // threads outside the grid only skip the evaluation.
+template <int VG>
+__device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v);
+template <int VG>
+__device__ __forceinline__ void combine_group(int op, float k, float* acc, const float* v);
+
 template <bool kCull>
 __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
                                const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
@@ -813,6 +818,7 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
         const double oz = G.z0 + (double)(bk * B) * G.pitch;
         const float side = (float)B * G.fpitch;
         float v[8];
+        bool edge = false;  // a corner sampled a grid table at its boundary: decide in float64
 #pragma unroll
         for (int c = 0; c < 8; ++c) v[c] = 0.f;
         for (int i = 0; i < len; ++i) {
@@ -826,14 +832,21 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
                 continue;
             }
             LocalPrim P;
-            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const float pv =
-                    local_eval(P, (c & 1) ? side : 0.f, ((c >> 1) & 1) ? side : 0.f, ((c >> 2) & 1) ? side : 0.f);
-                v[c] = chain_apply(op, v[c], pv, k);
+            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P, side);
+            // the corners as 4 (x, y) columns of 2 along z: one inlined evaluation body (the kind
+            // switch outside, the points inside) walked over the columns, the corner values rotated
+            // through registers -- 8 unrolled kind switches would not fit the instruction cache
+            const float dz2[2] = {0.f, side};
+            for (int col = 0; col < 4; ++col) {
+                float pv[2], acc2[2] = {v[0], v[4]};
+                edge |= eval_group<2>(P, (col & 1) ? side : 0.f, (col & 2) ? side : 0.f, dz2, pv) != 0;
+                combine_group<2>(op, k, acc2, pv);
+                const float t0 = acc2[0], t4 = acc2[1];
+                v[0] = v[1]; v[1] = v[2]; v[2] = v[3]; v[3] = t0;
+                v[4] = v[5]; v[5] = v[6]; v[6] = v[7]; v[7] = t4;
             }
         }
+        if (edge) v[0] = __int_as_float(0x7fc00000);  // NaN: decide_block takes the float64 path
         float m;
         kd = decide_block(G, v, m, [&](int c) {
             return list_eval_d(list, len, chain, prims, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
@@ -1090,8 +1103,11 @@ __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float 
     return fmaf(P.s, canon_f(P.type, P.p, x, y, z), -P.off);
 }
 
+// Returns bit k set where voxel k sampled a grid table next to its boundary (local_table_edge):
+// its value and the decisions on it are then taken in float64.
 template <int VG>
-__device__ __forceinline__ void eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+__device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+    uint32_t edge = 0;
     switch (P.type) {
     case P_SPHERE: eval_group_t<VG, P_SPHERE>(P, dx, dy, dz, v); break;
     case P_BOX: eval_group_t<VG, P_BOX>(P, dx, dy, dz, v); break;
@@ -1099,8 +1115,12 @@ __device__ __forceinline__ void eval_group(const LocalPrim& P, float dx, float d
     case P_TORUS: eval_group_t<VG, P_TORUS>(P, dx, dy, dz, v); break;
     default:
 #pragma unroll
-        for (int k = 0; k < VG; ++k) v[k] = eval_one_rare(P, dx, dy, dz[k]);
+        for (int k = 0; k < VG; ++k) {
+            v[k] = eval_one_rare(P, dx, dy, dz[k]);
+            edge |= (uint32_t)local_table_edge(P, dx, dy, dz[k]) << k;
+        }
     }
+    return edge;
 }
 
 // acc = op(acc, v) for the VG voxels; the operator switch is taken once.
@@ -1254,9 +1274,13 @@ __device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, co
             const int pi = col / P1, pj = col - pi * P1;
             const float dx = (float)(pi * B) * G.fpitch, dy = (float)(pj * B) * G.fpitch;
             float acc[P1], v[P1];
+            uint32_t edge = 0;
             float* out = val + col * P1;
 #pragma unroll
-            for (int k = 0; k < P1; ++k) acc[k] = first ? 0.f : out[k];
+            for (int k = 0; k < P1; ++k) {
+                acc[k] = first ? 0.f : out[k];
+                edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // marked in an earlier chunk
+            }
             for (int i = 0; i < clen; ++i) {
                 const LocalPrim& P = sp[i];
                 if (P.op == CH_OFFSET) {
@@ -1264,11 +1288,12 @@ __device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, co
                     for (int k = 0; k < P1; ++k) acc[k] -= P.k;
                     continue;
                 }
-                eval_group<P1>(P, dx, dy, dz, v);
+                edge |= eval_group<P1>(P, dx, dy, dz, v);
                 combine_group<P1>(P.op, P.k, acc, v);
             }
+            // a point that sampled a grid table at its boundary: NaN, so decide_block rechecks in float64
 #pragma unroll
-            for (int k = 0; k < P1; ++k) out[k] = acc[k];
+            for (int k = 0; k < P1; ++k) out[k] = (edge >> k) & 1u ? __int_as_float(0x7fc00000) : acc[k];
         }
     }
     __syncwarp();
@@ -1430,6 +1455,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
             const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
             const float dx = li * G.fpitch, dy = lj * G.fpitch;
             float dz[VG], acc[VG], v[VG];
+            uint32_t edge = 0;
 #pragma unroll
             for (int k = 0; k < VG; ++k) dz[k] = (lk0 + k) * G.fpitch;
             if (first) {
@@ -1437,6 +1463,8 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                 for (int k = 0; k < VG; ++k) acc[k] = 0.f;
             } else {
                 load_group<VG>(out, g * 32 + lane, acc);
+#pragma unroll
+                for (int k = 0; k < VG; ++k) edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // an earlier chunk's mark
             }
             for (int i = 0; i < clen; ++i) {
                 const LocalPrim& P = sp[i];
@@ -1446,8 +1474,13 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                     for (int k = 0; k < VG; ++k) acc[k] -= P.k;
                     continue;
                 }
-                eval_group<VG>(P, dx, dy, dz, v);
+                edge |= eval_group<VG>(P, dx, dy, dz, v);
                 combine_group<VG>(op, P.k, acc, v);
+            }
+            if (edge) {  // sampled a grid table at its boundary: carried to the last chunk as NaN
+#pragma unroll
+                for (int k = 0; k < VG; ++k)
+                    if ((edge >> k) & 1u) acc[k] = __int_as_float(0x7fc00000);
             }
             if (last) {
                 if (kDeferGuard) {

@@ -93,6 +93,22 @@ static __device__ __noinline__ float grid_sample_f(const float* __restrict__ p, 
     return p[5] != 0.f ? val : __fmul_rn(__fsub_rn(p[4], val), pitch);
 }
 
+// True where (x, y, z) lies within a thousandth of a cell of a sampled grid's boundary: there the
+// value jumps between the table and the outside constant, and a float32 inside test may decide
+// otherwise than the float64 one (the coordinate itself carries float32 rounding), so the caller
+// takes that sample's decisions in float64.
+static __device__ __noinline__ bool grid_edge_f(const float* __restrict__ p, float x, float y, float z) {
+    const float n[3] = {p[6] - 1.f, p[7] - 1.f, p[8] - 1.f};
+    const float f[3] = {(x - p[0]) / p[3], (y - p[1]) / p[3], (z - p[2]) / p[3]};
+    constexpr float tol = 1e-3f;
+    bool within = true, edge = false;
+    for (int a = 0; a < 3; ++a) {
+        within &= f[a] >= -tol && f[a] <= n[a] + tol;
+        edge |= fabsf(f[a]) < tol || fabsf(f[a] - n[a]) < tol;
+    }
+    return within && edge;
+}
+
 // Revolved (r, z) table, p = {r0, z0, pitch, nr, nz, -, ..., table}: bilinear at (r, z), r the
 // distance from the z axis, cell indices truncated and clamped to the table, weights clamped to [0, 1].
 static __device__ __noinline__ float revolve_sample_f(const float* __restrict__ p, float x, float y, float z) {
@@ -186,6 +202,28 @@ __device__ __forceinline__ float primf_world(const PrimF& P, float x, float y, f
     const float ly = fmaf(P.A[4], x, fmaf(P.A[5], y, fmaf(P.A[6], z, P.A[7])));
     const float lz = fmaf(P.A[8], x, fmaf(P.A[9], y, fmaf(P.A[10], z, P.A[11])));
     return fmaf(P.s, canon_f(P.type, P.p, lx, ly, lz), -P.off);
+}
+
+// Local coordinates of offset (dx, dy, dz) from the block origin.
+__device__ __forceinline__ void local_point(const LocalPrim& P, float dx, float dy, float dz, float& x, float& y,
+                                            float& z) {
+    if (P.ident) {
+        x = P.L[0] + dx;
+        y = P.L[1] + dy;
+        z = P.L[2] + dz;
+    } else {
+        x = fmaf(P.A[0], dx, fmaf(P.A[1], dy, fmaf(P.A[2], dz, P.L[0])));
+        y = fmaf(P.A[3], dx, fmaf(P.A[4], dy, fmaf(P.A[5], dz, P.L[1])));
+        z = fmaf(P.A[6], dx, fmaf(P.A[7], dy, fmaf(P.A[8], dz, P.L[2])));
+    }
+}
+
+// A sampled-grid leaf evaluated at offset (dx, dy, dz) next to its table's boundary (grid_edge_f).
+__device__ __forceinline__ bool local_table_edge(const LocalPrim& P, float dx, float dy, float dz) {
+    if (P.type != P_GRID) return false;
+    float x, y, z;
+    local_point(P, dx, dy, dz, x, y, z);
+    return grid_edge_f(P.p, x, y, z);
 }
 
 // Block-localised float32 value at offset (dx, dy, dz) from the block origin.
