@@ -27,5 +27,13 @@ enum {
 
 static inline int fb_div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Superblock edge in voxels, the middle level of the culling hierarchy (coarse regions are two
+// superblocks wide, blocks below): 32, or 16 for grids of at most 128 voxels per axis -- there a
+// 32-voxel superblock spans a quarter of the grid and culls little of a dense recipe.
+__host__ __device__ inline int fb_super_edge(int64_t nx, int64_t ny, int64_t nz) {
+    const int64_t m = nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz);
+    return m <= 128 ? 16 : 32;
+}
+
 // Number of SMs of the current device (148 on B200), cached per process.
 int fb_sm_count();

@@ -65,7 +65,6 @@ constexpr int kCapBlockWarp = 96;          // least per-block list of the warp-p
 constexpr int kCapBlockWarpMax = 1024;     // ... grown while the lists stay within kCapBlockBudget
 constexpr int64_t kCapBlockBudget = 4 << 20;
 constexpr int64_t kWarpCullBlocks = 1 << 17;  // grids up to this many blocks cull each block with a warp
-constexpr int kSuperEdge = 32;    // voxels per superblock edge
 constexpr int kCoarseDiv = 2;     // superblocks per coarse-region edge
 constexpr int kTile = 2048;       // compaction tile (256 threads x 8)
 constexpr int kLeafWarps = 4;     // warps per CTA in k_leaf
@@ -93,7 +92,7 @@ Geo make_geo(const FbGeom& g) {
     o.nby = (g.ny + g.block - 1) / g.block;
     o.nbz = (g.nz + g.block - 1) / g.block;
     o.nblocks = (int64_t)o.nbx * o.nby * o.nbz;
-    o.S = std::max(1, kSuperEdge / g.block);
+    o.S = std::max(1, fb_super_edge(g.nx, g.ny, g.nz) / g.block);
     o.nsx = (o.nbx + o.S - 1) / o.S;
     o.nsy = (o.nby + o.S - 1) / o.S;
     o.nsz = (o.nbz + o.S - 1) / o.S;
@@ -723,7 +722,10 @@ __device__ __noinline__ double list_eval_d(const uint32_t* __restrict__ list, in
 
 // Threads of one superblock are consecutive (a warp never spans two superblocks in the chain
 // mode), so the walk over the superblock's list runs in lockstep with broadcast loads.
-__host__ __device__ __forceinline__ int threads_per_super(int S) { return ((S * S * S + 31) / 32) * 32; }
+__host__ __device__ __forceinline__ int threads_per_super(int S) {
+    const int n = S * S * S;
+    return n >= 32 ? (n + 31) / 32 * 32 : n;  // 1 or 8: several superblocks share a warp
+}
 
 // Kind and corner_min_abs of one block from its 8 corner values: float32 decisions unless a corner
 // lies within the guard band of 0 or of the margin (or is NaN); then all 8 corners are re-evaluated
@@ -883,10 +885,9 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
     }
 }
 
-// 10 CTAs per SM (48 registers): the walk and the corner folds wait on loads and on the instruction
-// cache, and more resident warps hide that better than the few spills cost.
+// 6 CTAs per SM (80 registers): measured against 8 and 10 (64 / 48 registers, more spills) and 4.
 template <bool kCull>
-__global__ void __launch_bounds__(128, 10) k_classify_blocks(Geo G, const FbPrim* __restrict__ prims,
+__global__ void __launch_bounds__(128, 6) k_classify_blocks(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
                                                              const FbInsn* __restrict__ chain,
                                                              const uint32_t* __restrict__ pool,
@@ -1215,149 +1216,6 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
     }
 }
 
-// ------------------------------------------------------------------------------------ lattice classify
-// Block kinds of a chain recipe from the corner lattice of each superblock (grids of many blocks).
-// A block's 8 corners are lattice points of spacing B pitches shared with up to 7 neighbours; the
-// superblock evaluates its (S+1)^3 lattice once with its own culled list (exact for every point of
-// its closed region) instead of each block culling that list again and evaluating its corners.  A
-// warp per superblock: the list is localised to the superblock origin kLatChunk primitives at a
-// time into shared memory (a capsule re-anchored on its segment, as in localise), and each lane
-// evaluates whole lattice columns along z (the primitive switch taken once per column), keeping the
-// partial folds in shared memory between chunks.  Decisions then follow the per-block rule: a block
-// with a corner value within the guard band of 0 or of the margin (or NaN) re-evaluates all 8
-// corners in float64 with the superblock list and decides in float64, exactly as the oracle.
-constexpr bool kClassifyLattice = false;  // large grids: corner lattice per superblock (else a thread per block)
-constexpr int kLatWarps = 4;
-constexpr int kLatChunk = 32;
-
-// One superblock of the lattice classification (every lane of the warp calls it with the same s):
-// sp holds kLatChunk localised primitives, val the (S+1)^3 lattice values.  Also marks the
-// superblock's blocks as having no per-block list yet (blk_len = -1).
-template <int B>
-__device__ void lattice_super(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
-                              const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
-                              const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
-                              int32_t* __restrict__ kind, float* __restrict__ cma, int32_t* __restrict__ blk_off,
-                              int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int64_t blk_cap,
-                              int* __restrict__ cursor, int64_t s, LocalPrim* sp, float* val) {
-    constexpr int S = 32 / B;          // blocks per superblock edge
-    constexpr int P1 = S + 1;          // lattice points per edge
-    constexpr int NC = P1 * P1;        // lattice columns (along z)
-    const int lane = threadIdx.x & 31;
-    float dz[P1];
-#pragma unroll
-    for (int k = 0; k < P1; ++k) dz[k] = (float)(k * B) * G.fpitch;
-    const int sz = (int)(s % G.nsz), sy = (int)((s / G.nsz) % G.nsy), sx = (int)(s / ((int64_t)G.nsz * G.nsy));
-    const int64_t ix0 = (int64_t)sx * 32, iy0 = (int64_t)sy * 32, iz0 = (int64_t)sz * 32;
-    const double ox = G.x0 + (double)ix0 * G.pitch;
-    const double oy = G.y0 + (double)iy0 * G.pitch;
-    const double oz = G.z0 + (double)iz0 * G.pitch;
-    const uint32_t* list = pool + sb_off[s];
-    const int len = sb_len[s];
-    for (int c0 = 0; c0 == 0 || c0 < len; c0 += kLatChunk) {  // one pass even for an empty list
-        const int clen = max(0, min(kLatChunk, len - c0));
-        const bool first = c0 == 0;
-        __syncwarp();
-        for (int i = lane; i < clen; i += 32) {
-            const uint32_t e = list[c0 + i];
-            const FbInsn I = chain[e >> 2];
-            const int op = effective_op(e, I.op);
-            if (op == CH_OFFSET) {
-                sp[i].op = op;
-                sp[i].k = (float)I.k;
-            } else {
-                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], 32 * G.fpitch);
-            }
-        }
-        __syncwarp();
-        for (int col = lane; col < NC; col += 32) {
-            const int pi = col / P1, pj = col - pi * P1;
-            const float dx = (float)(pi * B) * G.fpitch, dy = (float)(pj * B) * G.fpitch;
-            float acc[P1], v[P1];
-            uint32_t edge = 0;
-            float* out = val + col * P1;
-#pragma unroll
-            for (int k = 0; k < P1; ++k) {
-                acc[k] = first ? 0.f : out[k];
-                edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // marked in an earlier chunk
-            }
-            for (int i = 0; i < clen; ++i) {
-                const LocalPrim& P = sp[i];
-                if (P.op == CH_OFFSET) {
-#pragma unroll
-                    for (int k = 0; k < P1; ++k) acc[k] -= P.k;
-                    continue;
-                }
-                edge |= eval_group<P1>(P, dx, dy, dz, v);
-                combine_group<P1>(P.op, P.k, acc, v);
-            }
-            // a point that sampled a grid table at its boundary: NaN, so decide_block rechecks in float64
-#pragma unroll
-            for (int k = 0; k < P1; ++k) out[k] = (edge >> k) & 1u ? __int_as_float(0x7fc00000) : acc[k];
-        }
-    }
-    __syncwarp();
-    // decisions of the superblock's blocks inside the grid
-    for (int t = lane; t < S * S * S; t += 32) {
-        const int li = t / (S * S), lj = (t / S) % S, lk = t % S;
-        const int bi = sx * S + li, bj = sy * S + lj, bk = sz * S + lk;
-        if (bi >= G.nbx || bj >= G.nby || bk >= G.nbz) continue;
-        const int64_t b = ((int64_t)bi * G.nby + bj) * G.nbz + bk;
-        float vc[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-            vc[c] = val[((li + (c & 1)) * P1 + (lj + ((c >> 1) & 1))) * P1 + lk + ((c >> 2) & 1)];
-        float m;
-        kind[b] = decide_block(G, vc, m, [&](int c) {
-            return list_eval_d(list, len, chain, prims, vertex_d(G.x0, (int64_t)bi * B + (c & 1) * B, G.pitch),
-                               vertex_d(G.y0, (int64_t)bj * B + ((c >> 1) & 1) * B, G.pitch),
-                               vertex_d(G.z0, (int64_t)bk * B + ((c >> 2) & 1) * B, G.pitch));
-        });
-        cma[b] = m;
-        int len_b = -1;
-        if (kind[b] == 0) {
-            // the block's own list, culled from the superblock's for the leaf pass and point queries
-            uint32_t blist[kCapBlock];
-            const float half = 0.5f * B;
-            const int n = seq_walk(list, len, chain, primf, G.fx0 + (bi * B + half) * G.fpitch,
-                                   G.fy0 + (bj * B + half) * G.fpitch, G.fz0 + (bk * B + half) * G.fpitch,
-                                   1.7320509f * half * G.fpitch, G.eps, blist, kCapBlock);
-            if (n <= kCapBlock) {
-                const int slot = atomicAdd(cursor, n);
-                if ((int64_t)slot + n <= blk_cap) {
-                    for (int i = 0; i < n; ++i) blk_pool[slot + i] = blist[i];
-                    blk_off[b] = slot;
-                    len_b = n;
-                }
-            }
-        }
-        blk_len[b] = len_b;  // -1: the leaf pass culls the block itself
-    }
-    __syncwarp();
-}
-
-template <int B>
-__global__ void __launch_bounds__(32 * kLatWarps) k_classify_lattice(Geo G, const FbPrim* __restrict__ prims,
-                                                                     const PrimF* __restrict__ primf,
-                                                                     const FbInsn* __restrict__ chain,
-                                                                     const uint32_t* __restrict__ pool,
-                                                                     const int64_t* __restrict__ sb_off,
-                                                                     const int32_t* __restrict__ sb_len,
-                                                                     int32_t* __restrict__ kind, float* __restrict__ cma,
-                                                                     int32_t* __restrict__ blk_off,
-                                                                     int32_t* __restrict__ blk_len,
-                                                                     uint32_t* __restrict__ blk_pool, int64_t blk_cap,
-                                                                     int* __restrict__ cursor) {
-    constexpr int P1 = 32 / B + 1;
-    __shared__ LocalPrim s_prim[kLatWarps][kLatChunk];
-    __shared__ float s_val[kLatWarps][P1 * P1 * P1];
-    const int warp = threadIdx.x >> 5;
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t s = gwarp; s < G.nsuper; s += nwarps)
-        lattice_super<B>(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, blk_cap,
-                         cursor, s, s_prim[warp], s_val[warp]);
-}
 
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
 // voxels along z (VG = 4, or 2 for 4^3 blocks) and stores each group with one vector store.
@@ -1768,13 +1626,11 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
     if (mode == 1) {
         k_full_list<<<fb_div_up(n_chain, 256), 256, 0, st>>>(S.pool + P.pool_full, n_chain);
         FB_LAUNCH();
-        const int coarse_edge = kSuperEdge * kCoarseDiv;
         // coarse regions from the full chain
         k_cull<true><<<fb_div_up(G.ncoarse * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, nullptr, nullptr, n_chain, 1,
                                                                1, 1, S.off, S.len, P.pool_coarse, P.cap_coarse,
                                                                G.S * G.B * kCoarseDiv, G.ncx, G.ncy, G.ncz);
         FB_LAUNCH();
-        (void)coarse_edge;
         // superblocks from their coarse region
         k_cull<false><<<fb_div_up(G.nsuper * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off, S.len, 0, kCoarseDiv,
                                                               G.ncy, G.ncz, S.off + G.ncoarse, S.len + G.ncoarse,
@@ -1789,32 +1645,11 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
             k_classify_blocks<false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
                 G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
                 S.blk_pool, P.blk_cap, S.misc + 2);
-        } else if (!kClassifyLattice) {
+        } else {
             // a thread per block: its own cull of the superblock list, kept for the active blocks
             k_classify_blocks<true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
                 G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
                 S.blk_pool, P.blk_cap, S.misc + 2);
-        } else {
-            // a warp per superblock: the corner lattice, lists culled for the active blocks
-            const int grid = (int)std::min<int64_t>(fb_div_up(G.nsuper, kLatWarps), (int64_t)fb_sm_count() * 64);
-            const int64_t* sb_off = S.off + G.ncoarse;
-            const int32_t* sb_len = S.len + G.ncoarse;
-            switch (G.B) {
-            case 4:
-                k_classify_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
-                                                                       kind, cma, S.blk_off, S.blk_len, S.blk_pool, P.blk_cap,
-                                                                       S.misc + 2);
-                break;
-            case 8:
-                k_classify_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
-                                                                       kind, cma, S.blk_off, S.blk_len, S.blk_pool, P.blk_cap,
-                                                                       S.misc + 2);
-                break;
-            default:
-                k_classify_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len,
-                                                                       kind, cma, S.blk_off, S.blk_len, S.blk_pool, P.blk_cap,
-                                                                       S.misc + 2);
-            }
         }
     } else {
         k_classify_program<<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, chain, n_chain, kind, cma);
@@ -1963,7 +1798,7 @@ __global__ void __launch_bounds__(128) k_b_cull_blocks(const RecDesc* __restrict
 // Each recipe's thread range is a multiple of 32 (nsuper x threads_per_super), so a warp never
 // spans two recipes.  kCull: recipes without k_cull_blocks lists cull their blocks here.
 template <bool kCull>
-__global__ void __launch_bounds__(128, 10) k_b_classify_blocks(const RecDesc* __restrict__ D, Group W, int64_t total,
+__global__ void __launch_bounds__(128, 6) k_b_classify_blocks(const RecDesc* __restrict__ D, Group W, int64_t total,
                                                                int* __restrict__ cursors) {
     const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= total) return;
@@ -1973,22 +1808,6 @@ __global__ void __launch_bounds__(128, 10) k_b_classify_blocks(const RecDesc* __
                           R.cma, R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[W.rec[j]], g - W.pre[j]);
 }
 
-template <int B>
-__global__ void __launch_bounds__(32 * kLatWarps) k_b_lattice(const RecDesc* __restrict__ D, Group W, int64_t total,
-                                                              int* __restrict__ cursors) {
-    constexpr int P1 = 32 / B + 1;
-    __shared__ LocalPrim s_prim[kLatWarps][kLatChunk];
-    __shared__ float s_val[kLatWarps][P1 * P1 * P1];
-    const int warp = threadIdx.x >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < total; g += nwarps) {
-        const int j = group_find(W, g);
-        const RecDesc& R = D[W.rec[j]];
-        lattice_super<B>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind,
-                         R.cma, R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[W.rec[j]], g - W.pre[j],
-                         s_prim[warp], s_val[warp]);
-    }
-}
 
 // Compaction of every recipe: tiles are taken from one ticket counter in the group's order, so a
 // recipe's predecessor tiles always hold smaller tickets (already running when a tile waits).
@@ -2104,7 +1923,7 @@ struct BatchHost {
     int64_t dev_bytes = 0;
     RecDesc* d_desc = nullptr;
     // static groups and their totals
-    Group prims{}, chain{}, coarse{}, super_{}, wblocks{}, wclass{}, cclass{}, lat[3]{}, tiles{};
+    Group prims{}, chain{}, coarse{}, super_{}, wblocks{}, wclass{}, cclass{}, lat[3]{}, tiles{};  // lat: unused
     int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_wblocks = 0, n_wclass = 0, n_cclass = 0,
             n_lat[3] = {0, 0, 0}, n_tiles = 0;
     // dynamic groups (prefixes written by k_batch_offsets)
@@ -2207,13 +2026,13 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             g_chain.add(r, d.n_chain);
             g_coarse.add(r, G.ncoarse);
             g_super.add(r, G.nsuper);
+            // classification threads rounded up to whole warps: a warp never spans two recipes
+            const int64_t cls_threads = (G.nsuper * threads_per_super(G.S) + 31) / 32 * 32;
             if (d.warp_blocks) {
                 g_wblocks.add(r, G.nblocks);
-                g_wclass.add(r, G.nsuper * threads_per_super(G.S));
-            } else if (!kClassifyLattice) {
-                g_cclass.add(r, G.nsuper * threads_per_super(G.S));
+                g_wclass.add(r, cls_threads);
             } else {
-                g_lat[b_index(G.B)].add(r, G.nsuper);
+                g_cclass.add(r, cls_threads);
             }
             g_tiles.add(r, d.ntiles);
             g_leaf[b_index(G.B)].add(r, 0);
@@ -2361,14 +2180,6 @@ int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, i
         k_b_classify_blocks<true><<<fb_div_up(H->n_cclass, 128), 128, 0, st>>>(D, H->cclass, H->n_cclass, H->cursors);
         FB_LAUNCH();
     }
-    for (int q = 0; q < 3; ++q) {
-        if (!H->n_lat[q]) continue;
-        const int grid = (int)std::min<int64_t>(fb_div_up(H->n_lat[q], kLatWarps), (int64_t)sms * 64);
-        if (q == 0) k_b_lattice<4><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[0], H->n_lat[0], H->cursors);
-        else if (q == 1) k_b_lattice<8><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[1], H->n_lat[1], H->cursors);
-        else k_b_lattice<16><<<grid, 32 * kLatWarps, 0, st>>>(D, H->lat[2], H->n_lat[2], H->cursors);
-        FB_LAUNCH();
-    }
     if (int rc = mark(2)) return rc;
     k_b_compact<<<(unsigned)H->n_tiles, 256, 0, st>>>(D, H->tiles, H->misc, kLookbackSpins);
     FB_LAUNCH();
@@ -2429,7 +2240,8 @@ int32_t fb_batch_launches(void* batch) noexcept {
     if (!H) return -1;
     int n = 1 + 4 + 2;  // memset; prepare, full list, two cull levels; compaction, offsets
     if (H->n_wblocks) n += 2;
-    for (int q = 0; q < 3; ++q) n += (H->n_lat[q] ? 1 : 0) + (H->leaf[q].m ? 1 : 0);
+    if (H->n_cclass) n += 1;
+    for (int q = 0; q < 3; ++q) n += H->leaf[q].m ? 1 : 0;
     return n;
 }
 

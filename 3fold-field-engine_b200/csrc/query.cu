@@ -309,7 +309,7 @@ int64_t accel_bins(const int32_t* dims) {
     const int B = dims[3];
     if (B < 1) return -1;
     const int64_t nbx = (dims[0] + B - 1) / B, nby = (dims[1] + B - 1) / B, nbz = (dims[2] + B - 1) / B;
-    const int64_t S = std::max(1, 32 / B);
+    const int64_t S = std::max(1, fb_super_edge(dims[0], dims[1], dims[2]) / B);
     const int64_t ns = ((nbx + S - 1) / S) * ((nby + S - 1) / S) * ((nbz + S - 1) / S);
     return nbx * nby * nbz + ns + 1;
 }
@@ -699,7 +699,7 @@ int fb_query_points_device(const void* d_primf, const FbInsn* d_chain, int32_t n
         A.x0 = accel_grid[0]; A.y0 = accel_grid[1]; A.z0 = accel_grid[2]; A.pitch = accel_grid[3];
         A.nx = accel_dims[0]; A.ny = accel_dims[1]; A.nz = accel_dims[2]; A.B = accel_dims[3];
         A.nbx = (A.nx + A.B - 1) / A.B; A.nby = (A.ny + A.B - 1) / A.B; A.nbz = (A.nz + A.B - 1) / A.B;
-        A.S = std::max(1, 32 / A.B);
+        A.S = std::max(1, fb_super_edge(A.nx, A.ny, A.nz) / A.B);
         A.nsy = (A.nby + A.S - 1) / A.S;
         A.nsz = (A.nbz + A.S - 1) / A.S;
         if (blk_off && blk_len && blk_pool && blk_cap > 0 && (blk_all || d_kind)) {
