@@ -1091,7 +1091,9 @@ __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float
 
 // The five kinds the milling recipes rarely use, out of line and one voxel per call (scalar
 // arguments stay in registers): the hot loop keeps only the four common kinds inlined, small enough
-// to stay in the instruction cache.
+// to stay in the instruction cache.  A sampled grid's voxel next to its table's boundary
+// (grid_edge_f) returns NaN: the caller marks it for the float64 recheck -- one call site, so the
+// hot loop keeps a single call on its rare path.
 __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float dy, float dz) {
     float x, y, z;
     if (P.ident) {
@@ -1101,10 +1103,11 @@ __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float 
         y = fmaf(P.A[5], dz, fmaf(P.A[3], dx, fmaf(P.A[4], dy, P.L[1])));
         z = fmaf(P.A[8], dz, fmaf(P.A[6], dx, fmaf(P.A[7], dy, P.L[2])));
     }
+    if (P.type == P_GRID && grid_edge_f(P.p, x, y, z)) return __int_as_float(0x7fc00000);
     return fmaf(P.s, canon_f(P.type, P.p, x, y, z), -P.off);
 }
 
-// Returns bit k set where voxel k sampled a grid table next to its boundary (local_table_edge):
+// Returns bit k set where voxel k sampled a grid table next to its boundary (eval_one_rare's NaN):
 // its value and the decisions on it are then taken in float64.
 template <int VG>
 __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
@@ -1118,7 +1121,7 @@ __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, flo
 #pragma unroll
         for (int k = 0; k < VG; ++k) {
             v[k] = eval_one_rare(P, dx, dy, dz[k]);
-            edge |= (uint32_t)local_table_edge(P, dx, dy, dz[k]) << k;
+            edge |= (uint32_t)!(v[k] == v[k]) << k;
         }
     }
     return edge;

@@ -204,28 +204,6 @@ __device__ __forceinline__ float primf_world(const PrimF& P, float x, float y, f
     return fmaf(P.s, canon_f(P.type, P.p, lx, ly, lz), -P.off);
 }
 
-// Local coordinates of offset (dx, dy, dz) from the block origin.
-__device__ __forceinline__ void local_point(const LocalPrim& P, float dx, float dy, float dz, float& x, float& y,
-                                            float& z) {
-    if (P.ident) {
-        x = P.L[0] + dx;
-        y = P.L[1] + dy;
-        z = P.L[2] + dz;
-    } else {
-        x = fmaf(P.A[0], dx, fmaf(P.A[1], dy, fmaf(P.A[2], dz, P.L[0])));
-        y = fmaf(P.A[3], dx, fmaf(P.A[4], dy, fmaf(P.A[5], dz, P.L[1])));
-        z = fmaf(P.A[6], dx, fmaf(P.A[7], dy, fmaf(P.A[8], dz, P.L[2])));
-    }
-}
-
-// A sampled-grid leaf evaluated at offset (dx, dy, dz) next to its table's boundary (grid_edge_f).
-__device__ __forceinline__ bool local_table_edge(const LocalPrim& P, float dx, float dy, float dz) {
-    if (P.type != P_GRID) return false;
-    float x, y, z;
-    local_point(P, dx, dy, dz, x, y, z);
-    return grid_edge_f(P.p, x, y, z);
-}
-
 // Block-localised float32 value at offset (dx, dy, dz) from the block origin.
 __device__ __forceinline__ float local_eval(const LocalPrim& P, float dx, float dy, float dz) {
     float x, y, z;

@@ -394,8 +394,22 @@ def e2e_leg(comp, meta, mask_np, dev, steps=3):
                + host_sq.numel() * 4)
         del sf  # the caller is done with this step's arrays: their page-locked blocks go back to the cache
     times = times[2:]
-    return {"value": leaf / statistics.median(times) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "seconds_per_step": statistics.median(times),
+    # the device->host link alone: the same byte count in one page-locked copy (the bound of this leg)
+    probe_d = torch.empty(int(d2h) // 4, dtype=torch.int32, device=dev)
+    probe_h = torch.empty(probe_d.shape, dtype=torch.int32, pin_memory=True)
+    link = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        probe_h.copy_(probe_d, non_blocking=True)
+        torch.cuda.synchronize()
+        link.append(time.perf_counter() - t0)
+    d2h_gbs = probe_d.numel() * 4 / min(link) / 1e9
+    del probe_d, probe_h
+    med = statistics.median(times)
+    return {"value": leaf / med / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "seconds_per_step": med,
+            "d2h_link_gbs": d2h_gbs, "link_bound_value": leaf / (d2h / (d2h_gbs * 1e9)) / 1e9,
             "api": "field_b200.build.FieldBuilder.build + DeviceField.to_host; field_b200.edt.squared_distance_device "
                    "with page-locked host mask and result (EDT on a second stream)"}
 
@@ -775,8 +789,19 @@ def e2e_batched(bb, steps):
         times.append(time.perf_counter() - t0)
     times = times[1:]
     sec = float(statistics.median(times))
-    return {"value": n and sum(int(c) * int(b) for c, b in zip(cnt, bb.b3)) / sec / 1e9, "unit": UNIT,
+    voxels = sum(int(c) * int(b) for c, b in zip(cnt, bb.b3))
+    # the device->host link alone on the tile bytes (one page-locked copy): the bound of this leg
+    link = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        host_tiles[:n].copy_(bb.tiles[:n], non_blocking=True)
+        torch.cuda.synchronize()
+        link.append(time.perf_counter() - t0)
+    d2h_gbs = n * 4 / min(link) / 1e9
+    return {"value": n and voxels / sec / 1e9, "unit": UNIT,
             "h2d_bytes_per_step": bb.table_bytes, "d2h_bytes_per_step": int(d2h), "seconds_per_step": sec,
+            "d2h_link_gbs": d2h_gbs, "link_bound_value": voxels / (d2h / (d2h_gbs * 1e9)) / 1e9,
             "api": "field_b200.batch.BatchBuilder (upload_tables, enqueue, tile_offsets / leaf_counts) with pinned "
                    "host buffers for the tiles, kinds and active ids"}
 
