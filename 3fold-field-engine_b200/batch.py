@@ -2,12 +2,12 @@
 
 ``BatchBuilder(recipes)`` keeps every recipe's compiled tables, culling scratch and outputs resident
 (one FieldBuilder slab each) and builds them all with ``fb_batch_build_device``: each phase -- the
-float32 mirror of the tables, two culling levels, classification (warp-culled blocks on grids of
-few blocks, the corner lattice with the active blocks' own lists on the others), compaction, the
-leaf tiles -- is one launch over a work-list spanning every recipe, so the small recipes fill
-the GPU beside the large ones.  The active counts, each recipe's place in the tile arena and the
-active-block work-lists are formed on the device: a build has no host synchronisation and
-allocates nothing, and the ~15 launches can be captured into one CUDA graph.  With ``edt=True``
+float32 mirror of the tables, two culling levels, classification (a thread per block culling its
+superblock's list; the active blocks keep their lists), compaction, the leaf tiles -- is one
+launch over a work-list spanning every recipe, so the small recipes fill the GPU beside the large
+ones.  The active counts, each recipe's place in the tile arena and the active-block work-lists
+are formed on the device: a build has no host synchronisation and allocates nothing, and the ~10
+launches can be captured into one CUDA graph.  With ``edt=True``
 every build is followed by each recipe's occupancy rasterisation (batched) and the squared EDT of
 that occupancy (distance to the solid), spread over side streams.
 

@@ -182,6 +182,9 @@ class FieldBuilder:
         if guard is None and c.tables:  # float32 table samples carry more error than the default band
             guard = max(meta.guard(), c.sampling_guard())
         self.geom = geom_of(meta, guard)
+        # fb_geom.reserved[0] bit 0: sampled-grid leaves present (the kernels then mark the voxels at
+        # a table's boundary for the float64 recheck)
+        self.geom.reserved[0] = int(bool(np.any(c.prims["type"] == X.P_GRID)))
         if tables is not None:
             # the caller placed the tables on the device (e.g. a batch's table arena); still checked
             _validate_program(c.prims, insns, self.mode, len(c.tables))

@@ -7,11 +7,12 @@
 //                    elements that can influence the region (Lipschitz interval arithmetic, exact
 //                    for min/max: a skipped element is strictly dominated everywhere in the
 //                    region, and an element that strictly dominates resets the list).  Two levels:
-//                    128-voxel coarse regions from the full chain, 32-voxel superblocks from those.
-//   k_classify       thread per block: culls the superblock list to the block, evaluates the 8
+//                    coarse regions (two superblocks wide) from the full chain, superblocks (32
+//                    voxels, 16 on grids of at most 128 per axis) from those.
+//   k_classify_blocks  thread per block: culls the superblock list to the block, evaluates the 8
 //                    corners in float32 in block-local coordinates, decides kind -1/0/+1 by the
 //                    reference rule, re-evaluating in float64 when a corner value lies within the
-//                    guard band of 0 or of the margin.
+//                    guard band of 0 or of the margin; the active blocks keep their lists.
 //   k_compact        single-pass decoupled look-back scan: ascending active block ids + count.
 //   k_leaf<B>        warp per active block: block-level culling, float64 -> float32 localisation of
 //                    each surviving primitive, float32 evaluation of all B^3 voxels, float64 recheck
@@ -61,10 +62,6 @@ constexpr int kCapCoarse = 1024;           // least list capacity of a coarse re
 constexpr int kCapSuper = 256;             // least list capacity of a superblock
 constexpr int64_t kCapBudget = 8 << 20;    // list entries per level beyond which capacities stop growing
 constexpr int kCapBlock = 48;              // leaf staging chunk and the leaf pass's own culled-list capacity
-constexpr int kCapBlockWarp = 96;          // least per-block list of the warp-per-block cull
-constexpr int kCapBlockWarpMax = 1024;     // ... grown while the lists stay within kCapBlockBudget
-constexpr int64_t kCapBlockBudget = 4 << 20;
-constexpr int64_t kWarpCullBlocks = 1 << 17;  // grids up to this many blocks cull each block with a warp
 constexpr int kCoarseDiv = 2;     // superblocks per coarse-region edge
 constexpr int kTile = 2048;       // compaction tile (256 threads x 8)
 constexpr int kLeafWarps = 4;     // warps per CTA in k_leaf
@@ -81,6 +78,7 @@ struct Geo {
     int ncx, ncy, ncz;
     int64_t ncoarse;
     float margin, guard, eps;
+    int grid_leaves;  // the recipe has sampled-grid leaves (fb_geom.reserved[0] bit 0)
 };
 
 Geo make_geo(const FbGeom& g) {
@@ -104,6 +102,7 @@ Geo make_geo(const FbGeom& g) {
     o.margin = g.margin;
     o.guard = g.guard;
     o.eps = 4.0f * g.guard;
+    o.grid_leaves = g.reserved[0] & 1;
     return o;
 }
 
@@ -124,8 +123,6 @@ struct Plan {
     int64_t pool_full, pool_coarse, pool_super;  // element offsets inside pool
     int64_t ntiles;
     int cap_coarse, cap_super;  // list capacities per coarse region / superblock
-    bool warp_blocks;           // per-block lists culled by one warp each, at blk_pool + b * cap_block
-    int cap_block;              // their capacity
 };
 
 // List capacity of a level: grows while the level's lists stay within kCapBudget entries, never
@@ -143,9 +140,6 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     p.primf = at; at += align256((int64_t)std::max(n_prims, 1) * sizeof(PrimF));
     p.cap_coarse = level_cap(G.ncoarse, kCapCoarse, n_chain);
     p.cap_super = level_cap(G.nsuper, kCapSuper, n_chain);
-    p.warp_blocks = G.nblocks <= kWarpCullBlocks;
-    p.cap_block = (int)std::min<int64_t>(
-        kCapBlockWarpMax, std::max<int64_t>(kCapBlockWarp, kCapBlockBudget / std::max<int64_t>(G.nblocks, 1)));
     p.pool_full = 0;
     p.pool_coarse = n_chain;
     p.pool_super = p.pool_coarse + G.ncoarse * p.cap_coarse;
@@ -158,7 +152,7 @@ Plan make_plan(const Geo& G, int n_prims, int n_chain) {
     p.misc = at; at += 256;  // [0] ticket, [1] error flag, [2] block-list pool cursor
     p.blk_off = at; at += align256(G.nblocks * 4);
     p.blk_len = at; at += align256(G.nblocks * 4);
-    p.blk_cap = p.warp_blocks ? G.nblocks * p.cap_block : std::max<int64_t>(G.nblocks * 12, 4096);
+    p.blk_cap = std::max<int64_t>(G.nblocks * 12, 4096);  // active blocks' lists (<= kCapBlock each)
     p.blk_pool = at; at += align256(p.blk_cap * 4);
     p.total = at;
     return p;
@@ -671,38 +665,6 @@ __global__ void k_cull(Geo G, const FbInsn* __restrict__ chain, const PrimF* __r
                        edge, rny, rnz, r);
 }
 
-// Block-level cull with one warp per block, for grids of few blocks (where one thread per block
-// would leave most of the GPU idle): the superblock list culled to the block's own list, stored at
-// blk_pool + b * cap.  blk_len[b] = -1 when it does not fit; that block then uses the superblock list
-// (exact, only slower).
-__device__ void cull_block(const Geo& G, const FbInsn* __restrict__ chain, const PrimF* __restrict__ primf,
-                           const uint32_t* __restrict__ pool, const int64_t* __restrict__ sb_off,
-                           const int32_t* __restrict__ sb_len, int32_t* __restrict__ blk_off,
-                           int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool, int cap, int64_t b) {
-    const int bk = (int)(b % G.nbz), bj = (int)((b / G.nbz) % G.nby), bi = (int)(b / ((int64_t)G.nbz * G.nby));
-    const int64_t s = ((int64_t)(bi / G.S) * G.nsy + bj / G.S) * G.nsz + bk / G.S;
-    const float half = 0.5f * G.B;
-    const float cx = G.fx0 + (bi * G.B + half) * G.fpitch;
-    const float cy = G.fy0 + (bj * G.B + half) * G.fpitch;
-    const float cz = G.fz0 + (bk * G.B + half) * G.fpitch;
-    const float R = 1.7320509f * half * G.fpitch;
-    const int n = warp_walk(pool + sb_off[s], sb_len[s], chain, primf, cx, cy, cz, R, G.eps, blk_pool + b * cap, cap);
-    if ((threadIdx.x & 31) == 0) {
-        blk_off[b] = (int32_t)(b * cap);
-        blk_len[b] = n <= cap ? n : -1;
-    }
-}
-
-__global__ void __launch_bounds__(128) k_cull_blocks(Geo G, const FbInsn* __restrict__ chain,
-                                                     const PrimF* __restrict__ primf, const uint32_t* __restrict__ pool,
-                                                     const int64_t* __restrict__ sb_off,
-                                                     const int32_t* __restrict__ sb_len, int32_t* __restrict__ blk_off,
-                                                     int32_t* __restrict__ blk_len, uint32_t* __restrict__ blk_pool,
-                                                     int cap) {
-    const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (b >= G.nblocks) return;
-    cull_block(G, chain, primf, pool, sb_off, sb_len, blk_off, blk_len, blk_pool, cap, b);
-}
 
 // ------------------------------------------------------------------------------------ localisation
 // ------------------------------------------------------------------------------------ classify
@@ -767,18 +729,16 @@ __device__ __forceinline__ double vertex_d(double origin, int64_t i, double pitc
 // Thread-per-block classification of a chain recipe: thread t of the superblock-major order --
 // threads of one superblock are consecutive, so a warp never spans two superblocks and walks in
 // lockstep with broadcast loads -- evaluates its block's 8 corners in float32 in block-local
-// coordinates.  kCull = false: the per-block lists k_cull_blocks left in blk_pool (grids of few
-// blocks).  kCull = true: the block culls the superblock list itself (seq_walk, kCapBlock entries)
-// and an active block keeps that list for the leaf pass and point queries: the warp's lists are
+// coordinates.  The block culls the superblock list itself (seq_walk, kCapBlock entries) and an
+// active block keeps that list for the leaf pass and point queries: the warp's lists are
 // placed with one atomicAdd on `cursor` (blk_len -1 where a list overflowed or the pool is full;
 // the leaf pass then culls the block itself).  Every lane of a warp reaches the placement, so
 // threads outside the grid only skip the evaluation.
-template <int VG>
+template <int VG, bool kEdge = true>
 __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v);
 template <int VG>
 __device__ __forceinline__ void combine_group(int op, float k, float* acc, const float* v);
 
-template <bool kCull>
 __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
                                const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
                                const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len,
@@ -794,27 +754,21 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
     const bool valid = s_id < G.nsuper && local < S * S * S && bi < G.nbx && bj < G.nby && bk < G.nbz;
     const int64_t b = ((int64_t)bi * G.nby + bj) * G.nbz + bk;
     const int B = G.B;
-    uint32_t blist[kCull ? kCapBlock : 1];
+    uint32_t blist[kCapBlock];
     int nblist = -1;
     int kd = 1;
     if (valid) {
         const uint32_t* list;
         int len;
-        if (kCull) {
-            const uint32_t* plist = pool + sb_off[s_id];
-            const int plen = sb_len[s_id];
-            const float half = 0.5f * B;
-            const int n = seq_walk(plist, plen, chain, primf, G.fx0 + (bi * B + half) * G.fpitch,
-                                   G.fy0 + (bj * B + half) * G.fpitch, G.fz0 + (bk * B + half) * G.fpitch,
-                                   1.7320509f * half * G.fpitch, G.eps, blist, kCapBlock);
-            nblist = n;
-            list = n <= kCapBlock ? blist : plist;
-            len = n <= kCapBlock ? n : plen;
-        } else {
-            const int n = blk_len[b];
-            list = n >= 0 ? blk_pool + blk_off[b] : pool + sb_off[s_id];
-            len = n >= 0 ? n : sb_len[s_id];
-        }
+        const uint32_t* plist = pool + sb_off[s_id];
+        const int plen = sb_len[s_id];
+        const float half = 0.5f * B;
+        const int n = seq_walk(plist, plen, chain, primf, G.fx0 + (bi * B + half) * G.fpitch,
+                               G.fy0 + (bj * B + half) * G.fpitch, G.fz0 + (bk * B + half) * G.fpitch,
+                               1.7320509f * half * G.fpitch, G.eps, blist, kCapBlock);
+        nblist = n;
+        list = n <= kCapBlock ? blist : plist;
+        len = n <= kCapBlock ? n : plen;
         const double ox = G.x0 + (double)(bi * B) * G.pitch;
         const double oy = G.y0 + (double)(bj * B) * G.pitch;
         const double oz = G.z0 + (double)(bk * B) * G.pitch;
@@ -858,7 +812,7 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
         kind[b] = kd;
         cma[b] = m;
     }
-    if (kCull) {
+    {
         // the warp's active blocks' lists: an inclusive scan of their lengths, one atomicAdd
         const int lane = threadIdx.x & 31;
         const bool keep = valid && kd == 0 && nblist >= 0 && nblist <= kCapBlock;
@@ -886,7 +840,6 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
 }
 
 // 6 CTAs per SM (80 registers): measured against 8 and 10 (64 / 48 registers, more spills) and 4.
-template <bool kCull>
 __global__ void __launch_bounds__(128, 6) k_classify_blocks(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
                                                              const FbInsn* __restrict__ chain,
@@ -898,8 +851,8 @@ __global__ void __launch_bounds__(128, 6) k_classify_blocks(Geo G, const FbPrim*
                                                              uint32_t* __restrict__ blk_pool, int64_t blk_cap,
                                                              int* __restrict__ cursor) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    classify_block<kCull>(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, blk_cap,
-                          cursor, t);
+    classify_block(G, prims, primf, chain, pool, sb_off, sb_len, kind, cma, blk_off, blk_len, blk_pool, blk_cap, cursor,
+                   t);
 }
 
 // General postfix programs: every corner of every block in float64, no culling.
@@ -1108,8 +1061,9 @@ __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float 
 }
 
 // Returns bit k set where voxel k sampled a grid table next to its boundary (eval_one_rare's NaN):
-// its value and the decisions on it are then taken in float64.
-template <int VG>
+// its value and the decisions on it are then taken in float64.  kEdge = false: recipes without
+// sampled-grid leaves, the marks left out.
+template <int VG, bool kEdge>
 __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
     uint32_t edge = 0;
     switch (P.type) {
@@ -1121,7 +1075,7 @@ __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, flo
 #pragma unroll
         for (int k = 0; k < VG; ++k) {
             v[k] = eval_one_rare(P, dx, dy, dz[k]);
-            edge |= (uint32_t)!(v[k] == v[k]) << k;
+            if (kEdge) edge |= (uint32_t)!(v[k] == v[k]) << k;
         }
     }
     return edge;
@@ -1225,8 +1179,10 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
 // One active block's tile: the block's culled list (as the classification left it, else culled
 // here from the superblock list into `sl`), localised kCapBlock primitives at a time into `sp`, each
 // lane evaluating groups of VG consecutive voxels along z (VG = 4, or 2 for 4^3 blocks) and storing
-// each group with one vector store.  Every lane of the warp calls it with the same block.
-template <int B>
+// each group with one vector store.  Every lane of the warp calls it with the same block.  kEdge:
+// the recipe has sampled-grid leaves, whose voxels at a table's boundary are marked for the float64
+// recheck (the marks cost registers in the hot loop, so recipes without such leaves leave them out).
+template <int B, bool kEdge>
 __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
                            const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
                            const int64_t* __restrict__ sb_off, const int32_t* __restrict__ sb_len, int64_t blk,
@@ -1324,8 +1280,10 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                 for (int k = 0; k < VG; ++k) acc[k] = 0.f;
             } else {
                 load_group<VG>(out, g * 32 + lane, acc);
+                if (kEdge) {
 #pragma unroll
-                for (int k = 0; k < VG; ++k) edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // an earlier chunk's mark
+                    for (int k = 0; k < VG; ++k) edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // an earlier chunk's mark
+                }
             }
             for (int i = 0; i < clen; ++i) {
                 const LocalPrim& P = sp[i];
@@ -1335,10 +1293,10 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                     for (int k = 0; k < VG; ++k) acc[k] -= P.k;
                     continue;
                 }
-                edge |= eval_group<VG>(P, dx, dy, dz, v);
+                edge |= eval_group<VG, kEdge>(P, dx, dy, dz, v);
                 combine_group<VG>(op, P.k, acc, v);
             }
-            if (edge) {  // sampled a grid table at its boundary: carried to the last chunk as NaN
+            if (kEdge && edge) {  // sampled a grid table at its boundary: carried to the last chunk as NaN
 #pragma unroll
                 for (int k = 0; k < VG; ++k)
                     if ((edge >> k) & 1u) acc[k] = __int_as_float(0x7fc00000);
@@ -1371,7 +1329,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
 }
 
 // Leaf tiles of a chain recipe: a warp per active block (leaf_block).
-template <int B>
+template <int B, bool kEdge>
 __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_leaf(Geo G, const FbPrim* __restrict__ prims,
                                                              const PrimF* __restrict__ primf,
                                                              const FbInsn* __restrict__ chain,
@@ -1393,8 +1351,8 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_leaf(Geo G, const FbPrim
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t n_active = min((int64_t)count[0], capacity);
     for (int64_t a = gwarp; a < n_active; a += nwarps)
-        leaf_block<B>(G, prims, primf, chain, pool, sb_off, sb_len, active[a], tiles + a * (B * B * B), work, kind,
-                      blk_off, blk_len, blk_pool, blk_cap, s_prim[warp], s_list[warp]);
+        leaf_block<B, kEdge>(G, prims, primf, chain, pool, sb_off, sb_len, active[a], tiles + a * (B * B * B), work,
+                             kind, blk_off, blk_len, blk_pool, blk_cap, s_prim[warp], s_list[warp]);
 }
 
 // Leaf tiles of a general postfix program: float64 per voxel, no culling.
@@ -1640,20 +1598,10 @@ int classify_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbIns
                                                               P.pool_super, P.cap_super, G.S * G.B, G.nsx, G.nsy, G.nsz);
         FB_LAUNCH();
         FB_CUDA(cudaMemsetAsync(S.misc, 0, 256, st));
-        if (P.warp_blocks) {
-            k_cull_blocks<<<fb_div_up(G.nblocks * 32, 128), 128, 0, st>>>(G, chain, S.primf, S.pool, S.off + G.ncoarse,
-                                                                         S.len + G.ncoarse, S.blk_off, S.blk_len,
-                                                                         S.blk_pool, P.cap_block);
-            FB_LAUNCH();
-            k_classify_blocks<false><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
-                G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
-                S.blk_pool, P.blk_cap, S.misc + 2);
-        } else {
-            // a thread per block: its own cull of the superblock list, kept for the active blocks
-            k_classify_blocks<true><<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
-                G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
-                S.blk_pool, P.blk_cap, S.misc + 2);
-        }
+        // a thread per block: its own cull of the superblock list, kept for the active blocks
+        k_classify_blocks<<<fb_div_up(G.nsuper * threads_per_super(G.S), 128), 128, 0, st>>>(
+            G, prims, S.primf, chain, S.pool, S.off + G.ncoarse, S.len + G.ncoarse, kind, cma, S.blk_off, S.blk_len,
+            S.blk_pool, P.blk_cap, S.misc + 2);
     } else {
         k_classify_program<<<fb_div_up(G.nblocks, 128), 128, 0, st>>>(G, prims, chain, n_chain, kind, cma);
     }
@@ -1682,22 +1630,17 @@ int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* c
         default: k_leaf_program<16><<<grid, 128, 0, st>>>(G, prims, chain, n_chain, active, count, capacity, tiles);
         }
     } else {
+#define FB_LEAF(BB, EDGE)                                                                                   \
+    k_leaf<BB, EDGE><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, \
+                                                       count, capacity, tiles, work, kind, S.blk_off, S.blk_len,  \
+                                                       S.blk_pool, P.blk_cap)
+        const bool edge = G.grid_leaves != 0;
         switch (G.B) {
-        case 4:
-            k_leaf<4><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, count,
-                                                       capacity, tiles, work, kind, S.blk_off, S.blk_len, S.blk_pool,
-                                                       P.blk_cap);
-            break;
-        case 8:
-            k_leaf<8><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, count,
-                                                       capacity, tiles, work, kind, S.blk_off, S.blk_len, S.blk_pool,
-                                                       P.blk_cap);
-            break;
-        default:
-            k_leaf<16><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active,
-                                                        count, capacity, tiles, work, kind, S.blk_off, S.blk_len,
-                                                        S.blk_pool, P.blk_cap);
+        case 4: if (edge) FB_LEAF(4, true); else FB_LEAF(4, false); break;
+        case 8: if (edge) FB_LEAF(8, true); else FB_LEAF(8, false); break;
+        default: if (edge) FB_LEAF(16, true); else FB_LEAF(16, false);
         }
+#undef FB_LEAF
     }
     FB_LAUNCH();
     return FB_OK;
@@ -1724,7 +1667,7 @@ struct RecDesc {
     int64_t* off;  // coarse regions then superblocks
     int32_t* len;
     int64_t pool_coarse, pool_super;
-    int32_t cap_coarse, cap_super, cap_block, warp_blocks;
+    int32_t cap_coarse, cap_super;
     int32_t* kind;
     float* cma;
     int32_t* active;
@@ -1789,25 +1732,16 @@ __global__ void __launch_bounds__(128) k_b_cull(const RecDesc* __restrict__ D, G
                            R.len + G.ncoarse, R.pool_super, R.cap_super, G.S * G.B, G.nsy, G.nsz, r);
 }
 
-__global__ void __launch_bounds__(128) k_b_cull_blocks(const RecDesc* __restrict__ D, Group W, int64_t total) {
-    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (g >= total) return;
-    const int j = group_find(W, g);
-    const RecDesc& R = D[W.rec[j]];
-    cull_block(R.G, R.chain, R.primf, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.blk_off, R.blk_len,
-               R.blk_pool, R.cap_block, g - W.pre[j]);
-}
 
 // Each recipe's thread range is a multiple of 32 (nsuper x threads_per_super), so a warp never
-// spans two recipes.  kCull: recipes without k_cull_blocks lists cull their blocks here.
-template <bool kCull>
+// spans two recipes.
 __global__ void __launch_bounds__(128, 6) k_b_classify_blocks(const RecDesc* __restrict__ D, Group W, int64_t total,
                                                                int* __restrict__ cursors) {
     const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= total) return;
     const int j = group_find(W, g);
     const RecDesc& R = D[W.rec[j]];
-    classify_block<kCull>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind,
+    classify_block(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.kind,
                           R.cma, R.blk_off, R.blk_len, R.blk_pool, R.blk_cap, &cursors[W.rec[j]], g - W.pre[j]);
 }
 
@@ -1826,12 +1760,17 @@ __global__ void __launch_bounds__(256) k_b_compact(const RecDesc* __restrict__ D
 
 // After the compaction: each recipe's tile offset in the arena (recipe order, floats), the tiles it
 // gets (count, clipped to the room left; the overflow flag misc[2] raised when clipped), and the
-// prefixes of the active-block groups leaf[0..2] (B = 4, 8, 16) and occ (recipes with a mask).  One
-// thread: a batch holds a few hundred to a few thousand recipes.
+// prefixes of the active-block groups leaf[0..5] (B = 4, 8, 16; then the same for recipes with
+// sampled-grid leaves) and occ (recipes with a mask).  One thread: a batch holds a few hundred to a
+// few thousand recipes.
+constexpr int kLeafGroups = 6;
+struct LeafGroups {
+    Group g[kLeafGroups];
+    int64_t* pre[kLeafGroups];
+};
+
 __global__ void k_batch_offsets(const RecDesc* __restrict__ D, int n, int64_t capacity,
-                                int64_t* __restrict__ tile_off, int32_t* __restrict__ leaf_count,
-                                Group l4, int64_t* __restrict__ l4_pre,
-                                Group l8, int64_t* __restrict__ l8_pre, Group l16, int64_t* __restrict__ l16_pre,
+                                int64_t* __restrict__ tile_off, int32_t* __restrict__ leaf_count, LeafGroups L,
                                 Group occ, int64_t* __restrict__ occ_pre, int* __restrict__ misc) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     int64_t at = 0;
@@ -1846,15 +1785,13 @@ __global__ void k_batch_offsets(const RecDesc* __restrict__ D, int n, int64_t ca
         at += take * b3;
     }
     int64_t t = 0;
-    const Group* L[3] = {&l4, &l8, &l16};
-    int64_t* P[3] = {l4_pre, l8_pre, l16_pre};
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < kLeafGroups; ++q) {
         t = 0;
-        for (int j = 0; j < L[q]->m; ++j) {
-            P[q][j] = t;
-            t += leaf_count[L[q]->rec[j]];
+        for (int j = 0; j < L.g[q].m; ++j) {
+            L.pre[q][j] = t;
+            t += leaf_count[L.g[q].rec[j]];
         }
-        P[q][L[q]->m] = t;
+        L.pre[q][L.g[q].m] = t;
     }
     t = 0;
     for (int j = 0; j < occ.m; ++j) {
@@ -1896,7 +1833,7 @@ __global__ void __launch_bounds__(256) k_b_occupancy(const RecDesc* __restrict__
     occupancy_item<B>(R.kind, R.slot, tiles + tile_off[r], G.nx, G.ny, G.nz, G.nby, G.nbz, R.mask, g - W.pre[j]);
 }
 
-template <int B>
+template <int B, bool kEdge>
 __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __restrict__ D, Group W,
                                                                float* __restrict__ tiles,
                                                                const int64_t* __restrict__ tile_off,
@@ -1911,7 +1848,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __
         const int r = W.rec[j];
         const RecDesc& R = D[r];
         const int64_t a = g - W.pre[j];
-        leaf_block<B>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.active[a],
+        leaf_block<B, kEdge>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.active[a],
                       tiles + tile_off[r] + a * (B * B * B), work, R.kind, R.blk_off, R.blk_len, R.blk_pool,
                       R.blk_cap, s_prim[warp], s_list[warp]);
     }
@@ -1926,12 +1863,11 @@ struct BatchHost {
     int64_t dev_bytes = 0;
     RecDesc* d_desc = nullptr;
     // static groups and their totals
-    Group prims{}, chain{}, coarse{}, super_{}, wblocks{}, wclass{}, cclass{}, lat[3]{}, tiles{};  // lat: unused
-    int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_wblocks = 0, n_wclass = 0, n_cclass = 0,
-            n_lat[3] = {0, 0, 0}, n_tiles = 0;
+    Group prims{}, chain{}, coarse{}, super_{}, cclass{}, tiles{};
+    int64_t n_prims = 0, n_chain = 0, n_coarse = 0, n_super = 0, n_cclass = 0, n_tiles = 0;
     // dynamic groups (prefixes written by k_batch_offsets)
-    Group leaf[3]{}, occ{};
-    int64_t* leaf_pre[3] = {nullptr, nullptr, nullptr};
+    Group leaf[kLeafGroups]{}, occ{};
+    int64_t* leaf_pre[kLeafGroups] = {};
     int64_t* occ_pre = nullptr;
     // occupancy groups (recipes carrying a mask): their blocks, and their rows of 16 z voxels per B
     Group occ_blocks{}, occ_rows[3]{};
@@ -1992,8 +1928,6 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             d.pool_super = P.pool_super;
             d.cap_coarse = P.cap_coarse;
             d.cap_super = P.cap_super;
-            d.cap_block = P.cap_block;
-            d.warp_blocks = P.warp_blocks ? 1 : 0;
             d.kind = it.d_kind;
             d.cma = it.d_cma;
             d.active = it.d_active;
@@ -2020,8 +1954,8 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
                 pre.push_back(pre.back() + items);
             }
         };
-        HostGroup g_prims, g_chain, g_coarse, g_super, g_wblocks, g_wclass, g_cclass, g_lat[3], g_tiles, g_leaf[3],
-            g_occ, g_occ_blocks, g_occ_rows[3];
+        HostGroup g_prims, g_chain, g_coarse, g_super, g_cclass, g_tiles, g_leaf[kLeafGroups], g_occ, g_occ_blocks,
+            g_occ_rows[3];
         for (int r = 0; r < n; ++r) {
             const RecDesc& d = H->desc[r];
             const Geo& G = d.G;
@@ -2031,14 +1965,9 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             g_super.add(r, G.nsuper);
             // classification threads rounded up to whole warps: a warp never spans two recipes
             const int64_t cls_threads = (G.nsuper * threads_per_super(G.S) + 31) / 32 * 32;
-            if (d.warp_blocks) {
-                g_wblocks.add(r, G.nblocks);
-                g_wclass.add(r, cls_threads);
-            } else {
-                g_cclass.add(r, cls_threads);
-            }
+            g_cclass.add(r, cls_threads);
             g_tiles.add(r, d.ntiles);
-            g_leaf[b_index(G.B)].add(r, 0);
+            g_leaf[b_index(G.B) + (G.grid_leaves ? 3 : 0)].add(r, 0);
             if (d.mask) {
                 g_occ.add(r, 0);
                 g_occ_blocks.add(r, G.nblocks);
@@ -2062,10 +1991,12 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             q.pre = place((int64_t)hg.pre.size() * 8);
             return q;
         };
-        HostGroup* statics[] = {&g_prims, &g_chain, &g_coarse, &g_super, &g_wblocks, &g_wclass,
-                                &g_lat[0], &g_lat[1], &g_lat[2], &g_tiles, &g_leaf[0], &g_leaf[1], &g_leaf[2],
-                                &g_occ, &g_occ_blocks, &g_occ_rows[0], &g_occ_rows[1], &g_occ_rows[2], &g_cclass};
-        constexpr int kGroups = 19;
+        // group slots: 0-3 prims, chain, coarse, super; 4 classification; 5 tiles; 6-11 leaves (B = 4,
+        // 8, 16, then with sampled-grid leaves); 12 occupancy recipes; 13 their blocks; 14-16 their rows
+        HostGroup* statics[] = {&g_prims, &g_chain, &g_coarse, &g_super, &g_cclass, &g_tiles, &g_leaf[0], &g_leaf[1],
+                                &g_leaf[2], &g_leaf[3], &g_leaf[4], &g_leaf[5], &g_occ, &g_occ_blocks,
+                                &g_occ_rows[0], &g_occ_rows[1], &g_occ_rows[2]};
+        constexpr int kGroups = 17;
         Placed placed[kGroups];
         for (int q = 0; q < kGroups; ++q) placed[q] = place_group(*statics[q]);
         const int64_t o_state = at;
@@ -2092,9 +2023,9 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
         // host image of the static part, copied in one transfer
         std::vector<char> image(o_state, 0);
         std::memcpy(image.data() + o_desc, H->desc.data(), (size_t)n * sizeof(RecDesc));
-        Group* dst[] = {&H->prims, &H->chain, &H->coarse, &H->super_, &H->wblocks, &H->wclass,
-                        &H->lat[0], &H->lat[1], &H->lat[2], &H->tiles, &H->leaf[0], &H->leaf[1], &H->leaf[2],
-                        &H->occ, &H->occ_blocks, &H->occ_rows[0], &H->occ_rows[1], &H->occ_rows[2], &H->cclass};
+        Group* dst[] = {&H->prims, &H->chain, &H->coarse, &H->super_, &H->cclass, &H->tiles, &H->leaf[0], &H->leaf[1],
+                        &H->leaf[2], &H->leaf[3], &H->leaf[4], &H->leaf[5], &H->occ, &H->occ_blocks,
+                        &H->occ_rows[0], &H->occ_rows[1], &H->occ_rows[2]};
         for (int q = 0; q < kGroups; ++q) {
             const HostGroup& hg = *statics[q];
             std::memcpy(image.data() + placed[q].rec, hg.rec.data(), hg.rec.size() * 4);
@@ -2103,18 +2034,15 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             dst[q]->pre = reinterpret_cast<const int64_t*>(D + placed[q].pre);
             dst[q]->m = (int32_t)hg.rec.size();
         }
-        for (int q = 0; q < 3; ++q) H->leaf_pre[q] = reinterpret_cast<int64_t*>(D + placed[10 + q].pre);
-        H->occ_pre = reinterpret_cast<int64_t*>(D + placed[13].pre);
+        for (int q = 0; q < kLeafGroups; ++q) H->leaf_pre[q] = reinterpret_cast<int64_t*>(D + placed[6 + q].pre);
+        H->occ_pre = reinterpret_cast<int64_t*>(D + placed[12].pre);
         H->n_occ_blocks = g_occ_blocks.pre.back();
         for (int q = 0; q < 3; ++q) H->n_occ_rows[q] = g_occ_rows[q].pre.back();
         H->n_prims = g_prims.pre.back();
         H->n_chain = g_chain.pre.back();
         H->n_coarse = g_coarse.pre.back();
         H->n_super = g_super.pre.back();
-        H->n_wblocks = g_wblocks.pre.back();
-        H->n_wclass = g_wclass.pre.back();
         H->n_cclass = g_cclass.pre.back();
-        for (int q = 0; q < 3; ++q) H->n_lat[q] = g_lat[q].pre.back();
         H->n_tiles = g_tiles.pre.back();
         if (cudaMemcpyAsync(D, image.data(), o_state, cudaMemcpyHostToDevice, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
@@ -2173,30 +2101,33 @@ int fb_batch_build_timed_device(void* batch, float* d_tiles, int64_t capacity, i
     k_b_cull<1><<<fb_div_up(H->n_super * 32, 128), 128, 0, st>>>(D, H->super_, H->n_super);
     FB_LAUNCH();
     if (int rc = mark(1)) return rc;
-    if (H->n_wblocks) {
-        k_b_cull_blocks<<<fb_div_up(H->n_wblocks * 32, 128), 128, 0, st>>>(D, H->wblocks, H->n_wblocks);
-        FB_LAUNCH();
-        k_b_classify_blocks<false><<<fb_div_up(H->n_wclass, 128), 128, 0, st>>>(D, H->wclass, H->n_wclass, H->cursors);
-        FB_LAUNCH();
-    }
     if (H->n_cclass) {
-        k_b_classify_blocks<true><<<fb_div_up(H->n_cclass, 128), 128, 0, st>>>(D, H->cclass, H->n_cclass, H->cursors);
+        k_b_classify_blocks<<<fb_div_up(H->n_cclass, 128), 128, 0, st>>>(D, H->cclass, H->n_cclass, H->cursors);
         FB_LAUNCH();
     }
     if (int rc = mark(2)) return rc;
     k_b_compact<<<(unsigned)H->n_tiles, 256, 0, st>>>(D, H->tiles, H->misc, kLookbackSpins);
     FB_LAUNCH();
-    k_batch_offsets<<<1, 32, 0, st>>>(D, H->n, capacity, H->tile_off, H->leaf_count, H->leaf[0],
-                                      H->leaf_pre[0], H->leaf[1], H->leaf_pre[1], H->leaf[2], H->leaf_pre[2], H->occ,
-                                      H->occ_pre, H->misc);
+    LeafGroups LG;
+    for (int q = 0; q < kLeafGroups; ++q) {
+        LG.g[q] = H->leaf[q];
+        LG.pre[q] = H->leaf_pre[q];
+    }
+    k_batch_offsets<<<1, 32, 0, st>>>(D, H->n, capacity, H->tile_off, H->leaf_count, LG, H->occ, H->occ_pre, H->misc);
     FB_LAUNCH();
     if (int rc = mark(3)) return rc;
     if (int rc = mark(4)) return rc;
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < kLeafGroups; ++q) {
         if (!H->leaf[q].m) continue;
-        if (q == 0) k_b_leaf<4><<<dyn, 32 * kLeafWarps, 0, st>>>(D, H->leaf[0], d_tiles, H->tile_off, work);
-        else if (q == 1) k_b_leaf<8><<<dyn, 32 * kLeafWarps, 0, st>>>(D, H->leaf[1], d_tiles, H->tile_off, work);
-        else k_b_leaf<16><<<dyn, 32 * kLeafWarps, 0, st>>>(D, H->leaf[2], d_tiles, H->tile_off, work);
+        const Group& W = H->leaf[q];
+        switch (q) {
+        case 0: k_b_leaf<4, false><<<dyn, 32 * kLeafWarps, 0, st>>>(D, W, d_tiles, H->tile_off, work); break;
+        case 1: k_b_leaf<8, false><<<dyn, 32 * kLeafWarps, 0, st>>>(D, W, d_tiles, H->tile_off, work); break;
+        case 2: k_b_leaf<16, false><<<dyn, 32 * kLeafWarps, 0, st>>>(D, W, d_tiles, H->tile_off, work); break;
+        case 3: k_b_leaf<4, true><<<dyn, 32 * kLeafWarps, 0, st>>>(D, W, d_tiles, H->tile_off, work); break;
+        case 4: k_b_leaf<8, true><<<dyn, 32 * kLeafWarps, 0, st>>>(D, W, d_tiles, H->tile_off, work); break;
+        default: k_b_leaf<16, true><<<dyn, 32 * kLeafWarps, 0, st>>>(D, W, d_tiles, H->tile_off, work);
+        }
         FB_LAUNCH();
     }
     return mark(5);
@@ -2242,9 +2173,8 @@ int32_t fb_batch_launches(void* batch) noexcept {
     BatchHost* H = static_cast<BatchHost*>(batch);
     if (!H) return -1;
     int n = 1 + 4 + 2;  // memset; prepare, full list, two cull levels; compaction, offsets
-    if (H->n_wblocks) n += 2;
     if (H->n_cclass) n += 1;
-    for (int q = 0; q < 3; ++q) n += H->leaf[q].m ? 1 : 0;
+    for (int q = 0; q < kLeafGroups; ++q) n += H->leaf[q].m ? 1 : 0;
     return n;
 }
 
@@ -2415,7 +2345,7 @@ int fb_field_accel(const FbGeom* g, int32_t n_prims, int32_t n_chain, const void
     if (blk_len) *blk_len = reinterpret_cast<const int32_t*>(b + P.blk_len);
     if (blk_pool) *blk_pool = reinterpret_cast<const uint32_t*>(b + P.blk_pool);
     if (blk_cap) *blk_cap = P.blk_cap;
-    if (blk_all) *blk_all = P.warp_blocks ? 1 : 0;  // every block has a list (else only kind == 0 blocks)
+    if (blk_all) *blk_all = 0;  // lists are kept for blocks of kind 0 only
     return FB_OK;
 }
 

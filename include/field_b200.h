@@ -34,7 +34,9 @@ typedef struct fb_geom {
     double x0, y0, z0, pitch;
     int32_t nx, ny, nz, block;
     float margin, guard;
-    int32_t reserved[2];
+    int32_t reserved[2]; /* [0] bit 0: the recipe has sampled-grid leaves (type 9), whose voxels at a
+                          * table's boundary the leaf and classification passes decide in float64;
+                          * other bits and [1]: 0 */
 } fb_geom; /* 64 bytes */
 
 /* One primitive: value = s * f(A x + t) - off, f canonical (type 0 sphere, 1 box, 2 cylinder, 3 cone,
