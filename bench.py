@@ -587,7 +587,7 @@ def run_headline(args, rank, world, local_rank):
     comps = batch_workload(args.recipes)
     t_compile = time.perf_counter() - t0
     t0 = time.perf_counter()
-    tuner = BT.Autotuner(TUNING if TUNING.exists() else None, device=dev)
+    tuner = BT.Autotuner(TUNING, device=dev)
     known = len(tuner.table)
     blocks = tuner.tune(comps)
     t_tune = time.perf_counter() - t0
