@@ -257,7 +257,9 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
 // active inside the block is the one near zero, which float32 holds to a relative 6e-8.
 //
 // A sphere takes the difference form (|L|^2 - r^2 + e.(2L + e)) / (|q| + r) when its radius exceeds
-// twice the block's extent in its frame, else the direct |q| - r.  Their float32 errors: about
+// twice the block's extent in its frame, else the direct |q| - r; a torus the same for its radial
+// distance to the ring, rho - R = (Lx^2 + Ly^2 - R^2 + ex (2 Lx + ex) + ey (2 Ly + ey)) / (rho + R),
+// when its ring radius R does.  Their float32 errors: about
 // u (|d| + 6 |e|) for the difference form (d = |L| - r, independent of r) and u (|L| + 2 |q|) ~ 3 u r for
 // the direct one (u = 2^-24): large spheres against small blocks favour the first, small spheres
 // against large blocks the second.  extent: the largest offset the block's evaluation uses.
@@ -290,10 +292,13 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     out.L[0] = (float)lx;
     out.L[1] = (float)ly;
     out.L[2] = (float)lz;
-    // sphere: |L|^2 - r^2 in float64, the constant term of the difference form of |q| - r
-    out.L[3] = F.type == P_SPHERE ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0]) : 0.f;
+    // the constant term of the difference form, in float64: sphere |L|^2 - r^2, torus (ring radius
+    // R = p[0]) Lx^2 + Ly^2 - R^2
+    out.L[3] = F.type == P_SPHERE   ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0])
+               : F.type == P_TORUS ? (float)(fma(lx, lx, ly * ly) - D.p[0] * D.p[0])
+                                   : 0.f;
     out.diff = 0;
-    if (F.type == P_SPHERE) {
+    if (F.type == P_SPHERE || F.type == P_TORUS) {
         // the extent in the sphere's frame: the Frobenius norm bounds the linear part's stretch
         const double a2 = A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
                           A[8] * A[8] + A[9] * A[9] + A[10] * A[10];
