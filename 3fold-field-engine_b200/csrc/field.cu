@@ -1019,28 +1019,20 @@ __device__ __forceinline__ void eval_group_sphere(const LocalPrim& P, float dx, 
     }
 }
 
-// Torus in difference form for its radial distance to the ring (localise): rho - R formed as
-// (Lx^2 + Ly^2 - R^2 + ex (2 Lx + ex) + ey (2 Ly + ey)) / (rho + R), the constant in float64 per block
-// (LocalPrim.L[3]), so the error no longer grows with the ring radius (~50 pitches of it put the
-// direct form above 1e-5 pitch).
+// Torus in its ring frame (localise): u = x - R and w = y of the rotated frame, rho - R =
+// u + w^2 / (rho + R + u); the quotient is a correction of a few pitches, so the fast division's two
+// ulps of it stay far below the float32 rounding of the coordinates themselves.
 template <int VG>
 __device__ __forceinline__ void eval_group_torus(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
-    const float L0 = P.L[0], L1 = P.L[1], L2 = P.L[2], K = P.L[3], R = P.p[0], r = P.p[1];
-    float ebx, eby, ebz, cx, cy, cz;  // e = eb + c * dz
-    if (P.ident) {
-        ebx = dx; eby = dy; ebz = 0.f; cx = 0.f; cy = 0.f; cz = 1.f;
-    } else {
-        ebx = fmaf(P.A[0], dx, P.A[1] * dy);
-        eby = fmaf(P.A[3], dx, P.A[4] * dy);
-        ebz = fmaf(P.A[6], dx, P.A[7] * dy);
-        cx = P.A[2]; cy = P.A[5]; cz = P.A[8];
-    }
+    const float L0 = P.L[0], L2 = P.L[2], R = P.p[0], r = P.p[1];
+    const float ebx = fmaf(P.A[0], dx, P.A[1] * dy), eby = fmaf(P.A[3], dx, P.A[4] * dy),
+                ebz = fmaf(P.A[6], dx, P.A[7] * dy);
 #pragma unroll
     for (int k = 0; k < VG; ++k) {
-        const float ex = fmaf(cx, dz[k], ebx), ey = fmaf(cy, dz[k], eby), ez = fmaf(cz, dz[k], ebz);
-        const float x = L0 + ex, y = L1 + ey, z = L2 + ez;
-        const float num = fmaf(ey, fmaf(2.f, L1, ey), fmaf(ex, fmaf(2.f, L0, ex), K));
-        const float qx = __fdiv_rn(num, sqrtf(fmaf(x, x, y * y)) + R);
+        const float u = L0 + fmaf(P.A[2], dz[k], ebx), w = fmaf(P.A[5], dz[k], eby), z = L2 + fmaf(P.A[8], dz[k], ebz);
+        const float t = R + u;  // x of the rotated frame: <= 0 only past the axis (a block across it)
+        const float rho = sqrtf(fmaf(t, t, w * w));
+        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
         v[k] = fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - r, -P.off);
     }
 }

@@ -257,9 +257,11 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
 // active inside the block is the one near zero, which float32 holds to a relative 6e-8.
 //
 // A sphere takes the difference form (|L|^2 - r^2 + e.(2L + e)) / (|q| + r) when its radius exceeds
-// twice the block's extent in its frame, else the direct |q| - r; a torus the same for its radial
-// distance to the ring, rho - R = (Lx^2 + Ly^2 - R^2 + ex (2 Lx + ex) + ey (2 Ly + ey)) / (rho + R),
-// when its ring radius R does.  Their float32 errors: about
+// twice the block's extent in its frame, else the direct |q| - r.  A torus whose ring radius R
+// does takes the ring frame: rotated about its axis so the block origin lies on +x, x measured from
+// the ring (u = x - R, w = y), where rho - R = u + w^2 / (rho + R + u) -- u carries the rounding of a
+// short offset instead of a coordinate of size R, and the quotient is a correction of a few
+// pitches.  Their float32 errors: about
 // u (|d| + 6 |e|) for the difference form (d = |L| - r, independent of r) and u (|L| + 2 |q|) ~ 3 u r for
 // the direct one (u = 2^-24): large spheres against small blocks favour the first, small spheres
 // against large blocks the second.  extent: the largest offset the block's evaluation uses.
@@ -292,21 +294,35 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     out.L[0] = (float)lx;
     out.L[1] = (float)ly;
     out.L[2] = (float)lz;
-    // the constant term of the difference form, in float64: sphere |L|^2 - r^2, torus (ring radius
-    // R = p[0]) Lx^2 + Ly^2 - R^2
-    out.L[3] = F.type == P_SPHERE   ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0])
-               : F.type == P_TORUS ? (float)(fma(lx, lx, ly * ly) - D.p[0] * D.p[0])
-                                   : 0.f;
+    // sphere: |L|^2 - r^2 in float64, the constant term of the difference form of |q| - r
+    out.L[3] = F.type == P_SPHERE ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0]) : 0.f;
     out.diff = 0;
     if (F.type == P_SPHERE || F.type == P_TORUS) {
-        // the extent in the sphere's frame: the Frobenius norm bounds the linear part's stretch
-        const double a2 = A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
-                          A[8] * A[8] + A[9] * A[9] + A[10] * A[10];
+        // the extent in the primitive's frame: the linear part's root-mean-square stretch (the
+        // Frobenius norm over sqrt 3; exact for a rotation or permutation times a uniform scale)
+        const double a2 = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
+                           A[8] * A[8] + A[9] * A[9] + A[10] * A[10]) / 3.0;
         out.diff = D.p[0] > 2.0 * (double)extent * (F.ident ? 1.0 : sqrt(a2)) ? 1 : 0;
     }
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
     out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
+    if (F.type == P_TORUS && out.diff) {
+        // ring frame: rotate about the torus axis so the block origin lies on +x, and measure x from
+        // the ring (the torus is symmetric under the rotation); only the offsets go through the
+        // rotation, whose float32 rounding then scales them by ~1 + 2^-24 at most
+        const double n = sqrt(fma(lx, lx, ly * ly));
+        const double cs = n > 0.0 ? lx / n : 1.0, sn = n > 0.0 ? ly / n : 0.0;
+        out.L[0] = (float)(n - D.p[0]);
+        out.L[1] = 0.f;
+        out.L[3] = 0.f;
+        for (int j = 0; j < 3; ++j) {
+            const double r0 = A[j], r1 = A[4 + j];
+            out.A[j] = (float)fma(cs, r0, sn * r1);
+            out.A[3 + j] = (float)fma(-sn, r0, cs * r1);
+        }
+        out.ident = 0;
+    }
 }
 
 // ------------------------------------------------------------------------------------ float64
