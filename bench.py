@@ -721,9 +721,10 @@ def run_headline(args, rank, world, local_rank):
     gc.collect()
     torch.cuda.empty_cache()
     if rank == 0 and not args.no_serve:
-        sv = run_serve(args, rate=1000.0, seconds=2.0, arena_gb=min(getattr(args, "arena_gb", 150.0), 100.0))
-        result["serve"] = {k: sv[k] for k in ("rate_req_s", "seconds", "requests", "throughput_req_s", "p50_ms",
-                                               "p99_ms", "errors", "worst_ms_per_half_second", "by_kind", "slots")}
+        sv = run_serve(args, rate=1000.0, seconds=3.0, arena_gb=min(getattr(args, "arena_gb", 150.0), 100.0))
+        result["serve"] = {k: sv[k] for k in ("rate_req_s", "seconds", "warmup", "requests", "throughput_req_s",
+                                               "p50_ms", "p99_ms", "errors", "worst_ms_per_half_second", "by_kind",
+                                               "slots")}
     return result
 
 
@@ -806,8 +807,10 @@ def e2e_batched(bb, steps):
                    "host buffers for the tiles, kinds and active ids"}
 
 
-def run_serve(args, rate=1000.0, seconds=10.0, seed=7, arena_gb=None):
-    """Poisson arrivals at `rate` req/s for `seconds`: 40 % builds (recipes as the batched
+def run_serve(args, rate=1000.0, seconds=10.0, seed=7, arena_gb=None, warmup_s=0.5):
+    """Poisson arrivals at `rate` req/s for `warmup_s` + `seconds`, the statistics over the requests
+    arriving after the first `warmup_s` (the same mix, run first so that the window measures the
+    steady state): 40 % builds (recipes as the batched
     workload), 30 % edits (1-64 tool capsules subtracted from a resident field), 20 % point queries
     (1e5-1e6 points, value + gradient), 10 % EDT recomputations; latency = completion - arrival.
     Request payloads (recipes, tool lists, point sets) are generated before the arrival window, as
@@ -820,7 +823,7 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7, arena_gb=None):
     torch.cuda.set_device(0)
     rng = np.random.default_rng(seed)
     pool = [(X.compile_recipe(r), n) for r, n, _ in R.batch_recipes(count=64, seed=11)]
-    n_req = int(rate * seconds)
+    n_req = int(rate * (seconds + warmup_s))
     gaps = rng.exponential(1.0 / rate, size=n_req)
     kinds = rng.choice(["build", "edit", "query", "edt"], size=n_req, p=[0.4, 0.3, 0.2, 0.1])
     # the client keeps its point sets in pinned host memory, which the server takes without a copy
@@ -908,20 +911,24 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7, arena_gb=None):
         gc.enable()
         gc.unfreeze()
         alloc1 = torch.cuda.memory_stats()
-        lat = np.array([(e - a) * 1e3 for _, a, _, e in srv.completed])
+        warm_n = sum(1 for _, a, _, _ in srv.completed if a < t0 + warmup_s)
+        done = [c for c in srv.completed if c[1] >= t0 + warmup_s]
+        t0 += warmup_s
+        lat = np.array([(e - a) * 1e3 for _, a, _, e in done])
         # worst latency of the requests arriving in each half second: a stall shows as one window
         windows = {}
-        for _, a, _, e in srv.completed:
+        for _, a, _, e in done:
             k = int((a - t0) / 0.5)
             windows[k] = max(windows.get(k, 0.0), (e - a) * 1e3)
         by_kind = {}
-        for kind, a, st, e in srv.completed:
+        for kind, a, st, e in done:
             by_kind.setdefault(kind, []).append(((e - a) * 1e3, (st - a) * 1e3))
     finally:
         srv.close()
     return {
-        "metric": METRIC, "workload": "serve_poisson", "rate_req_s": rate, "seconds": seconds, "requests": n_req,
-        "errors": errors, "offered_req_s": n_req / (t_submitted - t0),
+        "metric": METRIC, "workload": "serve_poisson", "rate_req_s": rate, "seconds": seconds,
+        "requests": len(done), "warmup": {"seconds": warmup_s, "requests": warm_n},
+        "errors": errors, "offered_req_s": n_req / (t_submitted - t0 + warmup_s),
         "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": float(np.percentile(lat, 50)),
         "p99_ms": float(np.percentile(lat, 99)),
         "by_kind": {k: {"n": len(v), "p50_ms": float(np.percentile([x for x, _ in v], 50)),
@@ -930,7 +937,7 @@ def run_serve(args, rate=1000.0, seconds=10.0, seed=7, arena_gb=None):
                     for k, v in by_kind.items()},
         "slowest": [{"kind": k, "arrival_s": round(a - t0, 3), "queue_ms": round((st - a) * 1e3, 1),
                      "service_ms": round((e - st) * 1e3, 1)}
-                    for k, a, st, e in sorted(srv.completed, key=lambda c: c[1] - c[3])[:5]],
+                    for k, a, st, e in sorted(done, key=lambda c: c[1] - c[3])[:5]],
         "worst_ms_per_half_second": [round(windows.get(k, 0.0), 1) for k in range(max(windows) + 1)] if windows else [],
         "allocator": {k: int(alloc1.get(k, 0) - alloc0.get(k, 0)) for k in ("num_device_alloc", "num_device_free",
                                                                            "num_alloc_retries")},
