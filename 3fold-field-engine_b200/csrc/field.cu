@@ -788,7 +788,8 @@ __device__ void classify_block(const Geo& G, const FbPrim* __restrict__ prims, c
                 continue;
             }
             LocalPrim P;
-            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P, side);
+            // canonical forms (no extent): the corner decisions have the float64 guard band
+            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, k, P);
             // the corners as 4 (x, y) columns of 2 along z: one inlined evaluation body (the kind
             // switch outside, the points inside) walked over the columns, the corner values rotated
             // through registers -- 8 unrolled kind switches would not fit the instruction cache

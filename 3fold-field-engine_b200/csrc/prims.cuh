@@ -261,7 +261,7 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
 // does takes the ring frame: rotated about its axis so the block origin lies on +x, x measured from
 // the ring (u = x - R, w = y), where rho - R = u + w^2 / (rho + R + u) -- u carries the rounding of a
 // short offset instead of a coordinate of size R, and the quotient is a correction of a few
-// pitches.  Their float32 errors: about
+// pitches.  extent 0 (callers that evaluate through local_eval) keeps the canonical forms.  Their float32 errors: about
 // u (|d| + 6 |e|) for the difference form (d = |L| - r, independent of r) and u (|L| + 2 |q|) ~ 3 u r for
 // the direct one (u = 2^-24): large spheres against small blocks favour the first, small spheres
 // against large blocks the second.  extent: the largest offset the block's evaluation uses.
@@ -302,7 +302,8 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
         // Frobenius norm over sqrt 3; exact for a rotation or permutation times a uniform scale)
         const double a2 = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
                            A[8] * A[8] + A[9] * A[9] + A[10] * A[10]) / 3.0;
-        out.diff = D.p[0] > 2.0 * (double)extent * (F.ident ? 1.0 : sqrt(a2)) ? 1 : 0;
+        // extent 0: the caller evaluates through local_eval (canonical forms only)
+        out.diff = extent > 0.f && D.p[0] > 2.0 * (double)extent * (F.ident ? 1.0 : sqrt(a2)) ? 1 : 0;
     }
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
@@ -311,8 +312,10 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
         // ring frame: rotate about the torus axis so the block origin lies on +x, and measure x from
         // the ring (the torus is symmetric under the rotation); only the offsets go through the
         // rotation, whose float32 rounding then scales them by ~1 + 2^-24 at most
-        const double n = sqrt(fma(lx, lx, ly * ly));
-        const double cs = n > 0.0 ? lx / n : 1.0, sn = n > 0.0 ? ly / n : 0.0;
+        const double n2 = fma(lx, lx, ly * ly);
+        const double inv = n2 > 0.0 ? rsqrt(n2) : 0.0;  // any rotation serves: only n must be accurate
+        const double n = n2 * inv;
+        const double cs = n2 > 0.0 ? lx * inv : 1.0, sn = n2 > 0.0 ? ly * inv : 0.0;
         out.L[0] = (float)(n - D.p[0]);
         out.L[1] = 0.f;
         out.L[3] = 0.f;
