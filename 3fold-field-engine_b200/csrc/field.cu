@@ -1028,6 +1028,18 @@ __device__ __forceinline__ void eval_group_torus(const LocalPrim& P, float dx, f
     const float L0 = P.L[0], L2 = P.L[2], R = P.p[0], r = P.p[1];
     const float ebx = fmaf(P.A[0], dx, P.A[1] * dy), eby = fmaf(P.A[3], dx, P.A[4] * dy),
                 ebz = fmaf(P.A[6], dx, P.A[7] * dy);
+    if (P.ident == 2) {  // axis along the grid's z: the ring distance is the column's, once
+        const float u = L0 + ebx, w = eby, t = R + u;
+        const float rho = sqrtf(fmaf(t, t, w * w));
+        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
+        const float q2 = qx * qx;
+#pragma unroll
+        for (int k = 0; k < VG; ++k) {
+            const float z = L2 + fmaf(P.A[8], dz[k], ebz);
+            v[k] = fmaf(P.s, sqrtf(fmaf(z, z, q2)) - r, -P.off);
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < VG; ++k) {
         const float u = L0 + fmaf(P.A[2], dz[k], ebx), w = fmaf(P.A[5], dz[k], eby), z = L2 + fmaf(P.A[8], dz[k], ebz);

@@ -324,7 +324,8 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
             out.A[j] = (float)fma(cs, r0, sn * r1);
             out.A[3 + j] = (float)fma(-sn, r0, cs * r1);
         }
-        out.ident = 0;
+        // 2: the torus axis along the grid's z, so a voxel column's u and w do not change along it
+        out.ident = (A[2] == 0.0 && A[6] == 0.0) ? 2 : 0;
     }
 }
 
