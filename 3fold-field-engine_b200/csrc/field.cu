@@ -1022,32 +1022,28 @@ __device__ __forceinline__ void eval_group_sphere(const LocalPrim& P, float dx, 
 
 // Torus in its ring frame (localise): u = x - R and w = y of the rotated frame, rho - R =
 // u + w^2 / (rho + R + u); the quotient is a correction of a few pitches, so the fast division's two
-// ulps of it stay far below the float32 rounding of the coordinates themselves.
+// ulps of it stay far below the float32 rounding of the coordinates themselves.  Out of line: the
+// leaf kernel's inlined body must stay small (inlined, this path cost the leaf pass 20 %).
 template <int VG>
-__device__ __forceinline__ void eval_group_torus(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
+struct Vals {
+    float v[VG];
+};
+
+template <int VG>
+__device__ __noinline__ Vals<VG> eval_group_torus(const LocalPrim& P, float dx, float dy, const float* dz) {
+    Vals<VG> out;
     const float L0 = P.L[0], L2 = P.L[2], R = P.p[0], r = P.p[1];
     const float ebx = fmaf(P.A[0], dx, P.A[1] * dy), eby = fmaf(P.A[3], dx, P.A[4] * dy),
                 ebz = fmaf(P.A[6], dx, P.A[7] * dy);
-    if (P.ident == 2) {  // axis along the grid's z: the ring distance is the column's, once
-        const float u = L0 + ebx, w = eby, t = R + u;
-        const float rho = sqrtf(fmaf(t, t, w * w));
-        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
-        const float q2 = qx * qx;
-#pragma unroll
-        for (int k = 0; k < VG; ++k) {
-            const float z = L2 + fmaf(P.A[8], dz[k], ebz);
-            v[k] = fmaf(P.s, sqrtf(fmaf(z, z, q2)) - r, -P.off);
-        }
-        return;
-    }
 #pragma unroll
     for (int k = 0; k < VG; ++k) {
         const float u = L0 + fmaf(P.A[2], dz[k], ebx), w = fmaf(P.A[5], dz[k], eby), z = L2 + fmaf(P.A[8], dz[k], ebz);
         const float t = R + u;  // x of the rotated frame: <= 0 only past the axis (a block across it)
         const float rho = sqrtf(fmaf(t, t, w * w));
         const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
-        v[k] = fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - r, -P.off);
+        out.v[k] = fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - r, -P.off);
     }
+    return out;
 }
 
 // VG voxels along z of one lane: values of primitive P at block offsets (dx, dy, dz0 + k*pz).
@@ -1058,7 +1054,9 @@ __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float
         return;
     }
     if (T == P_TORUS && P.diff) {
-        eval_group_torus<VG>(P, dx, dy, dz, v);
+        const Vals<VG> r = eval_group_torus<VG>(P, dx, dy, dz);
+#pragma unroll
+        for (int k = 0; k < VG; ++k) v[k] = r.v[k];
         return;
     }
     const float* p = P.p;

@@ -302,8 +302,11 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
         // Frobenius norm over sqrt 3; exact for a rotation or permutation times a uniform scale)
         const double a2 = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
                            A[8] * A[8] + A[9] * A[9] + A[10] * A[10]) / 3.0;
-        // extent 0: the caller evaluates through local_eval (canonical forms only)
-        out.diff = extent > 0.f && D.p[0] > 2.0 * (double)extent * (F.ident ? 1.0 : sqrt(a2)) ? 1 : 0;
+        // extent 0: the caller evaluates through local_eval (canonical forms only).  A torus's direct
+        // form is within 1e-5 pitch below four extents of ring radius (its tube's norm then bounds the
+        // error of either form), and its ring frame runs out of line
+        const double k = F.type == P_TORUS ? 4.0 : 2.0;
+        out.diff = extent > 0.f && D.p[0] > k * (double)extent * (F.ident ? 1.0 : sqrt(a2)) ? 1 : 0;
     }
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
@@ -324,8 +327,7 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
             out.A[j] = (float)fma(cs, r0, sn * r1);
             out.A[3 + j] = (float)fma(-sn, r0, cs * r1);
         }
-        // 2: the torus axis along the grid's z, so a voxel column's u and w do not change along it
-        out.ident = (A[2] == 0.0 && A[6] == 0.0) ? 2 : 0;
+        out.ident = 0;
     }
 }
 
