@@ -1020,43 +1020,11 @@ __device__ __forceinline__ void eval_group_sphere(const LocalPrim& P, float dx, 
     }
 }
 
-// Torus in its ring frame (localise): u = x - R and w = y of the rotated frame, rho - R =
-// u + w^2 / (rho + R + u); the quotient is a correction of a few pitches, so the fast division's two
-// ulps of it stay far below the float32 rounding of the coordinates themselves.  Out of line: the
-// leaf kernel's inlined body must stay small (inlined, this path cost the leaf pass 20 %).
-template <int VG>
-struct Vals {
-    float v[VG];
-};
-
-template <int VG>
-__device__ __noinline__ Vals<VG> eval_group_torus(const LocalPrim& P, float dx, float dy, const float* dz) {
-    Vals<VG> out;
-    const float L0 = P.L[0], L2 = P.L[2], R = P.p[0], r = P.p[1];
-    const float ebx = fmaf(P.A[0], dx, P.A[1] * dy), eby = fmaf(P.A[3], dx, P.A[4] * dy),
-                ebz = fmaf(P.A[6], dx, P.A[7] * dy);
-#pragma unroll
-    for (int k = 0; k < VG; ++k) {
-        const float u = L0 + fmaf(P.A[2], dz[k], ebx), w = fmaf(P.A[5], dz[k], eby), z = L2 + fmaf(P.A[8], dz[k], ebz);
-        const float t = R + u;  // x of the rotated frame: <= 0 only past the axis (a block across it)
-        const float rho = sqrtf(fmaf(t, t, w * w));
-        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
-        out.v[k] = fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - r, -P.off);
-    }
-    return out;
-}
-
 // VG voxels along z of one lane: values of primitive P at block offsets (dx, dy, dz0 + k*pz).
 template <int VG, int T>
 __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
     if (T == P_SPHERE && P.diff) {
         eval_group_sphere<VG>(P, dx, dy, dz, v);
-        return;
-    }
-    if (T == P_TORUS && P.diff) {
-        const Vals<VG> r = eval_group_torus<VG>(P, dx, dy, dz);
-#pragma unroll
-        for (int k = 0; k < VG; ++k) v[k] = r.v[k];
         return;
     }
     const float* p = P.p;
@@ -1075,12 +1043,25 @@ __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float
     }
 }
 
-// The five kinds the milling recipes rarely use, out of line and one voxel per call (scalar
-// arguments stay in registers): the hot loop keeps only the four common kinds inlined, small enough
-// to stay in the instruction cache.  A sampled grid's voxel next to its table's boundary
+// The kinds the milling recipes rarely use, and a torus in its ring frame, out of line and one voxel
+// per call (scalar arguments stay in registers): the hot loop keeps only the four common kinds'
+// plain forms inlined and one call site, small enough to stay in the instruction cache (a second
+// inlined or called torus path cost the leaf pass 20 % even where it never ran).  A sampled grid's voxel next to its table's boundary
 // (grid_edge_f) returns NaN: the caller marks it for the float64 recheck -- one call site, so the
 // hot loop keeps a single call on its rare path.
 __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float dy, float dz) {
+    if (P.type == P_TORUS) {
+        // a torus in its ring frame (localise): u = x - R and w = y of the rotated frame,
+        // rho - R = u + w^2 / (rho + R + u); the quotient is a correction of a few pitches, so the
+        // fast division's two ulps of it stay far below the float32 rounding of the coordinates
+        const float u = P.L[0] + fmaf(P.A[2], dz, fmaf(P.A[0], dx, P.A[1] * dy));
+        const float w = fmaf(P.A[5], dz, fmaf(P.A[3], dx, P.A[4] * dy));
+        const float z = P.L[2] + fmaf(P.A[8], dz, fmaf(P.A[6], dx, P.A[7] * dy));
+        const float t = P.p[0] + u;  // x of the rotated frame: <= 0 only past the axis
+        const float rho = sqrtf(fmaf(t, t, w * w));
+        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - P.p[0];
+        return fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - P.p[1], -P.off);
+    }
     float x, y, z;
     if (P.ident) {
         x = P.L[0] + dx; y = P.L[1] + dy; z = P.L[2] + dz;
@@ -1103,7 +1084,12 @@ __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, flo
     case P_SPHERE: eval_group_t<VG, P_SPHERE>(P, dx, dy, dz, v); break;
     case P_BOX: eval_group_t<VG, P_BOX>(P, dx, dy, dz, v); break;
     case P_CAPSULE: eval_group_t<VG, P_CAPSULE>(P, dx, dy, dz, v); break;
-    case P_TORUS: eval_group_t<VG, P_TORUS>(P, dx, dy, dz, v); break;
+    case P_TORUS:
+        if (!P.diff) {
+            eval_group_t<VG, P_TORUS>(P, dx, dy, dz, v);
+            break;
+        }
+        [[fallthrough]];
     default:
 #pragma unroll
         for (int k = 0; k < VG; ++k) {
