@@ -35,6 +35,17 @@ class FbGeom(ct.Structure):
                 ("margin", ct.c_float), ("guard", ct.c_float), ("reserved", ct.c_int32 * 2)]
 
 
+def _large_tori(c: Compiled, meta: GridMeta) -> bool:
+    """A torus whose ring radius exceeds four leaf extents (block * pitch) in its own frame, the
+    frame's stretch taken as the root-mean-square of its linear part (localise's rule)."""
+    tori = c.prims[c.prims["type"] == X.P_TORUS]
+    if not len(tori):
+        return False
+    a = tori["A"].reshape(-1, 3, 4)[:, :, :3]
+    scale = np.sqrt((a * a).sum(axis=(1, 2)) / 3.0)
+    return bool(np.any(tori["p"][:, 0] > 4.0 * meta.block * meta.pitch * scale))
+
+
 def geom_of(meta: GridMeta, guard=None) -> FbGeom:
     if meta.block not in (4, 8, 16):
         raise ValueError("block must be 4, 8 or 16")
@@ -183,8 +194,10 @@ class FieldBuilder:
             guard = max(meta.guard(), c.sampling_guard())
         self.geom = geom_of(meta, guard)
         # fb_geom.reserved[0] bit 0: sampled-grid leaves present (the kernels then mark the voxels at
-        # a table's boundary for the float64 recheck)
-        self.geom.reserved[0] = int(bool(np.any(c.prims["type"] == X.P_GRID)))
+        # a table's boundary for the float64 recheck); bit 1: a torus whose ring radius exceeds four
+        # leaf extents in its frame (the leaf evaluates it in its ring frame, float32 within 1e-5
+        # pitch there)
+        self.geom.reserved[0] = int(bool(np.any(c.prims["type"] == X.P_GRID))) | (2 * int(_large_tori(c, meta)))
         if tables is not None:
             # the caller placed the tables on the device (e.g. a batch's table arena); still checked
             _validate_program(c.prims, insns, self.mode, len(c.tables))

@@ -78,7 +78,7 @@ struct Geo {
     int ncx, ncy, ncz;
     int64_t ncoarse;
     float margin, guard, eps;
-    int grid_leaves;  // the recipe has sampled-grid leaves (fb_geom.reserved[0] bit 0)
+    int special;  // fb_geom.reserved[0] bits 0-1: sampled-grid leaves, or tori of a large ring radius
 };
 
 Geo make_geo(const FbGeom& g) {
@@ -102,7 +102,7 @@ Geo make_geo(const FbGeom& g) {
     o.margin = g.margin;
     o.guard = g.guard;
     o.eps = 4.0f * g.guard;
-    o.grid_leaves = g.reserved[0] & 1;
+    o.special = (g.reserved[0] & 3) != 0;
     return o;
 }
 
@@ -1043,25 +1043,12 @@ __device__ __forceinline__ void eval_group_t(const LocalPrim& P, float dx, float
     }
 }
 
-// The kinds the milling recipes rarely use, and a torus in its ring frame, out of line and one voxel
-// per call (scalar arguments stay in registers): the hot loop keeps only the four common kinds'
-// plain forms inlined and one call site, small enough to stay in the instruction cache (a second
-// inlined or called torus path cost the leaf pass 20 % even where it never ran).  A sampled grid's voxel next to its table's boundary
+// The kinds the milling recipes rarely use, out of line and one voxel per call (scalar arguments
+// stay in registers): the hot loop keeps only the four common kinds inlined, small enough to stay in
+// the instruction cache.  A sampled grid's voxel next to its table's boundary
 // (grid_edge_f) returns NaN: the caller marks it for the float64 recheck -- one call site, so the
 // hot loop keeps a single call on its rare path.
 __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float dy, float dz) {
-    if (P.type == P_TORUS) {
-        // a torus in its ring frame (localise): u = x - R and w = y of the rotated frame,
-        // rho - R = u + w^2 / (rho + R + u); the quotient is a correction of a few pitches, so the
-        // fast division's two ulps of it stay far below the float32 rounding of the coordinates
-        const float u = P.L[0] + fmaf(P.A[2], dz, fmaf(P.A[0], dx, P.A[1] * dy));
-        const float w = fmaf(P.A[5], dz, fmaf(P.A[3], dx, P.A[4] * dy));
-        const float z = P.L[2] + fmaf(P.A[8], dz, fmaf(P.A[6], dx, P.A[7] * dy));
-        const float t = P.p[0] + u;  // x of the rotated frame: <= 0 only past the axis
-        const float rho = sqrtf(fmaf(t, t, w * w));
-        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - P.p[0];
-        return fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - P.p[1], -P.off);
-    }
     float x, y, z;
     if (P.ident) {
         x = P.L[0] + dx; y = P.L[1] + dy; z = P.L[2] + dz;
@@ -1074,9 +1061,37 @@ __device__ __noinline__ float eval_one_rare(const LocalPrim& P, float dx, float 
     return fmaf(P.s, canon_f(P.type, P.p, x, y, z), -P.off);
 }
 
+// A torus in its ring frame (localise): u = x - R and w = y of the rotated frame, rho - R =
+// u + w^2 / (rho + R + u); the quotient is a correction of a few pitches, so the fast division's two
+// ulps of it stay far below the float32 rounding of the coordinates themselves.  Out of line, and
+// only in the leaf kernels built for recipes with such tori: in the common kernel's loop the extra
+// path cost the leaf pass 10-20 % even where it never ran.
+template <int VG>
+struct Vals {
+    float v[VG];
+};
+
+template <int VG>
+__device__ __noinline__ Vals<VG> eval_group_torus_ring(const LocalPrim& P, float dx, float dy, const float* dz) {
+    Vals<VG> out;
+    const float L0 = P.L[0], L2 = P.L[2], R = P.p[0], r = P.p[1];
+    const float ebx = fmaf(P.A[0], dx, P.A[1] * dy), eby = fmaf(P.A[3], dx, P.A[4] * dy),
+                ebz = fmaf(P.A[6], dx, P.A[7] * dy);
+#pragma unroll
+    for (int k = 0; k < VG; ++k) {
+        const float u = L0 + fmaf(P.A[2], dz[k], ebx), w = fmaf(P.A[5], dz[k], eby), z = L2 + fmaf(P.A[8], dz[k], ebz);
+        const float t = R + u;  // x of the rotated frame: <= 0 only past the axis (a block across it)
+        const float rho = sqrtf(fmaf(t, t, w * w));
+        const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
+        out.v[k] = fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - r, -P.off);
+    }
+    return out;
+}
+
 // Returns bit k set where voxel k sampled a grid table next to its boundary (eval_one_rare's NaN):
-// its value and the decisions on it are then taken in float64.  kEdge = false: recipes without
-// sampled-grid leaves, the marks left out.
+// its value and the decisions on it are then taken in float64.  kEdge = false: recipes with neither
+// sampled-grid leaves nor ring-frame tori (fb_geom.reserved[0] bits 0-1), whose leaf loop then
+// carries neither the marks nor the ring path.
 template <int VG, bool kEdge>
 __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, float dy, const float* dz, float* v) {
     uint32_t edge = 0;
@@ -1085,11 +1100,14 @@ __device__ __forceinline__ uint32_t eval_group(const LocalPrim& P, float dx, flo
     case P_BOX: eval_group_t<VG, P_BOX>(P, dx, dy, dz, v); break;
     case P_CAPSULE: eval_group_t<VG, P_CAPSULE>(P, dx, dy, dz, v); break;
     case P_TORUS:
-        if (!P.diff) {
+        if (kEdge && P.diff) {
+            const Vals<VG> r = eval_group_torus_ring<VG>(P, dx, dy, dz);
+#pragma unroll
+            for (int k = 0; k < VG; ++k) v[k] = r.v[k];
+        } else {
             eval_group_t<VG, P_TORUS>(P, dx, dy, dz, v);
-            break;
         }
-        [[fallthrough]];
+        break;
     default:
 #pragma unroll
         for (int k = 0; k < VG; ++k) {
@@ -1282,7 +1300,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                 sp[i].op = op;
                 sp[i].k = (float)I.k;
             } else {
-                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], B * G.fpitch);
+                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], B * G.fpitch, kEdge);
             }
         }
         __syncwarp();
@@ -1653,7 +1671,7 @@ int leaf_impl(const FbGeom& g, const FbPrim* prims, int n_prims, const FbInsn* c
     k_leaf<BB, EDGE><<<grid, 32 * kLeafWarps, 0, st>>>(G, prims, S.primf, chain, S.pool, sb_off, sb_len, active, \
                                                        count, capacity, tiles, work, kind, S.blk_off, S.blk_len,  \
                                                        S.blk_pool, P.blk_cap)
-        const bool edge = G.grid_leaves != 0;
+        const bool edge = G.special != 0;
         switch (G.B) {
         case 4: if (edge) FB_LEAF(4, true); else FB_LEAF(4, false); break;
         case 8: if (edge) FB_LEAF(8, true); else FB_LEAF(8, false); break;
@@ -1986,7 +2004,7 @@ void* fb_batch_create(const FbBatchItem* items, int32_t n, void* stream) noexcep
             const int64_t cls_threads = (G.nsuper * threads_per_super(G.S) + 31) / 32 * 32;
             g_cclass.add(r, cls_threads);
             g_tiles.add(r, d.ntiles);
-            g_leaf[b_index(G.B) + (G.grid_leaves ? 3 : 0)].add(r, 0);
+            g_leaf[b_index(G.B) + (G.special ? 3 : 0)].add(r, 0);
             if (d.mask) {
                 g_occ.add(r, 0);
                 g_occ_blocks.add(r, G.nblocks);

@@ -261,12 +261,13 @@ __device__ __forceinline__ float chain_apply(int op, float acc, float v, float k
 // does takes the ring frame: rotated about its axis so the block origin lies on +x, x measured from
 // the ring (u = x - R, w = y), where rho - R = u + w^2 / (rho + R + u) -- u carries the rounding of a
 // short offset instead of a coordinate of size R, and the quotient is a correction of a few
-// pitches.  extent 0 (callers that evaluate through local_eval) keeps the canonical forms.  Their float32 errors: about
+// pitches.  extent 0 (callers that evaluate through local_eval) keeps the canonical forms, and the
+// ring frame needs `ring` (leaf kernels built with its path).  Their float32 errors: about
 // u (|d| + 6 |e|) for the difference form (d = |L| - r, independent of r) and u (|L| + 2 |q|) ~ 3 u r for
 // the direct one (u = 2^-24): large spheres against small blocks favour the first, small spheres
 // against large blocks the second.  extent: the largest offset the block's evaluation uses.
 __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double ox, double oy, double oz, int op,
-                                         float k, LocalPrim& out, float extent = 0.f) {
+                                         float k, LocalPrim& out, float extent = 0.f, bool ring = false) {
     out.type = F.type;
     out.op = op;
     out.ident = F.ident;
@@ -297,7 +298,7 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     // sphere: |L|^2 - r^2 in float64, the constant term of the difference form of |q| - r
     out.L[3] = F.type == P_SPHERE ? (float)(fma(lx, lx, fma(ly, ly, lz * lz)) - D.p[0] * D.p[0]) : 0.f;
     out.diff = 0;
-    if (F.type == P_SPHERE || F.type == P_TORUS) {
+    if (F.type == P_SPHERE || (ring && F.type == P_TORUS)) {
         // the extent in the primitive's frame: the linear part's root-mean-square stretch (the
         // Frobenius norm over sqrt 3; exact for a rotation or permutation times a uniform scale)
         const double a2 = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2] + A[4] * A[4] + A[5] * A[5] + A[6] * A[6] +
