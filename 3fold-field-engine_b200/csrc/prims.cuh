@@ -312,7 +312,7 @@ __device__ __forceinline__ void localise(const FbPrim& D, const PrimF& F, double
     out.A[0] = F.A[0]; out.A[1] = F.A[1]; out.A[2] = F.A[2];
     out.A[3] = F.A[4]; out.A[4] = F.A[5]; out.A[5] = F.A[6];
     out.A[6] = F.A[8]; out.A[7] = F.A[9]; out.A[8] = F.A[10];
-    if (F.type == P_TORUS && out.diff) {
+    if (ring && F.type == P_TORUS && out.diff) {
         // ring frame: rotate about the torus axis so the block origin lies on +x, and measure x from
         // the ring (the torus is symmetric under the rotation); only the offsets go through the
         // rotation, whose float32 rounding then scales them by ~1 + 2^-24 at most
