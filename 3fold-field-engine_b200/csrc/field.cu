@@ -556,7 +556,7 @@ __device__ int warp_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn
     return n;
 }
 
-// The same walk by one thread (per-block lists in the lattice classification): the lanes of a warp
+// The same walk by one thread (each block's own list in k_classify_blocks): the lanes of a warp
 // walk the same superblock list together, so its loads are broadcasts.
 __device__ int seq_walk(const uint32_t* __restrict__ in, int n_in, const FbInsn* __restrict__ chain,
                         const PrimF* __restrict__ primf, float cx, float cy, float cz, float R, float eps,

@@ -42,7 +42,7 @@ def _batch_fields(bb):
 def test_batch_equals_plain_builds():
     """One batched build (work-lists over every recipe, device-side sizing) gives every recipe the
     kinds, ascending active ids and tiles of its own single build, bit for bit -- small grids
-    (warp-culled blocks) and large ones (corner lattice, 256^3 at 4^3 leaves and 512^3 at 8^3)."""
+    (16-voxel superblocks) and large ones (256^3 at 4^3 leaves and 512^3 at 8^3, above 2^17 blocks)."""
     import torch
     import field_b200.batch as BT
     import field_b200.expr as X
@@ -57,7 +57,7 @@ def test_batch_equals_plain_builds():
     assert bb.status() == 0
     got = _batch_fields(bb)
     want = _plain_fields(recipes)
-    assert any(fb.meta.n_blocks > (1 << 17) for fb in bb.builders)  # the lattice path is covered
+    assert any(fb.meta.n_blocks > (1 << 17) for fb in bb.builders)  # a large grid is covered
     for i, ((k1, a1, t1), (k2, a2, t2)) in enumerate(zip(got, want)):
         assert np.array_equal(k1, k2), i
         assert np.array_equal(a1, a2), i

@@ -28,7 +28,7 @@ def _restated(table, c, pts):
                                c["drill_r"], c["drill_z"], c["drill_x_half"])
 
 
-@pytest.mark.parametrize("pitch", [0.35, 0.2])  # warp-culled blocks; corner lattice (> 2^17 blocks)
+@pytest.mark.parametrize("pitch", [0.35, 0.2])  # a small grid; a large one (> 2^17 blocks)
 def test_machining_part_matches_oracle_and_reference_kernel(pitch):
     import field_b200.build as B
     comp, meta, table, c = _scene(pitch)
