@@ -274,6 +274,12 @@ __global__ void k_prepare_prims(const FbPrim* __restrict__ prims, int n, PrimF* 
     if (i < n) prepare_prim(prims, i, out);
 }
 
+// sqrt_sum over n inputs (the self-test export fb_sqrt_sum_probe).
+__global__ void k_sqrt_sum(const float* __restrict__ x, float* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = sqrt_sum(x[i]);
+}
+
 __global__ void k_full_list(uint32_t* __restrict__ list, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) list[i] = (uint32_t)i << 2;
@@ -975,20 +981,20 @@ __global__ void __launch_bounds__(256) k_compact(const int32_t* __restrict__ kin
 template <int T>
 __device__ __forceinline__ float canon_t(const float* __restrict__ p, float x, float y, float z) {
     // z-dependent terms outermost: across a group of voxels along z the x/y parts are shared
-    if (T == P_SPHERE) return sqrtf(fmaf(z, z, fmaf(x, x, y * y))) - p[0];
+    if (T == P_SPHERE) return sqrt_sum(fmaf(z, z, fmaf(x, x, y * y))) - p[0];
     if (T == P_BOX) {
         const float qx = fabsf(x) - p[0], qy = fabsf(y) - p[1], qz = fabsf(z) - p[2];
         const float ox = fmaxf(qx, 0.f), oy = fmaxf(qy, 0.f), oz = fmaxf(qz, 0.f);
-        return sqrtf(fmaf(oz, oz, fmaf(ox, ox, oy * oy))) + fminf(fmaxf(qz, fmaxf(qx, qy)), 0.f);
+        return sqrt_sum(fmaf(oz, oz, fmaf(ox, ox, oy * oy))) + fminf(fmaxf(qz, fmaxf(qx, qy)), 0.f);
     }
     if (T == P_CAPSULE) {
         const float h = fminf(fmaxf(fmaf(z, p[2], fmaf(x, p[0], y * p[1])) * p[4], p[5]), p[6]);
         const float dx = fmaf(-p[0], h, x), dy = fmaf(-p[1], h, y), dz = fmaf(-p[2], h, z);
-        return sqrtf(fmaf(dz, dz, fmaf(dx, dx, dy * dy))) - p[3];
+        return sqrt_sum(fmaf(dz, dz, fmaf(dx, dx, dy * dy))) - p[3];
     }
     if (T == P_TORUS) {
-        const float qx = sqrtf(fmaf(x, x, y * y)) - p[0];
-        return sqrtf(fmaf(z, z, qx * qx)) - p[1];
+        const float qx = sqrt_sum(fmaf(x, x, y * y)) - p[0];
+        return sqrt_sum(fmaf(z, z, qx * qx)) - p[1];
     }
     return canon_f(T, p, x, y, z);
 }
@@ -1015,7 +1021,7 @@ __device__ __forceinline__ void eval_group_sphere(const LocalPrim& P, float dx, 
         const float ex = fmaf(cx, dz[k], ebx), ey = fmaf(cy, dz[k], eby), ez = fmaf(cz, dz[k], ebz);
         const float x = L0 + ex, y = L1 + ey, z = L2 + ez;
         const float num = fmaf(ez, fmaf(2.f, L2, ez), fmaf(ey, fmaf(2.f, L1, ey), fmaf(ex, fmaf(2.f, L0, ex), K)));
-        const float den = sqrtf(fmaf(z, z, fmaf(x, x, y * y))) + r;
+        const float den = sqrt_sum(fmaf(z, z, fmaf(x, x, y * y))) + r;
         v[k] = fmaf(P.s, __fdiv_rn(num, den), -P.off);
     }
 }
@@ -1081,9 +1087,9 @@ __device__ __noinline__ Vals<VG> eval_group_torus_ring(const LocalPrim& P, float
     for (int k = 0; k < VG; ++k) {
         const float u = L0 + fmaf(P.A[2], dz[k], ebx), w = fmaf(P.A[5], dz[k], eby), z = L2 + fmaf(P.A[8], dz[k], ebz);
         const float t = R + u;  // x of the rotated frame: <= 0 only past the axis (a block across it)
-        const float rho = sqrtf(fmaf(t, t, w * w));
+        const float rho = sqrt_sum(fmaf(t, t, w * w));
         const float qx = t > 0.f ? u + __fdividef(w * w, rho + t) : rho - R;
-        out.v[k] = fmaf(P.s, sqrtf(fmaf(z, z, qx * qx)) - r, -P.off);
+        out.v[k] = fmaf(P.s, sqrt_sum(fmaf(z, z, qx * qx)) - r, -P.off);
     }
     return out;
 }
@@ -2461,6 +2467,16 @@ int fb_compact_timeout_probe(const int32_t* d_kind, int64_t n, int32_t* d_active
     FB_CUDA(cudaMemcpyAsync(flags, misc, 8, cudaMemcpyDeviceToHost, st));
     FB_CUDA(cudaStreamSynchronize(st));
     return flags[1] ? FB_TIMEOUT : FB_OK;
+}
+
+// The grouped evaluations' square root (sqrt_sum) over n device floats, stream-ordered.
+int fb_sqrt_sum_probe(const float* d_x, float* d_out, int64_t n, void* stream) noexcept {
+    if (!d_x || !d_out || n < 0) return FB_INVALID;
+    if (n == 0) return FB_OK;
+    const unsigned grid = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    k_sqrt_sum<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_x, d_out, n);
+    FB_LAUNCH();
+    return FB_OK;
 }
 
 // Error flag of the last compaction (1 when a bounded wait gave up), read from the scratch.

@@ -62,6 +62,20 @@ struct __align__(16) LocalPrim {
 __device__ __forceinline__ float sel_min(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float sel_max(float a, float b) { return a > b ? a : b; }
 
+// Square root of a sum of squares (x >= 0 or NaN) for the grouped float32 evaluations: one Newton
+// step on s^2 = x from the hardware's approximate reciprocal square root y, s = x*y, with the
+// residual x - s^2 formed exactly by one FMA (Markstein's correction, "IA-64 and Elementary
+// Functions", 2000): s + (y/2)(x - s^2).  Branch-free; correctly rounded on every input of [1, 4)
+// (tests/test_prims_gpu.py compares it with sqrtf across binades), so the tiles equal those of
+// sqrtf.  Inputs below 1e-30 (subnormal squares of offsets under 1e-15) give their root to within
+// 1e-15; x = 0 gives 0 and NaN stays NaN.
+__device__ __forceinline__ float sqrt_sum(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(fmaxf(x, 1e-30f)));
+    const float s = x * y;
+    return fmaf(0.5f * y, fmaf(-s, s, x), s);
+}
+
 // float32 lerp with the product form a*(1-t) + b*t, each operation rounded once.
 __device__ __forceinline__ float lerp_f(float a, float b, float t) {
     return __fadd_rn(__fmul_rn(a, __fsub_rn(1.f, t)), __fmul_rn(b, t));

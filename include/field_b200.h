@@ -186,6 +186,11 @@ void fb_batch_destroy(void* batch);
 int fb_compact_timeout_probe(const int32_t* d_kind, int64_t n, int32_t* d_active, int32_t* d_count,
                              void* d_scratch, int64_t scratch_len, int64_t spin_limit, void* stream);
 
+/* No counterpart in the reference.  Self-test of the square root the float32 leaf and corner
+ * evaluations use (a Newton step from the approximate reciprocal square root): d_out[i] = that root
+ * of d_x[i] for n device floats, stream-ordered.  Inputs are sums of squares (>= 0, or NaN). */
+int fb_sqrt_sum_probe(const float* d_x, float* d_out, int64_t n, void* stream);
+
 /* Replace meshsdf_classify_cpu / meshsdf_tiles_cpu, src/field_engine/mesh_sdf_native_v1/field.cpp:229,254,
  * and k_classify_dense / k_eval_tile_dense, src/field_engine/faltkarna_v1_mesh_to_sdf.py:602-657. */
 int64_t fb_dense_scratch_bytes(int64_t nx, int64_t ny, int64_t nz, int32_t block);
