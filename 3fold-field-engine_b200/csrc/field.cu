@@ -1217,6 +1217,364 @@ __device__ __forceinline__ void load_group(const float* out, int group, float* a
 }
 
 
+// ------------------------------------------------------------------------------------ 8^3 tiles
+// An 8^3 block's tile, primitive by primitive over all 512 voxels: lane l owns voxels
+// (2g + l/16, (l/2) % 8, 4 (l % 2) + k) for g, k in 0..3 -- the voxels, and the float operations in
+// their order, of the grouped loop below -- and keeps their running values in shared memory (one
+// float4 per group), so a staged primitive is read and dispatched once per 16 voxels rather than
+// once per 4, while the kind bodies stay one group long (a loop over the 4 groups, small enough for
+// the instruction cache).  The per-voxel arithmetic of the common kinds runs on float32 pairs
+// (FFMA2 / FADD2 / FMUL2 on sm_100: two voxels per instruction, each element rounded as its scalar
+// form), so the tiles equal the grouped loop's bit for bit.  Hard combines have the subtraction's
+// sign folded into the primitive's scale at staging and take one min or max per voxel; a set starts
+// from NaN, which min replaces.  Smooth combines, the rarely used kinds and the common kinds in a
+// general frame go voxel by voxel through the out-of-line evaluation.
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 abs2(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ float2 max2(float2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
+
+// sqrt_sum of both elements.
+__device__ __forceinline__ float2 sqrt_sum2(float2 x) {
+    float2 y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y.x) : "f"(fmaxf(x.x, 1e-30f)));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y.y) : "f"(fmaxf(x.y, 1e-30f)));
+    const float2 s = mul2(x, y);
+    return fma2(mul2(dup2(0.5f), y), fma2(neg2(s), s, x), s);
+}
+
+// One voxel of any staged primitive, as the grouped evaluation computes it (out of line: smooth
+// combines, the rarely used kinds and general frames).  NaN marks a sampled grid's voxel at its
+// table's boundary.
+__device__ __noinline__ float eval_one_any(const LocalPrim& P, float dx, float dy, float dz) {
+    if (P.type == P_SPHERE && P.diff) {
+        const float ex = fmaf(P.A[2], dz, fmaf(P.A[0], dx, P.A[1] * dy));
+        const float ey = fmaf(P.A[5], dz, fmaf(P.A[3], dx, P.A[4] * dy));
+        const float ez = fmaf(P.A[8], dz, fmaf(P.A[6], dx, P.A[7] * dy));
+        const float x = P.L[0] + ex, y = P.L[1] + ey, z = P.L[2] + ez;
+        const float num =
+            fmaf(ez, fmaf(2.f, P.L[2], ez), fmaf(ey, fmaf(2.f, P.L[1], ey), fmaf(ex, fmaf(2.f, P.L[0], ex), P.L[3])));
+        const float den = sqrt_sum(fmaf(z, z, fmaf(x, x, y * y))) + P.p[0];
+        return fmaf(P.s, __fdiv_rn(num, den), -P.off);
+    }
+    if (P.type == P_TORUS && P.diff) {
+        const float dzs[1] = {dz};
+        return eval_group_torus_ring<1>(P, dx, dy, dzs).v[0];
+    }
+    float x, y, z;
+    if (P.ident) {
+        x = P.L[0] + dx; y = P.L[1] + dy; z = P.L[2] + dz;
+    } else {
+        x = fmaf(P.A[2], dz, fmaf(P.A[0], dx, fmaf(P.A[1], dy, P.L[0])));
+        y = fmaf(P.A[5], dz, fmaf(P.A[3], dx, fmaf(P.A[4], dy, P.L[1])));
+        z = fmaf(P.A[8], dz, fmaf(P.A[6], dx, fmaf(P.A[7], dy, P.L[2])));
+    }
+    float c;
+    switch (P.type) {
+    case P_SPHERE: c = canon_t<P_SPHERE>(P.p, x, y, z); break;
+    case P_BOX: c = canon_t<P_BOX>(P.p, x, y, z); break;
+    case P_CAPSULE: c = canon_t<P_CAPSULE>(P.p, x, y, z); break;
+    case P_TORUS: c = canon_t<P_TORUS>(P.p, x, y, z); break;
+    default:
+        if (P.type == P_GRID && grid_edge_f(P.p, x, y, z)) return __int_as_float(0x7fc00000);
+        c = canon_f(P.type, P.p, x, y, z);
+    }
+    return fmaf(P.s, c, -P.off);
+}
+
+// One voxel's combine as the grouped loop applies it (smooth and hard, sign not folded).
+__device__ __forceinline__ float combine1(int op, float k, float acc, float v) {
+    if (k > 0.f) return chain_apply(op, acc, v, k);
+    switch (op) {
+    case CH_SET: return v;
+    case CH_SETNEG: return -v;
+    case CH_UNION: return sel_min(acc, v);
+    case CH_INTERSECT: return sel_max(acc, v);
+    default: return sel_max(acc, -v);
+    }
+}
+
+// Lane geometry of a tile: group g's x offset is (2g + hi) * fpitch, then dy and the z offset pairs.
+struct Lane16 {
+    int hi;
+    float fpitch, dy;
+    float2 dz[2];
+    __device__ __forceinline__ float dx(int g) const { return (2 * g + hi) * fpitch; }
+};
+
+// Running values of a lane's group g (acc: the lane's slot of group 0; groups 32 float4 apart) and
+// the hard combine of a group's 4 values into them.  mode 2 (set) replaces them.
+struct Group4 {
+    float2 a0, a1;
+    __device__ __forceinline__ Group4(const float4* acc, int g, int mode) {
+        const float4 v = mode == 2 ? make_float4(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000),
+                                                 __int_as_float(0x7fc00000), __int_as_float(0x7fc00000))
+                                   : acc[g * 32];
+        a0 = make_float2(v.x, v.y);
+        a1 = make_float2(v.z, v.w);
+    }
+    __device__ __forceinline__ void combine(bool mx, float2 v0, float2 v1) {
+        a0.x = mx ? fmaxf(a0.x, v0.x) : fminf(a0.x, v0.x);
+        a0.y = mx ? fmaxf(a0.y, v0.y) : fminf(a0.y, v0.y);
+        a1.x = mx ? fmaxf(a1.x, v1.x) : fminf(a1.x, v1.x);
+        a1.y = mx ? fmaxf(a1.y, v1.y) : fminf(a1.y, v1.y);
+    }
+    __device__ __forceinline__ void store(float4* acc, int g) const { acc[g * 32] = make_float4(a0.x, a0.y, a1.x, a1.y); }
+};
+
+// Sphere in the difference form (any frame: the identity frame gives the grouped loop's values).
+__device__ __forceinline__ void tile16_sphere_diff(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
+    const float2 L0 = dup2(P.L[0]), L1 = dup2(P.L[1]), L2 = dup2(P.L[2]), K = dup2(P.L[3]), r = dup2(P.p[0]);
+    const float2 s = dup2(P.s), noff = dup2(-P.off), two = dup2(2.f);
+    const float2 c2 = dup2(P.A[2]), c5 = dup2(P.A[5]), c8 = dup2(P.A[8]);
+    const float a0 = P.A[0], a3 = P.A[3], a6 = P.A[6];
+    const float a1 = P.A[1] * Q.dy, a4 = P.A[4] * Q.dy, a7 = P.A[7] * Q.dy;
+    const bool mx = mode == 1;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const float dx = Q.dx(g);
+        const float2 ebx = dup2(fmaf(a0, dx, a1)), eby = dup2(fmaf(a3, dx, a4)), ebz = dup2(fmaf(a6, dx, a7));
+        float2 v[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float2 ex = fma2(c2, Q.dz[j], ebx), ey = fma2(c5, Q.dz[j], eby), ez = fma2(c8, Q.dz[j], ebz);
+            const float2 x = add2(L0, ex), y = add2(L1, ey), z = add2(L2, ez);
+            const float2 num = fma2(ez, fma2(two, L2, ez), fma2(ey, fma2(two, L1, ey), fma2(ex, fma2(two, L0, ex), K)));
+            const float2 den = add2(sqrt_sum2(fma2(z, z, fma2(x, x, mul2(y, y)))), r);
+            v[j] = fma2(s, make_float2(__fdiv_rn(num.x, den.x), __fdiv_rn(num.y, den.y)), noff);
+        }
+        Group4 a(acc, g, mode);
+        a.combine(mx, v[0], v[1]);
+        a.store(acc, g);
+    }
+}
+
+// Sphere, direct form, identity frame.
+__device__ __forceinline__ void tile16_sphere(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
+    const float L0 = P.L[0], y = P.L[1] + Q.dy, yy = y * y;
+    const float2 z0 = add2(dup2(P.L[2]), Q.dz[0]), z1 = add2(dup2(P.L[2]), Q.dz[1]);
+    const float2 s = dup2(P.s), noff = dup2(-P.off), nr = dup2(-P.p[0]);
+    const bool mx = mode == 1;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const float x = L0 + Q.dx(g);
+        const float2 xy = dup2(fmaf(x, x, yy));
+        const float2 v0 = fma2(s, add2(sqrt_sum2(fma2(z0, z0, xy)), nr), noff);
+        const float2 v1 = fma2(s, add2(sqrt_sum2(fma2(z1, z1, xy)), nr), noff);
+        Group4 a(acc, g, mode);
+        a.combine(mx, v0, v1);
+        a.store(acc, g);
+    }
+}
+
+// Box, identity frame.
+__device__ __forceinline__ void tile16_box(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
+    const float L0 = P.L[0], p0 = P.p[0];
+    const float y = P.L[1] + Q.dy, qy = fabsf(y) - P.p[1], oy = fmaxf(qy, 0.f), oyy = oy * oy;
+    const float2 qz0 = add2(abs2(add2(dup2(P.L[2]), Q.dz[0])), dup2(-P.p[2]));
+    const float2 qz1 = add2(abs2(add2(dup2(P.L[2]), Q.dz[1])), dup2(-P.p[2]));
+    const float2 oz0 = max2(qz0, 0.f), oz1 = max2(qz1, 0.f);
+    const float2 s = dup2(P.s), noff = dup2(-P.off);
+    const bool mx = mode == 1;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const float qx = fabsf(L0 + Q.dx(g)) - p0, ox = fmaxf(qx, 0.f);
+        const float2 oxy = dup2(fmaf(ox, ox, oyy));
+        const float mxy = fmaxf(qx, qy);
+        const float2 in0 = make_float2(fminf(fmaxf(qz0.x, mxy), 0.f), fminf(fmaxf(qz0.y, mxy), 0.f));
+        const float2 in1 = make_float2(fminf(fmaxf(qz1.x, mxy), 0.f), fminf(fmaxf(qz1.y, mxy), 0.f));
+        const float2 v0 = fma2(s, add2(sqrt_sum2(fma2(oz0, oz0, oxy)), in0), noff);
+        const float2 v1 = fma2(s, add2(sqrt_sum2(fma2(oz1, oz1, oxy)), in1), noff);
+        Group4 a(acc, g, mode);
+        a.combine(mx, v0, v1);
+        a.store(acc, g);
+    }
+}
+
+// Capsule, identity frame.
+__device__ __forceinline__ void tile16_capsule(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
+    const float* p = P.p;
+    const float L0 = P.L[0], p0 = p[0], p5 = p[5], p6 = p[6];
+    const float y = P.L[1] + Q.dy, yp1 = y * p[1];
+    const float2 z[2] = {add2(dup2(P.L[2]), Q.dz[0]), add2(dup2(P.L[2]), Q.dz[1])};
+    const float2 s = dup2(P.s), noff = dup2(-P.off), nr = dup2(-p[3]), p2 = dup2(p[2]), p4 = dup2(p[4]);
+    const float2 np0 = dup2(-p0), np1 = dup2(-p[1]), np2 = dup2(-p[2]), y2 = dup2(y);
+    const bool mx = mode == 1;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const float x = L0 + Q.dx(g);
+        const float2 xy = dup2(fmaf(x, p0, yp1)), x2 = dup2(x);
+        float2 v[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float2 t = mul2(fma2(z[j], p2, xy), p4);
+            const float2 h = make_float2(fminf(fmaxf(t.x, p5), p6), fminf(fmaxf(t.y, p5), p6));
+            const float2 ex = fma2(np0, h, x2), ey = fma2(np1, h, y2), ez = fma2(np2, h, z[j]);
+            v[j] = fma2(s, add2(sqrt_sum2(fma2(ez, ez, fma2(ex, ex, mul2(ey, ey)))), nr), noff);
+        }
+        Group4 a(acc, g, mode);
+        a.combine(mx, v[0], v[1]);
+        a.store(acc, g);
+    }
+}
+
+// Torus, any frame (the identity frame gives the grouped loop's values).
+__device__ __forceinline__ void tile16_torus(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
+    const float t0 = fmaf(P.A[1], Q.dy, P.L[0]), t1 = fmaf(P.A[4], Q.dy, P.L[1]), t2 = fmaf(P.A[7], Q.dy, P.L[2]);
+    const float a0 = P.A[0], a3 = P.A[3], a6 = P.A[6];
+    const float2 c2 = dup2(P.A[2]), c5 = dup2(P.A[5]), c8 = dup2(P.A[8]);
+    const float2 s = dup2(P.s), noff = dup2(-P.off), nR = dup2(-P.p[0]), nr = dup2(-P.p[1]);
+    const bool mx = mode == 1;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const float dx = Q.dx(g);
+        const float2 bx = dup2(fmaf(a0, dx, t0)), by = dup2(fmaf(a3, dx, t1)), bz = dup2(fmaf(a6, dx, t2));
+        float2 v[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float2 x = fma2(c2, Q.dz[j], bx), y = fma2(c5, Q.dz[j], by), z = fma2(c8, Q.dz[j], bz);
+            const float2 qx = add2(sqrt_sum2(fma2(x, x, mul2(y, y))), nR);
+            v[j] = fma2(s, add2(sqrt_sum2(fma2(z, z, mul2(qx, qx))), nr), noff);
+        }
+        Group4 a(acc, g, mode);
+        a.combine(mx, v[0], v[1]);
+        a.store(acc, g);
+    }
+}
+
+// A torus in its ring frame (leaf kernels built for recipes with such tori).
+__device__ __forceinline__ void tile16_torus_ring(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
+    const float dzs[4] = {Q.dz[0].x, Q.dz[0].y, Q.dz[1].x, Q.dz[1].y};
+    const bool mx = mode == 1;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        const Vals<4> r = eval_group_torus_ring<4>(P, Q.dx(g), Q.dy, dzs);
+        Group4 a(acc, g, mode);
+        a.combine(mx, make_float2(r.v[0], r.v[1]), make_float2(r.v[2], r.v[3]));
+        a.store(acc, g);
+    }
+}
+
+// Any other staged element (mode 3): an offset, a smooth combine, a rarely used kind or a common
+// kind in a general frame, voxel by voxel.  Returns the voxels that sampled a grid table at its
+// boundary (bit 4g + k).
+__device__ __forceinline__ uint32_t tile16_other(const LocalPrim& P, const Lane16& Q, float4* acc) {
+    const int op = P.op;
+    const float k = P.k;
+    uint32_t edge = 0;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        float4 a = acc[g * 32];
+        if (op == CH_OFFSET) {
+            a.x -= k; a.y -= k; a.z -= k; a.w -= k;
+        } else {
+            const float dx = Q.dx(g);
+            const float v0 = eval_one_any(P, dx, Q.dy, Q.dz[0].x), v1 = eval_one_any(P, dx, Q.dy, Q.dz[0].y);
+            const float v2 = eval_one_any(P, dx, Q.dy, Q.dz[1].x), v3 = eval_one_any(P, dx, Q.dy, Q.dz[1].y);
+            edge |= ((uint32_t)!(v0 == v0) | (uint32_t)!(v1 == v1) << 1 | (uint32_t)!(v2 == v2) << 2 |
+                     (uint32_t)!(v3 == v3) << 3) << (4 * g);
+            a.x = combine1(op, k, a.x, v0);
+            a.y = combine1(op, k, a.y, v1);
+            a.z = combine1(op, k, a.z, v2);
+            a.w = combine1(op, k, a.w, v3);
+        }
+        acc[g * 32] = a;
+    }
+    return edge;
+}
+
+// The tile of one 8^3 block from its culled list (leaf_block's list and frame), with the running
+// values in this warp's `acc` (4 groups x 32 lanes float4, shared memory); returns the lane's
+// guard-band bits (bit 4g + k: voxel k of group g), as the grouped loop's deferred recheck reads
+// them.  Every lane of the warp calls it with the same block.
+template <bool kEdge>
+__device__ __forceinline__ uint32_t tile16(const Geo& G, const FbPrim* __restrict__ prims,
+                                           const PrimF* __restrict__ primf, const FbInsn* __restrict__ chain,
+                                           const uint32_t* list, int len, double ox, double oy, double oz,
+                                           float* __restrict__ out, LocalPrim* sp, float4* acc_warp) {
+    const int lane = threadIdx.x & 31;
+    Lane16 Q;
+    Q.hi = lane >> 4;
+    Q.fpitch = G.fpitch;
+    Q.dy = ((lane >> 1) & 7) * G.fpitch;
+    const int lk0 = 4 * (lane & 1);
+    Q.dz[0] = make_float2(lk0 * G.fpitch, (lk0 + 1) * G.fpitch);
+    Q.dz[1] = make_float2((lk0 + 2) * G.fpitch, (lk0 + 3) * G.fpitch);
+    float4* acc = acc_warp + lane;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) acc[g * 32] = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t edge = 0;  // kEdge: bit 4g + k marks a voxel that sampled a grid table at its boundary
+    for (int c0 = 0; c0 < len; c0 += kCapBlock) {
+        const int clen = min(kCapBlock, len - c0);
+        __syncwarp();
+        for (int i = lane; i < clen; i += 32) {
+            const uint32_t e = list[c0 + i];
+            const FbInsn I = chain[e >> 2];
+            const int op = effective_op(e, I.op);
+            LocalPrim& S = sp[i];
+            if (op == CH_OFFSET) {
+                S.op = op;
+                S.k = (float)I.k;
+                S.mode = 3;
+                continue;
+            }
+            localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, S, 8 * G.fpitch, kEdge);
+            const int t = S.type;
+            const bool fast = t == P_TORUS || (t == P_SPHERE && S.diff) ||
+                              (S.ident && (t == P_SPHERE || t == P_BOX || t == P_CAPSULE));
+            int mode = 3;
+            if (fast && !(S.k > 0.f)) {
+                mode = (op == CH_SET || op == CH_SETNEG) ? 2 : (op == CH_INTERSECT || op == CH_SUBTRACT) ? 1 : 0;
+                if (op == CH_SUBTRACT || op == CH_SETNEG) {
+                    S.s = -S.s;
+                    S.off = -S.off;
+                }
+            }
+            S.mode = mode;
+        }
+        __syncwarp();
+        for (int i = 0; i < clen; ++i) {
+            const LocalPrim& P = sp[i];
+            const int mode = P.mode;
+            if (mode == 3) {
+                const uint32_t e = tile16_other(P, Q, acc);
+                if (kEdge) edge |= e;
+                continue;
+            }
+            switch (P.type) {
+            case P_SPHERE:
+                if (P.diff) tile16_sphere_diff(P, Q, mode, acc);
+                else tile16_sphere(P, Q, mode, acc);
+                break;
+            case P_BOX: tile16_box(P, Q, mode, acc); break;
+            case P_CAPSULE: tile16_capsule(P, Q, mode, acc); break;
+            default:  // P_TORUS: the staging gives modes 0-2 to the kinds above only
+                if (kEdge && P.diff) tile16_torus_ring(P, Q, mode, acc);
+                else tile16_torus(P, Q, mode, acc);
+            }
+        }
+    }
+    uint32_t near = 0;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+        float4 a = acc[g * 32];
+        if (kEdge) {  // sampled a grid table at its boundary: decided in float64
+            const float nan = __int_as_float(0x7fc00000);
+            if ((edge >> (4 * g)) & 1u) a.x = nan;
+            if ((edge >> (4 * g + 1)) & 1u) a.y = nan;
+            if ((edge >> (4 * g + 2)) & 1u) a.z = nan;
+            if ((edge >> (4 * g + 3)) & 1u) a.w = nan;
+        }
+        near |= ((uint32_t)!(fabsf(a.x) >= G.guard) | (uint32_t)!(fabsf(a.y) >= G.guard) << 1 |
+                 (uint32_t)!(fabsf(a.z) >= G.guard) << 2 | (uint32_t)!(fabsf(a.w) >= G.guard) << 3) << (4 * g);
+        reinterpret_cast<float4*>(out)[g * 32 + lane] = a;
+    }
+    return near;
+}
+
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
 // voxels along z (VG = 4, or 2 for 4^3 blocks) and stores each group with one vector store.
 // One active block's tile: the block's culled list (as the classification left it, else culled
@@ -1232,7 +1590,7 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
                            float* __restrict__ out, unsigned long long* __restrict__ work,
                            const int32_t* __restrict__ kind, const int32_t* __restrict__ blk_off,
                            const int32_t* __restrict__ blk_len, const uint32_t* __restrict__ blk_pool, int64_t blk_cap,
-                           LocalPrim* sp, uint32_t* sl) {
+                           LocalPrim* sp, uint32_t* sl, float4* acc) {
     constexpr int kVox = B * B * B;
     constexpr int VG = B == 4 ? 2 : 4;
     constexpr int kGroups = kVox / (32 * VG);
@@ -1294,69 +1652,73 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
     // the list in chunks of kCapBlock localised primitives; between chunks each lane keeps its
     // partial fold in its own part of the tile (the same float operations in the same order)
     uint32_t near = 0;  // bit g * VG + k: voxel k of this lane's group g lies in the guard band
-    for (int c0 = 0; c0 == 0 || c0 < len; c0 += kCapBlock) {  // one pass even for an empty list
-        const int clen = max(0, min(kCapBlock, len - c0));
-        const bool first = c0 == 0, last = c0 + clen >= len;
-        __syncwarp();
-        for (int i = lane; i < clen; i += 32) {
-            const uint32_t e = list[c0 + i];
-            const FbInsn I = chain[e >> 2];
-            const int op = effective_op(e, I.op);
-            if (op == CH_OFFSET) {
-                sp[i].op = op;
-                sp[i].k = (float)I.k;
-            } else {
-                localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], B * G.fpitch, kEdge);
-            }
-        }
-        __syncwarp();
-        for (int g = 0; g < kGroups; ++g) {
-            const int v0 = (g * 32 + lane) * VG;
-            const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
-            const float dx = li * G.fpitch, dy = lj * G.fpitch;
-            float dz[VG], acc[VG], v[VG];
-            uint32_t edge = 0;
-#pragma unroll
-            for (int k = 0; k < VG; ++k) dz[k] = (lk0 + k) * G.fpitch;
-            if (first) {
-#pragma unroll
-                for (int k = 0; k < VG; ++k) acc[k] = 0.f;
-            } else {
-                load_group<VG>(out, g * 32 + lane, acc);
-                if (kEdge) {
-#pragma unroll
-                    for (int k = 0; k < VG; ++k) edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // an earlier chunk's mark
-                }
-            }
-            for (int i = 0; i < clen; ++i) {
-                const LocalPrim& P = sp[i];
-                const int op = P.op;
+    if constexpr (B == 8) {
+        near = tile16<kEdge>(G, prims, primf, chain, list, len, ox, oy, oz, out, sp, acc);
+    } else {
+        for (int c0 = 0; c0 == 0 || c0 < len; c0 += kCapBlock) {  // one pass even for an empty list
+            const int clen = max(0, min(kCapBlock, len - c0));
+            const bool first = c0 == 0, last = c0 + clen >= len;
+            __syncwarp();
+            for (int i = lane; i < clen; i += 32) {
+                const uint32_t e = list[c0 + i];
+                const FbInsn I = chain[e >> 2];
+                const int op = effective_op(e, I.op);
                 if (op == CH_OFFSET) {
-#pragma unroll
-                    for (int k = 0; k < VG; ++k) acc[k] -= P.k;
-                    continue;
-                }
-                edge |= eval_group<VG, kEdge>(P, dx, dy, dz, v);
-                combine_group<VG>(op, P.k, acc, v);
-            }
-            if (kEdge && edge) {  // sampled a grid table at its boundary: carried to the last chunk as NaN
-#pragma unroll
-                for (int k = 0; k < VG; ++k)
-                    if ((edge >> k) & 1u) acc[k] = __int_as_float(0x7fc00000);
-            }
-            if (last) {
-                if (kDeferGuard) {
-#pragma unroll
-                    for (int k = 0; k < VG; ++k) near |= (uint32_t)!(fabsf(acc[k]) >= G.guard) << (g * VG + k);
+                    sp[i].op = op;
+                    sp[i].k = (float)I.k;
                 } else {
-#pragma unroll
-                    for (int k = 0; k < VG; ++k)
-                        if (!(fabsf(acc[k]) >= G.guard))
-                            acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
-                                                        (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
+                    localise(prims[I.arg], primf[I.arg], ox, oy, oz, op, (float)I.k, sp[i], B * G.fpitch, kEdge);
                 }
             }
-            store_group<VG>(out, g * 32 + lane, acc);
+            __syncwarp();
+            for (int g = 0; g < kGroups; ++g) {
+                const int v0 = (g * 32 + lane) * VG;
+                const int li = v0 / (B * B), lj = (v0 / B) % B, lk0 = v0 % B;
+                const float dx = li * G.fpitch, dy = lj * G.fpitch;
+                float dz[VG], acc[VG], v[VG];
+                uint32_t edge = 0;
+    #pragma unroll
+                for (int k = 0; k < VG; ++k) dz[k] = (lk0 + k) * G.fpitch;
+                if (first) {
+    #pragma unroll
+                    for (int k = 0; k < VG; ++k) acc[k] = 0.f;
+                } else {
+                    load_group<VG>(out, g * 32 + lane, acc);
+                    if (kEdge) {
+    #pragma unroll
+                        for (int k = 0; k < VG; ++k) edge |= (uint32_t)!(acc[k] == acc[k]) << k;  // an earlier chunk's mark
+                    }
+                }
+                for (int i = 0; i < clen; ++i) {
+                    const LocalPrim& P = sp[i];
+                    const int op = P.op;
+                    if (op == CH_OFFSET) {
+    #pragma unroll
+                        for (int k = 0; k < VG; ++k) acc[k] -= P.k;
+                        continue;
+                    }
+                    edge |= eval_group<VG, kEdge>(P, dx, dy, dz, v);
+                    combine_group<VG>(op, P.k, acc, v);
+                }
+                if (kEdge && edge) {  // sampled a grid table at its boundary: carried to the last chunk as NaN
+    #pragma unroll
+                    for (int k = 0; k < VG; ++k)
+                        if ((edge >> k) & 1u) acc[k] = __int_as_float(0x7fc00000);
+                }
+                if (last) {
+                    if (kDeferGuard) {
+    #pragma unroll
+                        for (int k = 0; k < VG; ++k) near |= (uint32_t)!(fabsf(acc[k]) >= G.guard) << (g * VG + k);
+                    } else {
+    #pragma unroll
+                        for (int k = 0; k < VG; ++k)
+                            if (!(fabsf(acc[k]) >= G.guard))
+                                acc[k] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li,
+                                                            (int64_t)bj * B + lj, (int64_t)bk * B + lk0 + k);
+                    }
+                }
+                store_group<VG>(out, g * 32 + lane, acc);
+            }
         }
     }
     // guard band: a float64 recheck of the few voxels near zero, so the sign never disagrees with
@@ -1389,13 +1751,14 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_leaf(Geo G, const FbPrim
                                                              const uint32_t* __restrict__ blk_pool, int64_t blk_cap) {
     __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
     __shared__ uint32_t s_list[kLeafWarps][kCapBlock];
+    __shared__ float4 s_acc[kLeafWarps][B == 8 ? 128 : 1];  // 8^3 tiles: running values, 4 groups x 32 lanes
     const int warp = threadIdx.x >> 5;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t n_active = min((int64_t)count[0], capacity);
     for (int64_t a = gwarp; a < n_active; a += nwarps)
         leaf_block<B, kEdge>(G, prims, primf, chain, pool, sb_off, sb_len, active[a], tiles + a * (B * B * B), work,
-                             kind, blk_off, blk_len, blk_pool, blk_cap, s_prim[warp], s_list[warp]);
+                             kind, blk_off, blk_len, blk_pool, blk_cap, s_prim[warp], s_list[warp], s_acc[warp]);
 }
 
 // Leaf tiles of a general postfix program: float64 per voxel, no culling.
@@ -1883,6 +2246,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __
                                                                unsigned long long* __restrict__ work) {
     __shared__ LocalPrim s_prim[kLeafWarps][kCapBlock];
     __shared__ uint32_t s_list[kLeafWarps][kCapBlock];
+    __shared__ float4 s_acc[kLeafWarps][B == 8 ? 128 : 1];  // 8^3 tiles: running values, 4 groups x 32 lanes
     const int warp = threadIdx.x >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = W.pre[W.m];
@@ -1893,7 +2257,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __
         const int64_t a = g - W.pre[j];
         leaf_block<B, kEdge>(R.G, R.prims, R.primf, R.chain, R.pool, R.off + R.G.ncoarse, R.len + R.G.ncoarse, R.active[a],
                       tiles + tile_off[r] + a * (B * B * B), work, R.kind, R.blk_off, R.blk_len, R.blk_pool,
-                      R.blk_cap, s_prim[warp], s_list[warp]);
+                      R.blk_cap, s_prim[warp], s_list[warp], s_acc[warp]);
     }
 }
 

@@ -52,7 +52,8 @@ struct __align__(16) PrimF {
 // sphere's difference form for this block.
 struct __align__(16) LocalPrim {
     int32_t type, op, ident, diff;
-    float k, s, off, pad1;
+    float k, s, off;
+    int32_t mode;  // 8^3 leaf tiles: 0 min, 1 max, 2 set (hard combines, sign folded into s/off), 3 other
     float L[4];
     float A[12];   // A_lin rows (9 used)
     float p[12];
