@@ -43,6 +43,7 @@ SIGNATURES = {
     "fb_field_compact_error": (I, [P, I, I, P, P]),
     "fb_compact_timeout_probe": (I, [P, I64, P, P, P, I64, I64, P]),
     "fb_sqrt_sum_probe": (I, [P, P, I64, P]),
+    "fb_quotient_probe": (I, [P, P, P, I64, P]),
     # batched builds
     "fb_batch_create": (P, [P, I, P]),
     "fb_batch_build_device": (I, [P, P, I64, I, P]),

@@ -1237,6 +1237,18 @@ __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y
 __device__ __forceinline__ float2 abs2(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
 __device__ __forceinline__ float2 max2(float2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
 
+// num / den for den > 0 (a sum with a positive radius): one Newton step from the approximate
+// reciprocal y, q = q0 + y (num - q0 den) with q0 = num y and the residual formed exactly by one FMA
+// (Markstein's correction, as for sqrt_sum).  Branch-free; tests/test_prims_gpu.py compares it with
+// the IEEE quotient.
+__device__ __forceinline__ float2 quotient2(float2 num, float2 den) {
+    float2 y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y.x) : "f"(den.x));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y.y) : "f"(den.y));
+    const float2 q0 = mul2(num, y);
+    return fma2(fma2(neg2(q0), den, num), y, q0);
+}
+
 // sqrt_sum of both elements.
 __device__ __forceinline__ float2 sqrt_sum2(float2 x) {
     float2 y;
@@ -1333,7 +1345,7 @@ __device__ __forceinline__ void tile16_sphere_diff(const LocalPrim& P, const Lan
     const float a0 = P.A[0], a3 = P.A[3], a6 = P.A[6];
     const float a1 = P.A[1] * Q.dy, a4 = P.A[4] * Q.dy, a7 = P.A[7] * Q.dy;
     const bool mx = mode == 1;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         const float dx = Q.dx(g);
         const float2 ebx = dup2(fmaf(a0, dx, a1)), eby = dup2(fmaf(a3, dx, a4)), ebz = dup2(fmaf(a6, dx, a7));
@@ -1344,7 +1356,7 @@ __device__ __forceinline__ void tile16_sphere_diff(const LocalPrim& P, const Lan
             const float2 x = add2(L0, ex), y = add2(L1, ey), z = add2(L2, ez);
             const float2 num = fma2(ez, fma2(two, L2, ez), fma2(ey, fma2(two, L1, ey), fma2(ex, fma2(two, L0, ex), K)));
             const float2 den = add2(sqrt_sum2(fma2(z, z, fma2(x, x, mul2(y, y)))), r);
-            v[j] = fma2(s, make_float2(__fdiv_rn(num.x, den.x), __fdiv_rn(num.y, den.y)), noff);
+            v[j] = fma2(s, quotient2(num, den), noff);
         }
         Group4 a(acc, g, mode);
         a.combine(mx, v[0], v[1]);
@@ -1358,7 +1370,7 @@ __device__ __forceinline__ void tile16_sphere(const LocalPrim& P, const Lane16& 
     const float2 z0 = add2(dup2(P.L[2]), Q.dz[0]), z1 = add2(dup2(P.L[2]), Q.dz[1]);
     const float2 s = dup2(P.s), noff = dup2(-P.off), nr = dup2(-P.p[0]);
     const bool mx = mode == 1;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         const float x = L0 + Q.dx(g);
         const float2 xy = dup2(fmaf(x, x, yy));
@@ -1379,7 +1391,7 @@ __device__ __forceinline__ void tile16_box(const LocalPrim& P, const Lane16& Q, 
     const float2 oz0 = max2(qz0, 0.f), oz1 = max2(qz1, 0.f);
     const float2 s = dup2(P.s), noff = dup2(-P.off);
     const bool mx = mode == 1;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         const float qx = fabsf(L0 + Q.dx(g)) - p0, ox = fmaxf(qx, 0.f);
         const float2 oxy = dup2(fmaf(ox, ox, oyy));
@@ -1403,7 +1415,7 @@ __device__ __forceinline__ void tile16_capsule(const LocalPrim& P, const Lane16&
     const float2 s = dup2(P.s), noff = dup2(-P.off), nr = dup2(-p[3]), p2 = dup2(p[2]), p4 = dup2(p[4]);
     const float2 np0 = dup2(-p0), np1 = dup2(-p[1]), np2 = dup2(-p[2]), y2 = dup2(y);
     const bool mx = mode == 1;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         const float x = L0 + Q.dx(g);
         const float2 xy = dup2(fmaf(x, p0, yp1)), x2 = dup2(x);
@@ -1428,7 +1440,7 @@ __device__ __forceinline__ void tile16_torus(const LocalPrim& P, const Lane16& Q
     const float2 c2 = dup2(P.A[2]), c5 = dup2(P.A[5]), c8 = dup2(P.A[8]);
     const float2 s = dup2(P.s), noff = dup2(-P.off), nR = dup2(-P.p[0]), nr = dup2(-P.p[1]);
     const bool mx = mode == 1;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         const float dx = Q.dx(g);
         const float2 bx = dup2(fmaf(a0, dx, t0)), by = dup2(fmaf(a3, dx, t1)), bz = dup2(fmaf(a6, dx, t2));
@@ -1449,7 +1461,7 @@ __device__ __forceinline__ void tile16_torus(const LocalPrim& P, const Lane16& Q
 __device__ __forceinline__ void tile16_torus_ring(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
     const float dzs[4] = {Q.dz[0].x, Q.dz[0].y, Q.dz[1].x, Q.dz[1].y};
     const bool mx = mode == 1;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         const Vals<4> r = eval_group_torus_ring<4>(P, Q.dx(g), Q.dy, dzs);
         Group4 a(acc, g, mode);
@@ -1465,7 +1477,7 @@ __device__ __forceinline__ uint32_t tile16_other(const LocalPrim& P, const Lane1
     const int op = P.op;
     const float k = P.k;
     uint32_t edge = 0;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = 0; g < 4; ++g) {
         float4 a = acc[g * 32];
         if (op == CH_OFFSET) {
@@ -1573,6 +1585,13 @@ __device__ __forceinline__ uint32_t tile16(const Geo& G, const FbPrim* __restric
         reinterpret_cast<float4*>(out)[g * 32 + lane] = a;
     }
     return near;
+}
+
+// quotient2 over n pairs (the self-test export fb_quotient_probe).
+__global__ void k_quotient(const float* __restrict__ num, const float* __restrict__ den, float* __restrict__ out,
+                           int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = quotient2(make_float2(num[i], 0.f), make_float2(den[i], 1.f)).x;
 }
 
 // Leaf tiles of a chain recipe: warp per active block.  Each lane owns groups of VG consecutive
@@ -2839,6 +2858,16 @@ int fb_sqrt_sum_probe(const float* d_x, float* d_out, int64_t n, void* stream) n
     if (n == 0) return FB_OK;
     const unsigned grid = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
     k_sqrt_sum<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_x, d_out, n);
+    FB_LAUNCH();
+    return FB_OK;
+}
+
+// The 8^3 tiles' quotient (quotient2) of n device float pairs, stream-ordered.
+int fb_quotient_probe(const float* d_num, const float* d_den, float* d_out, int64_t n, void* stream) noexcept {
+    if (!d_num || !d_den || !d_out || n < 0) return FB_INVALID;
+    if (n == 0) return FB_OK;
+    const unsigned grid = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    k_quotient<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_num, d_den, d_out, n);
     FB_LAUNCH();
     return FB_OK;
 }

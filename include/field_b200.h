@@ -190,6 +190,10 @@ int fb_compact_timeout_probe(const int32_t* d_kind, int64_t n, int32_t* d_active
  * evaluations use (a Newton step from the approximate reciprocal square root): d_out[i] = that root
  * of d_x[i] for n device floats, stream-ordered.  Inputs are sums of squares (>= 0, or NaN). */
 int fb_sqrt_sum_probe(const float* d_x, float* d_out, int64_t n, void* stream);
+/* No counterpart in the reference.  Self-test of the quotient the 8^3 leaf tiles use for the sphere's
+ * difference form (a Newton step from the approximate reciprocal): d_out[i] = d_num[i] / d_den[i] for
+ * n device floats, d_den[i] > 0, stream-ordered. */
+int fb_quotient_probe(const float* d_num, const float* d_den, float* d_out, int64_t n, void* stream);
 
 /* Replace meshsdf_classify_cpu / meshsdf_tiles_cpu, src/field_engine/mesh_sdf_native_v1/field.cpp:229,254,
  * and k_classify_dense / k_eval_tile_dense, src/field_engine/faltkarna_v1_mesh_to_sdf.py:602-657. */
