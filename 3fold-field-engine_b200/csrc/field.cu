@@ -1602,6 +1602,21 @@ __global__ void k_quotient(const float* __restrict__ num, const float* __restric
 // each group with one vector store.  Every lane of the warp calls it with the same block.  kEdge:
 // the recipe has sampled-grid leaves, whose voxels at a table's boundary are marked for the float64
 // recheck (the marks cost registers in the hot loop, so recipes without such leaves leave them out).
+// The float64 recheck of a lane's guard-band voxels (bit g * VG + k: voxel k of its group g).
+template <int B, int VG>
+__device__ __noinline__ void recheck_near(uint32_t near, int lane, float* out, const uint32_t* list, int len,
+                                          const FbInsn* __restrict__ chain, const FbPrim* __restrict__ prims,
+                                          const Geo& G, int bi, int bj, int bk) {
+    while (near) {
+        const int bit = __ffs(near) - 1;
+        near &= near - 1;
+        const int v = ((bit / VG) * 32 + lane) * VG + bit % VG;
+        const int li = v / (B * B), lj = (v / B) % B, lk = v % B;
+        out[v] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li, (int64_t)bj * B + lj,
+                                    (int64_t)bk * B + lk);
+    }
+}
+
 template <int B, bool kEdge>
 __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const PrimF* __restrict__ primf,
                            const FbInsn* __restrict__ chain, const uint32_t* __restrict__ pool,
@@ -1619,7 +1634,17 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
         for (int v = lane; v < kVox; v += 32) out[v] = kBig;
         return;
     }
-    const int bk = (int)(blk % G.nbz), bj = (int)((blk / G.nbz) % G.nby), bi = (int)(blk / ((int64_t)G.nbz * G.nby));
+    int bi, bj, bk;
+    if (G.nblocks <= 0xffffffffll) {  // 32-bit division (grids below 2^32 blocks)
+        const uint32_t b32 = (uint32_t)blk, q = b32 / (uint32_t)G.nbz;
+        bk = (int)(b32 - q * (uint32_t)G.nbz);
+        bj = (int)(q % (uint32_t)G.nby);
+        bi = (int)(q / (uint32_t)G.nby);
+    } else {
+        bk = (int)(blk % G.nbz);
+        bj = (int)((blk / G.nbz) % G.nby);
+        bi = (int)(blk / ((int64_t)G.nbz * G.nby));
+    }
     const double ox = G.x0 + (double)(bi * B) * G.pitch;
     const double oy = G.y0 + (double)(bj * B) * G.pitch;
     const double oz = G.z0 + (double)(bk * B) * G.pitch;
@@ -1741,15 +1766,9 @@ __device__ void leaf_block(const Geo& G, const FbPrim* __restrict__ prims, const
         }
     }
     // guard band: a float64 recheck of the few voxels near zero, so the sign never disagrees with
-    // the float64 value -- after the tile is stored, where little else is live across the call
-    while (near) {
-        const int bit = __ffs(near) - 1;
-        near &= near - 1;
-        const int v = ((bit / VG) * 32 + lane) * VG + bit % VG;
-        const int li = v / (B * B), lj = (v / B) % B, lk = v % B;
-        out[v] = (float)guard_value(list, len, chain, prims, G, (int64_t)bi * B + li, (int64_t)bj * B + lj,
-                                    (int64_t)bk * B + lk);
-    }
+    // the float64 value -- after the tile is stored, in one out-of-line call only where a lane has
+    // such voxels (the call inside the kernel's own loop cost the leaf pass 8 % in registers)
+    if (near) recheck_near<B, VG>(near, lane, out, list, len, chain, prims, G, bi, bj, bk);
 }
 
 // Leaf tiles of a chain recipe: a warp per active block (leaf_block).
