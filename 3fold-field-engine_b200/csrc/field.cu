@@ -1457,15 +1457,33 @@ __device__ __forceinline__ void tile16_torus(const LocalPrim& P, const Lane16& Q
     }
 }
 
-// A torus in its ring frame (leaf kernels built for recipes with such tori).
+// A torus in its ring frame (leaf kernels built for recipes with such tori), on pairs: the
+// operations of eval_group_torus_ring in their order, the fast division per element.
 __device__ __forceinline__ void tile16_torus_ring(const LocalPrim& P, const Lane16& Q, int mode, float4* acc) {
-    const float dzs[4] = {Q.dz[0].x, Q.dz[0].y, Q.dz[1].x, Q.dz[1].y};
+    const float2 L0 = dup2(P.L[0]), L2 = dup2(P.L[2]), R = dup2(P.p[0]), nR = dup2(-P.p[0]), nr = dup2(-P.p[1]);
+    const float2 s = dup2(P.s), noff = dup2(-P.off);
+    const float2 c2 = dup2(P.A[2]), c5 = dup2(P.A[5]), c8 = dup2(P.A[8]);
+    const float a0 = P.A[0], a3 = P.A[3], a6 = P.A[6];
+    const float a1 = P.A[1] * Q.dy, a4 = P.A[4] * Q.dy, a7 = P.A[7] * Q.dy;
     const bool mx = mode == 1;
 #pragma unroll 2
     for (int g = 0; g < 4; ++g) {
-        const Vals<4> r = eval_group_torus_ring<4>(P, Q.dx(g), Q.dy, dzs);
+        const float dx = Q.dx(g);
+        const float2 ebx = dup2(fmaf(a0, dx, a1)), eby = dup2(fmaf(a3, dx, a4)), ebz = dup2(fmaf(a6, dx, a7));
+        float2 v[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float2 u = add2(L0, fma2(c2, Q.dz[j], ebx)), w = fma2(c5, Q.dz[j], eby);
+            const float2 z = add2(L2, fma2(c8, Q.dz[j], ebz));
+            const float2 t = add2(R, u), ww = mul2(w, w);
+            const float2 rho = sqrt_sum2(fma2(t, t, ww));
+            const float2 den = add2(rho, t), far = add2(rho, nR);
+            const float2 qx = make_float2(t.x > 0.f ? u.x + __fdividef(ww.x, den.x) : far.x,
+                                          t.y > 0.f ? u.y + __fdividef(ww.y, den.y) : far.y);
+            v[j] = fma2(s, add2(sqrt_sum2(fma2(z, z, mul2(qx, qx))), nr), noff);
+        }
         Group4 a(acc, g, mode);
-        a.combine(mx, make_float2(r.v[0], r.v[1]), make_float2(r.v[2], r.v[3]));
+        a.combine(mx, v[0], v[1]);
         a.store(acc, g);
     }
 }
