@@ -91,6 +91,12 @@ SIGNATURES = {
     "fb_multires_query_device": (I, [P, D, I, P, D, P, P, P, P, P, I64, P, P, P]),
     "fb_grid_pairs_device": (I, [P, I, P, P, I64, P, P, I, P, P]),
     "fb_multires_band_device": (I, [P, D, I, P, P, P, P, P, I64, P, P, P, P, P]),
+    # EDT consumers: clearance, valid mask, lattice Laplacian
+    "fb_edt_mm_device": (I, [P, I64, D, P, P]),
+    "fb_clearance_mask_device": (I, [P, P, I64, D, P, P]),
+    "fb_lattice_scratch_bytes": (I64, [I, I, I]),
+    "fb_lattice_count_device": (I, [P, I, I, I, P, P, I64, P]),
+    "fb_lattice_emit_device": (I, [P, P, I, I, I, D, D, P, P, P, P, P, P, P, P, I64, P]),
 }
 
 

@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--check-bricks", type=int, default=24, help="precision: bricks checked per level")
-    ap.add_argument("--workload", choices=("batched", "plain", "serve", "precision", "tree", "mesh"), default="batched",
+    ap.add_argument("--workload", choices=("batched", "plain", "serve", "precision", "tree", "mesh", "clearance"), default="batched",
                     help="batched: 256 recipes built as one batch against recipe by recipe (default line); plain: "
                          "the plain method at scale; serve: the request loop; precision: float32 vs float64 at "
                          "mixed pitch; tree: packed adaptive block tree of a dense 512^3 field, built and sampled; "
@@ -1027,6 +1027,135 @@ def run_tree(args, n=512, samples=50_000_000):
     }
 
 
+def run_clearance(args, pitch=0.01):
+    """EDT consumers on the default EDT's obstacle grid (n^3, 2000 boxes, 8 % fill) as the route
+    network of laplaceflode_v1.rutt_genom_flode's first steps: the squared EDT to the occupied cells,
+    the clearance in mm, the validity mask, and the lattice Laplacian (count pass, scans, node map,
+    edges and CSR).  Device-resident steps through the C ABI with preallocated outputs (CUDA events,
+    L2 flushed between steps); end to end through field_b200.clearance.fritt_natverk with NumPy in
+    and NumPy/scipy out; the oracle's NumPy restatement timed on a 128^3 crop beside it."""
+    import torch
+    import field_b200._lib as L_
+    import field_b200.clearance as C
+    import field_b200.recipes as R
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n = args.edt_n
+    occ_np = R.obstacle_grid(seed=2, n=n, n_boxes=2000, fill=0.08).astype(bool)
+    occ = torch.from_numpy(occ_np.view(np.uint8)).to(dev)
+    L = L_.lib()
+    st = L_.stream_handle()
+    V = occ.numel()
+    sq = torch.empty(occ.shape, dtype=torch.int32, device=dev)
+    edt_scr = torch.empty(int(L.fb_edt_scratch_bytes(n, n, n, 0)), dtype=torch.uint8, device=dev)
+    E = torch.empty(occ.shape, dtype=torch.float64, device=dev)
+    valid = torch.empty(occ.shape, dtype=torch.uint8, device=dev)
+    lat_scr = torch.empty(int(L.fb_lattice_scratch_bytes(n, n, n)), dtype=torch.uint8, device=dev)
+    totals = torch.empty(3, dtype=torch.int32, device=dev)
+    L.fb_lattice_count_device(occ.data_ptr(), n, n, n, totals.data_ptr(), lat_scr.data_ptr(), lat_scr.numel(), st)
+    nodes, n_edges, nnz = (int(x) for x in totals.cpu().tolist())
+    node_map = torch.empty(occ.shape, dtype=torch.int32, device=dev)
+    u = torch.empty(n_edges, dtype=torch.int32, device=dev)
+    v = torch.empty(n_edges, dtype=torch.int32, device=dev)
+    kond = torch.empty(n_edges, dtype=torch.float64, device=dev)
+    indptr = torch.empty(nodes + 1, dtype=torch.int32, device=dev)
+    indices = torch.empty(nnz, dtype=torch.int32, device=dev)
+    data = torch.empty(nnz, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    threshold = 1.0 + 2.0 * pitch
+
+    def step():
+        rc = [0] * 5
+        ev[0].record()
+        rc[0] = L.fb_edt_squared_device(occ.data_ptr(), n, n, n, 1, sq.data_ptr(), edt_scr.data_ptr(), edt_scr.numel(), st)
+        rc[1] = L.fb_edt_mm_device(sq.data_ptr(), V, pitch, E.data_ptr(), st)
+        ev[1].record()
+        rc[2] = L.fb_clearance_mask_device(occ.data_ptr(), E.data_ptr(), V, threshold, valid.data_ptr(), st)
+        ev[2].record()
+        rc[3] = L.fb_lattice_count_device(occ.data_ptr(), n, n, n, totals.data_ptr(), lat_scr.data_ptr(),
+                                          lat_scr.numel(), st)
+        ev[3].record()
+        rc[4] = L.fb_lattice_emit_device(occ.data_ptr(), E.data_ptr(), n, n, n, pitch, 1.5, node_map.data_ptr(),
+                                         u.data_ptr(), v.data_ptr(), kond.data_ptr(), indptr.data_ptr(),
+                                         indices.data_ptr(), data.data_ptr(), lat_scr.data_ptr(), lat_scr.numel(), st)
+        ev[4].record()
+        assert not any(rc), rc
+
+    phases = []
+    for i in range(max(args.warmup, 3) + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        step()
+        torch.cuda.synchronize()
+        if i >= max(args.warmup, 3):
+            phases.append([ev[k].elapsed_time(ev[k + 1]) for k in range(4)])
+    clocks = ClockSampler(0)
+    clocks.start()
+    tt = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        tt.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    assert [int(x) for x in totals.cpu().tolist()] == [nodes, n_edges, nnz]
+    ms = statistics.median(tt)
+    ph = [statistics.median(p[k] for p in phases) for k in range(4)]
+    peak, peak_src = measured_peaks()
+    # algorithmic bytes of the lattice passes: occupancy read by the count, node and emit passes
+    # (3 B per cell), node map written and read (8 B), clearance read (8 B), row starts (4 B per node),
+    # edges (16 B), CSR entries (12 B)
+    lat_bytes = 3.0 * V + 8.0 * V + 8.0 * V + 4.0 * (nodes + 1) + 16.0 * n_edges + 12.0 * nnz
+    lat_ms = ph[2] + ph[3]
+    lat_gbs = lat_bytes / (lat_ms * 1e-3) / 1e9
+    # end to end: NumPy occupancy in, NumPy arrays and a scipy CSR out
+    e2e_ms, d2h = [], 0
+    for _ in range(0 if args.no_e2e else 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = C.fritt_natverk(occ_np, pitch)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        d2h = sum(int(getattr(a, "nbytes", 0)) for a in res if isinstance(a, np.ndarray))
+        d2h += res[-1].data.nbytes + res[-1].indices.nbytes + res[-1].indptr.nbytes
+        del res
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        crop = np.ascontiguousarray(occ_np[:128, :128, :128])
+        t0 = time.perf_counter()
+        Ec = oracle.clearance_mm(crop, pitch)
+        oracle.lattice_laplacian(crop, Ec, pitch, 1.5)
+        dt = time.perf_counter() - t0
+        cpu = {"value": crop.size / dt / 1e9, "unit": "Gvox/s", "cores": len(os.sched_getaffinity(0)), "kind": "port",
+               "sample": "oracle clearance (C EDT) + NumPy lattice Laplacian of a 128^3 crop of the same grid"}
+    e2e = min(e2e_ms) if e2e_ms else None
+    return {
+        "metric": "EDT consumers: grid cells/s (clearance, validity mask, lattice Laplacian)",
+        "workload": f"clearance_network_{n}^3", "value": V / (ms * 1e-3) / 1e9, "unit": "Gvox/s",
+        "higher_is_better": True, "steps": args.steps, "ms_per_step": ms,
+        "phases_ms": {"edt_and_clearance": ph[0], "validity_mask": ph[1], "lattice_count": ph[2],
+                      "lattice_nodes_and_emit": ph[3]},
+        "nodes": nodes, "edges": n_edges, "csr_entries": nnz,
+        "roofline": {"bound": "hbm", "kernel": "lattice passes (count, scans, nodes, emit)", "achieved": lat_gbs,
+                     "peak": peak, "unit": "GB/s", "frac": lat_gbs / peak, "peak_source": peak_src,
+                     "basis": "3 B occupancy + 8 B node map + 8 B clearance per cell, 4 B per node, "
+                              "16 B per edge, 12 B per CSR entry", "bytes": lat_bytes},
+        "e2e": None if e2e is None else {"value": V / (e2e * 1e-3) / 1e9, "unit": "Gvox/s", "ms": e2e,
+                                         "h2d_bytes_per_step": int(occ_np.nbytes), "d2h_bytes_per_step": int(d2h)},
+        # per step: squared EDT 3 (bits, zy, x), clearance 1, mask 1, lattice count 1 + three
+        # two-level scans of 3 each, node map 1, emit 1
+        "gpu_launches": 17 * args.steps, "cpu_baseline": cpu, "clocks": clk, "dtype": "u8 in, int32 + f64 out",
+        "data": "synthetic",
+        "config": {"workload": f"clearance_network_{n}^3_2000boxes_8pct", "grid": [n, n, n], "pitch_mm": pitch,
+                   "p_kond": 1.5, "l2": "256 MiB flush between steps"},
+    }
+
+
 def run_mesh(args, pitch=0.08):
     """Mesh -> signed distance field (ray-winding solid, paired exact EDT, surface layer) of a seeded
     scene of a sphere, a rotated box and a torus (about 55 k triangles) on a grid of pitch 0.08 mm
@@ -1173,8 +1302,8 @@ def main():
     args = parse()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(spawn_ranks(args.gpus))
-    if args.impl == "ours" and args.workload in ("serve", "precision", "tree", "mesh"):
-        fn = {"precision": run_precision, "tree": run_tree, "mesh": run_mesh,
+    if args.impl == "ours" and args.workload in ("serve", "precision", "tree", "mesh", "clearance"):
+        fn = {"precision": run_precision, "tree": run_tree, "mesh": run_mesh, "clearance": run_clearance,
               "serve": lambda a: run_serve(a, rate=a.rate, seconds=a.seconds)}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return

@@ -374,6 +374,32 @@ int fb_mesh_components_device(const int32_t* d_faces, int64_t n_faces, const flo
                               int32_t* d_parent, int32_t* d_label, double* d_comp_volume, int32_t* d_count,
                               int32_t* d_err, void* stream);
 
+/* ------------------------------------------------------------------------------------------ EDT consumers */
+
+/* Clearance in millimetres, float64(sqrt(sq)) * pitch: replaces `distance_transform_edt(~occ) * pitch_mm`
+ * of src/field_engine/opt/laplaceflode_v1.py:313-314 and opt/f33_1_topologi_v1.py:205-206, fed by
+ * fb_edt_squared_device with sites_nonzero = 1 on the occupancy. */
+int fb_edt_mm_device(const int32_t* d_sq, int64_t n, double pitch, double* d_out, void* stream);
+/* d_valid[i] = !occ[i] && edt_mm[i] >= threshold (threshold = min_r + margin, formed by the caller in
+ * float64): replaces `free & (edt_mm >= min_r_mm + margin_mm)`, opt/f33_1_topologi_v1.py:207-208. */
+int fb_clearance_mask_device(const uint8_t* d_occ, const double* d_edt_mm, int64_t n, double threshold,
+                             uint8_t* d_valid, void* stream);
+/* The free space of an occupancy grid as a resistor network, replacing bygg_gitterlaplacian,
+ * src/field_engine/opt/laplaceflode_v1.py:69-97.  Two calls on one stream with the same scratch:
+ * fb_lattice_count_device writes d_totals = {nodes, edges, CSR entries} (int32, device); the caller
+ * sizes the outputs from them and fb_lattice_emit_device writes the node map (nx*ny*nz int32, -1 on
+ * occupied cells), the edges u, v, kond (axis 0, 1, 2; lower cell ascending; kond = max(0.5 (E_u +
+ * E_v) / pitch, 0.1)^p_kond) and the CSR Laplacian (indptr[nodes + 1], indices and data[entries]:
+ * columns ascending, -kond off the diagonal, the diagonal summed in scipy's COO order).  At most
+ * (2^31 - 1) / 7 cells (status 1 beyond); fb_lattice_scratch_bytes returns -1 for such shapes. */
+int64_t fb_lattice_scratch_bytes(int nx, int ny, int nz);
+int fb_lattice_count_device(const uint8_t* d_occ, int nx, int ny, int nz, int32_t* d_totals, void* d_scratch,
+                            int64_t scratch_len, void* stream);
+int fb_lattice_emit_device(const uint8_t* d_occ, const double* d_edt_mm, int nx, int ny, int nz, double pitch,
+                           double p_kond, int32_t* d_node_map, int32_t* d_u, int32_t* d_v, double* d_kond,
+                           int32_t* d_indptr, int32_t* d_indices, double* d_data, const void* d_scratch,
+                           int64_t scratch_len, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

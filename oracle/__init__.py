@@ -755,3 +755,74 @@ def mesh_volume(verts, faces):
     v = np.asarray(verts, np.float64)
     a, b, c = v[faces[:, 0]], v[faces[:, 1]], v[faces[:, 2]]
     return float(np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6.0)
+
+
+# ------------------------------------------------------------------------- EDT consumers
+def clearance_mm(occ, pitch):
+    """float64 clearance of every cell to the nearest occupied one times the pitch: scipy's
+    ``distance_transform_edt(~occ) * pitch`` (src/field_engine/opt/laplaceflode_v1.py:313-314),
+    restated as the float64 root of the oracle's exact squared EDT to the occupied cells."""
+    occ = np.asarray(occ, bool)
+    sq = edt_squared(~occ)  # zeros of ~occ are the occupied cells
+    return np.sqrt(sq.astype(np.float64)) * float(pitch)
+
+
+def lattice_laplacian(occ, edt_mm, pitch, p_kond=1.5):
+    """Restatement of bygg_gitterlaplacian (src/field_engine/opt/laplaceflode_v1.py:69-97) that
+    builds the CSR directly instead of through a COO sum: returns (n, node_map, u, v, kond, indptr,
+    indices, data).  Rows list their columns ascending (p - sx, p - sy, p - 1, p, p + 1, p + sy,
+    p + sx in C order); the diagonal is the left-to-right sum of the row's conductances in the COO's
+    order (the cell as lower end of its axis 0, 1, 2 edges, then as upper end), which is the order
+    scipy's sum_duplicates adds them in.  Absent edges add 0.0, which leaves every sum unchanged."""
+    occ = np.asarray(occ, bool)
+    shape3 = (1,) * (3 - occ.ndim) + occ.shape
+    fri = ~occ.reshape(shape3)
+    E = np.asarray(edt_mm, np.float64).reshape(shape3)
+    n = int(fri.sum())
+    node = np.full(shape3, -1, np.int32)
+    node[fri] = np.arange(n, dtype=np.int32)
+    fwd, bwd, kf, kb = [], [], [], []
+    U, V, K = [], [], []
+    for a in range(3):
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[a], hi[a] = slice(None, -1), slice(1, None)
+        lo, hi = tuple(lo), tuple(hi)
+        e = np.zeros(shape3, bool)
+        e[lo] = fri[lo] & fri[hi]          # cell is the lower end of an axis-a edge
+        b = np.zeros(shape3, bool)
+        b[hi] = e[lo]                      # cell is the upper end of one
+        c = np.zeros(shape3)
+        c[lo] = 0.5 * (E[lo] + E[hi]) / pitch
+        k = np.where(e, np.maximum(c, 0.1) ** p_kond, 0.0)
+        kup = np.zeros(shape3)
+        kup[hi] = k[lo]
+        fwd.append(e)
+        bwd.append(b)
+        kf.append(k)
+        kb.append(kup)
+        U.append(node[lo][e[lo]])
+        V.append(node[hi][e[lo]])
+        K.append(k[lo][e[lo]])
+    u, v, kond = np.concatenate(U), np.concatenate(V), np.concatenate(K)
+    strides = (shape3[1] * shape3[2], shape3[2], 1)
+    lin = np.arange(fri.size).reshape(shape3)
+    diag = ((((kf[0] + kf[1]) + kf[2]) + kb[0]) + kb[1]) + kb[2]
+    deg = sum(x.astype(np.int64) for x in fwd + bwd)
+    has = fri & (deg > 0)
+    # slots in column order: -x, -y, -z, diagonal, +z, +y, +x
+    present = [bwd[0], bwd[1], bwd[2], has, fwd[2], fwd[1], fwd[0]]
+    cols = [lin - strides[0], lin - strides[1], lin - strides[2], lin, lin + strides[2], lin + strides[1],
+            lin + strides[0]]
+    vals = [-kb[0], -kb[1], -kb[2], diag, -kf[2], -kf[1], -kf[0]]
+    cells = np.nonzero(fri.ravel())[0]
+    P = np.stack([p.ravel()[cells] for p in present], axis=1)
+    C = np.stack([np.where(p.ravel()[cells], node.ravel()[np.clip(c.ravel()[cells], 0, fri.size - 1)], 0)
+                  for p, c in zip(present, cols)], axis=1)
+    Vv = np.stack([x.ravel()[cells] for x in vals], axis=1)
+    counts = P.sum(axis=1)
+    indptr = np.zeros(n + 1, np.int32)
+    np.cumsum(counts, out=indptr[1:])
+    indices = C[P].astype(np.int32)
+    data = Vv[P]
+    return n, node.reshape(occ.shape), u, v, kond, indptr, indices, data
