@@ -445,42 +445,100 @@ class _Compiler:
         return len(self.prims) - 1
 
     # ---- general postfix emission (no re-association)
-    def emit(self, node, M, sigma, out):
+    # The deeper operand of each boolean is evaluated first (Sethi-Ullman order), so a tree of N
+    # leaves needs at most log2(N) + 1 stack slots whatever its shape.  Union and intersection are
+    # symmetric in their operands (the same value bits: min / max and |a - b| do not depend on the
+    # order); subtract(a, b) with the deeper b is evaluated as intersect(-b, a), the same float64
+    # operations as max(a, -b) + h^2 k / 4 with h from |a + b|.  A negated subtree is emitted with a
+    # negative output scale: leaves get s < 0 and off < 0 (value = s f - off, negation is exact in
+    # round-to-nearest), offsets flip with it, union and intersection swap, and -subtract(a, b) is
+    # union(-a, b).
+    def _stack_need(self, node, memo):
+        """Stack slots the postfix program of ``node`` needs in the deeper-operand-first order."""
+        key = id(node)
+        if key in memo:
+            return memo[key]
+        op = node["op"]
+        if op in LEAF_OPS:
+            r = 1
+        elif op in ("transform", "scale", "axis_project", "offset"):
+            r = self._stack_need(node["child"], memo)
+        elif op in ("union", "intersect", "subtract"):
+            spine = []
+            cur = node
+            while cur["op"] in ("union", "intersect", "subtract") and id(cur) not in memo:
+                spine.append(cur)
+                cur = cur["a"]
+            r = self._stack_need(cur, memo)
+            for nd in reversed(spine):
+                nb = self._stack_need(nd["b"], memo)
+                r = max(r, nb) if r != nb else r + 1
+                memo[id(nd)] = r
+        else:
+            raise ValueError(f"unknown op {op!r}")
+        memo[key] = r
+        return r
+
+    def emit(self, node, M, sigma, out, memo=None):
+        if memo is None:
+            memo = {}
         op = node["op"]
         if op in LEAF_OPS:
             out.append((OP_PUSH, self.leaf(node, M, sigma), 0.0))
         elif op == "transform":
-            self.emit(node["child"], np.asarray(mat4_inverse_affine(node["mat4"])) @ M, sigma, out)
+            self.emit(node["child"], np.asarray(mat4_inverse_affine(node["mat4"])) @ M, sigma, out, memo)
         elif op == "scale":
             s = float(node["s"])
             if not s > 0:
                 raise ValueError("scale factor must be positive")
-            self.emit(node["child"], np.diag([1 / s, 1 / s, 1 / s, 1.0]) @ M, sigma * s, out)
+            self.emit(node["child"], np.diag([1 / s, 1 / s, 1 / s, 1.0]) @ M, sigma * s, out, memo)
         elif op == "axis_project":
             Pm = np.eye(4)
             Pm[node["axis"], :] = 0.0
             Pm[node["axis"], 3] = node["ref"]
-            self.emit(node["child"], Pm @ M, sigma, out)
+            self.emit(node["child"], Pm @ M, sigma, out, memo)
         elif op == "offset":
             n0 = len(out)
-            self.emit(node["child"], M, sigma, out)
+            self.emit(node["child"], M, sigma, out, memo)
             if len(out) == n0 + 1 and out[-1][0] == OP_PUSH:
                 self.prims[out[-1][1]]["off"] += sigma * node["delta"]
             else:
                 out.append((OP_OFFSET, -1, sigma * node["delta"]))
         elif op in ("union", "intersect", "subtract"):
-            spine = []
+            # the run of the left spine evaluated left operand first, iteratively (recipes are
+            # left-deep chains thousands of operations long); it ends at a leaf-side operand or at a
+            # node whose right operand is the deeper one, which recurses
+            run = []
             cur = node
-            while cur["op"] in ("union", "intersect", "subtract"):
-                spine.append(cur)
+            while cur["op"] in ("union", "intersect", "subtract") and (
+                    self._stack_need(cur["b"], memo) <= self._stack_need(cur["a"], memo)):
+                run.append(cur)
                 cur = cur["a"]
-            self.emit(cur, M, sigma, out)
-            for nd in reversed(spine):
-                self.emit(nd["b"], M, sigma, out)
-                code = {"union": OP_UNION, "intersect": OP_INTERSECT, "subtract": OP_SUBTRACT}[nd["op"]]
-                out.append((code, -1, sigma * nd["k"]))
+            if cur["op"] in ("union", "intersect", "subtract"):
+                code, sb = self._bool_code(cur["op"], sigma, b_first=True)
+                self.emit(cur["b"], M, sb, out, memo)
+                self.emit(cur["a"], M, sigma, out, memo)
+                out.append((code, -1, abs(sigma) * cur["k"]))
+            else:
+                self.emit(cur, M, sigma, out, memo)
+            for nd in reversed(run):
+                code, sb = self._bool_code(nd["op"], sigma, b_first=False)
+                self.emit(nd["b"], M, sb, out, memo)
+                out.append((code, -1, abs(sigma) * nd["k"]))
         else:
             raise ValueError(f"unknown op {op!r}")
+
+    @staticmethod
+    def _bool_code(op, sigma, b_first):
+        """Opcode and the right operand's output scale of boolean `op` under output scale `sigma`
+        (the left operand always keeps `sigma`)."""
+        if sigma > 0:
+            if op == "subtract":
+                return (OP_INTERSECT, -sigma) if b_first else (OP_SUBTRACT, sigma)
+            return (OP_UNION if op == "union" else OP_INTERSECT), sigma
+        if op == "subtract":  # -(a - b) = union(-a, b)
+            return OP_UNION, -sigma
+        return (OP_INTERSECT if op == "union" else OP_UNION), sigma
 
     # ---- chain emission: returns list of (CH_op, prim, k) or None
     def chain(self, node, M, sigma):
@@ -608,7 +666,7 @@ def compile_recipe(node) -> Compiled:
     for op, _, _ in prog:
         depth += 1 if op == OP_PUSH else (0 if op == OP_OFFSET else -1)
         max_depth = max(max_depth, depth)
-    if max_depth > 32:
+    if max_depth > 32:  # reachable only with more than 2^31 leaves (deeper operand first)
         raise ValueError("expression tree too deep for the GPU stack evaluator (depth > 32)")
     prims = np.array(c.prims, dtype=PRIM) if c.prims else np.zeros(0, PRIM)
     return Compiled(prims, _records(prog), None, c.tables)

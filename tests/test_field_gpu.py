@@ -152,3 +152,26 @@ def test_compaction_wait_runs_out_and_reports():
     dense = np.random.default_rng(3).normal(size=(40, 36, 44)).astype(np.float32)
     r = B.klassificera_och_evaluera_fran_tatt_falt(None, dense, 0.5, 4)
     assert (r["active_ids"] == np.where(r["kind"] == 0)[0]).all()
+
+
+def test_deep_general_programs_match_oracle(fb):
+    """Right-deep smooth trees (120 operands; a deep subtracted subtree; a negated subtract inside
+    one) compile in the deeper-operand-first order and build on the GPU's float64 program path."""
+    import field_b200.expr as X
+    from field_b200.grid import GridMeta
+    rng = np.random.default_rng(5)
+    sph = [X.sphere(float(rng.uniform(0.03, 0.1)), tuple(rng.uniform(0.15, 0.85, 3))) for _ in range(160)]
+    chain = sph[119]
+    for nd in reversed(sph[:119]):
+        chain = X.union(nd, chain, k=float(rng.choice([0.0, 0.02])))
+    inner = sph[159]
+    for nd in reversed(sph[120:159]):
+        inner = X.intersect(X.offset(nd, -0.1), inner, k=0.01)
+    trees = [X.subtract(X.box((0.4, 0.4, 0.4), (0.5, 0.5, 0.5)), chain, k=0.03),
+             X.subtract(X.sphere(0.45, (0.5, 0.5, 0.5)), X.subtract(X.box((0.3, 0.3, 0.3), (0.5, 0.5, 0.5)), inner,
+                                                                      k=0.02), k=0.02)]
+    meta = GridMeta(0.0, 0.0, 0.0, 1.0 / 64, 65, 64, 66, 8)
+    for t in trees:
+        comp = X.compile_recipe(t)
+        assert comp.chain is None and (comp.prims["s"] < 0).any()
+        _check_against_oracle(t, meta, fb)
