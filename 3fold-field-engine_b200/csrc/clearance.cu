@@ -48,16 +48,23 @@ struct VoxelFlags {
 
 __device__ __forceinline__ VoxelFlags voxel_flags(const uint8_t* __restrict__ occ, const LatGrid& g, int64_t p) {
     VoxelFlags f{};
-    if (p >= g.n || occ[p]) return f;
-    const int64_t yz = p % g.sx;
-    const int x = (int)(p / g.sx), y = (int)(yz / g.nz), z = (int)(yz - (int64_t)y * g.nz);
+    if (p >= g.n) return f;
+    // cell counts stay below 2^31 (the entry points' limit): 32-bit index arithmetic; the seven
+    // occupancy bytes are loaded independently of each other
+    const uint32_t q = (uint32_t)p, sx = (uint32_t)g.sx, nz = (uint32_t)g.nz;
+    const uint32_t x = q / sx, yz = q - x * sx, y = yz / nz, z = yz - y * nz;
+    const bool self = occ[q] != 0;
+    const bool fx = x + 1 < (uint32_t)g.nx && !occ[q + sx], bx = x > 0 && !occ[q - sx];
+    const bool fy = y + 1 < (uint32_t)g.ny && !occ[q + nz], by = y > 0 && !occ[q - nz];
+    const bool fz = z + 1 < nz && !occ[q + 1], bz = z > 0 && !occ[q - 1];
+    if (self) return f;
     f.free = 1;
-    f.e0 = (x + 1 < g.nx && !occ[p + g.sx]) ? 1u : 0u;
-    f.e1 = (y + 1 < g.ny && !occ[p + g.sy]) ? 1u : 0u;
-    f.e2 = (z + 1 < g.nz && !occ[p + 1]) ? 1u : 0u;
-    f.b0 = (x > 0 && !occ[p - g.sx]) ? 1u : 0u;
-    f.b1 = (y > 0 && !occ[p - g.sy]) ? 1u : 0u;
-    f.b2 = (z > 0 && !occ[p - 1]) ? 1u : 0u;
+    f.e0 = fx;
+    f.e1 = fy;
+    f.e2 = fz;
+    f.b0 = bx;
+    f.b1 = by;
+    f.b2 = bz;
     const uint32_t deg = f.e0 + f.e1 + f.e2 + f.b0 + f.b1 + f.b2;
     f.row = deg ? deg + 1 : 0;
     return f;
@@ -157,13 +164,12 @@ __global__ void __launch_bounds__(kLatThreads) k_lat_nodes(const uint8_t* __rest
     }
 }
 
-// Conductance of the edge between voxels a < b: max(0.5 (E_a + E_b) / pitch, 0.1)^p, in the
+// Conductance of the edge between cells a < b from their clearances: max(0.5 (E_a + E_b) / pitch, 0.1)^p, in the
 // reference's operation order (NaN propagates through the max as in np.maximum).  The reference's
 // exponent 1.5 is m * sqrt(m) (correctly rounded root, one rounding of the product: within 2 ulp
 // of libm's pow, as CUDA's pow is), 0 and 1 are exact; other exponents call pow.
-__device__ __forceinline__ double conductance(const double* __restrict__ edt_mm, int64_t a, int64_t b, double pitch,
-                                              double p_kond) {
-    const double c = __ddiv_rn(__dmul_rn(0.5, __dadd_rn(edt_mm[a], edt_mm[b])), pitch);
+__device__ __forceinline__ double conductance(double ea, double eb, double pitch, double p_kond) {
+    const double c = __ddiv_rn(__dmul_rn(0.5, __dadd_rn(ea, eb)), pitch);
     const double m = (c != c) ? c : (c > kConductanceFloor ? c : kConductanceFloor);
     if (p_kond == 1.5) return __dmul_rn(m, __dsqrt_rn(m));
     if (p_kond == 1.0) return m;
@@ -198,21 +204,32 @@ __global__ void __launch_bounds__(kLatThreads, 4) k_lat_emit(const uint8_t* __re
     for (int r = 0; r < kLatRounds; ++r) {
         const int64_t p = base + r * kLatThreads + threadIdx.x;
         const VoxelFlags f = voxel_flags(occ, g, p);
+        // every load of the cell's row is issued before the round's block scan, so its latency
+        // overlaps the scan's barriers
+        double ec = 0.0, exp_ = 0.0, eyp = 0.0, ezp = 0.0, exm = 0.0, eym = 0.0, ezm = 0.0;
+        int32_t id = 0, nxp = 0, nyp = 0, nxm = 0, nym = 0;
+        if (f.free) {
+            ec = edt_mm[p];
+            id = node_map[p];
+            if (f.e0) { exp_ = edt_mm[p + g.sx]; nxp = node_map[p + g.sx]; }
+            if (f.e1) { eyp = edt_mm[p + g.sy]; nyp = node_map[p + g.sy]; }
+            if (f.e2) ezp = edt_mm[p + 1];
+            if (f.b0) { exm = edt_mm[p - g.sx]; nxm = node_map[p - g.sx]; }
+            if (f.b1) { eym = edt_mm[p - g.sy]; nym = node_map[p - g.sy]; }
+            if (f.b2) ezm = edt_mm[p - 1];
+        }
         uint64_t tot;
         const uint64_t pre = block_scan4((uint64_t)f.e0 | ((uint64_t)f.e1 << 16) | ((uint64_t)f.e2 << 32) |
                                              ((uint64_t)f.row << 48),
                                          s_warp, tot);
         if (f.free) {
-            const int32_t id = node_map[p];
-            // conductances: forward edges (p is the lower end), then backward ones
-            const double kf0 = f.e0 ? conductance(edt_mm, p, p + g.sx, pitch, p_kond) : 0.0;
-            const double kf1 = f.e1 ? conductance(edt_mm, p, p + g.sy, pitch, p_kond) : 0.0;
-            const double kf2 = f.e2 ? conductance(edt_mm, p, p + 1, pitch, p_kond) : 0.0;
-            const double kb0 = f.b0 ? conductance(edt_mm, p - g.sx, p, pitch, p_kond) : 0.0;
-            const double kb1 = f.b1 ? conductance(edt_mm, p - g.sy, p, pitch, p_kond) : 0.0;
-            const double kb2 = f.b2 ? conductance(edt_mm, p - 1, p, pitch, p_kond) : 0.0;
-            const int32_t nxp = f.e0 ? node_map[p + g.sx] : 0, nyp = f.e1 ? node_map[p + g.sy] : 0;
-            const int32_t nxm = f.b0 ? node_map[p - g.sx] : 0, nym = f.b1 ? node_map[p - g.sy] : 0;
+            // conductances: forward edges (the cell is the lower end), then backward ones
+            const double kf0 = f.e0 ? conductance(ec, exp_, pitch, p_kond) : 0.0;
+            const double kf1 = f.e1 ? conductance(ec, eyp, pitch, p_kond) : 0.0;
+            const double kf2 = f.e2 ? conductance(ec, ezp, pitch, p_kond) : 0.0;
+            const double kb0 = f.b0 ? conductance(exm, ec, pitch, p_kond) : 0.0;
+            const double kb1 = f.b1 ? conductance(eym, ec, pitch, p_kond) : 0.0;
+            const double kb2 = f.b2 ? conductance(ezm, ec, pitch, p_kond) : 0.0;
             if (f.e0) {
                 const int k = (int)field16(pre, 0);
                 s_eu[0][k] = id;
