@@ -35,9 +35,30 @@ constexpr int kLatRounds = 8;
 constexpr int kLatTile = kLatThreads * kLatRounds;
 constexpr double kConductanceFloor = 0.1;  // laplaceflode_v1.py KONDUKTANS_GOLV
 
+// Division of 32-bit unsigned integers by an invariant divisor d >= 1 through a multiply
+// (Granlund and Montgomery, "Division by invariant integers using multiplication", PLDI 1994):
+// s = ceil(log2 d), m = floor(2^32 (2^s - d) / d) + 1, n / d = (mulhi(n, m) + n) >> s for every
+// 32-bit n (the sum taken in 64 bits).
+struct FastDiv {
+    uint32_t d, m;
+    int s;
+    static FastDiv of(uint32_t d) {
+        FastDiv f;
+        f.d = d;
+        f.s = 0;
+        while (f.s < 32 && (uint64_t(1) << f.s) < d) ++f.s;
+        f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << f.s) - d)) / d + 1);
+        return f;
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const {
+        return (uint32_t)(((uint64_t)__umulhi(n, m) + n) >> s);
+    }
+};
+
 struct LatGrid {
     int nx, ny, nz;
     int64_t sx, sy, n;  // strides of axes 0 and 1 (axis 2 is contiguous), voxel count
+    FastDiv div_sx, div_nz;
 };
 
 // Occupancy flags of voxel p: free, free forward neighbours along axes 0/1/2 (the edges p owns as
@@ -52,7 +73,7 @@ __device__ __forceinline__ VoxelFlags voxel_flags(const uint8_t* __restrict__ oc
     // cell counts stay below 2^31 (the entry points' limit): 32-bit index arithmetic; the seven
     // occupancy bytes are loaded independently of each other
     const uint32_t q = (uint32_t)p, sx = (uint32_t)g.sx, nz = (uint32_t)g.nz;
-    const uint32_t x = q / sx, yz = q - x * sx, y = yz / nz, z = yz - y * nz;
+    const uint32_t x = g.div_sx.div(q), yz = q - x * sx, y = g.div_nz.div(yz), z = yz - y * nz;
     const bool self = occ[q] != 0;
     const bool fx = x + 1 < (uint32_t)g.nx && !occ[q + sx], bx = x > 0 && !occ[q - sx];
     const bool fy = y + 1 < (uint32_t)g.ny && !occ[q + nz], by = y > 0 && !occ[q - nz];
@@ -321,6 +342,8 @@ bool lat_shape(int nx, int ny, int nz, LatGrid& g) {
     g.sy = nz;
     g.sx = (int64_t)ny * nz;
     g.n = n;
+    g.div_sx = FastDiv::of((uint32_t)g.sx);
+    g.div_nz = FastDiv::of((uint32_t)nz);
     return true;
 }
 
