@@ -17,7 +17,9 @@ as a resistor network, with the reference's signatures.
 
 Arguments given as NumPy arrays return NumPy arrays (and a ``scipy.sparse.csr_matrix`` for the
 Laplacian, as the reference does); CUDA tensors return CUDA tensors (the Laplacian as a
-``torch.sparse_csr_tensor``).  Every computation runs on the GPU.
+``torch.sparse_csr_tensor``).  Every computation runs on the GPU.  Host results are NumPy arrays
+over pooled page-locked blocks, read back with one synchronisation; a block returns to the pool when
+its array is dropped.
 
 Bit-exact against the reference: the node map, ``u``, ``v``, the CSR structure, the clearance and the
 mask.  The conductances take ``pow`` from CUDA's math library where NumPy takes the host's libm, so
@@ -43,6 +45,39 @@ MAX_CELLS = (2 ** 31 - 1) // 7
 def _torch():
     import torch
     return torch
+
+
+_POOL = None
+
+
+def _host_arrays(tensors):
+    """NumPy arrays of device tensors over pooled page-locked blocks: every copy is enqueued on the
+    current stream, then one synchronisation.  A block returns to the pool when its array (or the
+    last object sharing its memory) is dropped, so repeated calls reuse page-locked memory instead
+    of faulting in fresh pageable pages at every call."""
+    global _POOL
+    torch = _torch()
+    if _POOL is None:
+        from .serve import PinnedPool
+        _POOL = PinnedPool()
+    staged = []
+    for t in tensors:
+        nbytes = t.numel() * t.element_size()
+        if nbytes == 0:
+            staged.append((torch.empty(tuple(t.shape), dtype=t.dtype), None))
+            continue
+        blk, handle = _POOL.take(nbytes)
+        view = blk.view(t.dtype).view(tuple(t.shape))
+        view.copy_(t, non_blocking=True)
+        staged.append((view, handle))
+    torch.cuda.current_stream().synchronize()
+    out = []
+    for view, handle in staged:
+        a = view.numpy()
+        if handle is not None:
+            _POOL.bind(a, handle)
+        out.append(a)
+    return out
 
 
 def _as_device_occ(occ):
@@ -106,7 +141,7 @@ def edt_mm(occ, pitch_mm):
     st = _lib.lib().fb_edt_mm_device(sq.data_ptr(), sq.numel(), pitch, out.data_ptr(), _lib.stream_handle())
     _lib.check(st, 'edt_mm')
     out = out.reshape(shape)
-    return out.cpu().numpy() if host else out
+    return _host_arrays([out])[0] if host else out
 
 
 def giltig_frirum(occ, edt_mm, min_r_mm, margin_mm):
@@ -120,7 +155,7 @@ def giltig_frirum(occ, edt_mm, min_r_mm, margin_mm):
                                              valid.data_ptr(), _lib.stream_handle())
     _lib.check(st, 'giltig_frirum')
     valid = valid.view(torch.bool).reshape(shape)
-    return valid.cpu().numpy() if host else valid
+    return _host_arrays([valid])[0] if host else valid
 
 
 def bygg_gitterlaplacian(occ, edt_mm, pitch_mm, p_kond=1.5):
@@ -156,9 +191,11 @@ def bygg_gitterlaplacian(occ, edt_mm, pitch_mm, p_kond=1.5):
     node_map = node_map.reshape(shape)
     if host:
         from scipy import sparse
-        Lh = sparse.csr_matrix((data.cpu().numpy(), indices.cpu().numpy(), indptr.cpu().numpy()), shape=(n, n))
-        return n, node_map.cpu().numpy(), u.cpu().numpy(), v.cpu().numpy(), kond.cpu().numpy(), Lh
-    Ld = torch.sparse_csr_tensor(indptr, indices, data, size=(n, n))
+        node_h, u_h, v_h, kond_h, indptr_h, indices_h, data_h = _host_arrays(
+            [node_map, u, v, kond, indptr, indices, data])
+        Lh = sparse.csr_matrix((data_h, indices_h, indptr_h), shape=(n, n))
+        return n, node_h, u_h, v_h, kond_h, Lh
+    Ld = torch.sparse_csr_tensor(indptr, indices, data, size=(n, n), check_invariants=False)
     return n, node_map, u, v, kond, Ld
 
 

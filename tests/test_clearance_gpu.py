@@ -135,3 +135,22 @@ def test_full_size_properties():
     import field_b200.edt as ED
     sq = ED.squared_distance_device(occ.view(torch.uint8), sites_nonzero=True)
     assert torch.equal(E, sq.double().sqrt() * 0.01)
+
+
+def test_host_results_reuse_the_page_locked_pool():
+    """Host results are views of pooled page-locked blocks: once a call's arrays are dropped, the
+    next call of the same size allocates no new page-locked memory, and its arrays are correct."""
+    import gc
+    import field_b200.clearance as C
+    rng = np.random.default_rng(21)
+    occ = rng.random((30, 40, 50)) < 0.15
+    E = C.edt_mm(occ, 0.3)
+    first = C.bygg_gitterlaplacian(occ, E, 0.3)
+    want_n, want = oracle_dict(occ, E, 0.3, 1.5)
+    check_network(first, want_n, want)
+    del first
+    gc.collect()
+    before = C._POOL.allocated
+    second = C.bygg_gitterlaplacian(occ, E, 0.3)
+    assert C._POOL.allocated == before
+    check_network(second, want_n, want)
