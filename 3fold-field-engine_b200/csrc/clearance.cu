@@ -185,10 +185,10 @@ __global__ void __launch_bounds__(kLatThreads) k_lat_nodes(const uint8_t* __rest
     }
 }
 
-// Conductance of the edge between cells a < b from their clearances: max(0.5 (E_a + E_b) / pitch, 0.1)^p, in the
-// reference's operation order (NaN propagates through the max as in np.maximum).  The reference's
-// exponent 1.5 is m * sqrt(m) (correctly rounded root, one rounding of the product: within 2 ulp
-// of libm's pow, as CUDA's pow is), 0 and 1 are exact; other exponents call pow.
+// Conductance of the edge between cells a < b from their clearances, max(0.5 (E_a + E_b) / pitch,
+// 0.1)^p, in the reference's operation order (NaN propagates through the max as in np.maximum).
+// The reference's exponent 1.5 is m * sqrt(m) (correctly rounded root, one rounding of the product:
+// within 2 ulp of libm's pow, as CUDA's pow is), 0 and 1 are exact; other exponents call pow.
 __device__ __forceinline__ double conductance(double ea, double eb, double pitch, double p_kond) {
     const double c = __ddiv_rn(__dmul_rn(0.5, __dadd_rn(ea, eb)), pitch);
     const double m = (c != c) ? c : (c > kConductanceFloor ? c : kConductanceFloor);
