@@ -96,7 +96,7 @@ SIGNATURES = {
     "fb_clearance_mask_device": (I, [P, P, I64, D, P, P]),
     "fb_lattice_scratch_bytes": (I64, [I, I, I]),
     "fb_lattice_count_device": (I, [P, I, I, I, P, P, I64, P]),
-    "fb_lattice_emit_device": (I, [P, P, I, I, I, D, D, P, P, P, P, P, P, P, P, I64, P]),
+    "fb_lattice_emit_device": (I, [P, P, I, I, I, D, D, P, P, P, P, I64, P, I64, P, P, I64, P, I64, P]),
 }
 
 

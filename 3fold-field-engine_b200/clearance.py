@@ -185,8 +185,8 @@ def bygg_gitterlaplacian(occ, edt_mm, pitch_mm, p_kond=1.5):
     indices = torch.empty(nnz, dtype=torch.int32, device=dev)
     data = torch.empty(nnz, dtype=torch.float64, device=dev)
     _lib.check(L.fb_lattice_emit_device(occ3.data_ptr(), e.data_ptr(), nx, ny, nz, pitch, p,
-                                        node_map.data_ptr(), u.data_ptr(), v.data_ptr(), kond.data_ptr(),
-                                        indptr.data_ptr(), indices.data_ptr(), data.data_ptr(),
+                                        node_map.data_ptr(), u.data_ptr(), v.data_ptr(), kond.data_ptr(), n_edges,
+                                        indptr.data_ptr(), n + 1, indices.data_ptr(), data.data_ptr(), nnz,
                                         scratch.data_ptr(), scratch.numel(), stream), 'bygg_gitterlaplacian')
     node_map = node_map.reshape(shape)
     if host:

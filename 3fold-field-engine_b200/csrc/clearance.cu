@@ -159,13 +159,13 @@ __global__ void __launch_bounds__(kLatThreads) k_lat_count(const uint8_t* __rest
 }
 
 // Node map (-1 on occupied voxels) and CSR row starts; the thread of the last voxel also closes the
-// row pointer array with the entry total.
+// row pointer array with the entry total.  Row starts beyond the caller's capacity are not written.
 __global__ void __launch_bounds__(kLatThreads) k_lat_nodes(const uint8_t* __restrict__ occ, LatGrid g,
                                                            const int32_t* __restrict__ node_base,
                                                            const int32_t* __restrict__ entry_base,
                                                            const int32_t* __restrict__ totals,
                                                            int32_t* __restrict__ node_map,
-                                                           int32_t* __restrict__ indptr) {
+                                                           int32_t* __restrict__ indptr, int64_t indptr_cap) {
     __shared__ uint64_t s_warp[kLatThreads / 32];
     const int64_t base = (int64_t)blockIdx.x * kLatTile;
     int32_t node = node_base[blockIdx.x], entry = entry_base[blockIdx.x];
@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(kLatThreads) k_lat_nodes(const uint8_t* __rest
         if (p < g.n) {
             const int32_t id = node + (int32_t)field16(pre, 0);
             node_map[p] = f.free ? id : -1;
-            if (f.free) indptr[id] = entry + (int32_t)field16(pre, 1);
-            if (p == g.n - 1) indptr[totals[0]] = totals[2];
+            if (f.free && id < indptr_cap) indptr[id] = entry + (int32_t)field16(pre, 1);
+            if (p == g.n - 1 && totals[0] < indptr_cap) indptr[totals[0]] = totals[2];
         }
         node += (int32_t)field16(tot, 0);
         entry += (int32_t)field16(tot, 1);
@@ -211,8 +211,9 @@ __global__ void __launch_bounds__(kLatThreads, 4) k_lat_emit(const uint8_t* __re
                                                              const int32_t* __restrict__ entry_base,
                                                              const int32_t* __restrict__ node_map,
                                                              int32_t* __restrict__ u, int32_t* __restrict__ v,
-                                                             double* __restrict__ kond,
-                                                             int32_t* __restrict__ indices, double* __restrict__ data) {
+                                                             double* __restrict__ kond, int64_t edge_cap,
+                                                             int32_t* __restrict__ indices, double* __restrict__ data,
+                                                             int64_t entry_cap) {
     __shared__ uint64_t s_warp[kLatThreads / 32];
     __shared__ double s_val[kLatThreads * kLatRowMax];
     __shared__ int32_t s_idx[kLatThreads * kLatRowMax];
@@ -288,24 +289,20 @@ __global__ void __launch_bounds__(kLatThreads, 4) k_lat_emit(const uint8_t* __re
         __syncthreads();
         const int ne0 = (int)field16(tot, 0), ne1 = (int)field16(tot, 1), ne2 = (int)field16(tot, 2);
         const int nrow = (int)field16(tot, 3);
+        // outputs beyond the caller's capacities are not written
         for (int i = threadIdx.x; i < nrow; i += kLatThreads) {
+            if ((int64_t)cb + i >= entry_cap) break;
             indices[cb + i] = s_idx[i];
             data[cb + i] = s_val[i];
         }
-        for (int i = threadIdx.x; i < ne0; i += kLatThreads) {
-            u[eb[0] + i] = s_eu[0][i];
-            v[eb[0] + i] = s_ev[0][i];
-            kond[eb[0] + i] = s_ek[0][i];
-        }
-        for (int i = threadIdx.x; i < ne1; i += kLatThreads) {
-            u[eb[1] + i] = s_eu[1][i];
-            v[eb[1] + i] = s_ev[1][i];
-            kond[eb[1] + i] = s_ek[1][i];
-        }
-        for (int i = threadIdx.x; i < ne2; i += kLatThreads) {
-            u[eb[2] + i] = s_eu[2][i];
-            v[eb[2] + i] = s_ev[2][i];
-            kond[eb[2] + i] = s_ek[2][i];
+        for (int a = 0; a < 3; ++a) {
+            const int ne = a == 0 ? ne0 : (a == 1 ? ne1 : ne2);
+            for (int i = threadIdx.x; i < ne; i += kLatThreads) {
+                if ((int64_t)eb[a] + i >= edge_cap) break;
+                u[eb[a] + i] = s_eu[a][i];
+                v[eb[a] + i] = s_ev[a][i];
+                kond[eb[a] + i] = s_ek[a][i];
+            }
         }
         __syncthreads();
         eb[0] += ne0;
@@ -402,20 +399,24 @@ int fb_lattice_count_device(const uint8_t* d_occ, int nx, int ny, int nz, int32_
 
 int fb_lattice_emit_device(const uint8_t* d_occ, const double* d_edt_mm, int nx, int ny, int nz, double pitch,
                            double p_kond, int32_t* d_node_map, int32_t* d_u, int32_t* d_v, double* d_kond,
-                           int32_t* d_indptr, int32_t* d_indices, double* d_data, const void* d_scratch,
-                           int64_t scratch_len, void* stream) noexcept {
+                           int64_t edge_cap, int32_t* d_indptr, int64_t indptr_cap, int32_t* d_indices,
+                           double* d_data, int64_t entry_cap, const void* d_scratch, int64_t scratch_len,
+                           void* stream) noexcept {
     LatGrid g;
-    if (!d_occ || !d_edt_mm || !d_node_map || !d_indptr || !d_scratch || !lat_shape(nx, ny, nz, g))
-        return FB_INVALID;
+    if (!d_occ || !d_edt_mm || !d_node_map || !d_scratch || !lat_shape(nx, ny, nz, g)) return FB_INVALID;
+    if (edge_cap < 0 || indptr_cap < 1 || entry_cap < 0 || !d_indptr) return FB_INVALID;
+    if (edge_cap > 0 && (!d_u || !d_v || !d_kond)) return FB_INVALID;
+    if (entry_cap > 0 && (!d_indices || !d_data)) return FB_INVALID;
     const int64_t tiles = (g.n + kLatTile - 1) / kLatTile;
     if (scratch_len < 4 * lat_scratch_words(tiles)) return FB_INVALID;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const LatScratch s = lat_scratch(const_cast<void*>(d_scratch), tiles);
     k_lat_nodes<<<(unsigned)tiles, kLatThreads, 0, st>>>(d_occ, g, s.nodes, s.entries, s.totals, d_node_map,
-                                                           d_indptr);
+                                                           d_indptr, indptr_cap);
     FB_LAUNCH();
     k_lat_emit<<<(unsigned)tiles, kLatThreads, 0, st>>>(d_occ, d_edt_mm, g, pitch, p_kond, (int)tiles, s.edges,
-                                                          s.entries, d_node_map, d_u, d_v, d_kond, d_indices, d_data);
+                                                          s.entries, d_node_map, d_u, d_v, d_kond, edge_cap, d_indices,
+                                                          d_data, entry_cap);
     FB_LAUNCH();
     return FB_OK;
 }

@@ -1077,8 +1077,9 @@ def run_clearance(args, pitch=0.01):
                                           lat_scr.numel(), st)
         ev[3].record()
         rc[4] = L.fb_lattice_emit_device(occ.data_ptr(), E.data_ptr(), n, n, n, pitch, 1.5, node_map.data_ptr(),
-                                         u.data_ptr(), v.data_ptr(), kond.data_ptr(), indptr.data_ptr(),
-                                         indices.data_ptr(), data.data_ptr(), lat_scr.data_ptr(), lat_scr.numel(), st)
+                                         u.data_ptr(), v.data_ptr(), kond.data_ptr(), n_edges, indptr.data_ptr(),
+                                         nodes + 1, indices.data_ptr(), data.data_ptr(), nnz, lat_scr.data_ptr(),
+                                         lat_scr.numel(), st)
         ev[4].record()
         assert not any(rc), rc
 

@@ -390,15 +390,19 @@ int fb_clearance_mask_device(const uint8_t* d_occ, const double* d_edt_mm, int64
  * sizes the outputs from them and fb_lattice_emit_device writes the node map (nx*ny*nz int32, -1 on
  * occupied cells), the edges u, v, kond (axis 0, 1, 2; lower cell ascending; kond = max(0.5 (E_u +
  * E_v) / pitch, 0.1)^p_kond) and the CSR Laplacian (indptr[nodes + 1], indices and data[entries]:
- * columns ascending, -kond off the diagonal, the diagonal summed in scipy's COO order).  At most
- * (2^31 - 1) / 7 cells (status 1 beyond); fb_lattice_scratch_bytes returns -1 for such shapes. */
+ * columns ascending, -kond off the diagonal, the diagonal summed in scipy's COO order).  The
+ * capacities are the lengths of the caller's u / v / kond (edges), indptr (nodes + 1) and indices /
+ * data (entries) buffers: outputs beyond them are not written, and a null pointer is accepted only
+ * where its capacity is 0.  At most (2^31 - 1) / 7 cells (status 1 beyond);
+ * fb_lattice_scratch_bytes returns -1 for such shapes. */
 int64_t fb_lattice_scratch_bytes(int nx, int ny, int nz);
 int fb_lattice_count_device(const uint8_t* d_occ, int nx, int ny, int nz, int32_t* d_totals, void* d_scratch,
                             int64_t scratch_len, void* stream);
 int fb_lattice_emit_device(const uint8_t* d_occ, const double* d_edt_mm, int nx, int ny, int nz, double pitch,
                            double p_kond, int32_t* d_node_map, int32_t* d_u, int32_t* d_v, double* d_kond,
-                           int32_t* d_indptr, int32_t* d_indices, double* d_data, const void* d_scratch,
-                           int64_t scratch_len, void* stream);
+                           int64_t edge_cap, int32_t* d_indptr, int64_t indptr_cap, int32_t* d_indices,
+                           double* d_data, int64_t entry_cap, const void* d_scratch, int64_t scratch_len,
+                           void* stream);
 
 #ifdef __cplusplus
 }
