@@ -2295,8 +2295,10 @@ __global__ void __launch_bounds__(256) k_b_occupancy(const RecDesc* __restrict__
     occupancy_item<B>(R.kind, R.slot, tiles + tile_off[r], G.nx, G.ny, G.nz, G.nby, G.nbz, R.mask, g - W.pre[j]);
 }
 
+// 5 CTAs per SM (96 registers; the 8^3 form's spill stores 108 -> 16 bytes): the batch's leaf phase
+// 16.55 -> 15.59 ms, where the single-recipe k_leaf keeps 6 (at 5 its 1024^3 pass went 1.50 -> 1.57 ms).
 template <int B, bool kEdge>
-__global__ void __launch_bounds__(32 * kLeafWarps, 6) k_b_leaf(const RecDesc* __restrict__ D, Group W,
+__global__ void __launch_bounds__(32 * kLeafWarps, 5) k_b_leaf(const RecDesc* __restrict__ D, Group W,
                                                                float* __restrict__ tiles,
                                                                const int64_t* __restrict__ tile_off,
                                                                unsigned long long* __restrict__ work) {
